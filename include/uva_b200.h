@@ -1,0 +1,175 @@
+/*
+ * uva_b200.h - C ABI of the B200 (sm_100a) parameterization and validation
+ * kernels of Ultimate UV Artist's per-island hot path.
+ *
+ * Conventions
+ *   - Every function returns an int status: UVA_OK (0) or a negative
+ *     UVA_E_* code; uva_last_error() gives a message for the calling thread.
+ *   - Device pointers are plain pointers into CUDA global memory on the
+ *     current device; `stream` is a cudaStream_t passed as void*. Nothing is
+ *     synchronised unless the function says so.
+ *   - No global mutable state: calls on different streams/threads are
+ *     independent (the reference calls its flatten path from thread pools).
+ *   - A batch is many charts ("islands") concatenated block-diagonally:
+ *     vertices [vofs[i], vofs[i+1]) and triangles [tofs[i], tofs[i+1]) belong
+ *     to island i. Triangles hold island-LOCAL vertex indices.
+ *
+ * Reference interfaces replaced (paths inside the Ultimate UV Artist project):
+ *   engine/gpu.py   Batch.__init__ :69-124, _build_laplacian :126-142,
+ *                   _rhs :165-182, _cg :184-202, _max_step :204-227,
+ *                   arap :230-249, repair_flips :251-273,
+ *                   orient_positive :275-281, flips_per_chart :158-163,
+ *                   signed_area :153-156, jacobians :145-151, shrink :283-295
+ *   engine/param.py local_frames :19-32, cot_weights :35-44, lscm :136-169,
+ *                   _far_pair :172-179, refine (arap) :379-414,
+ *                   _arap_rotations :206-256, _arap_rhs :457-474,
+ *                   _max_step :259-291, _energy :294-319,
+ *                   repair_flips :477-516, chart_quality :520-551
+ *   engine/validate.py, engine/metrics.py: see the validation block below.
+ */
+#ifndef UVA_B200_H
+#define UVA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UVA_OK            0
+#define UVA_E_ARG        -1   /* bad argument (null pointer, negative size) */
+#define UVA_E_CUDA       -2   /* a CUDA runtime call failed                 */
+#define UVA_E_NOBOUNDARY -3   /* LSCM on an island with no boundary         */
+#define UVA_E_TOOBIG     -4   /* size above a documented maximum            */
+#define UVA_E_NODEVICE   -5   /* no CUDA device / not sm_100                */
+
+/* Frame / weight semantics: the two reference solvers differ in how they
+ * treat thin triangles (gpu.py:102-120 vs param.py:19-44).                 */
+#define UVA_SEM_BATCH 0
+#define UVA_SEM_PARAM 1
+
+/* Per-island solver status bits (uva_island_status.flags).                 */
+#define UVA_ST_MAXITER    1   /* an inner CG or the refinement hit its cap  */
+#define UVA_ST_NONFINITE  2   /* the solve went non-finite; U kept          */
+#define UVA_ST_ENERGYSTOP 4   /* relative-energy stop (param.refine)        */
+#define UVA_ST_NOBOUNDARY 8   /* LSCM: no boundary loop                     */
+
+typedef struct uva_island_status {
+    int32_t cg_iters;      /* inner FP32 CG iterations executed             */
+    int32_t refinements;   /* FP64 residual recomputations                  */
+    int32_t outer_iters;   /* ARAP local/global iterations executed         */
+    int32_t flags;         /* UVA_ST_* bits                                 */
+    double  resid[2];      /* last FP64 relative residual per column        */
+    double  energy;        /* last ARAP energy (param semantics)            */
+    double  step;          /* last line-search step                         */
+} uva_island_status;
+
+/* --------------------------------------------------------------------------
+ * Topology plan (host). Built from the triangle lists only, in parallel over
+ * islands; replaces gpu.unique_edges / sym_csr (gpu.py:39-63) and the
+ * boundary searches of param.boundary_edges_oriented (param.py:59-68).
+ * ------------------------------------------------------------------------ */
+typedef struct uva_plan uva_plan;
+
+enum {
+    UVA_PLAN_NC = 0, UVA_PLAN_N, UVA_PLAN_T, UVA_PLAN_E, UVA_PLAN_NSLICES,
+    UVA_PLAN_NSLOTS, UVA_PLAN_NBVERTS, UVA_PLAN_MAXROWS, UVA_PLAN_NSIZES
+};
+
+/* tris: t*3 island-LOCAL vertex ids (int64, host); vofs/tofs: nc+1 offsets.
+ * Returns UVA_E_ARG if an index is out of its island's range.              */
+int uva_plan_create(const int64_t* tris, const int64_t* vofs, const int64_t* tofs,
+                    int32_t nc, int32_t nthreads, uva_plan** out);
+int uva_plan_sizes(const uva_plan* plan, int64_t* sizes /* UVA_PLAN_NSIZES */);
+/* Copies the plan into caller-owned HOST arrays (sizes from uva_plan_sizes):
+ *   tri4      t*4   local a,b,c and island id
+ *   tri_edge  t*3   global unique-edge id of edge k (corners k+1 -> k+2)
+ *   sofs      nc+1  first SELL slice of each island
+ *   slice_ptr nslices+1 first slot of each slice (32 rows per slice)
+ *   slot_col  nslots island-local column (padding: the row itself)
+ *   slot_edge nslots global unique-edge id (padding: -1)
+ *   slot_c    nslots LSCM boundary coupling H[i, j+n] (param.py:147-150)
+ *   vt_ptr    n+1   incidence offsets; vt 3t entries f*3+corner, ascending
+ *   vflags    n     bit0: endpoint of an edge used once (gpu.py:256-258)
+ *                   bit1: endpoint of a twin-less half-edge (param.py:513-514)
+ *   bofs      nc+1, bverts: sorted boundary source vertices (param.py:152)  */
+int uva_plan_export(const uva_plan* plan, int32_t* tri4, int32_t* tri_edge, int32_t* sofs,
+                    int32_t* slice_ptr, int32_t* slot_col, int32_t* slot_edge, float* slot_c,
+                    int32_t* vt_ptr, int32_t* vt, uint8_t* vflags, int32_t* bofs, int32_t* bverts);
+void uva_plan_destroy(uva_plan* plan);
+
+/* --------------------------------------------------------------------------
+ * Device batch descriptor: plain device pointers, filled by the host layer.
+ * ------------------------------------------------------------------------ */
+typedef struct uva_batch {
+    int32_t nc, n, t, E, nslices, nslots, semantics, maxrows;
+    /* topology (from the plan) */
+    const int32_t* vofs;      const int32_t* tofs;      const int32_t* sofs;
+    const int32_t* tri4;      const int32_t* tri_edge;
+    const int32_t* slice_ptr; const int32_t* slot_col;  const int32_t* slot_edge;
+    const float*   slot_c;    const int32_t* vt_ptr;    const int32_t* vt;
+    const uint8_t* vflags;    const int32_t* bofs;      const int32_t* bverts;
+    const int32_t* order;     /* nc island ids, largest first (work order)    */
+    /* geometry, written by uva_batch_setup */
+    const double*  P;         /* n*3 positions (FP64)                          */
+    double* frame;            /* t*4: x1, x2, y2, area                          */
+    double* wtri;             /* t*4: w0, w1, w2 (half cotangents), ok (1/0)    */
+    float*  tscale;           /* t: target size (Batch.shrink)                  */
+    double* wedge;            /* E: summed edge weight                          */
+    float*  slot_w;           /* nslots: FP32 edge weight of each SELL slot     */
+    double* wdiag;            /* n: exact FP64 row sum of slot_w                */
+    float*  dinv;             /* n: Jacobi inverse of wdiag (pin row: on the fly)*/
+    int32_t* pins;            /* nc*3: ARAP pin, LSCM p0, LSCM p1 (local ids)   */
+    double* wpin;             /* nc: soft-pin weight                            */
+    double* U;                /* n*2 UVs (FP64 master copy)                     */
+    /* scratch (device, sized n / t) */
+    double* x64;  double* b64;  double* rc;     /* x64, b64: max(n,nc)*2;     */
+                                                /* rc: t*3*2 corner RHS terms */
+    float*  r32;  float*  d32;  float*  p32;  float* q32;
+    uva_island_status* status;                  /* nc                         */
+    int32_t* work;            /* >= 4 ints, zeroed by the callee per launch     */
+} uva_batch;
+
+typedef struct uva_solve_params {
+    int32_t iters;            /* ARAP outer iterations                          */
+    int32_t line_search;      /* 1: flip-safe step (param: only if flip-free)   */
+    double  tol;              /* FP64 relative residual per column              */
+    double  energy_tol;       /* >0: param.refine relative-energy stop          */
+    double  inner_eta;        /* inner FP32 CG relative reduction floor         */
+    int32_t max_inner;        /* inner CG iteration cap per refinement          */
+    int32_t max_refine;       /* refinement cap per global step                 */
+    int32_t threads;          /* threads per island team (0: autotuned)         */
+    int32_t reserved;
+} uva_solve_params;
+
+/* Frames, weights, matrix values, Jacobi diagonal, pins and pin weights.
+ * Batch semantics: global wpin = max|w| (gpu.py:138); param: per island.   */
+int uva_batch_setup(uva_batch* b, void* stream);
+/* LSCM of every island (hard pins at the far boundary pair, param.py:136-169)
+ * solved by FP32 PCG with FP64 residual refinement; writes b->U.           */
+int uva_lscm(uva_batch* b, const uva_solve_params* prm, void* stream);
+/* ARAP local/global iterations of every island in one persistent launch
+ * (gpu.py:230-249 with semantics BATCH, param.py:379-414 with PARAM).      */
+int uva_arap(uva_batch* b, const uva_solve_params* prm, void* stream);
+
+/* Batch utilities (gpu.py:145-299). */
+int uva_orient_positive(uva_batch* b, void* stream);
+int uva_repair_flips(uva_batch* b, int32_t rounds, void* stream);
+int uva_flips_per_chart(const uva_batch* b, float* out /* nc */, void* stream);
+int uva_signed_area(const uva_batch* b, const double* U, double* out /* t */, void* stream);
+int uva_jacobians(const uva_batch* b, const double* U, double* out /* t*4 */, void* stream);
+/* Serial in-order flip repair of param.repair_flips (param.py:477-516). */
+int uva_repair_flips_serial(uva_batch* b, int32_t rounds, void* stream);
+/* gpu.py:283-295: sel (t bytes, in/out) grown by `rings` vertex rings, then
+ * tscale = max(tscale * factor, floor) on the selection; vmark: n bytes.   */
+int uva_shrink(uva_batch* b, uint8_t* sel, uint8_t* vmark, int32_t rings, float factor, float floor_,
+               void* stream);
+
+/* Library info. */
+const char* uva_last_error(void);
+int uva_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UVA_B200_H */

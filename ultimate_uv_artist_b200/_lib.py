@@ -1,0 +1,138 @@
+"""ctypes binding of the C ABI in include/uva_b200.h (libuva_b200.so).
+
+The library is required: there is no CPU fallback. Importing this module
+loads the in-tree ``libuva_b200.so`` (building it with nvcc if it is missing
+and a compiler is present) and raises ``RuntimeError`` otherwise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libuva_b200.so")
+
+UVA_OK = 0
+UVA_E_ARG = -1
+UVA_E_CUDA = -2
+UVA_E_NOBOUNDARY = -3
+UVA_E_TOOBIG = -4
+UVA_E_NODEVICE = -5
+SEM_BATCH = 0
+SEM_PARAM = 1
+ST_MAXITER = 1
+ST_NONFINITE = 2
+ST_ENERGYSTOP = 4
+ST_NOBOUNDARY = 8
+
+PLAN_NSIZES = 8
+(PLAN_NC, PLAN_N, PLAN_T, PLAN_E, PLAN_NSLICES, PLAN_NSLOTS, PLAN_NBVERTS, PLAN_MAXROWS) = range(8)
+
+vp = C.c_void_p
+i32 = C.c_int32
+
+
+class IslandStatus(C.Structure):
+    _fields_ = [("cg_iters", i32), ("refinements", i32), ("outer_iters", i32), ("flags", i32),
+                ("resid", C.c_double * 2), ("energy", C.c_double), ("step", C.c_double)]
+
+
+class BatchDesc(C.Structure):
+    """Mirror of ``uva_batch`` (field order and types must match the header)."""
+    _fields_ = [("nc", i32), ("n", i32), ("t", i32), ("E", i32), ("nslices", i32), ("nslots", i32),
+                ("semantics", i32), ("maxrows", i32),
+                ("vofs", vp), ("tofs", vp), ("sofs", vp), ("tri4", vp), ("tri_edge", vp),
+                ("slice_ptr", vp), ("slot_col", vp), ("slot_edge", vp), ("slot_c", vp),
+                ("vt_ptr", vp), ("vt", vp), ("vflags", vp), ("bofs", vp), ("bverts", vp), ("order", vp),
+                ("P", vp), ("frame", vp), ("wtri", vp), ("tscale", vp), ("wedge", vp), ("slot_w", vp),
+                ("wdiag", vp), ("dinv", vp), ("pins", vp), ("wpin", vp), ("U", vp),
+                ("x64", vp), ("b64", vp), ("rc", vp), ("r32", vp), ("d32", vp), ("p32", vp), ("q32", vp),
+                ("status", vp), ("work", vp)]
+
+
+class SolveParams(C.Structure):
+    _fields_ = [("iters", i32), ("line_search", i32), ("tol", C.c_double), ("energy_tol", C.c_double),
+                ("inner_eta", C.c_double), ("max_inner", i32), ("max_refine", i32), ("threads", i32),
+                ("reserved", i32)]
+
+
+_SIGS = {
+    "uva_plan_create": [vp, vp, vp, i32, i32, vp],
+    "uva_plan_sizes": [vp, vp],
+    "uva_plan_export": [vp] * 13,
+    "uva_plan_destroy": [vp],
+    "uva_batch_setup": [vp, vp],
+    "uva_lscm": [vp, vp, vp],
+    "uva_arap": [vp, vp, vp],
+    "uva_orient_positive": [vp, vp],
+    "uva_repair_flips": [vp, i32, vp],
+    "uva_repair_flips_serial": [vp, i32, vp],
+    "uva_flips_per_chart": [vp, vp, vp],
+    "uva_signed_area": [vp, vp, vp, vp],
+    "uva_jacobians": [vp, vp, vp, vp],
+    "uva_shrink": [vp, vp, vp, i32, C.c_float, C.c_float, vp],
+    "uva_last_error": [],
+    "uva_version": [],
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def _load():
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            try:
+                from . import build as _build
+                _build.build()
+            except Exception as exc:  # noqa: BLE001 - re-raised with context
+                raise RuntimeError(f"uva_b200: {LIB_PATH} is missing and could not be built: {exc}") from exc
+        lib = C.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = i32
+        lib.uva_last_error.restype = C.c_char_p
+        lib.uva_plan_destroy.restype = None
+        _lib = lib
+        return lib
+
+
+def lib():
+    return _load()
+
+
+def exported_symbols():
+    """Names this binding expects the library to export."""
+    return sorted(_SIGS)
+
+
+def check(status, what=""):
+    """Raise on a non-zero status, with the library's thread-local message."""
+    if status == UVA_OK:
+        return
+    msg = lib().uva_last_error().decode(errors="replace")
+    if status == UVA_E_NOBOUNDARY:
+        raise ValueError(msg or "chart has no boundary (closed surface): needs a cut")
+    if status == UVA_E_ARG:
+        raise ValueError(f"{what}: {msg}")
+    raise RuntimeError(f"{what}: uva_b200 status {status}: {msg}")
+
+
+def ptr(t):
+    """Raw device/host address of a torch tensor or numpy array (None -> 0)."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return C.c_void_p(t.data_ptr())
+    return C.c_void_p(t.ctypes.data)
+
+
+def stream_handle(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)

@@ -1,0 +1,296 @@
+// Topology plan of a batch of islands (host, C++17, parallel over islands).
+//
+// Everything here depends on the triangle lists only, so a plan is built once
+// per batch and reused by every solve. It replaces the edge deduplication and
+// CSR assembly of engine/gpu.py:39-63 (unique_edges, sym_csr) and the boundary
+// searches of engine/param.py:59-68 (boundary_edges_oriented) with per-island
+// sorts that run on all host cores, and lays the Laplacian pattern out as a
+// sliced-ELL matrix (32-row slices, column-major inside a slice) so that a warp
+// reads one slot of 32 consecutive rows with one coalesced load.
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <numeric>
+#include <thread>
+#include <vector>
+
+#include "../../include/uva_b200.h"
+
+extern "C" void uva_set_error(const char* msg);
+
+namespace {
+
+struct IslandPlan {
+    int32_t n = 0, t = 0;
+    std::vector<int32_t> tri_edge;     // 3t local edge ids (-1: never)
+    std::vector<int32_t> edge_info;    // per local edge: count | fwd<<10 | rev<<20
+    std::vector<int32_t> row_ptr;      // n+1 (non-self-loop neighbours)
+    std::vector<int32_t> row_col;      // neighbour ids, ascending per row
+    std::vector<int32_t> row_edge;     // local edge id of each neighbour entry
+    std::vector<uint8_t> vflags;       // n
+    std::vector<int32_t> bverts;       // sorted unique boundary sources
+    int32_t nedges = 0, nslices = 0, nslots = 0;
+    std::vector<int32_t> slice_w;      // per slice width
+};
+
+void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& bad) {
+    ip.n = n; ip.t = t;
+    struct HE { int64_t key; int32_t he; };
+    std::vector<HE> he(static_cast<size_t>(3) * t);
+    for (int32_t f = 0; f < t; ++f) {
+        for (int k = 0; k < 3; ++k) {
+            int64_t a = T[3 * f + (k + 1) % 3], b = T[3 * f + (k + 2) % 3];
+            if (a < 0 || a >= n || b < 0 || b >= n) { bad = true; return; }
+            int64_t lo = a < b ? a : b, hi = a < b ? b : a;
+            he[3 * f + k] = {lo * n + hi, 3 * f + k};
+        }
+    }
+    std::sort(he.begin(), he.end(), [](const HE& x, const HE& y) {
+        return x.key < y.key || (x.key == y.key && x.he < y.he);
+    });
+    ip.tri_edge.assign(static_cast<size_t>(3) * t, -1);
+    ip.edge_info.clear();
+    std::vector<int64_t> ekey;
+    for (size_t s = 0; s < he.size();) {
+        size_t e = s;
+        int32_t fwd = 0, rev = 0;
+        const int64_t key = he[s].key;
+        const int64_t lo = key / n;
+        while (e < he.size() && he[e].key == key) {
+            const int32_t h = he[e].he;
+            const int32_t f = h / 3, k = h % 3;
+            const int64_t a = T[3 * f + (k + 1) % 3];
+            if (a == lo) ++fwd; else ++rev;
+            ip.tri_edge[h] = static_cast<int32_t>(ekey.size());
+            ++e;
+        }
+        const int32_t cnt = static_cast<int32_t>(e - s);
+        ip.edge_info.push_back(std::min(cnt, 1023) | (std::min(fwd, 1023) << 10) | (std::min(rev, 1023) << 20));
+        ekey.push_back(key);
+        s = e;
+    }
+    ip.nedges = static_cast<int32_t>(ekey.size());
+    // rows: appending in key order keeps each row sorted (see file comment)
+    std::vector<int32_t> deg(n, 0);
+    for (int64_t key : ekey) {
+        const int64_t lo = key / n, hi = key % n;
+        if (lo == hi) continue;
+        ++deg[lo]; ++deg[hi];
+    }
+    ip.row_ptr.assign(n + 1, 0);
+    for (int32_t v = 0; v < n; ++v) ip.row_ptr[v + 1] = ip.row_ptr[v] + deg[v];
+    ip.row_col.assign(ip.row_ptr[n], 0);
+    ip.row_edge.assign(ip.row_ptr[n], 0);
+    std::vector<int32_t> fill(ip.row_ptr.begin(), ip.row_ptr.end() - 1);
+    for (int32_t e = 0; e < ip.nedges; ++e) {
+        const int64_t lo = ekey[e] / n, hi = ekey[e] % n;
+        if (lo == hi) continue;
+        ip.row_col[fill[lo]] = static_cast<int32_t>(hi); ip.row_edge[fill[lo]++] = e;
+        ip.row_col[fill[hi]] = static_cast<int32_t>(lo); ip.row_edge[fill[hi]++] = e;
+    }
+    // the fill above appends hi-entries of row `lo` before lo-entries of rows
+    // met later; restore ascending column order per row
+    for (int32_t v = 0; v < n; ++v) {
+        const int32_t a = ip.row_ptr[v], b = ip.row_ptr[v + 1];
+        bool sorted = true;
+        for (int32_t q = a + 1; q < b; ++q) if (ip.row_col[q - 1] > ip.row_col[q]) { sorted = false; break; }
+        if (!sorted) {
+            std::vector<std::pair<int32_t, int32_t>> tmp;
+            for (int32_t q = a; q < b; ++q) tmp.emplace_back(ip.row_col[q], ip.row_edge[q]);
+            std::sort(tmp.begin(), tmp.end());
+            for (int32_t q = a; q < b; ++q) { ip.row_col[q] = tmp[q - a].first; ip.row_edge[q] = tmp[q - a].second; }
+        }
+    }
+    // vertex flags and boundary sources
+    ip.vflags.assign(n, 0);
+    std::vector<uint8_t> isb(n, 0);
+    for (int32_t e = 0; e < ip.nedges; ++e) {
+        const int32_t info = ip.edge_info[e];
+        const int32_t cnt = info & 1023, fwd = (info >> 10) & 1023, rev = (info >> 20) & 1023;
+        const int64_t lo = ekey[e] / n, hi = ekey[e] % n;
+        if (cnt == 1) { ip.vflags[lo] |= 1; ip.vflags[hi] |= 1; }
+        if (lo == hi) continue;
+        if (fwd > 0 && rev == 0) { ip.vflags[lo] |= 2; ip.vflags[hi] |= 2; isb[lo] = 1; }
+        if (rev > 0 && fwd == 0) { ip.vflags[lo] |= 2; ip.vflags[hi] |= 2; isb[hi] = 1; }
+    }
+    ip.bverts.clear();
+    for (int32_t v = 0; v < n; ++v) if (isb[v]) ip.bverts.push_back(v);
+    // sliced ELL: 32 rows per slice
+    ip.nslices = (n + 31) / 32;
+    ip.slice_w.assign(ip.nslices, 0);
+    ip.nslots = 0;
+    for (int32_t s = 0; s < ip.nslices; ++s) {
+        int32_t w = 0;
+        for (int32_t r = s * 32; r < std::min(n, s * 32 + 32); ++r) w = std::max(w, deg[r]);
+        ip.slice_w[s] = w;
+        ip.nslots += 32 * w;
+    }
+}
+
+}  // namespace
+
+struct uva_plan {
+    int32_t nc = 0;
+    int64_t n = 0, t = 0, E = 0, nslices = 0, nslots = 0, nbverts = 0, maxrows = 0;
+    std::vector<int64_t> vofs, tofs;
+    std::vector<IslandPlan> isl;
+    std::vector<int64_t> eofs, sofs, slotofs, bofs;
+    const int64_t* tris = nullptr;   // not owned; only valid during create
+    std::vector<int32_t> tri_local;  // 3t local ids (copied)
+};
+
+extern "C" int uva_plan_create(const int64_t* tris, const int64_t* vofs, const int64_t* tofs, int32_t nc,
+                               int32_t nthreads, uva_plan** out) {
+    if (!out || nc < 0 || (nc > 0 && (!vofs || !tofs))) { uva_set_error("uva_plan_create: bad arguments"); return UVA_E_ARG; }
+    *out = nullptr;
+    auto* p = new uva_plan();
+    p->nc = nc;
+    p->vofs.assign(vofs, vofs + nc + 1);
+    p->tofs.assign(tofs, tofs + nc + 1);
+    for (int32_t i = 0; i < nc; ++i) {
+        if (p->vofs[i + 1] < p->vofs[i] || p->tofs[i + 1] < p->tofs[i]) {
+            delete p; uva_set_error("uva_plan_create: offsets must be non-decreasing"); return UVA_E_ARG;
+        }
+    }
+    p->n = p->vofs[nc] - p->vofs[0];
+    p->t = p->tofs[nc] - p->tofs[0];
+    if (p->n > (int64_t(1) << 30) || 3 * p->t > (int64_t(1) << 30)) {
+        delete p; uva_set_error("uva_plan_create: batch too large for 32-bit indices"); return UVA_E_TOOBIG;
+    }
+    if (p->t > 0 && !tris) { delete p; uva_set_error("uva_plan_create: null triangles"); return UVA_E_ARG; }
+    p->isl.resize(nc);
+    p->tri_local.assign(tris, tris + 3 * p->t);
+    // largest islands first for load balance
+    std::vector<int32_t> order(nc);
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+        return (p->tofs[a + 1] - p->tofs[a]) > (p->tofs[b + 1] - p->tofs[b]);
+    });
+    std::atomic<int32_t> next{0};
+    std::atomic<bool> anybad{false};
+    auto worker = [&]() {
+        for (;;) {
+            const int32_t q = next.fetch_add(1);
+            if (q >= nc) break;
+            const int32_t i = order[q];
+            bool bad = false;
+            build_island(tris + 3 * (p->tofs[i] - p->tofs[0]), static_cast<int32_t>(p->vofs[i + 1] - p->vofs[i]),
+                         static_cast<int32_t>(p->tofs[i + 1] - p->tofs[i]), p->isl[i], bad);
+            if (bad) anybad = true;
+        }
+    };
+    int32_t nt = nthreads > 0 ? nthreads : static_cast<int32_t>(std::thread::hardware_concurrency());
+    nt = std::max(1, std::min(nt, std::max(nc, 1)));
+    std::vector<std::thread> pool;
+    for (int32_t k = 1; k < nt; ++k) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    if (anybad) { delete p; uva_set_error("uva_plan_create: triangle index outside its island"); return UVA_E_ARG; }
+    p->eofs.assign(nc + 1, 0); p->sofs.assign(nc + 1, 0); p->slotofs.assign(nc + 1, 0); p->bofs.assign(nc + 1, 0);
+    for (int32_t i = 0; i < nc; ++i) {
+        p->eofs[i + 1] = p->eofs[i] + p->isl[i].nedges;
+        p->sofs[i + 1] = p->sofs[i] + p->isl[i].nslices;
+        p->slotofs[i + 1] = p->slotofs[i] + p->isl[i].nslots;
+        p->bofs[i + 1] = p->bofs[i] + static_cast<int64_t>(p->isl[i].bverts.size());
+        p->maxrows = std::max<int64_t>(p->maxrows, p->isl[i].n);
+    }
+    p->E = p->eofs[nc]; p->nslices = p->sofs[nc]; p->nslots = p->slotofs[nc]; p->nbverts = p->bofs[nc];
+    if (p->nslots > (int64_t(1) << 31) - 1 || p->E > (int64_t(1) << 31) - 1) {
+        delete p; uva_set_error("uva_plan_create: plan too large for 32-bit offsets"); return UVA_E_TOOBIG;
+    }
+    *out = p;
+    return UVA_OK;
+}
+
+extern "C" int uva_plan_sizes(const uva_plan* p, int64_t* s) {
+    if (!p || !s) { uva_set_error("uva_plan_sizes: null argument"); return UVA_E_ARG; }
+    s[UVA_PLAN_NC] = p->nc; s[UVA_PLAN_N] = p->n; s[UVA_PLAN_T] = p->t; s[UVA_PLAN_E] = p->E;
+    s[UVA_PLAN_NSLICES] = p->nslices; s[UVA_PLAN_NSLOTS] = p->nslots; s[UVA_PLAN_NBVERTS] = p->nbverts;
+    s[UVA_PLAN_MAXROWS] = p->maxrows;
+    return UVA_OK;
+}
+
+extern "C" int uva_plan_export(const uva_plan* p, int32_t* tri4, int32_t* tri_edge, int32_t* sofs,
+                               int32_t* slice_ptr, int32_t* slot_col, int32_t* slot_edge, float* slot_c,
+                               int32_t* vt_ptr, int32_t* vt, uint8_t* vflags, int32_t* bofs, int32_t* bverts) {
+    if (!p) { uva_set_error("uva_plan_export: null plan"); return UVA_E_ARG; }
+    const int32_t nc = p->nc;
+    const int64_t v0 = p->vofs.empty() ? 0 : p->vofs[0];
+    const int64_t t0 = p->tofs.empty() ? 0 : p->tofs[0];
+    auto worker = [&](int32_t lo, int32_t hi) {
+        for (int32_t i = lo; i < hi; ++i) {
+            const IslandPlan& ip = p->isl[i];
+            const int64_t fb = p->tofs[i] - t0, vb = p->vofs[i] - v0;
+            const int64_t eb = p->eofs[i], sb = p->sofs[i], slb = p->slotofs[i];
+            for (int32_t f = 0; f < ip.t; ++f) {
+                for (int k = 0; k < 3; ++k) {
+                    tri4[4 * (fb + f) + k] = static_cast<int32_t>(p->tri_local[3 * (fb + f) + k]);
+                    const int32_t e = ip.tri_edge[3 * f + k];
+                    tri_edge[3 * (fb + f) + k] = e < 0 ? -1 : static_cast<int32_t>(eb + e);
+                }
+                tri4[4 * (fb + f) + 3] = i;
+            }
+            if (sofs) sofs[i] = static_cast<int32_t>(sb);
+            int64_t slot = slb;
+            for (int32_t s = 0; s < ip.nslices; ++s) {
+                slice_ptr[sb + s] = static_cast<int32_t>(slot);
+                const int32_t w = ip.slice_w[s];
+                for (int32_t k = 0; k < w; ++k) {
+                    for (int32_t lane = 0; lane < 32; ++lane) {
+                        const int32_t r = s * 32 + lane;
+                        const int64_t q = slot + static_cast<int64_t>(k) * 32 + lane;
+                        if (r < ip.n && k < ip.row_ptr[r + 1] - ip.row_ptr[r]) {
+                            const int32_t j = ip.row_col[ip.row_ptr[r] + k];
+                            const int32_t e = ip.row_edge[ip.row_ptr[r] + k];
+                            slot_col[q] = j;
+                            slot_edge[q] = static_cast<int32_t>(eb + e);
+                            const int32_t info = ip.edge_info[e];
+                            const int32_t nf = (info >> 10) & 1023, nr = (info >> 20) & 1023;
+                            // half-edges r->j and j->r (fwd is lo->hi)
+                            const int32_t n_rj = r < j ? nf : nr, n_jr = r < j ? nr : nf;
+                            const int32_t b_rj = n_jr == 0 ? n_rj : 0, b_jr = n_rj == 0 ? n_jr : 0;
+                            slot_c[q] = -0.5f * static_cast<float>(b_rj) + 0.5f * static_cast<float>(b_jr);
+                        } else {
+                            slot_col[q] = r < ip.n ? r : 0;
+                            slot_edge[q] = -1;
+                            slot_c[q] = 0.0f;
+                        }
+                    }
+                }
+                slot += static_cast<int64_t>(w) * 32;
+            }
+            for (int32_t v = 0; v < ip.n; ++v) vflags[vb + v] = ip.vflags[v];
+            if (bofs) bofs[i] = static_cast<int32_t>(p->bofs[i]);
+            for (size_t q = 0; q < ip.bverts.size(); ++q) bverts[p->bofs[i] + q] = ip.bverts[q];
+        }
+    };
+    const int32_t nt = std::max(1, std::min<int32_t>(static_cast<int32_t>(std::thread::hardware_concurrency()), nc));
+    std::vector<std::thread> pool;
+    const int32_t chunk = (nc + nt - 1) / std::max(nt, 1);
+    for (int32_t k = 0; k < nt; ++k) {
+        const int32_t lo = k * chunk, hi = std::min(nc, lo + chunk);
+        if (lo < hi) pool.emplace_back(worker, lo, hi);
+    }
+    for (auto& th : pool) th.join();
+    if (sofs) sofs[nc] = static_cast<int32_t>(p->nslices);
+    slice_ptr[p->nslices] = static_cast<int32_t>(p->nslots);
+    if (bofs) bofs[nc] = static_cast<int32_t>(p->nbverts);
+    // vertex -> (triangle, corner) incidence, ascending by f*3+corner
+    std::vector<int32_t> cnt(p->n + 1, 0);
+    for (int32_t i = 0; i < nc; ++i) {
+        const int64_t fb = p->tofs[i] - t0, vb = p->vofs[i] - v0;
+        for (int32_t f = 0; f < p->isl[i].t; ++f)
+            for (int k = 0; k < 3; ++k) ++cnt[vb + p->tri_local[3 * (fb + f) + k] + 1];
+    }
+    for (int64_t v = 0; v < p->n; ++v) cnt[v + 1] += cnt[v];
+    for (int64_t v = 0; v <= p->n; ++v) vt_ptr[v] = cnt[v];
+    std::vector<int32_t> fillp(cnt.begin(), cnt.end() - 1);
+    for (int32_t i = 0; i < nc; ++i) {
+        const int64_t fb = p->tofs[i] - t0, vb = p->vofs[i] - v0;
+        for (int32_t f = 0; f < p->isl[i].t; ++f)
+            for (int k = 0; k < 3; ++k) vt[fillp[vb + p->tri_local[3 * (fb + f) + k]]++] = static_cast<int32_t>(3 * (fb + f) + k);
+    }
+    return UVA_OK;
+}
+
+extern "C" void uva_plan_destroy(uva_plan* p) { delete p; }

@@ -1,0 +1,238 @@
+"""Device-resident batch of islands and the calls into the CUDA library.
+
+A ``DeviceBatch`` concatenates many charts block-diagonally, builds the
+topology plan on the host cores (C++, parallel over islands), uploads it once,
+and keeps every per-island array in HBM: frames, weights, the sliced-ELL
+Laplacian, UVs and solver scratch. All solver calls run on one CUDA stream and
+never synchronise the host.
+
+Memory: about 80 bytes per triangle plus about 170 bytes per vertex
+(UVs and solver vectors), so a 180 GB B200 holds batches of several hundred
+million triangles.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, ptr
+
+DEFAULTS = {
+    "arap": {"tol": 1e-6, "inner_eta": 1e-3, "max_inner": 4000, "max_refine": 12},
+    "lscm": {"tol": 1e-9, "inner_eta": 1e-4, "max_inner": 20000, "max_refine": 16},
+}
+
+
+def require_cuda(dev=None):
+    """The product path has no CPU fallback: fail loudly without a CUDA device."""
+    if not torch.cuda.is_available():
+        raise RuntimeError("ultimate_uv_artist_b200 needs a CUDA device (sm_100a); none is available")
+    d = torch.device(dev) if dev is not None else torch.device("cuda", torch.cuda.current_device())
+    if d.type != "cuda":
+        raise RuntimeError(f"ultimate_uv_artist_b200 runs on CUDA devices only, got {d}")
+    return d
+
+
+class Plan:
+    """Host topology plan (wraps uva_plan_create / uva_plan_export)."""
+
+    def __init__(self, T_local, vofs, tofs, nthreads=0):
+        L = _lib.lib()
+        T_local = np.ascontiguousarray(T_local, np.int64).reshape(-1, 3)
+        vofs = np.ascontiguousarray(vofs, np.int64)
+        tofs = np.ascontiguousarray(tofs, np.int64)
+        nc = len(vofs) - 1
+        h = C.c_void_p()
+        check(L.uva_plan_create(ptr(T_local), ptr(vofs), ptr(tofs), nc, int(nthreads), C.byref(h)),
+              "uva_plan_create")
+        try:
+            sz = np.zeros(_lib.PLAN_NSIZES, np.int64)
+            check(L.uva_plan_sizes(h, ptr(sz)), "uva_plan_sizes")
+            self.nc, self.n, self.t, self.E = int(sz[0]), int(sz[1]), int(sz[2]), int(sz[3])
+            self.nslices, self.nslots, self.nbverts, self.maxrows = int(sz[4]), int(sz[5]), int(sz[6]), int(sz[7])
+            self.tri4 = np.empty((self.t, 4), np.int32)
+            self.tri_edge = np.empty((self.t, 3), np.int32)
+            self.sofs = np.empty(nc + 1, np.int32)
+            self.slice_ptr = np.empty(self.nslices + 1, np.int32)
+            self.slot_col = np.empty(self.nslots, np.int32)
+            self.slot_edge = np.empty(self.nslots, np.int32)
+            self.slot_c = np.empty(self.nslots, np.float32)
+            self.vt_ptr = np.empty(self.n + 1, np.int32)
+            self.vt = np.empty(3 * self.t, np.int32)
+            self.vflags = np.empty(self.n, np.uint8)
+            self.bofs = np.empty(nc + 1, np.int32)
+            self.bverts = np.empty(max(self.nbverts, 1), np.int32)
+            check(L.uva_plan_export(h, ptr(self.tri4), ptr(self.tri_edge), ptr(self.sofs), ptr(self.slice_ptr),
+                                    ptr(self.slot_col), ptr(self.slot_edge), ptr(self.slot_c), ptr(self.vt_ptr),
+                                    ptr(self.vt), ptr(self.vflags), ptr(self.bofs), ptr(self.bverts)),
+                  "uva_plan_export")
+        finally:
+            L.uva_plan_destroy(h)
+        self.vofs = vofs.astype(np.int32)
+        self.tofs = tofs.astype(np.int32)
+        sizes = np.diff(tofs)
+        self.order = np.argsort(-sizes, kind="stable").astype(np.int32)
+
+
+def concat_charts(charts, with_uv=True):
+    """(P, T, U) per chart -> concatenated FP64 P, local int64 T, FP64 U, offsets."""
+    nc = len(charts)
+    vofs = np.zeros(nc + 1, np.int64)
+    tofs = np.zeros(nc + 1, np.int64)
+    for i, ch in enumerate(charts):
+        vofs[i + 1] = vofs[i] + len(ch[0])
+        tofs[i + 1] = tofs[i] + len(ch[1])
+    P = np.empty((int(vofs[-1]), 3), np.float64)
+    T = np.empty((int(tofs[-1]), 3), np.int64)
+    U = np.zeros((int(vofs[-1]), 2), np.float64)
+    for i, ch in enumerate(charts):
+        P[vofs[i]:vofs[i + 1]] = np.asarray(ch[0], np.float64).reshape(-1, 3)
+        T[tofs[i]:tofs[i + 1]] = np.asarray(ch[1], np.int64).reshape(-1, 3)
+        if with_uv and len(ch) > 2 and ch[2] is not None:
+            U[vofs[i]:vofs[i + 1]] = np.asarray(ch[2], np.float64).reshape(-1, 2)
+    return P, T, U, vofs, tofs
+
+
+class DeviceBatch:
+    """Islands resident on one CUDA device, ready for the uva_* kernels."""
+
+    def __init__(self, P, T_local, vofs, tofs, U=None, semantics=_lib.SEM_BATCH, device=None, stream=None,
+                 plan=None):
+        self.dev = require_cuda(device)
+        self.stream = stream
+        self.semantics = int(semantics)
+        plan = plan if plan is not None else Plan(T_local, vofs, tofs)
+        self.plan = plan
+        self.nc, self.n, self.t = plan.nc, plan.n, plan.t
+        d = self.dev
+
+        def up(a, dtype=None):
+            t = torch.from_numpy(np.ascontiguousarray(a))
+            if t.numel() == 0:
+                t = torch.zeros(1, dtype=t.dtype)
+            return t.to(d, non_blocking=False) if dtype is None else t.to(d, dtype)
+
+        # topology
+        self.vofs = up(plan.vofs); self.tofs = up(plan.tofs); self.sofs = up(plan.sofs)
+        self.tri4 = up(plan.tri4); self.tri_edge = up(plan.tri_edge)
+        self.slice_ptr = up(plan.slice_ptr); self.slot_col = up(plan.slot_col)
+        self.slot_edge = up(plan.slot_edge); self.slot_c = up(plan.slot_c)
+        self.vt_ptr = up(plan.vt_ptr); self.vt = up(plan.vt); self.vflags = up(plan.vflags)
+        self.bofs = up(plan.bofs); self.bverts = up(plan.bverts); self.order = up(plan.order)
+        # geometry
+        n, t, nc = max(self.n, 1), max(self.t, 1), max(self.nc, 1)
+        f64, f32 = torch.float64, torch.float32
+        self.P = up(np.asarray(P, np.float64).reshape(-1, 3)) if self.n else torch.zeros((1, 3), dtype=f64, device=d)
+        self.frame = torch.empty((t, 4), dtype=f64, device=d)
+        self.wtri = torch.empty((t, 4), dtype=f64, device=d)
+        self.tscale = torch.ones(t, dtype=f32, device=d)
+        self.wedge = torch.empty(max(plan.E, 1), dtype=f64, device=d)
+        self.slot_w = torch.empty(max(plan.nslots, 1), dtype=f32, device=d)
+        self.wdiag = torch.empty(n, dtype=f64, device=d)
+        self.dinv = torch.empty(n, dtype=f32, device=d)
+        self.pins = torch.zeros((nc, 3), dtype=torch.int32, device=d)
+        self.wpin = torch.empty(nc, dtype=f64, device=d)
+        if U is None:
+            self.U = torch.zeros((n, 2), dtype=f64, device=d)
+        else:
+            self.U = up(np.asarray(U, np.float64).reshape(-1, 2)) if self.n else torch.zeros((1, 2), dtype=f64, device=d)
+        m = max(n, nc)
+        self.x64 = torch.empty((m, 2), dtype=f64, device=d)
+        self.b64 = torch.empty((m, 2), dtype=f64, device=d)
+        self.rc = torch.empty((t, 3, 2), dtype=f64, device=d)
+        self.r32 = torch.empty((n, 2), dtype=f32, device=d)
+        self.d32 = torch.empty((n, 2), dtype=f32, device=d)
+        self.p32 = torch.empty((n, 2), dtype=f32, device=d)
+        self.q32 = torch.empty((n, 2), dtype=f32, device=d)
+        self.status = torch.zeros((nc, C.sizeof(_lib.IslandStatus)), dtype=torch.uint8, device=d)
+        self.work = torch.zeros(8, dtype=torch.int32, device=d)
+        self.desc = self._make_desc()
+        self.setup()
+
+    # ------------------------------------------------------------ plumbing
+    def _make_desc(self):
+        D = _lib.BatchDesc()
+        p = self.plan
+        D.nc, D.n, D.t, D.E = self.nc, self.n, self.t, p.E
+        D.nslices, D.nslots, D.semantics, D.maxrows = p.nslices, p.nslots, self.semantics, p.maxrows
+        for name in ("vofs", "tofs", "sofs", "tri4", "tri_edge", "slice_ptr", "slot_col", "slot_edge", "slot_c",
+                     "vt_ptr", "vt", "vflags", "bofs", "bverts", "order", "P", "frame", "wtri", "tscale", "wedge",
+                     "slot_w", "wdiag", "dinv", "pins", "wpin", "U", "x64", "b64", "rc", "r32", "d32", "p32",
+                     "q32", "status", "work"):
+            setattr(D, name, getattr(self, name).data_ptr())
+        return D
+
+    def _refresh_u(self):
+        """Re-point the descriptor after U was replaced by a new tensor."""
+        self.desc.U = self.U.data_ptr()
+
+    def _stream(self):
+        s = self.stream if self.stream is not None else torch.cuda.current_stream(self.dev)
+        return C.c_void_p(s.cuda_stream)
+
+    def setup(self):
+        check(_lib.lib().uva_batch_setup(C.byref(self.desc), self._stream()), "uva_batch_setup")
+
+    @staticmethod
+    def params(kind="arap", iters=1, line_search=True, energy_tol=0.0, threads=0, **over):
+        base = dict(DEFAULTS[kind])
+        base.update({k: v for k, v in over.items() if v is not None})
+        P = _lib.SolveParams()
+        P.iters = int(iters); P.line_search = 1 if line_search else 0
+        P.tol = float(base["tol"]); P.energy_tol = float(energy_tol)
+        P.inner_eta = float(base["inner_eta"]); P.max_inner = int(base["max_inner"])
+        P.max_refine = int(base["max_refine"]); P.threads = int(threads)
+        return P
+
+    # ------------------------------------------------------------ solvers
+    def lscm(self, **kw):
+        prm = self.params("lscm", **kw)
+        check(_lib.lib().uva_lscm(C.byref(self.desc), C.byref(prm), self._stream()), "uva_lscm")
+
+    def arap(self, iters=8, line_search=True, energy_tol=0.0, **kw):
+        prm = self.params("arap", iters=iters, line_search=line_search, energy_tol=energy_tol, **kw)
+        check(_lib.lib().uva_arap(C.byref(self.desc), C.byref(prm), self._stream()), "uva_arap")
+
+    def orient_positive(self):
+        check(_lib.lib().uva_orient_positive(C.byref(self.desc), self._stream()), "uva_orient_positive")
+
+    def repair_flips(self, rounds=60, serial=False):
+        fn = _lib.lib().uva_repair_flips_serial if serial else _lib.lib().uva_repair_flips
+        check(fn(C.byref(self.desc), int(rounds), self._stream()), "uva_repair_flips")
+
+    def flips_per_chart(self):
+        out = torch.empty(max(self.nc, 1), dtype=torch.float32, device=self.dev)
+        check(_lib.lib().uva_flips_per_chart(C.byref(self.desc), ptr(out), self._stream()), "uva_flips_per_chart")
+        return out[:self.nc]
+
+    def signed_area(self, U=None):
+        U = self.U if U is None else U.to(self.dev, torch.float64).contiguous()
+        out = torch.empty(max(self.t, 1), dtype=torch.float64, device=self.dev)
+        check(_lib.lib().uva_signed_area(C.byref(self.desc), ptr(U), ptr(out), self._stream()), "uva_signed_area")
+        return out[:self.t]
+
+    def jacobians(self, U=None):
+        U = self.U if U is None else U.to(self.dev, torch.float64).contiguous()
+        out = torch.empty((max(self.t, 1), 4), dtype=torch.float64, device=self.dev)
+        check(_lib.lib().uva_jacobians(C.byref(self.desc), ptr(U), ptr(out), self._stream()), "uva_jacobians")
+        return out[:self.t]
+
+    def shrink(self, tri_idx, factor=0.6, floor=0.05, rings=3):
+        sel = torch.zeros(max(self.t, 1), dtype=torch.uint8, device=self.dev)
+        sel[torch.as_tensor(np.asarray(tri_idx, np.int64), device=self.dev)] = 1
+        vmark = torch.empty(max(self.n, 1), dtype=torch.uint8, device=self.dev)
+        check(_lib.lib().uva_shrink(C.byref(self.desc), ptr(sel), ptr(vmark), int(rings), float(factor),
+                                    float(floor), self._stream()), "uva_shrink")
+
+    def island_status(self):
+        """Per-island solver status (host numpy structured array)."""
+        raw = self.status[:self.nc].cpu().numpy()
+        dt = np.dtype([("cg_iters", np.int32), ("refinements", np.int32), ("outer_iters", np.int32),
+                       ("flags", np.int32), ("resid", np.float64, 2), ("energy", np.float64), ("step", np.float64)])
+        return raw.view(dt).reshape(-1)
+
+    def uvs(self):
+        return self.U[:self.n].double().cpu().numpy()
