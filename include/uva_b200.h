@@ -152,6 +152,22 @@ int uva_lscm(uva_batch* b, const uva_solve_params* prm, void* stream);
  * (gpu.py:230-249 with semantics BATCH, param.py:379-414 with PARAM).      */
 int uva_arap(uva_batch* b, const uva_solve_params* prm, void* stream);
 
+/* No counterpart in the reference. The same ARAP iterations as uva_arap, for
+ * callers that cannot allocate device memory while they run (for example a
+ * host application that owns a fixed device pool, or code that must not call
+ * cudaMalloc between frames). It allocates nothing: the solver scratch of `b`
+ * (x64, b64, rc, r32, d32, p32, q32, work) is ignored and replaced by one
+ * static device array of 5,243,136 bytes that every GPU loading the library
+ * holds until exit. The caller still passes the inputs (topology, geometry,
+ * pins, order) and the outputs (U, status). Limits: at most 32768 vertices
+ * and 65536 triangles per call, else UVA_E_TOOBIG. The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture. All calls share the array and it keeps the
+ * last call's contents (the work counter is cleared per call): calls that
+ * overlap on the GPU, from any stream or thread, race and must be serialised
+ * by the caller.                                                            */
+int uva_arap_noalloc(const uva_batch* b, const uva_solve_params* prm, void* stream);
+
 /* Batch utilities (gpu.py:145-299). */
 int uva_orient_positive(uva_batch* b, void* stream);
 int uva_repair_flips(uva_batch* b, int32_t rounds, void* stream);

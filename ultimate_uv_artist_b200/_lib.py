@@ -65,6 +65,7 @@ _SIGS = {
     "uva_batch_setup": [vp, vp],
     "uva_lscm": [vp, vp, vp],
     "uva_arap": [vp, vp, vp],
+    "uva_arap_noalloc": [vp, vp, vp],
     "uva_orient_positive": [vp, vp],
     "uva_repair_flips": [vp, i32, vp],
     "uva_repair_flips_serial": [vp, i32, vp],

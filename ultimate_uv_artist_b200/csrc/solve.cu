@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -808,4 +809,75 @@ extern "C" int uva_lscm(uva_batch* b, const uva_solve_params* prm, void* stream)
         case 512: return launch_arap<512>(b, prm, s, true);
         default: return launch_arap<256>(b, prm, s, true);
     }
+}
+
+// ------------------------------------------------------------------ no-allocation ARAP
+// Fixed solver scratch for uva_arap_noalloc. Some callers of this library
+// cannot allocate device memory while they run ARAP: a host application that
+// owns a fixed device pool, or code that must not call cudaMalloc between
+// frames. They pass their own inputs and outputs and the solver borrows this
+// static array instead of caller-provided scratch. Every GPU that loads the
+// library holds the array until the process exits.
+namespace {
+
+constexpr int64_t kNoAllocMaxVerts = 32768;
+constexpr int64_t kNoAllocMaxTris = 65536;
+constexpr size_t kAlignUp(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+constexpr size_t kNaWork = 256;                                                   // work counter
+constexpr size_t kNaX64 = kAlignUp(sizeof(double) * 2 * kNoAllocMaxVerts);        // x64
+constexpr size_t kNaB64 = kAlignUp(sizeof(double) * 2 * kNoAllocMaxVerts);        // b64
+constexpr size_t kNaRc = kAlignUp(sizeof(double) * 6 * kNoAllocMaxTris);          // rc
+constexpr size_t kNaF32 = kAlignUp(sizeof(float) * 2 * kNoAllocMaxVerts);         // r32, d32, p32, q32
+constexpr size_t kNoAllocBytes = kNaWork + kNaX64 + kNaB64 + kNaRc + 4 * kNaF32;   // 5,243,136 bytes
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device (the host-side symbol is only a stand-in for the device array).
+int noalloc_scratch(unsigned char** out) {
+    static std::mutex mu;
+    static std::vector<unsigned char*> cache;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return uva_cuda_status(e, "uva_arap_noalloc/cudaGetDevice");
+    std::lock_guard<std::mutex> lk(mu);
+    if (static_cast<int>(cache.size()) <= dev) cache.resize(dev + 1, nullptr);
+    if (!cache[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return uva_cuda_status(e, "uva_arap_noalloc/cudaGetSymbolAddress");
+        cache[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = cache[dev];
+    return UVA_OK;
+}
+
+}  // namespace
+
+extern "C" int uva_arap_noalloc(const uva_batch* b, const uva_solve_params* prm, void* stream) {
+    if (!check_batch(b) || !prm || !b->status || !b->U) {
+        uva_set_error("uva_arap_noalloc: bad arguments (status and U are required outputs)");
+        return UVA_E_ARG;
+    }
+    if (b->n > kNoAllocMaxVerts || b->t > kNoAllocMaxTris) {
+        uva_set_error("uva_arap_noalloc: batch above the fixed scratch limit of 32768 vertices / 65536 triangles");
+        return UVA_E_TOOBIG;
+    }
+    if (b->nc == 0 || prm->iters <= 0) return UVA_OK;
+    unsigned char* base = nullptr;
+    const int rc = noalloc_scratch(&base);
+    if (rc != UVA_OK) return rc;
+    uva_batch w = *b;
+    size_t off = 0;
+    w.work = reinterpret_cast<int32_t*>(base + off); off += kNaWork;
+    w.x64 = reinterpret_cast<double*>(base + off); off += kNaX64;
+    w.b64 = reinterpret_cast<double*>(base + off); off += kNaB64;
+    w.rc = reinterpret_cast<double*>(base + off); off += kNaRc;
+    w.r32 = reinterpret_cast<float*>(base + off); off += kNaF32;
+    w.d32 = reinterpret_cast<float*>(base + off); off += kNaF32;
+    w.p32 = reinterpret_cast<float*>(base + off); off += kNaF32;
+    w.q32 = reinterpret_cast<float*>(base + off);
+    // the work counter is the only scratch that must start at zero; launch_arap
+    // clears it on the stream before the launch
+    return launch_arap<256>(&w, prm, static_cast<cudaStream_t>(stream), false);
 }
