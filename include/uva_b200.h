@@ -85,7 +85,8 @@ int uva_plan_sizes(const uva_plan* plan, int64_t* sizes /* UVA_PLAN_NSIZES */);
  *   tri4      t*4   local a,b,c and island id
  *   tri_edge  t*3   global unique-edge id of edge k (corners k+1 -> k+2)
  *   sofs      nc+1  first SELL slice of each island
- *   slice_ptr nslices+1 first slot of each slice (32 rows per slice)
+ *   slice_ptr nslices+1 first slot of each slice (32 rows per slice, width
+ *             padded to a multiple of 4 slots)
  *   slot_col  nslots island-local column (padding: the row itself)
  *   slot_edge nslots global unique-edge id (padding: -1)
  *   slot_c    nslots LSCM boundary coupling H[i, j+n] (param.py:147-150)
@@ -109,15 +110,16 @@ typedef struct uva_batch {
     const int32_t* slice_ptr; const int32_t* slot_col;  const int32_t* slot_edge;
     const float*   slot_c;    const int32_t* vt_ptr;    const int32_t* vt;
     const uint8_t* vflags;    const int32_t* bofs;      const int32_t* bverts;
-    const int32_t* order;     /* nc island ids, largest first (work order)    */
+    const int32_t* order;     /* nc island ids by class, largest first        */
+    int32_t class_ofs[5];     /* host values: class c owns order[ofs[c]..ofs[c+1]) */
     /* geometry, written by uva_batch_setup */
     const double*  P;         /* n*3 positions (FP64)                          */
     double* frame;            /* t*4: x1, x2, y2, area                          */
     double* wtri;             /* t*4: w0, w1, w2 (half cotangents), ok (1/0)    */
     float*  tscale;           /* t: target size (Batch.shrink)                  */
     double* wedge;            /* E: summed edge weight                          */
-    float*  slot_w;           /* nslots: FP32 edge weight of each SELL slot     */
-    double* wdiag;            /* n: exact FP64 row sum of slot_w                */
+    int32_t* slot_cw;         /* nslots*2: packed (column, FP32 weight bits)    */
+    double* wdiag;            /* n: exact FP64 row sum of the slot weights      */
     float*  dinv;             /* n: Jacobi inverse of wdiag (pin row: on the fly)*/
     int32_t* pins;            /* nc*3: ARAP pin, LSCM p0, LSCM p1 (local ids)   */
     double* wpin;             /* nc: soft-pin weight                            */
@@ -129,6 +131,13 @@ typedef struct uva_batch {
     uva_island_status* status;                  /* nc                         */
     int32_t* work;            /* >= 4 ints, zeroed by the callee per launch     */
 } uva_batch;
+
+/* Island size classes of one persistent launch (see uva_arap): islands are
+ * solved by a whole 1024-thread CTA (more than UVA_CLASS_MID vertices), by a
+ * 256-thread sub-team (more than UVA_CLASS_SMALL) or by one warp.           */
+#define UVA_CLASS_BIG   8192   /* above: CG vectors in global memory          */
+#define UVA_CLASS_MID   2048
+#define UVA_CLASS_SMALL 256
 
 typedef struct uva_solve_params {
     int32_t iters;            /* ARAP outer iterations                          */

@@ -27,6 +27,7 @@ ST_ENERGYSTOP = 4
 ST_NOBOUNDARY = 8
 
 PLAN_NSIZES = 8
+CLASS_BIG, CLASS_MID, CLASS_SMALL = 8192, 2048, 256
 (PLAN_NC, PLAN_N, PLAN_T, PLAN_E, PLAN_NSLICES, PLAN_NSLOTS, PLAN_NBVERTS, PLAN_MAXROWS) = range(8)
 
 vp = C.c_void_p
@@ -45,7 +46,8 @@ class BatchDesc(C.Structure):
                 ("vofs", vp), ("tofs", vp), ("sofs", vp), ("tri4", vp), ("tri_edge", vp),
                 ("slice_ptr", vp), ("slot_col", vp), ("slot_edge", vp), ("slot_c", vp),
                 ("vt_ptr", vp), ("vt", vp), ("vflags", vp), ("bofs", vp), ("bverts", vp), ("order", vp),
-                ("P", vp), ("frame", vp), ("wtri", vp), ("tscale", vp), ("wedge", vp), ("slot_w", vp),
+                ("class_ofs", i32 * 5),
+                ("P", vp), ("frame", vp), ("wtri", vp), ("tscale", vp), ("wedge", vp), ("slot_cw", vp),
                 ("wdiag", vp), ("dinv", vp), ("pins", vp), ("wpin", vp), ("U", vp),
                 ("x64", vp), ("b64", vp), ("rc", vp), ("r32", vp), ("d32", vp), ("p32", vp), ("q32", vp),
                 ("status", vp), ("work", vp)]

@@ -6,7 +6,8 @@
 // searches of engine/param.py:59-68 (boundary_edges_oriented) with per-island
 // sorts that run on all host cores, and lays the Laplacian pattern out as a
 // sliced-ELL matrix (32-row slices, column-major inside a slice) so that a warp
-// reads one slot of 32 consecutive rows with one coalesced load.
+// reads one slot of 32 consecutive rows with one coalesced load. Slice widths
+// are padded to a multiple of 4 slots (padding: weight 0, column = the row).
 #include <algorithm>
 #include <atomic>
 #include <cstring>
@@ -122,6 +123,7 @@ void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& 
     for (int32_t s = 0; s < ip.nslices; ++s) {
         int32_t w = 0;
         for (int32_t r = s * 32; r < std::min(n, s * 32 + 32); ++r) w = std::max(w, deg[r]);
+        w = (w + 3) & ~3;            // multiple of 4: the SpMV loads slots 4 at a time
         ip.slice_w[s] = w;
         ip.nslots += 32 * w;
     }

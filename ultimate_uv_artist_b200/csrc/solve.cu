@@ -124,7 +124,7 @@ __global__ void k_rows(uva_batch b, const int32_t* vert_isl) {
         const int q = q0 + 32 * k;
         const int e = b.slot_edge[q];
         const float w32 = e >= 0 ? static_cast<float>(b.wedge[e]) : 0.0f;
-        b.slot_w[q] = w32;
+        reinterpret_cast<int2*>(b.slot_cw)[q] = make_int2(b.slot_col[q], __float_as_int(w32));
         sum += static_cast<double>(w32);
     }
     b.wdiag[v] = sum;
@@ -177,8 +177,128 @@ __global__ void k_vert_isl(const int32_t* vofs, int nc, int32_t* vert_isl) {
 }
 
 // ------------------------------------------------------------------ island solver
+// One persistent launch of 1024-thread CTAs serves four island size classes
+// (islands pre-sorted by vertex count and grouped by class in b.order):
+//   G  n > 8192          whole CTA, CG vectors in global memory (L2)
+//   A  2048 < n <= 8192  whole CTA, CG vectors p, r, d in shared memory
+//   B  256 < n <= 2048   256-thread sub-team (named barrier), shared memory
+//   C  n <= 256          one warp, shared memory
+// A CTA drains class G, then A, then splits into sub-teams for B and warps
+// for C, so small islands fill the SMs while the large ones finish.
+constexpr int KB = 1024;              // CTA size
+constexpr int RB = 8;                 // rows per thread in the shared-memory classes
+constexpr int SUB = 256;              // sub-team size of class B
+constexpr size_t kDynSmem = sizeof(float2) * 3 * KB * RB;   // 196,608 bytes
+
+enum Op { OP_ARAP = 0, OP_LSCM = 1 };
+
+template <int NTT>
+__device__ __forceinline__ void team_sync(int bar) {
+    if constexpr (NTT == 32) {
+        __syncwarp();
+    } else if constexpr (NTT == KB) {
+        __syncthreads();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(NTT) : "memory");
+    }
+}
+
+template <int NTT>
+struct Team {
+    int tid, bar, phase;
+    double* redd;
+    float* redf;
+    int* redi;
+    int* slot;
+    float2 *sp, *sr, *sd;   // CG vectors (shared memory, or null for class G)
+    __device__ __forceinline__ void sync() { team_sync<NTT>(bar); }
+};
+
+// All-reduce of K values over the team; every thread gets bitwise-identical
+// totals (xor butterflies are symmetric; the cross-warp sum runs in one order).
+template <int NTT, int K, typename T>
+__device__ __forceinline__ void team_sum(Team<NTT>& tm, T (&v)[K], T* red) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    }
+    if constexpr (NTT > 32) {
+        constexpr int NW = NTT / 32;
+        const int lane = tm.tid & 31, warp = tm.tid >> 5;
+        T* buf = red + tm.phase * K * NW;
+        tm.phase ^= 1;
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) buf[k * NW + warp] = v[k];
+        }
+        tm.sync();
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            T s = T(0);
+#pragma unroll
+            for (int w = 0; w < NW; ++w) s += buf[k * NW + w];
+            v[k] = s;
+        }
+    } else {
+        __syncwarp();
+    }
+}
+
+template <int NTT>
+__device__ __forceinline__ double team_min(Team<NTT>& tm, double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if constexpr (NTT > 32) {
+        constexpr int NW = NTT / 32;
+        double* buf = tm.redd + tm.phase * 4 * NW;
+        tm.phase ^= 1;
+        if ((tm.tid & 31) == 0) buf[tm.tid >> 5] = v;
+        tm.sync();
+        v = buf[0];
+#pragma unroll
+        for (int w = 1; w < NW; ++w) v = fmin(v, buf[w]);
+    } else {
+        __syncwarp();
+    }
+    return v;
+}
+
+template <int NTT>
+__device__ __forceinline__ int team_or(Team<NTT>& tm, int v) {
+    v = __any_sync(0xffffffffu, v) ? 1 : 0;
+    if constexpr (NTT > 32) {
+        constexpr int NW = NTT / 32;
+        int* buf = tm.redi + tm.phase * NW;
+        tm.phase ^= 1;
+        if ((tm.tid & 31) == 0) buf[tm.tid >> 5] = v;
+        tm.sync();
+        v = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) v |= buf[w];
+    } else {
+        __syncwarp();
+    }
+    return v;
+}
+
+// Rows of the island owned by this thread: i = tid + j*NTT. R > 0: at most R
+// rows (unrolled); R == 0: any number (class G).
+template <int NTT, int R, typename F>
+__device__ __forceinline__ void for_rows(int tid, int n, F&& f) {
+    if constexpr (R > 0) {
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            const int i = tid + j * NTT;
+            if (i < n) f(i, j);
+        }
+    } else {
+        for (int i = tid; i < n; i += NTT) f(i, 0);
+    }
+}
+
 struct Isl {
-    int id, v0, n, f0, nt, s0, pin;
+    int id, v0, n, f0, nt, s0, pin, p0, p1;
     double wpin;
 };
 
@@ -189,38 +309,37 @@ __device__ __forceinline__ Isl load_island(const uva_batch& b, int isl) {
     I.f0 = b.tofs[isl]; I.nt = b.tofs[isl + 1] - I.f0;
     I.s0 = b.sofs[isl];
     I.pin = b.pins[3 * isl];
+    I.p0 = b.pins[3 * isl + 1];
+    I.p1 = b.pins[3 * isl + 2];
     I.wpin = b.wpin[isl];
     return I;
 }
 
-// Sliced-ELL row cursor: row i of the island lives in slice s0 + i/32, lane i%32.
-struct Row {
-    int q0, width;
-};
-__device__ __forceinline__ Row row_of(const uva_batch& b, const Isl& I, int i) {
+__device__ __forceinline__ void row_slots(const uva_batch& b, const Isl& I, int i, int& q0, int& width) {
     const int s = I.s0 + (i >> 5);
-    const int p = b.slice_ptr[s];
-    Row r;
-    r.q0 = p + (i & 31);
-    r.width = (b.slice_ptr[s + 1] - p) >> 5;
-    return r;
+    const int p = __ldg(b.slice_ptr + s);
+    q0 = p + (i & 31);
+    width = (__ldg(b.slice_ptr + s + 1) - p) >> 5;
 }
 
-// Operator modes of the shared CG machinery.
-enum Op { OP_ARAP = 0, OP_LSCM = 1 };
-
-// y = A x for one row (FP64): ARAP Laplacian + soft pin, or the LSCM
-// conformal operator H = [[L, C], [-C, L]] (param.py:145-150).
 template <Op OP>
-__device__ __forceinline__ double2 apply_row64(const uva_batch& b, const Isl& I, int i, const double2* x) {
-    const Row r = row_of(b, I, i);
-    const double2 xi = x[I.v0 + i];
+__device__ __forceinline__ bool is_pinned(const Isl& I, int i) {
+    return OP == OP_LSCM && (i == I.p0 || i == I.p1);
+}
+
+// (A x)_i in FP64 from an FP64 vector (global memory, island-local indices).
+template <Op OP>
+__device__ __forceinline__ double2 apply64(const uva_batch& b, const Isl& I, int i, const double2* x) {
+    int q0, width;
+    row_slots(b, I, i, q0, width);
+    const int2* cw = reinterpret_cast<const int2*>(b.slot_cw);
+    const double2 xi = x[i];
     double ax = 0.0, ay = 0.0;
-    for (int k = 0; k < r.width; ++k) {
-        const int q = r.q0 + 32 * k;
-        const int j = __ldg(b.slot_col + q);
-        const double w = static_cast<double>(__ldg(b.slot_w + q));
-        const double2 xj = x[I.v0 + j];
+    for (int k = 0; k < width; ++k) {
+        const int q = q0 + 32 * k;
+        const int2 s = __ldg(cw + q);
+        const double w = static_cast<double>(__int_as_float(s.y));
+        const double2 xj = x[s.x];
         ax += w * (xi.x - xj.x);
         ay += w * (xi.y - xj.y);
         if (OP == OP_LSCM) {
@@ -233,199 +352,191 @@ __device__ __forceinline__ double2 apply_row64(const uva_batch& b, const Isl& I,
     return make_double2(ax, ay);
 }
 
+// (A p)_i in FP32, four slots per step (slice widths are multiples of 4).
 template <Op OP>
-__device__ __forceinline__ float2 apply_row32(const uva_batch& b, const Isl& I, int i, const float2* x, float wpin32) {
-    const Row r = row_of(b, I, i);
-    const float2 xi = x[I.v0 + i];
-    float ax = 0.0f, ay = 0.0f;
-    for (int k = 0; k < r.width; ++k) {
-        const int q = r.q0 + 32 * k;
-        const int j = __ldg(b.slot_col + q);
-        const float w = __ldg(b.slot_w + q);
-        const float2 xj = x[I.v0 + j];
-        ax = fmaf(w, xi.x - xj.x, ax);
-        ay = fmaf(w, xi.y - xj.y, ay);
+__device__ __forceinline__ float2 apply32(const uva_batch& b, const Isl& I, int i, const float2* p, float wpin32) {
+    int q0, width;
+    row_slots(b, I, i, q0, width);
+    const int2* cw = reinterpret_cast<const int2*>(b.slot_cw);
+    const float2 xi = p[i];
+    float ax = 0.f, ay = 0.f;
+    for (int k = 0; k < width; k += 4) {
+        int2 s[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s[u] = __ldg(cw + q0 + 32 * (k + u));
+        float c[4];
         if (OP == OP_LSCM) {
-            const float c = __ldg(b.slot_c + q);
-            ax = fmaf(c, xj.y, ax);
-            ay = fmaf(-c, xj.x, ay);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) c[u] = __ldg(b.slot_c + q0 + 32 * (k + u));
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float2 xj = p[s[u].x];
+            const float w = __int_as_float(s[u].y);
+            ax = fmaf(w, xi.x - xj.x, ax);
+            ay = fmaf(w, xi.y - xj.y, ay);
+            if (OP == OP_LSCM) {
+                ax = fmaf(c[u], xj.y, ax);
+                ay = fmaf(-c[u], xj.x, ay);
+            }
         }
     }
     if (OP == OP_ARAP && i == I.pin) { ax = fmaf(wpin32, xi.x, ax); ay = fmaf(wpin32, xi.y, ay); }
     return make_float2(ax, ay);
 }
 
-struct Lscm {
-    int p0, p1;   // pinned vertices (local); -1 when unused
-};
-
-__device__ __forceinline__ bool pinned(const Lscm& L, int i) { return i == L.p0 || i == L.p1; }
-
-__device__ __forceinline__ float jacobi(const uva_batch& b, const Isl& I, int i, Op op) {
-    const float d = b.dinv[I.v0 + i];
-    if (op == OP_ARAP && i == I.pin) {
+template <Op OP>
+__device__ __forceinline__ float jacobi(const uva_batch& b, const Isl& I, int i) {
+    if (is_pinned<OP>(I, i)) return 0.0f;
+    if (OP == OP_ARAP && i == I.pin) {
         const double diag = b.wdiag[I.v0 + i] + I.wpin;
         return diag > 1e-30 ? static_cast<float>(1.0 / diag) : 1.0f;
     }
-    return d;
+    return __ldg(b.dinv + I.v0 + i);
 }
 
-// Shared-memory workspace of one team.
-template <int NT>
-struct Smem {
-    double redd[2 * 4 * (NT / 32)];
-    float redf[2 * 4 * (NT / 32)];
-    int redi[2 * (NT / 32)];
-    int island;
-};
-
-// Solves A x = rhs for one island: x64 holds the start on entry and the
-// solution on exit. FP64 residual recomputation (refinement) around FP32
-// Jacobi-PCG corrections. NCOL = 2 (ARAP: u and v separately) or 1 (LSCM:
-// one vector of 2n unknowns). Returns inner iterations; writes residuals.
-template <int NT, Op OP, int NCOL>
-__device__ int refine_solve(const uva_batch& b, const Isl& I, const Lscm& LS, const uva_solve_params& prm,
-                            const double bb[2], Smem<NT>& sm, int& phase, double res_out[2], int& nref,
-                            bool& capped) {
-    const int tid = threadIdx.x;
-    double2* x64 = reinterpret_cast<double2*>(b.x64);
-    const double2* b64 = reinterpret_cast<const double2*>(b.b64);
-    float2* r32 = reinterpret_cast<float2*>(b.r32);
-    float2* d32 = reinterpret_cast<float2*>(b.d32);
-    float2* p32 = reinterpret_cast<float2*>(b.p32);
-    float2* q32 = reinterpret_cast<float2*>(b.q32);
+// Solves A x = rhs for one island. x64 (global, FP64) holds the start on entry
+// and the solution on exit. FP64 residual refinement around FP32 Jacobi-PCG
+// corrections; NCOL = 2 (ARAP: u and v separately) or 1 (LSCM: one vector of
+// 2n unknowns). Returns the inner CG iterations executed.
+template <int NTT, int R, Op OP, int NCOL>
+__device__ int refine_solve(const uva_batch& b, const Isl& I, const uva_solve_params& prm, Team<NTT>& tm,
+                            const double bb[2], double res_out[2], int& nref, bool& capped) {
+    double2* x64 = reinterpret_cast<double2*>(b.x64) + I.v0;
+    const double2* b64 = reinterpret_cast<const double2*>(b.b64) + I.v0;
+    float2* sp = tm.sp ? tm.sp : reinterpret_cast<float2*>(b.p32) + I.v0;
+    float2* sr = tm.sr ? tm.sr : reinterpret_cast<float2*>(b.r32) + I.v0;
+    float2* sd = tm.sd ? tm.sd : reinterpret_cast<float2*>(b.d32) + I.v0;
+    float2* sq = reinterpret_cast<float2*>(b.q32) + I.v0;   // class G only
     const float wpin32 = static_cast<float>(I.wpin);
+    const int tid = tm.tid, n = I.n;
+    float2 qreg[R > 0 ? R : 1];
     int total = 0;
     capped = false;
     nref = 0;
     for (int ref = 0;; ++ref) {
         // ---- FP64 residual r = rhs - A x
         double rr[2] = {0.0, 0.0};
-        for (int i = tid; i < I.n; i += NT) {
-            double2 r;
-            if (OP == OP_LSCM && pinned(LS, i)) {
-                r = make_double2(0.0, 0.0);
-            } else {
-                const double2 ax = apply_row64<OP>(b, I, i, x64);
-                const double2 rhs = OP == OP_ARAP ? b64[I.v0 + i] : make_double2(0.0, 0.0);
-                r = rhs - ax;
+        for_rows<NTT, R>(tid, n, [&](int i, int) {
+            double2 r = make_double2(0.0, 0.0);
+            if (!is_pinned<OP>(I, i)) {
+                const double2 ax = apply64<OP>(b, I, i, x64);
+                const double2 rhs = OP == OP_ARAP ? b64[i] : make_double2(0.0, 0.0);
+                r = make_double2(rhs.x - ax.x, rhs.y - ax.y);
             }
-            r32[I.v0 + i] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
+            sr[i] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
             rr[0] += r.x * r.x;
             rr[1] += r.y * r.y;
-        }
-        block_sum<NT, 2>(rr, sm.redd, phase);
+        });
+        team_sum<NTT, 2>(tm, rr, tm.redd);
         ++nref;
-        double res[2];
-        bool done = true;
+        bool done;
         if (NCOL == 2) {
-            for (int c = 0; c < 2; ++c) {
-                res[c] = sqrt(rr[c] / fmax(bb[c], 1e-300));
-                if (!(rr[c] <= prm.tol * prm.tol * fmax(bb[c], 1e-300))) done = false;
-            }
+            res_out[0] = sqrt(rr[0] / fmax(bb[0], 1e-300));
+            res_out[1] = sqrt(rr[1] / fmax(bb[1], 1e-300));
+            done = rr[0] <= prm.tol * prm.tol * fmax(bb[0], 1e-300) && rr[1] <= prm.tol * prm.tol * fmax(bb[1], 1e-300);
         } else {
             const double s = rr[0] + rr[1];
-            res[0] = res[1] = sqrt(s / fmax(bb[0], 1e-300));
+            res_out[0] = res_out[1] = sqrt(s / fmax(bb[0], 1e-300));
             done = s <= prm.tol * prm.tol * fmax(bb[0], 1e-300);
         }
-        res_out[0] = res[0]; res_out[1] = res[1];
         if (done) break;
         if (ref >= prm.max_refine || !isfinite(rr[0] + rr[1])) { capped = true; break; }
-        // ---- inner FP32 PCG on A d = r (d0 = 0)
-        float rz[2] = {0.f, 0.f}, r0[2] = {0.f, 0.f};
-        for (int i = tid; i < I.n; i += NT) {
-            const float2 r = r32[I.v0 + i];
-            const float m = (OP == OP_LSCM && pinned(LS, i)) ? 0.0f : jacobi(b, I, i, OP);
-            const float2 z = make_float2(m * r.x, m * r.y);
-            d32[I.v0 + i] = make_float2(0.f, 0.f);
-            p32[I.v0 + i] = z;
-            rz[0] += r.x * z.x; rz[1] += r.y * z.y;
-            r0[0] += r.x * r.x; r0[1] += r.y * r.y;
-        }
-        float red4[4] = {rz[0], rz[1], r0[0], r0[1]};
-        block_sum<NT, 4>(red4, sm.redf, phase);
-        float thr[2];
+        // ---- inner FP32 PCG on A d = r, d0 = 0
+        float red4[4] = {0.f, 0.f, 0.f, 0.f};   // r.z (2), r.r (2)
+        for_rows<NTT, R>(tid, n, [&](int i, int) {
+            const float2 r = sr[i];
+            const float m = jacobi<OP>(b, I, i);
+            sd[i] = make_float2(0.f, 0.f);
+            sp[i] = make_float2(m * r.x, m * r.y);
+            red4[0] += m * r.x * r.x; red4[1] += m * r.y * r.y;
+            red4[2] += r.x * r.x; red4[3] += r.y * r.y;
+        });
+        team_sum<NTT, 4>(tm, red4, tm.redf);
+        float rz[2], thr2[2];
         bool act[2];
         if (NCOL == 2) {
+#pragma unroll
             for (int c = 0; c < 2; ++c) {
                 rz[c] = red4[c];
-                const float a = static_cast<float>(prm.inner_eta) * sqrtf(red4[2 + c]);
-                const float t = static_cast<float>(0.5 * prm.tol * sqrt(bb[c]));
-                thr[c] = fmaxf(a, t);
-                act[c] = red4[2 + c] > thr[c] * thr[c] && rz[c] > 0.f;
+                const float t = fmaxf(static_cast<float>(prm.inner_eta) * sqrtf(red4[2 + c]),
+                                      static_cast<float>(0.5 * prm.tol * sqrt(bb[c])));
+                thr2[c] = t * t;
+                act[c] = red4[2 + c] > thr2[c] && rz[c] > 0.f;
             }
         } else {
-            rz[0] = red4[0] + red4[1]; rz[1] = rz[0];
-            const float a = static_cast<float>(prm.inner_eta) * sqrtf(red4[2] + red4[3]);
-            const float t = static_cast<float>(0.5 * prm.tol * sqrt(bb[0]));
-            thr[0] = thr[1] = fmaxf(a, t);
-            act[0] = act[1] = (red4[2] + red4[3]) > thr[0] * thr[0] && rz[0] > 0.f;
+            rz[0] = rz[1] = red4[0] + red4[1];
+            const float t = fmaxf(static_cast<float>(prm.inner_eta) * sqrtf(red4[2] + red4[3]),
+                                  static_cast<float>(0.5 * prm.tol * sqrt(bb[0])));
+            thr2[0] = thr2[1] = t * t;
+            act[0] = act[1] = (red4[2] + red4[3]) > thr2[0] && rz[0] > 0.f;
         }
         int it = 0;
         while ((act[0] || act[1]) && it < prm.max_inner) {
-            __syncthreads();   // p complete
+            tm.sync();   // p complete
             float pq[2] = {0.f, 0.f};
-            for (int i = tid; i < I.n; i += NT) {
-                float2 q;
-                if (OP == OP_LSCM && pinned(LS, i)) q = make_float2(0.f, 0.f);
-                else q = apply_row32<OP>(b, I, i, p32, wpin32);
-                q32[I.v0 + i] = q;
-                const float2 p = p32[I.v0 + i];
+            for_rows<NTT, R>(tid, n, [&](int i, int j) {
+                float2 q = make_float2(0.f, 0.f);
+                if (!is_pinned<OP>(I, i)) q = apply32<OP>(b, I, i, sp, wpin32);
+                if constexpr (R > 0) qreg[j] = q; else sq[i] = q;
+                const float2 p = sp[i];
                 pq[0] += p.x * q.x; pq[1] += p.y * q.y;
-            }
-            block_sum<NT, 2>(pq, sm.redf, phase);
+            });
+            team_sum<NTT, 2>(tm, pq, tm.redf);
             float alpha[2];
             if (NCOL == 2) {
-                for (int c = 0; c < 2; ++c) alpha[c] = (act[c] && pq[c] > 0.f) ? rz[c] / pq[c] : 0.f;
+                alpha[0] = (act[0] && pq[0] > 0.f) ? rz[0] / pq[0] : 0.f;
+                alpha[1] = (act[1] && pq[1] > 0.f) ? rz[1] / pq[1] : 0.f;
             } else {
                 const float s = pq[0] + pq[1];
                 alpha[0] = alpha[1] = (act[0] && s > 0.f) ? rz[0] / s : 0.f;
             }
-            float acc[4] = {0.f, 0.f, 0.f, 0.f};   // rz_new (2), rr (2)
-            for (int i = tid; i < I.n; i += NT) {
-                const float2 p = p32[I.v0 + i], q = q32[I.v0 + i];
-                float2 d = d32[I.v0 + i], r = r32[I.v0 + i];
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            for_rows<NTT, R>(tid, n, [&](int i, int j) {
+                float2 q;
+                if constexpr (R > 0) q = qreg[j]; else q = sq[i];
+                const float2 p = sp[i];
+                float2 d = sd[i], r = sr[i];
                 d.x = fmaf(alpha[0], p.x, d.x); d.y = fmaf(alpha[1], p.y, d.y);
                 r.x = fmaf(-alpha[0], q.x, r.x); r.y = fmaf(-alpha[1], q.y, r.y);
-                d32[I.v0 + i] = d; r32[I.v0 + i] = r;
-                const float m = (OP == OP_LSCM && pinned(LS, i)) ? 0.0f : jacobi(b, I, i, OP);
-                acc[0] += r.x * m * r.x; acc[1] += r.y * m * r.y;
+                sd[i] = d; sr[i] = r;
+                const float m = jacobi<OP>(b, I, i);
+                acc[0] += m * r.x * r.x; acc[1] += m * r.y * r.y;
                 acc[2] += r.x * r.x; acc[3] += r.y * r.y;
-            }
-            block_sum<NT, 4>(acc, sm.redf, phase);
+            });
+            team_sum<NTT, 4>(tm, acc, tm.redf);
             ++it;
             float beta[2];
             if (NCOL == 2) {
+#pragma unroll
                 for (int c = 0; c < 2; ++c) {
-                    const bool conv = acc[2 + c] <= thr[c] * thr[c];
                     beta[c] = (act[c] && rz[c] > 0.f) ? acc[c] / rz[c] : 0.f;
                     if (act[c]) rz[c] = acc[c];
-                    if (conv || !(acc[c] > 0.f)) act[c] = false;
+                    if (acc[2 + c] <= thr2[c] || !(acc[c] > 0.f)) act[c] = false;
                 }
             } else {
-                const float s = acc[0] + acc[1], rrs = acc[2] + acc[3];
-                const bool conv = rrs <= thr[0] * thr[0];
+                const float s = acc[0] + acc[1];
                 beta[0] = beta[1] = (act[0] && rz[0] > 0.f) ? s / rz[0] : 0.f;
                 rz[0] = rz[1] = s;
-                if (conv || !(s > 0.f)) act[0] = act[1] = false;
+                if (acc[2] + acc[3] <= thr2[0] || !(s > 0.f)) act[0] = act[1] = false;
             }
             if (!(act[0] || act[1])) break;
-            for (int i = tid; i < I.n; i += NT) {
-                const float2 r = r32[I.v0 + i], p = p32[I.v0 + i];
-                const float m = (OP == OP_LSCM && pinned(LS, i)) ? 0.0f : jacobi(b, I, i, OP);
-                p32[I.v0 + i] = make_float2(fmaf(beta[0], p.x, m * r.x), fmaf(beta[1], p.y, m * r.y));
-            }
+            for_rows<NTT, R>(tid, n, [&](int i, int) {
+                const float2 r = sr[i], p = sp[i];
+                const float m = jacobi<OP>(b, I, i);
+                sp[i] = make_float2(fmaf(beta[0], p.x, m * r.x), fmaf(beta[1], p.y, m * r.y));
+            });
         }
         if (it >= prm.max_inner) capped = true;
         total += it;
-        __syncthreads();
-        for (int i = tid; i < I.n; i += NT) {
-            const float2 d = d32[I.v0 + i];
-            double2 x = x64[I.v0 + i];
+        tm.sync();
+        for_rows<NTT, R>(tid, n, [&](int i, int) {
+            const float2 d = sd[i];
+            double2 x = x64[i];
             x.x += static_cast<double>(d.x); x.y += static_cast<double>(d.y);
-            x64[I.v0 + i] = x;
-        }
-        __syncthreads();
+            x64[i] = x;
+        });
+        tm.sync();
     }
     return total;
 }
@@ -443,6 +554,7 @@ __device__ __forceinline__ void local_terms(const uva_batch& b, const Isl& I, in
     double c = 1.0, s = 0.0;
     const double sar = du1x * du2y - du2x * du1y;
     flip = sar <= 0.0 ? 1 : 0;
+    energy = 0.0;
     if (batch) {
         if (wt.w != 0.0) {
             const double j00 = du1x / x1, j10 = du1y / x1;
@@ -458,26 +570,22 @@ __device__ __forceinline__ void local_terms(const uva_batch& b, const Isl& I, in
         }
         const double sc = static_cast<double>(b.tscale[f]);
         c *= sc; s *= sc;
-        energy = 0.0;
-    } else {
-        energy = 0.0;
-        if (fabs(x1 * y2) >= 1e-300) {
-            const double j00 = du1x / x1, j10 = du1y / x1;
-            const double j01 = (du2x - j00 * x2) / y2, j11 = (du2y - j10 * x2) / y2;
-            double ca = j00 + j11, cb = j10 - j01;
-            double h = sqrt(ca * ca + cb * cb);
-            if (h < 1e-300) { ca = 1.0; cb = 0.0; h = 1.0; }
-            c = ca / h; s = cb / h;
-            const double qe = 0.5 * (j00 + j11), qh = 0.5 * (j10 - j01);
-            const double rf = 0.5 * (j00 - j11), rg = 0.5 * (j10 + j01);
-            const double q = sqrt(qe * qe + qh * qh), r = sqrt(rf * rf + rg * rg);
-            energy = fr.w * ((q + r - 1.0) * (q + r - 1.0) + (q - r - 1.0) * (q - r - 1.0));
-        }
+    } else if (fabs(x1 * y2) >= 1e-300) {
+        const double j00 = du1x / x1, j10 = du1y / x1;
+        const double j01 = (du2x - j00 * x2) / y2, j11 = (du2y - j10 * x2) / y2;
+        double ca = j00 + j11, cb = j10 - j01;
+        double h = sqrt(ca * ca + cb * cb);
+        if (h < 1e-300) { ca = 1.0; cb = 0.0; h = 1.0; }
+        c = ca / h; s = cb / h;
+        const double qe = 0.5 * (j00 + j11), qh = 0.5 * (j10 - j01);
+        const double rf = 0.5 * (j00 - j11), rg = 0.5 * (j10 + j01);
+        const double q = sqrt(qe * qe + qh * qh), r = sqrt(rf * rf + rg * rg);
+        energy = fr.w * ((q + r - 1.0) * (q + r - 1.0) + (q - r - 1.0) * (q - r - 1.0));
     }
     // edge k runs corner k+1 -> k+2; frame corners (0,0), (x1,0), (x2,y2)
     const double cxs[3] = {0.0, x1, x2}, cys[3] = {0.0, 0.0, y2};
-    double vx[3], vy[3];
     const double wk[3] = {wt.x, wt.y, wt.z};
+    double vx[3], vy[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const int i = (k + 1) % 3, j = (k + 2) % 3;
@@ -499,7 +607,9 @@ __device__ __forceinline__ double step_bound(const uva_batch& b, const Isl& I, i
                                              bool batch) {
     const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
     const double2 u0 = U[I.v0 + tv.x], u1 = U[I.v0 + tv.y], u2 = U[I.v0 + tv.z];
-    const double2 d0 = X[I.v0 + tv.x] - u0, d1 = X[I.v0 + tv.y] - u1, d2 = X[I.v0 + tv.z] - u2;
+    const double2 x0 = X[I.v0 + tv.x], x1 = X[I.v0 + tv.y], x2 = X[I.v0 + tv.z];
+    const double2 d0 = make_double2(x0.x - u0.x, x0.y - u0.y), d1 = make_double2(x1.x - u1.x, x1.y - u1.y),
+                  d2 = make_double2(x2.x - u2.x, x2.y - u2.y);
     const double ux1 = u1.x - u0.x, uy1 = u1.y - u0.y, ux2 = u2.x - u0.x, uy2 = u2.y - u0.y;
     const double dx1 = d1.x - d0.x, dy1 = d1.y - d0.y, dx2 = d2.x - d0.x, dy2 = d2.y - d0.y;
     const double C = ux1 * uy2 - ux2 * uy1;
@@ -522,9 +632,7 @@ __device__ __forceinline__ double step_bound(const uva_batch& b, const Isl& I, i
         }
         return isnan(t) ? big : t;
     }
-    if (A == 0.0 || fabs(A) < 1e-30 * fmax(fabs(B), 1e-300)) {
-        return B < 0.0 ? -C / B : big;
-    }
+    if (A == 0.0 || fabs(A) < 1e-30 * fmax(fabs(B), 1e-300)) return B < 0.0 ? -C / B : big;
     const double disc = B * B - 4.0 * A * C;
     if (disc < 0.0) return big;
     const double sq = sqrt(disc);
@@ -535,207 +643,228 @@ __device__ __forceinline__ double step_bound(const uva_batch& b, const Isl& I, i
     return t;
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT) k_arap(uva_batch b, uva_solve_params prm, const int32_t* order, int count) {
-    __shared__ Smem<NT> sm;
-    int phase = 0;
-    const int tid = threadIdx.x;
+// ---- ARAP outer iterations of one island (gpu.py:230-249 / param.py:379-414)
+template <int NTT, int R>
+__device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, const Isl& I) {
+    const int tid = tm.tid;
     const bool batch = b.semantics == UVA_SEM_BATCH;
     double2* U = reinterpret_cast<double2*>(b.U);
     double2* x64 = reinterpret_cast<double2*>(b.x64);
     double2* b64 = reinterpret_cast<double2*>(b.b64);
     const double2* rc = reinterpret_cast<const double2*>(b.rc);
-    for (;;) {
-        if (tid == 0) sm.island = atomicAdd(b.work, 1);
-        __syncthreads();
-        const int qi = sm.island;
-        __syncthreads();
-        if (qi >= count) break;
-        const Isl I = load_island(b, order[qi]);
-        const Lscm LS{-1, -1};
-        uva_island_status st{};
-        bool use_ls = prm.line_search != 0;
-        double prev_e = 0.0;
-        for (int it = 0; it < prm.iters; ++it) {
-            // ---- local step over the island's triangles
-            double e_loc[1] = {0.0};
-            int flips = 0;
-            for (int f = I.f0 + tid; f < I.f0 + I.nt; f += NT) {
-                double e; int fl;
-                local_terms(b, I, f, U, batch, e, fl);
-                e_loc[0] += e;
-                flips += fl;
-            }
-            if (!batch) {
-                double ev[2] = {e_loc[0], static_cast<double>(flips)};
-                block_sum<NT, 2>(ev, sm.redd, phase);
-                if (it == 0) {
-                    use_ls = prm.line_search != 0 && ev[1] == 0.0;
-                    prev_e = ev[0];
-                } else if (prm.energy_tol > 0.0 && fabs(prev_e - ev[0]) <= prm.energy_tol * fmax(prev_e, 1e-300)) {
-                    st.flags |= UVA_ST_ENERGYSTOP;
-                    st.energy = ev[0];
-                    break;
-                } else {
-                    prev_e = ev[0];
-                }
-                st.energy = ev[0];
-            }
-            __syncthreads();   // corner terms complete
-            // ---- gather the right-hand side per vertex, warm start x = U
-            double bb[2] = {0.0, 0.0};
-            for (int i = tid; i < I.n; i += NT) {
-                const int v = I.v0 + i;
-                double bx = 0.0, by = 0.0;
-                for (int p = b.vt_ptr[v]; p < b.vt_ptr[v + 1]; ++p) {
-                    const double2 c = rc[b.vt[p]];
-                    bx += c.x; by += c.y;
-                }
-                const double2 u = U[v];
-                if (i == I.pin) { bx += I.wpin * u.x; by += I.wpin * u.y; }
-                b64[v] = make_double2(bx, by);
-                x64[v] = u;
-                bb[0] += bx * bx; bb[1] += by * by;
-            }
-            block_sum<NT, 2>(bb, sm.redd, phase);
-            // ---- global step
-            int nref = 0;
-            bool capped = false;
-            st.cg_iters += refine_solve<NT, OP_ARAP, 2>(b, I, LS, prm, bb, sm, phase, st.resid, nref, capped);
-            st.refinements += nref;
-            if (capped) st.flags |= UVA_ST_MAXITER;
-            // ---- non-finite charts keep their layout (gpu.py:235-240)
-            int bad = 0;
-            for (int i = tid; i < I.n; i += NT) bad |= finite2(x64[I.v0 + i]) ? 0 : 1;
-            bad = block_or<NT>(bad, sm.redi, phase);
-            if (bad) {
-                st.flags |= UVA_ST_NONFINITE;
-                st.outer_iters = it + 1;
-                continue;
-            }
-            double step = 1.0;
-            if (use_ls) {
-                double tmin = 1e30;
-                for (int f = I.f0 + tid; f < I.f0 + I.nt; f += NT) tmin = fmin(tmin, step_bound(b, I, f, U, x64, batch));
-                tmin = block_min<NT, double>(tmin, sm.redd, phase);
-                step = batch ? fmin(0.9 * tmin, 1.0) : fmin(1.0, 0.9 * tmin);
-            }
-            st.step = step;
-            for (int i = tid; i < I.n; i += NT) {
-                const int v = I.v0 + i;
-                const double2 u = U[v], x = x64[v];
-                U[v] = use_ls ? make_double2(u.x + (x.x - u.x) * step, u.y + (x.y - u.y) * step) : x;
-            }
-            st.outer_iters = it + 1;
-            __syncthreads();
+    uva_island_status st{};
+    bool use_ls = prm.line_search != 0;
+    double prev_e = 0.0;
+    for (int it = 0; it < prm.iters; ++it) {
+        double ev[2] = {0.0, 0.0};
+        for (int f = I.f0 + tid; f < I.f0 + I.nt; f += NTT) {
+            double e; int fl;
+            local_terms(b, I, f, U, batch, e, fl);
+            ev[0] += e; ev[1] += fl;
         }
-        if (tid == 0) b.status[I.id] = st;
-        __syncthreads();
+        if (!batch) {
+            team_sum<NTT, 2>(tm, ev, tm.redd);
+            if (it == 0) {
+                use_ls = prm.line_search != 0 && ev[1] == 0.0;
+                prev_e = ev[0];
+            } else if (prm.energy_tol > 0.0 && fabs(prev_e - ev[0]) <= prm.energy_tol * fmax(prev_e, 1e-300)) {
+                st.flags |= UVA_ST_ENERGYSTOP;
+                st.energy = ev[0];
+                break;
+            } else {
+                prev_e = ev[0];
+            }
+            st.energy = ev[0];
+        }
+        tm.sync();   // corner terms complete
+        double bb[2] = {0.0, 0.0};
+        for_rows<NTT, R>(tid, I.n, [&](int i, int) {
+            const int v = I.v0 + i;
+            double bx = 0.0, by = 0.0;
+            const int pe = __ldg(b.vt_ptr + v + 1);
+            for (int p = __ldg(b.vt_ptr + v); p < pe; ++p) {
+                const double2 c = rc[__ldg(b.vt + p)];
+                bx += c.x; by += c.y;
+            }
+            const double2 u = U[v];
+            if (i == I.pin) { bx += I.wpin * u.x; by += I.wpin * u.y; }
+            b64[v] = make_double2(bx, by);
+            x64[v] = u;
+            bb[0] += bx * bx; bb[1] += by * by;
+        });
+        team_sum<NTT, 2>(tm, bb, tm.redd);   // also publishes x64 / b64 to the team
+        int nref = 0;
+        bool capped = false;
+        st.cg_iters += refine_solve<NTT, R, OP_ARAP, 2>(b, I, prm, tm, bb, st.resid, nref, capped);
+        st.refinements += nref;
+        if (capped) st.flags |= UVA_ST_MAXITER;
+        int bad = 0;
+        for_rows<NTT, R>(tid, I.n, [&](int i, int) { bad |= finite2(x64[I.v0 + i]) ? 0 : 1; });
+        bad = team_or(tm, bad);
+        st.outer_iters = it + 1;
+        if (bad) {   // non-finite charts keep their layout (gpu.py:235-240)
+            st.flags |= UVA_ST_NONFINITE;
+            continue;
+        }
+        double step = 1.0;
+        if (use_ls) {
+            double tmin = 1e30;
+            for (int f = I.f0 + tid; f < I.f0 + I.nt; f += NTT) tmin = fmin(tmin, step_bound(b, I, f, U, x64, batch));
+            tmin = team_min(tm, tmin);
+            step = fmin(0.9 * tmin, 1.0);
+        }
+        st.step = step;
+        tm.sync();   // all line-search reads of U done
+        for_rows<NTT, R>(tid, I.n, [&](int i, int) {
+            const int v = I.v0 + i;
+            const double2 u = U[v], x = x64[v];
+            U[v] = use_ls ? make_double2(u.x + (x.x - u.x) * step, u.y + (x.y - u.y) * step) : x;
+        });
+        tm.sync();
     }
+    if (tid == 0) b.status[I.id] = st;
 }
 
-// LSCM per island: hard pins p0 -> (0,0), p1 -> (|P[p1]-P[p0]|, 0); start
-// from the projection onto the mean-normal plane aligned with the pins.
-template <int NT>
-__global__ void __launch_bounds__(NT) k_lscm(uva_batch b, uva_solve_params prm, const int32_t* order, int count) {
-    __shared__ Smem<NT> sm;
-    __shared__ double basis[8];
-    int phase = 0;
-    const int tid = threadIdx.x;
+// ---- LSCM of one island: hard pins p0 -> (0,0), p1 -> (|P[p1]-P[p0]|, 0);
+// start from the projection on the mean-normal plane aligned with the pins.
+template <int NTT, int R>
+__device__ void solve_lscm(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, const Isl& I) {
+    const int tid = tm.tid;
     double2* x64 = reinterpret_cast<double2*>(b.x64);
     double2* U = reinterpret_cast<double2*>(b.U);
     const double* P = b.P;
-    for (;;) {
-        if (tid == 0) sm.island = atomicAdd(b.work, 1);
-        __syncthreads();
-        const int qi = sm.island;
-        __syncthreads();
-        if (qi >= count) break;
-        const Isl I = load_island(b, order[qi]);
-        Lscm LS{b.pins[3 * I.id + 1], b.pins[3 * I.id + 2]};
-        uva_island_status st{};
-        if (LS.p0 < 0 || I.n == 0) {
-            st.flags |= UVA_ST_NOBOUNDARY;
-            for (int i = tid; i < I.n; i += NT) U[I.v0 + i] = make_double2(0.0, 0.0);
-            if (tid == 0) b.status[I.id] = st;
-            __syncthreads();
-            continue;
-        }
-        // mean normal (sum of triangle cross products)
-        double nrm[3] = {0.0, 0.0, 0.0};
-        for (int f = I.f0 + tid; f < I.f0 + I.nt; f += NT) {
-            const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
-            const double* a = P + 3 * (I.v0 + tv.x);
-            const double* c1 = P + 3 * (I.v0 + tv.y);
-            const double* c2 = P + 3 * (I.v0 + tv.z);
-            const double e1x = c1[0] - a[0], e1y = c1[1] - a[1], e1z = c1[2] - a[2];
-            const double e2x = c2[0] - a[0], e2y = c2[1] - a[1], e2z = c2[2] - a[2];
-            nrm[0] += e1y * e2z - e1z * e2y;
-            nrm[1] += e1z * e2x - e1x * e2z;
-            nrm[2] += e1x * e2y - e1y * e2x;
-        }
-        block_sum<NT, 3>(nrm, sm.redd, phase);
-        const double* pp0 = P + 3 * (I.v0 + LS.p0);
-        const double* pp1 = P + 3 * (I.v0 + LS.p1);
-        if (tid == 0) {
-            double nl = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
-            double nx = 0.0, ny = 0.0, nz = 1.0;
-            if (nl > 0.0 && isfinite(nl)) { nx = nrm[0] / nl; ny = nrm[1] / nl; nz = nrm[2] / nl; }
-            double ax = pp1[0] - pp0[0], ay = pp1[1] - pp0[1], az = pp1[2] - pp0[2];
-            const double d = sqrt(ax * ax + ay * ay + az * az);
-            const double dn = ax * nx + ay * ny + az * nz;
-            ax -= dn * nx; ay -= dn * ny; az -= dn * nz;
-            double al = sqrt(ax * ax + ay * ay + az * az);
-            double s = 1.0;
-            if (al > 0.0 && isfinite(al)) { s = d / al; ax /= al; ay /= al; az /= al; }
-            else { ax = 1.0; ay = 0.0; az = 0.0; }
-            basis[0] = ax * s; basis[1] = ay * s; basis[2] = az * s;
-            basis[3] = (ny * az - nz * ay) * s; basis[4] = (nz * ax - nx * az) * s; basis[5] = (nx * ay - ny * ax) * s;
-            basis[6] = d;
-        }
-        __syncthreads();
-        for (int i = tid; i < I.n; i += NT) {
-            const double* pi = P + 3 * (I.v0 + i);
-            const double dx = pi[0] - pp0[0], dy = pi[1] - pp0[1], dz = pi[2] - pp0[2];
-            double2 x = make_double2(dx * basis[0] + dy * basis[1] + dz * basis[2], dx * basis[3] + dy * basis[4] + dz * basis[5]);
-            if (i == LS.p0) x = make_double2(0.0, 0.0);
-            if (i == LS.p1) x = make_double2(basis[6], 0.0);
-            x64[I.v0 + i] = x;
-        }
-        __syncthreads();
-        // ||rhs||^2 of the reduced system: A applied to the pinned values only
-        double bb[2] = {0.0, 0.0};
-        {
-            const double dpin = basis[6];
-            for (int i = tid; i < I.n; i += NT) {
-                if (pinned(LS, i)) continue;
-                const Row r = row_of(b, I, i);
-                double ax = 0.0, ay = 0.0;
-                for (int k = 0; k < r.width; ++k) {
-                    const int q = r.q0 + 32 * k;
-                    const int j = b.slot_col[q];
-                    if (j != LS.p1) continue;   // p0 sits at the origin
-                    const double w = static_cast<double>(b.slot_w[q]);
-                    const double c = static_cast<double>(b.slot_c[q]);
-                    ax += -w * dpin;
-                    ay -= c * dpin;
-                }
-                bb[0] += ax * ax + ay * ay;
-            }
-            block_sum<NT, 2>(bb, sm.redd, phase);
-        }
-        int nref = 0;
-        bool capped = false;
-        st.cg_iters = refine_solve<NT, OP_LSCM, 1>(b, I, LS, prm, bb, sm, phase, st.resid, nref, capped);
-        st.refinements = nref;
-        if (capped) st.flags |= UVA_ST_MAXITER;
-        int bad = 0;
-        for (int i = tid; i < I.n; i += NT) bad |= finite2(x64[I.v0 + i]) ? 0 : 1;
-        bad = block_or<NT>(bad, sm.redi, phase);
-        if (bad) st.flags |= UVA_ST_NONFINITE;
-        for (int i = tid; i < I.n; i += NT) U[I.v0 + i] = x64[I.v0 + i];
+    uva_island_status st{};
+    if (I.p0 < 0 || I.n == 0) {
+        st.flags |= UVA_ST_NOBOUNDARY;
+        for_rows<NTT, R>(tid, I.n, [&](int i, int) { U[I.v0 + i] = make_double2(0.0, 0.0); });
         if (tid == 0) b.status[I.id] = st;
-        __syncthreads();
+        tm.sync();
+        return;
+    }
+    double nrm[3] = {0.0, 0.0, 0.0};
+    for (int f = I.f0 + tid; f < I.f0 + I.nt; f += NTT) {
+        const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
+        const double* a = P + 3 * (I.v0 + tv.x);
+        const double* c1 = P + 3 * (I.v0 + tv.y);
+        const double* c2 = P + 3 * (I.v0 + tv.z);
+        const double e1x = c1[0] - a[0], e1y = c1[1] - a[1], e1z = c1[2] - a[2];
+        const double e2x = c2[0] - a[0], e2y = c2[1] - a[1], e2z = c2[2] - a[2];
+        nrm[0] += e1y * e2z - e1z * e2y;
+        nrm[1] += e1z * e2x - e1x * e2z;
+        nrm[2] += e1x * e2y - e1y * e2x;
+    }
+    team_sum<NTT, 3>(tm, nrm, tm.redd);
+    const double* pp0 = P + 3 * (I.v0 + I.p0);
+    const double* pp1 = P + 3 * (I.v0 + I.p1);
+    // every thread derives the same basis from the same totals
+    const double nl = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+    double nx = 0.0, ny = 0.0, nz = 1.0;
+    if (nl > 0.0 && isfinite(nl)) { nx = nrm[0] / nl; ny = nrm[1] / nl; nz = nrm[2] / nl; }
+    double ax = pp1[0] - pp0[0], ay = pp1[1] - pp0[1], az = pp1[2] - pp0[2];
+    const double dpin = sqrt(ax * ax + ay * ay + az * az);
+    const double dn = ax * nx + ay * ny + az * nz;
+    ax -= dn * nx; ay -= dn * ny; az -= dn * nz;
+    const double al = sqrt(ax * ax + ay * ay + az * az);
+    double s = 1.0;
+    if (al > 0.0 && isfinite(al)) { s = dpin / al; ax /= al; ay /= al; az /= al; }
+    else { ax = 1.0; ay = 0.0; az = 0.0; }
+    const double bx = ny * az - nz * ay, by = nz * ax - nx * az, bz = nx * ay - ny * ax;
+    for_rows<NTT, R>(tid, I.n, [&](int i, int) {
+        const double* pi = P + 3 * (I.v0 + i);
+        const double dx = pi[0] - pp0[0], dy = pi[1] - pp0[1], dz = pi[2] - pp0[2];
+        double2 x = make_double2(s * (dx * ax + dy * ay + dz * az), s * (dx * bx + dy * by + dz * bz));
+        if (i == I.p0) x = make_double2(0.0, 0.0);
+        if (i == I.p1) x = make_double2(dpin, 0.0);
+        x64[I.v0 + i] = x;
+    });
+    // ||rhs||^2 of the reduced system: A applied to the pinned values only
+    double bb[2] = {0.0, 0.0};
+    const int2* cw = reinterpret_cast<const int2*>(b.slot_cw);
+    for_rows<NTT, R>(tid, I.n, [&](int i, int) {
+        if (is_pinned<OP_LSCM>(I, i)) return;
+        int q0, width;
+        row_slots(b, I, i, q0, width);
+        double rx = 0.0, ry = 0.0;
+        for (int k = 0; k < width; ++k) {
+            const int q = q0 + 32 * k;
+            const int2 sl = __ldg(cw + q);
+            if (sl.x != I.p1) continue;   // p0 sits at the origin
+            const double w = static_cast<double>(__int_as_float(sl.y));
+            const double c = static_cast<double>(__ldg(b.slot_c + q));
+            rx -= w * dpin;
+            ry -= c * dpin;
+        }
+        bb[0] += rx * rx + ry * ry;
+    });
+    team_sum<NTT, 2>(tm, bb, tm.redd);   // also publishes x64 to the team
+    int nref = 0;
+    bool capped = false;
+    st.cg_iters = refine_solve<NTT, R, OP_LSCM, 1>(b, I, prm, tm, bb, st.resid, nref, capped);
+    st.refinements = nref;
+    st.outer_iters = 1;
+    if (capped) st.flags |= UVA_ST_MAXITER;
+    int bad = 0;
+    for_rows<NTT, R>(tid, I.n, [&](int i, int) {
+        const double2 x = x64[I.v0 + i];
+        bad |= finite2(x) ? 0 : 1;
+        U[I.v0 + i] = x;
+    });
+    bad = team_or(tm, bad);
+    if (bad) st.flags |= UVA_ST_NONFINITE;
+    if (tid == 0) b.status[I.id] = st;
+    tm.sync();
+}
+
+template <int NTT, int R, Op OP>
+__device__ void run_class(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, int cls) {
+    const int lo = b.class_ofs[cls], hi = b.class_ofs[cls + 1];
+    if (lo >= hi) return;
+    for (;;) {
+        int qi;
+        if constexpr (NTT == 32) {
+            qi = 0;
+            if (tm.tid == 0) qi = atomicAdd(b.work + cls, 1);
+            qi = __shfl_sync(0xffffffffu, qi, 0);
+        } else {
+            if (tm.tid == 0) *tm.slot = atomicAdd(b.work + cls, 1);
+            tm.sync();
+            qi = *tm.slot;
+            tm.sync();
+        }
+        if (lo + qi >= hi) break;
+        const Isl I = load_island(b, b.order[lo + qi]);
+        if (OP == OP_ARAP) solve_arap<NTT, R>(b, prm, tm, I);
+        else solve_lscm<NTT, R>(b, prm, tm, I);
+    }
+}
+
+template <Op OP>
+__global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params prm) {
+    extern __shared__ float2 dyn[];
+    __shared__ double redd[2 * 4 * 32];
+    __shared__ float redf[2 * 4 * 32];
+    __shared__ int redi[2 * 32];
+    __shared__ int slots[8];
+    {
+        Team<KB> tm{static_cast<int>(threadIdx.x), 0, 0, redd, redf, redi, &slots[0], nullptr, nullptr, nullptr};
+        run_class<KB, 0, OP>(b, prm, tm, 0);
+        tm.sp = dyn; tm.sr = dyn + KB * RB; tm.sd = dyn + 2 * KB * RB;
+        run_class<KB, RB, OP>(b, prm, tm, 1);
+    }
+    __syncthreads();
+    const int s = threadIdx.x / SUB;
+    {
+        float2* base = dyn + s * (3 * SUB * RB);
+        Team<SUB> tm{static_cast<int>(threadIdx.x % SUB), 1 + s, 0, redd + s * 64, redf + s * 64, redi + s * 16,
+                     &slots[1 + s], base, base + SUB * RB, base + 2 * SUB * RB};
+        run_class<SUB, RB, OP>(b, prm, tm, 2);
+    }
+    {
+        const int w = threadIdx.x / 32;
+        float2* base = dyn + w * (3 * 32 * RB);
+        Team<32> tm{static_cast<int>(threadIdx.x % 32), 0, 0, nullptr, nullptr, nullptr, nullptr,
+                    base, base + 32 * RB, base + 2 * 32 * RB};
+        run_class<32, RB, OP>(b, prm, tm, 3);
     }
 }
 
@@ -748,20 +877,33 @@ int sm_count() {
 
 bool check_batch(const uva_batch* b) {
     return b && b->nc >= 0 && b->n >= 0 && b->t >= 0 &&
-           (b->nc == 0 || (b->vofs && b->tofs && b->sofs && b->order && b->work));
+           (b->nc == 0 || (b->vofs && b->tofs && b->sofs && b->order && b->work && b->slot_cw));
 }
 
-template <int NT>
-int launch_arap(uva_batch* b, const uva_solve_params* prm, cudaStream_t s, bool lscm) {
-    const int32_t* order = b->order;
-    cudaMemsetAsync(b->work, 0, sizeof(int32_t) * 4, s);
-    int occ = 0;
-    if (lscm) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_lscm<NT>, NT, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_arap<NT>, NT, 0);
-    const int grid = std::max(1, std::min(b->nc, sm_count() * std::max(occ, 1)));
-    if (lscm) k_lscm<NT><<<grid, NT, 0, s>>>(*b, *prm, order, b->nc);
-    else k_arap<NT><<<grid, NT, 0, s>>>(*b, *prm, order, b->nc);
-    UVA_CHECK_LAUNCH(lscm ? "uva_lscm" : "uva_arap");
+bool check_classes(const uva_batch* b) {
+    if (b->class_ofs[0] != 0 || b->class_ofs[4] != b->nc) return false;
+    for (int c = 0; c < 4; ++c)
+        if (b->class_ofs[c + 1] < b->class_ofs[c]) return false;
+    return true;
+}
+
+template <Op OP>
+int launch_islands(const uva_batch* b, const uva_solve_params* prm, cudaStream_t s) {
+    if (!check_classes(b)) {
+        uva_set_error("uva_arap/uva_lscm: class_ofs must be 0 <= ... <= nc, non-decreasing");
+        return UVA_E_ARG;
+    }
+    cudaError_t e = cudaFuncSetAttribute(k_islands<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kDynSmem));
+    if (e != cudaSuccess) return uva_cuda_status(e, "uva_islands/cudaFuncSetAttribute");
+    e = cudaMemsetAsync(b->work, 0, sizeof(int32_t) * 4, s);
+    if (e != cudaSuccess) return uva_cuda_status(e, "uva_islands/memset");
+    const int big = b->class_ofs[2];                        // islands that take a whole CTA
+    const int small = b->class_ofs[4] - b->class_ofs[2];    // islands for sub-teams / warps
+    const int want = big + (small + 3) / 4;
+    const int grid = std::max(1, std::min(sm_count(), want));
+    k_islands<OP><<<grid, KB, kDynSmem, s>>>(*b, *prm);
+    UVA_CHECK_LAUNCH(OP == OP_ARAP ? "uva_arap" : "uva_lscm");
     return UVA_OK;
 }
 
@@ -792,23 +934,13 @@ extern "C" int uva_batch_setup(uva_batch* b, void* stream) {
 extern "C" int uva_arap(uva_batch* b, const uva_solve_params* prm, void* stream) {
     if (!check_batch(b) || !prm) { uva_set_error("uva_arap: bad arguments"); return UVA_E_ARG; }
     if (b->nc == 0 || prm->iters <= 0) return UVA_OK;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    switch (prm->threads) {
-        case 128: return launch_arap<128>(b, prm, s, false);
-        case 512: return launch_arap<512>(b, prm, s, false);
-        default: return launch_arap<256>(b, prm, s, false);
-    }
+    return launch_islands<OP_ARAP>(b, prm, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int uva_lscm(uva_batch* b, const uva_solve_params* prm, void* stream) {
     if (!check_batch(b) || !prm) { uva_set_error("uva_lscm: bad arguments"); return UVA_E_ARG; }
     if (b->nc == 0) return UVA_OK;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    switch (prm->threads) {
-        case 128: return launch_arap<128>(b, prm, s, true);
-        case 512: return launch_arap<512>(b, prm, s, true);
-        default: return launch_arap<256>(b, prm, s, true);
-    }
+    return launch_islands<OP_LSCM>(b, prm, static_cast<cudaStream_t>(stream));
 }
 
 // ------------------------------------------------------------------ no-allocation ARAP
@@ -877,7 +1009,7 @@ extern "C" int uva_arap_noalloc(const uva_batch* b, const uva_solve_params* prm,
     w.d32 = reinterpret_cast<float*>(base + off); off += kNaF32;
     w.p32 = reinterpret_cast<float*>(base + off); off += kNaF32;
     w.q32 = reinterpret_cast<float*>(base + off);
-    // the work counter is the only scratch that must start at zero; launch_arap
-    // clears it on the stream before the launch
-    return launch_arap<256>(&w, prm, static_cast<cudaStream_t>(stream), false);
+    // the work counters are the only scratch that must start at zero;
+    // launch_islands clears them on the stream before the launch
+    return launch_islands<OP_ARAP>(&w, prm, static_cast<cudaStream_t>(stream));
 }

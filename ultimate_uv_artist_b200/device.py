@@ -73,8 +73,12 @@ class Plan:
             L.uva_plan_destroy(h)
         self.vofs = vofs.astype(np.int32)
         self.tofs = tofs.astype(np.int32)
-        sizes = np.diff(tofs)
-        self.order = np.argsort(-sizes, kind="stable").astype(np.int32)
+        # island work order: grouped by size class (whole CTA with global or
+        # shared-memory vectors, 256-thread sub-team, warp), largest first
+        nv = np.diff(vofs)
+        cls = np.where(nv > _lib.CLASS_BIG, 0, np.where(nv > _lib.CLASS_MID, 1, np.where(nv > _lib.CLASS_SMALL, 2, 3)))
+        self.order = np.lexsort((-nv, cls)).astype(np.int32)
+        self.class_ofs = np.searchsorted(cls[self.order], np.arange(5)).astype(np.int32)
 
 
 def concat_charts(charts, with_uv=True):
@@ -130,7 +134,7 @@ class DeviceBatch:
         self.wtri = torch.empty((t, 4), dtype=f64, device=d)
         self.tscale = torch.ones(t, dtype=f32, device=d)
         self.wedge = torch.empty(max(plan.E, 1), dtype=f64, device=d)
-        self.slot_w = torch.empty(max(plan.nslots, 1), dtype=f32, device=d)
+        self.slot_cw = torch.empty((max(plan.nslots, 1), 2), dtype=torch.int32, device=d)
         self.wdiag = torch.empty(n, dtype=f64, device=d)
         self.dinv = torch.empty(n, dtype=f32, device=d)
         self.pins = torch.zeros((nc, 3), dtype=torch.int32, device=d)
@@ -158,9 +162,11 @@ class DeviceBatch:
         p = self.plan
         D.nc, D.n, D.t, D.E = self.nc, self.n, self.t, p.E
         D.nslices, D.nslots, D.semantics, D.maxrows = p.nslices, p.nslots, self.semantics, p.maxrows
+        for c in range(5):
+            D.class_ofs[c] = int(p.class_ofs[c])
         for name in ("vofs", "tofs", "sofs", "tri4", "tri_edge", "slice_ptr", "slot_col", "slot_edge", "slot_c",
                      "vt_ptr", "vt", "vflags", "bofs", "bverts", "order", "P", "frame", "wtri", "tscale", "wedge",
-                     "slot_w", "wdiag", "dinv", "pins", "wpin", "U", "x64", "b64", "rc", "r32", "d32", "p32",
+                     "slot_cw", "wdiag", "dinv", "pins", "wpin", "U", "x64", "b64", "rc", "r32", "d32", "p32",
                      "q32", "status", "work"):
             setattr(D, name, getattr(self, name).data_ptr())
         return D
