@@ -190,6 +190,132 @@ int uva_repair_flips_serial(uva_batch* b, int32_t rounds, void* stream);
 int uva_shrink(uva_batch* b, uint8_t* sel, uint8_t* vmark, int32_t rings, float factor, float floor_,
                void* stream);
 
+/* --------------------------------------------------------------------------
+ * Exact validation of exported float32 UVs (engine/validate.py:139-209,
+ * _overlaps :95-136, _overlaps_strict :258-300; islands of
+ * engine/metrics.py:91-103). Bit-exact FP64 predicates (no FMA contraction).
+ * ------------------------------------------------------------------------ */
+enum {
+    UVA_VC_NONFINITE = 0,   /* UV rows with a non-finite coordinate          */
+    UVA_VC_OUTSIDE,         /* UV rows outside [0,1]                         */
+    UVA_VC_DEGENERATE,      /* has 3D area, zero UV area                     */
+    UVA_VC_SLIVERS,         /* has 3D area, below float32 UV resolution      */
+    UVA_VC_FLIPPED,         /* against the island's dominant orientation     */
+    UVA_VC_MIRRORED,        /* islands with negative dominant orientation    */
+    UVA_VC_ISLANDS,         /* islands                                       */
+    UVA_VC_OVERLAP,         /* triangles in a positive-area overlap          */
+    UVA_VC_CONTACTS,        /* strict-only overlaps (float32 contacts)       */
+    UVA_VC_ISLANDS_OV,      /* islands holding an overlapping triangle       */
+    UVA_VC_PAIRS,           /* candidate pairs with intersecting FP64 boxes  */
+    UVA_VC_BIG,             /* triangles tested outside the grid (> 16 cells)*/
+    UVA_VC_AMBIGUOUS,       /* islands whose orientation was re-summed exactly */
+    UVA_VC_N = 16
+};
+
+typedef struct uva_val_desc {
+    int32_t n, m;           /* vertices, triangles                            */
+    int32_t grid;           /* grid cells per side (0: clip(sqrt(m)/2, 64, 4096)) */
+    int32_t reserved;
+    const double* V;        /* n*3 positions (FP64)                           */
+    const float* UV;        /* n*2 exported UVs (float32)                     */
+    const int32_t* F;       /* m*3                                            */
+    double rel;             /* tolerant predicate, relative to edge^2 (1e-6)  */
+    uint8_t* tflags;        /* out, m bytes rounded up to a multiple of 4:
+                               1 has3d, 2 sliver, 4 skipped, 8 flipped,
+                               16 overlap, 32 strict overlap                  */
+    int32_t* labels;        /* out, m: island of each face (0..islands-1, by
+                               smallest welded vertex id; the partition is the
+                               reference's, its numbering depends on union order) */
+    double* sa;             /* out, m: signed UV area                         */
+    int64_t* counts;        /* out, UVA_VC_N counters                         */
+    void* scratch;          /* device scratch of uva_validate_scratch_bytes   */
+    int64_t scratch_bytes;
+} uva_val_desc;
+
+int uva_validate_scratch_bytes(int64_t n, int64_t m, int32_t grid, int64_t* bytes);
+int uva_validate(const uva_val_desc* d, void* stream);
+/* engine/metrics.py:91-103: face islands; weld != 0 merges vertices with
+ * identical float32 (position, uv) bytes. count: device int64.
+ * Scratch: uva_validate_scratch_bytes(n, m, 0).                            */
+int uva_islands(const double* V, const float* UV, const int32_t* F, int32_t n, int32_t m, int32_t weld,
+                int32_t* labels, int64_t* count, void* scratch, int64_t scratch_bytes, void* stream);
+/* engine/validate.py:212-226: overlap flags (bit 16 of tflags, m bytes
+ * rounded up to a multiple of 4) of one chart whose FP64 UVs the caller has
+ * normalised to [0, 0.999999]; triangles with |area| <= 1e-14 are skipped.
+ * Scratch: uva_validate_scratch_bytes(n, m, 0).                            */
+int uva_chart_overlaps(const double* U, const int32_t* F, int32_t n, int32_t m, uint8_t* tflags,
+                       void* scratch, int64_t scratch_bytes, void* stream);
+
+/* --------------------------------------------------------------------------
+ * Gutter and coverage rasters (engine/metrics.py:13-62, 314-373).
+ * ------------------------------------------------------------------------ */
+int uva_gutter_scratch_bytes(int32_t res, int64_t m, int64_t* bytes);
+/* Label raster (last triangle wins, like the reference's serial loop) into
+ * img (res*res int32, -1 empty) and the gap between islands from an exact,
+ * radius-limited Euclidean distance transform that breaks ties like
+ * scipy.ndimage.distance_transform_edt (smallest column, then row).
+ * out (device, 4 doubles): [0] min d(p)+d(q) over 4-neighbour pairs with
+ * different nearest labels and both distances <= radius (1e300: none),
+ * [1] filled texels, [2] 1 if two islands touch, [3] radius. The gap is exact
+ * when out[0] <= radius; otherwise call again with a larger radius. UV is
+ * FP64 as given (validate_uvs passes float32-rounded values).             */
+int uva_gutter(const double* UV, const int32_t* F, const int32_t* labels, int32_t m, int32_t res, int32_t radius,
+               int32_t* img, void* scratch, int64_t scratch_bytes, double* out, void* stream);
+/* Coverage counts per texel centre with the top-left rule, saturating at 255
+ * (uv: FP64 as given); stats (device, 2 int64): covered, covered twice.    */
+int uva_raster_counts(const double* uv, const int32_t* F, int32_t m, int32_t res, uint8_t* counts, int64_t* stats,
+                      void* scratch, int64_t scratch_bytes, void* stream);
+
+/* --------------------------------------------------------------------------
+ * Distortion metrics (engine/metrics.py:106-210, engine/param.py:520-551).
+ * ------------------------------------------------------------------------ */
+/* Weighted quantile per segment (argsort, cumsum, searchsorted semantics of
+ * metrics._wquantile :107-112): the smallest x whose cumulative weight
+ * reaches q * total; weight-0 entries are ignored; seg may be null (one
+ * segment). out: nseg doubles (device), NaN for an empty segment.          */
+int uva_wquantile_scratch_bytes(int32_t nseg, int64_t* bytes);
+int uva_wquantile(const double* x, const double* w, const int32_t* seg, int32_t n, int32_t nseg, double q,
+                  double* out, void* scratch, int64_t scratch_bytes, void* stream);
+int uva_metrics_scratch_bytes(int64_t m, int64_t n_islands, int64_t* bytes);
+/* distortion_report (metrics.py:148-210). out (device, 32 doubles):
+ * [0] sum a3, [1] sum |sa|, [2] collapsed, [3] collapsed w, [4] aniso*w (ok),
+ * [5] w (aniso ok), [6] angle*w (valid), [7] w (valid), [8] lg*w (ok),
+ * [9] w (ok), [10] stretch^2*w (ok), [11] lc*w (ok), [12] flipped,
+ * [13] flipped w, [16] mirrored islands, [17] sum ia3, [24] anisotropy p95,
+ * [25] log2 density-ratio p95, [26] log2 chart-area p95, [27] log2 island
+ * density p95. islands may be null. per_tri (device, m*6, may be null):
+ * s1, s2, signed UV area, 3D area, good, angle error (triangle_jacobians). */
+int uva_distortion_report(const double* V, const double* UV, const int32_t* F, const int32_t* islands,
+                          int32_t n, int32_t m, int32_t n_islands, double* out, double* per_tri,
+                          void* scratch, int64_t scratch_bytes, void* stream);
+int uva_quality_scratch_bytes(int64_t t, int64_t nc, int64_t* bytes);
+/* chart_quality (param.py:520-551) of every island of a PARAM-semantics
+ * batch. out (device, nc*8): flips, aniso_p95, aniso_mean, area_p95,
+ * area_logdev, stretch, scale, area. per_aniso, per_area: t doubles.       */
+int uva_chart_quality(const uva_batch* b, double* out, double* per_aniso, double* per_area, void* scratch,
+                      int64_t scratch_bytes, void* stream);
+
+/* --------------------------------------------------------------------------
+ * Per-chart helpers of engine/param.py (one chart, global int64 triangles).
+ * ------------------------------------------------------------------------ */
+enum {
+    UVA_OP_FRAMES = 0,      /* local_frames :19-32  -> out X (t*6), out2 area */
+    UVA_OP_COTS,            /* cot_weights :35-44   X -> out (t*3)            */
+    UVA_OP_SIGNED_AREA,     /* signed_areas :97-99  U -> out (t)              */
+    UVA_OP_ROTATIONS,       /* _arap_rotations mode 0 :206-233 -> out (t*4)   */
+    UVA_OP_RHS,             /* _arap_rhs :457-474   -> out (n*2)              */
+    UVA_OP_MAX_STEP,        /* _max_step :259-291   U, D -> out (1)           */
+    UVA_OP_ENERGY           /* _energy :294-319, kind = arg -> out (1)        */
+};
+int uva_chart_op(int32_t op, int32_t arg, const double* P, const int64_t* T, const double* U, const double* D,
+                 const double* X, const double* cots, const double* R, const double* area, int32_t n, int32_t t,
+                 double* out, double* out2, void* stream);
+/* SPDSolver (param.py:103-132): FP64 Jacobi-PCG on a CSR SPD matrix, one
+ * right-hand side per column (b, x: ncol*n column-major), warm start in x,
+ * stop at ||r|| <= tol ||b||. scratch: 3*n*ncol doubles; iters: ncol.      */
+int uva_csr_pcg(int32_t n, const int32_t* rowptr, const int32_t* col, const double* val, const double* b, double* x,
+                int32_t ncol, double tol, int32_t maxiter, double* scratch, int32_t* iters, void* stream);
+
 /* Library info. */
 const char* uva_last_error(void);
 int uva_version(void);

@@ -138,6 +138,17 @@ def main(ref_root):
     uchart = U64[info["vofs"][0]:info["vofs"][1]].copy()
     uchart[5] += np.array([0.004, 0.003])
     cov = validate.chart_overlaps(uchart, fchart)
+    # a clean atlas (one mirrored island, no overlaps): non-zero gutter
+    V2, F2, UV2, _ = synth.validation_atlas(seed=33, islands=40, tris_per_island=50, atlas=512, padding=4,
+                                            overlap_rate=0.0, fold_rate=0.0, mirrored=1, outside=0)
+    rep2, prob2 = validate.validate_uvs(V2, F2, UV2, atlas=512, padding=4)
+    U2_64 = UV2.astype(np.float32).astype(np.float64)
+    isl2, _ = metrics.uv_islands(F2, len(V2), U2_64, V2)
+    g2, img2 = metrics.min_gutter(U2_64, F2, isl2, 512)
+    keys2 = sorted(k for k in rep2 if isinstance(rep2[k], (int, float, bool, np.integer, np.floating)))
+    out.update(w_V=V2, w_F=F2, w_UV=UV2, w_problems=prob2, w_isl=isl2, w_gutter=np.array(g2),
+               w_img=img2.astype(np.int32), w_rep_keys=np.array(keys2),
+               w_rep_vals=np.array([float(rep2[k]) for k in keys2]))
     keys = sorted(k for k in rep if isinstance(rep[k], (int, float, bool, np.integer, np.floating)))
     out.update(v_V=V, v_F=F, v_UV=UV, v_problems=problems, v_ov=ov, v_ovs=ovs, v_isl=isl_lab,
                v_nisl=np.array(n_isl), v_gutter=np.array(g), v_img=img.astype(np.int32),

@@ -1,0 +1,160 @@
+"""CPU tests: the oracle against the reference's golden fixtures, the C ABI
+(library loads, every declared symbol exported), the host topology plan, and
+the synthetic generators. No GPU needed."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import arap as O
+from oracle import validate as OV
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+# ---------------------------------------------------------------- oracle vs reference
+def test_oracle_param_matches_reference(golden):
+    P, T = golden["p_P"], golden["p_T"]
+    X, area = O.local_frames(P, T)
+    assert np.array_equal(X, golden["p_X"]) and np.array_equal(area, golden["p_area"])
+    cots = O.cot_weights(X)
+    assert np.array_equal(cots, golden["p_cots"])
+    assert np.abs(O.lscm(P, T) - golden["p_U0"]).max() < 1e-12
+    bi, _ = O.boundary_edges_oriented(T)
+    assert O.far_pair(P, np.unique(bi)) == tuple(golden["p_pins"].tolist())
+    R = O.arap_rotations(golden["p_U0"], T, X)
+    assert np.abs(R - golden["p_R"]).max() < 1e-14
+    assert np.abs(O.arap_rhs(len(P), T, X, cots, R) - golden["p_b"]).max() < 1e-13
+    assert np.abs(O.refine_arap(P, T, golden["p_U0"], iters=10, tol=0.0) - golden["p_U1"]).max() < 1e-12
+    assert np.abs(O.refine_arap(P, T, golden["p_U0"], iters=10, tol=1e-5) - golden["p_U2"]).max() < 1e-12
+    assert O.max_step_param(golden["p_U0"], golden["p_U1"] - golden["p_U0"], T) == float(golden["p_maxstep"])
+    assert abs(O.energy(golden["p_U1"], T, X, area, 0) - float(golden["p_E0"])) < 1e-12
+    assert np.array_equal(O.repair_flips_param(golden["p_Uf"], T), golden["p_Ur"])
+
+
+def test_oracle_batch_matches_reference(golden):
+    nc = int(golden["b_nc"])
+    items = [(golden[f"b_P{k}"], golden[f"b_T{k}"], golden[f"b_U{k}"]) for k in range(nc)]
+    B = O.BatchRef(items)
+    assert B.wpin == float(golden["b_wpin"])
+    B.orient_positive()
+    assert np.abs(B.U - golden["b_Ua"]).max() < 1e-15
+    assert np.abs(B.rhs(B.U) - golden["b_rhs0"]).max() < 1e-12
+    B.arap(6, True)
+    assert O.uv_rel_error(B.U, golden["b_Ub"], B.offsets) < 1e-9
+    B.arap(3, False)
+    assert O.uv_rel_error(B.U, golden["b_Uc"], B.offsets) < 1e-9
+    B.U = golden["b_Ud"].copy()
+    assert np.array_equal(B.flips_per_chart(), golden["b_flips"])
+    B.repair_flips(40)
+    assert np.abs(B.U - golden["b_Ue"]).max() < 1e-12
+
+
+@pytest.mark.parametrize("prefix", ["v", "w"])
+def test_oracle_validation_matches_reference(golden, prefix):
+    V, F, UV = golden[f"{prefix}_V"], golden[f"{prefix}_F"], golden[f"{prefix}_UV"]
+    rep, prob, ex = OV.validate_uvs(V, F, UV, atlas=512, padding=4)
+    ref = dict(zip(golden[f"{prefix}_rep_keys"].tolist(), golden[f"{prefix}_rep_vals"].tolist()))
+    for k, v in ref.items():
+        assert float(rep[k]) == v, (k, rep[k], v)
+    assert np.array_equal(prob, golden[f"{prefix}_problems"])
+    assert OV.same_partition(ex["islands"], golden[f"{prefix}_isl"])
+    if prefix == "v":
+        assert np.array_equal(ex["ov"], golden["v_ov"]) and np.array_equal(ex["ov_strict"], golden["v_ovs"])
+        U64 = UV.astype(np.float32).astype(np.float64)
+        assert np.array_equal(OV.raster_labels(U64, F, golden["v_isl"], 512), golden["v_img"])
+        assert np.array_equal(OV.raster_counts(U64, F, 256), golden["v_counts"])
+        assert np.array_equal(OV.chart_overlaps(golden["v_cU"], golden["v_cF"]), golden["v_cov"])
+
+
+def test_numpy_predicates_agree_with_c_loops(golden):
+    """The vectorised numpy predicates and the C restatement of the serial
+    loops give the same flags (two independent restatements)."""
+    V, F, UV = golden["v_V"], golden["v_F"], golden["v_UV"]
+    U = UV.astype(np.float32).astype(np.float64)
+    skip = np.zeros(len(F), bool)
+    for strict in (False, True):
+        a, _ = OV.overlaps(U, F, skip, 0.0 if strict else 1e-6, strict=strict)
+        b, _ = OV.overlaps_c(U, F, skip, 64, 0.0 if strict else 1e-6, strict=strict)
+        assert np.array_equal(a, b)
+    lab = golden["v_isl"]
+    assert np.array_equal(OV.raster_labels_numpy(U, F, lab, 128), OV.raster_labels(U, F, lab, 128))
+
+
+# ---------------------------------------------------------------- C ABI
+def _declared_functions():
+    src = open(os.path.join(ROOT, "include", "uva_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(uva_[a-z_0-9]+)\s*\(", src, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    from ultimate_uv_artist_b200 import _lib
+    L = _lib.lib()
+    names = _declared_functions()
+    assert len(names) >= 30, names
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert L.uva_version() >= 1
+
+
+def test_plan_matches_numpy_topology():
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.device import Plan, concat_charts
+    rng = np.random.default_rng(1)
+    isl = [synth.disk_patch(rng, t) for t in (20, 150, 900)] + [synth.hemisphere_patch(seed=3, n=9)]
+    P, T, _, vofs, tofs = concat_charts([(p, t) for p, t in isl], with_uv=False)
+    pl = Plan(T, vofs, tofs)
+    assert pl.n == len(P) and pl.t == len(T)
+    for i in range(pl.nc):
+        Ti = T[tofs[i]:tofs[i + 1]]
+        n = vofs[i + 1] - vofs[i]
+        a = np.r_[Ti[:, 1], Ti[:, 2], Ti[:, 0]]
+        b = np.r_[Ti[:, 2], Ti[:, 0], Ti[:, 1]]
+        key = np.unique(np.minimum(a, b) * n + np.maximum(a, b))
+        ea, eb = key // n, key % n
+        for v in range(n):
+            s = pl.sofs[i] + v // 32
+            w = (pl.slice_ptr[s + 1] - pl.slice_ptr[s]) // 32
+            assert w % 4 == 0
+            q = pl.slice_ptr[s] + v % 32 + 32 * np.arange(w)
+            cols = [int(c) for c, e in zip(pl.slot_col[q], pl.slot_edge[q]) if e >= 0]
+            assert cols == sorted(set(eb[ea == v].tolist()) | set(ea[eb == v].tolist()))
+        bi, bj = O.boundary_edges_oriented(Ti)
+        assert np.array_equal(np.unique(bi), pl.bverts[pl.bofs[i]:pl.bofs[i + 1]])
+    # island work order: classes by vertex count, each class largest first
+    nv = np.diff(vofs)[pl.order]
+    assert np.all(np.diff(pl.class_ofs) >= 0) and pl.class_ofs[-1] == pl.nc
+
+
+def test_plan_rejects_bad_indices():
+    from ultimate_uv_artist_b200.device import Plan
+    T = np.array([[0, 1, 5]])
+    with pytest.raises(ValueError):
+        Plan(T, [0, 3], [0, 1])
+
+
+def test_product_path_requires_cuda():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("CUDA present")
+    from ultimate_uv_artist_b200.engine import gpu
+    with pytest.raises(RuntimeError):
+        gpu.Batch([(np.zeros((3, 3)), np.array([[0, 1, 2]]), np.zeros((3, 2)))])
+
+
+# ---------------------------------------------------------------- generators
+def test_validation_atlas_faults():
+    from ultimate_uv_artist_b200 import synth
+    V, F, UV, info = synth.validation_atlas(seed=31, islands=60, tris_per_island=50, atlas=512, padding=4,
+                                            overlap_rate=2e-3, fold_rate=2e-3, mirrored=2, outside=5)
+    assert len(info["mirrored"]) == 2 and len(info["outside"]) == 5
+    assert ((UV < 0) | (UV > 1)).any(1).sum() == 5
+
+
+def test_uneven_islands_sizes():
+    from ultimate_uv_artist_b200 import synth
+    isl = synth.uneven_islands(seed=7, count=50)
+    t = np.array([len(T) for _, T in isl])
+    assert t.min() >= 8 and t.max() <= 20000

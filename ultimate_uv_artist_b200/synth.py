@@ -104,7 +104,7 @@ def validation_atlas(seed=3000, islands=5000, tris_per_island=200, atlas=4096, p
     * folds: one vertex of a triangle reflected across its opposite edge, at
       ``fold_rate`` per triangle;
     * ``mirrored`` islands mirrored u -> 1 - u inside their bounding box;
-    * ``outside`` vertices pushed outside [0, 1].
+    * ``outside`` vertices near the atlas border pushed 1-4 texels outside [0, 1].
     """
     rng = np.random.default_rng(seed)
     side = max(2, int(round(np.sqrt(tris_per_island / 2.0))))
@@ -144,7 +144,9 @@ def validation_atlas(seed=3000, islands=5000, tris_per_island=200, atlas=4096, p
     m = len(F)
     info = {"shifted": [], "folded": [], "mirrored": [], "outside": []}
     # overlaps: shift whole islands by U(0, 8) texels (u and v)
-    n_shift = max(1, int(rng.binomial(m, overlap_rate)))
+    n_shift = int(rng.binomial(m, overlap_rate))
+    if overlap_rate > 0:
+        n_shift = max(1, n_shift)
     for i in rng.choice(islands, n_shift, replace=False):
         d = rng.uniform(0, 8, 2) / atlas
         U[vofs[i]:vofs[i + 1]] += d
@@ -156,7 +158,9 @@ def validation_atlas(seed=3000, islands=5000, tris_per_island=200, atlas=4096, p
         seg[:, 0] = lo + hi - seg[:, 0]
         info["mirrored"].append(int(i))
     # folds: reflect one vertex of a triangle across the opposite edge
-    n_fold = max(1, int(rng.binomial(m, fold_rate)))
+    n_fold = int(rng.binomial(m, fold_rate))
+    if fold_rate > 0:
+        n_fold = max(1, n_fold)
     for t in rng.choice(m, n_fold, replace=False):
         a, b, c = F[t]
         p, q = U[b], U[c]
@@ -165,9 +169,11 @@ def validation_atlas(seed=3000, islands=5000, tris_per_island=200, atlas=4096, p
         proj = p + e * (r @ e) / max(e @ e, 1e-30)
         U[a] = 2 * proj - U[a]
         info["folded"].append(int(t))
-    # out of range vertices
-    for vtx in rng.choice(len(U), outside, replace=False):
-        U[vtx] = U[vtx] + np.where(rng.random(2) < 0.5, -1.0, 1.0) * rng.uniform(1.0, 1.5, 2)
+    # out of range vertices: vertices of islands next to the atlas border,
+    # pushed 1-4 texels past that border
+    lo_v = np.argsort(U[:, 1])[: max(outside * 50, 1)]
+    for vtx in rng.choice(lo_v, min(outside, len(lo_v)), replace=False):
+        U[vtx, 1] = -rng.uniform(1.0, 4.0) / atlas
         info["outside"].append(int(vtx))
     return V.astype(np.float32), F.astype(np.int64), U.astype(np.float32), {**info, "vofs": vofs, "tofs": tofs}
 
