@@ -316,6 +316,24 @@ int uva_chart_op(int32_t op, int32_t arg, const double* P, const int64_t* T, con
 int uva_csr_pcg(int32_t n, const int32_t* rowptr, const int32_t* col, const double* val, const double* b, double* x,
                 int32_t ncol, double tol, int32_t maxiter, double* scratch, int32_t* iters, void* stream);
 
+/* --------------------------------------------------------------------------
+ * Distortion energies with backward passes (engine/param.py:294-319):
+ * kind 0 ARAP, kind 1 symmetric Dirichlet (inf for inverted triangles),
+ * frames from P as param.local_frames; per island.
+ * ------------------------------------------------------------------------ */
+int uva_energy_fwd(const uva_batch* b, const double* P, const double* U, int32_t kind, double* e_isl,
+                   double* e_tri, void* stream);
+/* dE/dU (n*2) and, if gP is not null, dE/dP (n*3); gscale (nc, may be null)
+ * scales each island's energy (the upstream gradient).                     */
+int uva_energy_bwd(const uva_batch* b, const double* P, const double* U, int32_t kind, const double* gscale,
+                   double* gU, double* gP, void* stream);
+/* p95-stretch refinement: `steps` Jacobi-preconditioned, flip-safe, monotone
+ * descent steps on the symmetric Dirichlet energy of every island; updates
+ * b->U; e_isl (nc) gets the final energies. scratch: 8n + 8nc + n + 2
+ * doubles.                                                                 */
+int uva_sd_refine(uva_batch* b, int32_t steps, int32_t halvings, double cap, double* e_isl, void* scratch,
+                  void* stream);
+
 /* Library info. */
 const char* uva_last_error(void);
 int uva_version(void);

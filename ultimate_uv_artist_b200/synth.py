@@ -184,13 +184,19 @@ def energy_islands(seed=4000, count=512, tmin=500, tmax=50000, degenerate=0.05, 
 
     Near-degenerate triangles are made by sliding one vertex of a triangle
     towards the midpoint of its opposite edge until the aspect ratio reaches
-    U(10, max_aspect). Returns a list of (P, T)."""
+    U(10, max_aspect); a move that would invert an incident triangle of the
+    xy projection is skipped, so the projection stays a flip-free
+    parameterization. Returns a list of (P, T)."""
     rng = np.random.default_rng(seed)
     targets = np.exp(rng.uniform(np.log(tmin), np.log(tmax), count))
     out = []
     for t in targets:
         P, T = disk_patch(rng, t / 0.785, bumps=8, amp=0.3)
         P = P.astype(np.float64)
+        inc = [[] for _ in range(len(P))]
+        for f, tri in enumerate(T):
+            for v in tri:
+                inc[v].append(f)
         k = int(degenerate * len(T))
         for f in rng.choice(len(T), k, replace=False):
             a, b, c = T[f]
@@ -198,8 +204,15 @@ def energy_islands(seed=4000, count=512, tmin=500, tmax=50000, degenerate=0.05, 
             base = np.linalg.norm(P[c] - P[b])
             h = np.linalg.norm(P[a] - mid)
             target_h = base / rng.uniform(10.0, max_aspect)
-            if h > target_h:
-                P[a] = mid + (P[a] - mid) * (target_h / h)
+            if h <= target_h:
+                continue
+            old = P[a].copy()
+            P[a] = mid + (P[a] - mid) * (target_h / h)
+            tri = T[inc[a]]
+            u = P[tri][:, :, :2].astype(np.float32).astype(np.float64)   # as stored
+            sa = (u[:, 1, 0] - u[:, 0, 0]) * (u[:, 2, 1] - u[:, 0, 1]) - (u[:, 2, 0] - u[:, 0, 0]) * (u[:, 1, 1] - u[:, 0, 1])
+            if (sa <= 0).any():
+                P[a] = old
         out.append((P.astype(np.float32), T))
     return out
 
