@@ -73,7 +73,7 @@ typedef struct uva_plan uva_plan;
 
 enum {
     UVA_PLAN_NC = 0, UVA_PLAN_N, UVA_PLAN_T, UVA_PLAN_E, UVA_PLAN_NSLICES,
-    UVA_PLAN_NSLOTS, UVA_PLAN_NBVERTS, UVA_PLAN_MAXROWS, UVA_PLAN_NSIZES
+    UVA_PLAN_NSLOTS, UVA_PLAN_NBVERTS, UVA_PLAN_MAXROWS, UVA_PLAN_NCOARSE, UVA_PLAN_NSIZES
 };
 
 /* tris: t*3 island-LOCAL vertex ids (int64, host); vofs/tofs: nc+1 offsets.
@@ -87,7 +87,8 @@ int uva_plan_sizes(const uva_plan* plan, int64_t* sizes /* UVA_PLAN_NSIZES */);
  *   sofs      nc+1  first SELL slice of each island
  *   slice_ptr nslices+1 first slot of each slice (32 rows per slice, width
  *             padded to a multiple of 4 slots)
- *   slot_col  nslots island-local column (padding: the row itself)
+ *   slot_col  nslots island-local column = solver ROW of the neighbour
+ *             (padding: the row itself); slots of a row in vertex order
  *   slot_edge nslots global unique-edge id (padding: -1)
  *   slot_c    nslots LSCM boundary coupling H[i, j+n] (param.py:147-150)
  *   vt_ptr    n+1   incidence offsets; vt 3t entries f*3+corner, ascending
@@ -97,6 +98,12 @@ int uva_plan_sizes(const uva_plan* plan, int64_t* sizes /* UVA_PLAN_NSIZES */);
 int uva_plan_export(const uva_plan* plan, int32_t* tri4, int32_t* tri_edge, int32_t* sofs,
                     int32_t* slice_ptr, int32_t* slot_col, int32_t* slot_edge, float* slot_c,
                     int32_t* vt_ptr, int32_t* vt, uint8_t* vflags, int32_t* bofs, int32_t* bverts);
+/* Solver row order (island-local): row_vert / vert_row (n each), rows per
+ * coarse aggregate per island (0: none) and offsets of each island's m*m
+ * coarse block (nc+1). Rows are grouped in compact breadth-first blobs of
+ * agg_rows vertices so that aggregates are whole 32-row slices.           */
+int uva_plan_export_rows(const uva_plan* plan, int32_t* row_vert, int32_t* vert_row, int32_t* agg_rows,
+                         int32_t* cofs);
 void uva_plan_destroy(uva_plan* plan);
 
 /* --------------------------------------------------------------------------
@@ -111,6 +118,14 @@ typedef struct uva_batch {
     const float*   slot_c;    const int32_t* vt_ptr;    const int32_t* vt;
     const uint8_t* vflags;    const int32_t* bofs;      const int32_t* bverts;
     const int32_t* order;     /* nc island ids by class, largest first        */
+    const int32_t* row_vert;  /* n: solver row -> vertex (island-local)       */
+    const int32_t* vert_row;  /* n: vertex -> solver row (island-local)       */
+    const int32_t* agg_rows;  /* nc: rows per coarse aggregate (0: none)      */
+    const int32_t* cofs;      /* nc+1: offset of the island's m*m coarse block */
+    float*  coarse_a;         /* cofs[nc]: inverse coarse ARAP operators (FP32) */
+    float*  coarse_l;         /* 4*cofs[nc]: inverse coarse LSCM operators     */
+    double* coarse_work;      /* 4*cofs[nc]: FP64 workspace of the setup        */
+    float*  cpart;            /* 2*nslices: per-slice residual sums (solve scratch) */
     int32_t class_ofs[5];     /* host values: class c owns order[ofs[c]..ofs[c+1]) */
     /* geometry, written by uva_batch_setup */
     const double*  P;         /* n*3 positions (FP64)                          */
@@ -119,13 +134,14 @@ typedef struct uva_batch {
     float*  tscale;           /* t: target size (Batch.shrink)                  */
     double* wedge;            /* E: summed edge weight                          */
     int32_t* slot_cw;         /* nslots*2: packed (column, FP32 weight bits)    */
-    double* wdiag;            /* n: exact FP64 row sum of the slot weights      */
-    float*  dinv;             /* n: Jacobi inverse of wdiag (pin row: on the fly)*/
+    double* wdiag;            /* n (by solver row): FP64 row sum of the weights */
+    float*  dinv;             /* n (by row): inverse of wdiag (pin row on the fly) */
     int32_t* pins;            /* nc*3: ARAP pin, LSCM p0, LSCM p1 (local ids)   */
     double* wpin;             /* nc: soft-pin weight                            */
     double* U;                /* n*2 UVs (FP64 master copy)                     */
     /* scratch (device, sized n / t) */
-    double* x64;  double* b64;  double* rc;     /* x64, b64: max(n,nc)*2;     */
+    double* x64;  double* b64;  double* rc;     /* x64, b64: max(n,nc)*2, by  */
+                                                /* solver row;                */
                                                 /* rc: t*3*2 corner RHS terms */
     float*  r32;  float*  d32;  float*  p32;  float* q32;
     uva_island_status* status;                  /* nc                         */
@@ -165,8 +181,8 @@ int uva_arap(uva_batch* b, const uva_solve_params* prm, void* stream);
  * callers that cannot allocate device memory while they run (for example a
  * host application that owns a fixed device pool, or code that must not call
  * cudaMalloc between frames). It allocates nothing: the solver scratch of `b`
- * (x64, b64, rc, r32, d32, p32, q32, work) is ignored and replaced by one
- * static device array of 5,243,136 bytes that every GPU loading the library
+ * (x64, b64, rc, r32, d32, p32, q32, cpart, work) is ignored and replaced by one
+ * static device array of 5,505,280 bytes that every GPU loading the library
  * holds until exit. The caller still passes the inputs (topology, geometry,
  * pins, order) and the outputs (U, status). Limits: at most 32768 vertices
  * and 65536 triangles per call, else UVA_E_TOOBIG. The first call on a device

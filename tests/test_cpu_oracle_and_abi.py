@@ -114,12 +114,20 @@ def test_plan_matches_numpy_topology():
         b = np.r_[Ti[:, 2], Ti[:, 0], Ti[:, 1]]
         key = np.unique(np.minimum(a, b) * n + np.maximum(a, b))
         ea, eb = key // n, key % n
+        rv, vr = pl.row_vert[vofs[i]:vofs[i + 1]], pl.vert_row[vofs[i]:vofs[i + 1]]
+        assert np.array_equal(np.sort(rv), np.arange(n)) and np.array_equal(rv[vr], np.arange(n))
+        if n > 256:   # aggregates of agg_rows consecutive rows, at most 256 of them
+            m = -(-n // pl.agg_rows[i])
+            assert pl.agg_rows[i] % 128 == 0 and m <= 256 and pl.cofs[i + 1] - pl.cofs[i] == m * m
+        else:
+            assert pl.agg_rows[i] == 0 and pl.cofs[i + 1] == pl.cofs[i] and np.array_equal(rv, np.arange(n))
         for v in range(n):
-            s = pl.sofs[i] + v // 32
+            row = vr[v]
+            s = pl.sofs[i] + row // 32
             w = (pl.slice_ptr[s + 1] - pl.slice_ptr[s]) // 32
             assert w % 4 == 0
-            q = pl.slice_ptr[s] + v % 32 + 32 * np.arange(w)
-            cols = [int(c) for c, e in zip(pl.slot_col[q], pl.slot_edge[q]) if e >= 0]
+            q = pl.slice_ptr[s] + row % 32 + 32 * np.arange(w)
+            cols = [int(rv[c]) for c, e in zip(pl.slot_col[q], pl.slot_edge[q]) if e >= 0]
             assert cols == sorted(set(eb[ea == v].tolist()) | set(ea[eb == v].tolist()))
         bi, bj = O.boundary_edges_oriented(Ti)
         assert np.array_equal(np.unique(bi), pl.bverts[pl.bofs[i]:pl.bofs[i + 1]])

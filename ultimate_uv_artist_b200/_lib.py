@@ -26,9 +26,9 @@ ST_NONFINITE = 2
 ST_ENERGYSTOP = 4
 ST_NOBOUNDARY = 8
 
-PLAN_NSIZES = 8
+PLAN_NSIZES = 9
 CLASS_BIG, CLASS_MID, CLASS_SMALL = 8192, 2048, 256
-(PLAN_NC, PLAN_N, PLAN_T, PLAN_E, PLAN_NSLICES, PLAN_NSLOTS, PLAN_NBVERTS, PLAN_MAXROWS) = range(8)
+(PLAN_NC, PLAN_N, PLAN_T, PLAN_E, PLAN_NSLICES, PLAN_NSLOTS, PLAN_NBVERTS, PLAN_MAXROWS, PLAN_NCOARSE) = range(9)
 
 vp = C.c_void_p
 i32 = C.c_int32
@@ -46,6 +46,8 @@ class BatchDesc(C.Structure):
                 ("vofs", vp), ("tofs", vp), ("sofs", vp), ("tri4", vp), ("tri_edge", vp),
                 ("slice_ptr", vp), ("slot_col", vp), ("slot_edge", vp), ("slot_c", vp),
                 ("vt_ptr", vp), ("vt", vp), ("vflags", vp), ("bofs", vp), ("bverts", vp), ("order", vp),
+                ("row_vert", vp), ("vert_row", vp), ("agg_rows", vp), ("cofs", vp),
+                ("coarse_a", vp), ("coarse_l", vp), ("coarse_work", vp), ("cpart", vp),
                 ("class_ofs", i32 * 5),
                 ("P", vp), ("frame", vp), ("wtri", vp), ("tscale", vp), ("wedge", vp), ("slot_cw", vp),
                 ("wdiag", vp), ("dinv", vp), ("pins", vp), ("wpin", vp), ("U", vp),
@@ -63,6 +65,7 @@ _SIGS = {
     "uva_plan_create": [vp, vp, vp, i32, i32, vp],
     "uva_plan_sizes": [vp, vp],
     "uva_plan_export": [vp] * 13,
+    "uva_plan_export_rows": [vp] * 5,
     "uva_plan_destroy": [vp],
     "uva_batch_setup": [vp, vp],
     "uva_lscm": [vp, vp, vp],

@@ -168,10 +168,11 @@ __global__ void k_energy_bwd(const uva_batch b, const double* P, const double* U
 
 // ---- p95-stretch refinement: Jacobi-preconditioned descent on the
 // symmetric Dirichlet energy, flip-safe and monotone per island.
-__global__ void k_descent_dir(int n, const uva_batch b, const double* gU, double* Dd) {
+__global__ void k_descent_dir(int n, const uva_batch b, const int32_t* vert_isl, const double* gU, double* Dd) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
-    const double d = b.wdiag[v];
+    const int v0 = b.vofs[vert_isl[v]];
+    const double d = b.wdiag[v0 + b.vert_row[v]];   // the diagonal is stored by solver row
     const double m = d > 1e-30 ? 1.0 / d : 0.0;
     Dd[2 * v] = -m * gU[2 * v];
     Dd[2 * v + 1] = -m * gU[2 * v + 1];
@@ -305,7 +306,7 @@ extern "C" int uva_sd_refine(uva_batch* b, int32_t steps, int32_t halvings, doub
     for (int it = 0; it < steps; ++it) {
         uva_energy_fwd(b, b->P, b->U, 1, e_isl, nullptr, s);
         uva_energy_bwd(b, b->P, b->U, 1, nullptr, gU, nullptr, s);
-        k_descent_dir<<<nb(n), 256, 0, s>>>(n, *b, gU, Dd);
+        k_descent_dir<<<nb(n), 256, 0, s>>>(n, *b, vert_isl, gU, Dd);
         k_fill_d<<<nb(nc), 256, 0, s>>>(tmax, nc, 1e30);
         k_island_max_step<<<nb(b->t), 256, 0, s>>>(*b, b->U, Dd, tmax);
         k_init_alpha<<<nb(nc), 256, 0, s>>>(nc, tmax, alpha, accepted, cap);

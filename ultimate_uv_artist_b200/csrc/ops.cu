@@ -66,14 +66,15 @@ __global__ void k_repair(uva_batch b, int rounds, uint8_t* mark) {
             const int v = v0 + i;
             double2 u = U[v];
             if (mark[v] && !(b.vflags[v] & 1)) {
-                const int s = s0 + (i >> 5);
-                const int q0 = b.slice_ptr[s] + (i & 31), width = (b.slice_ptr[s + 1] - b.slice_ptr[s]) >> 5;
+                const int row = b.vert_row[v];   // solver row of vertex i
+                const int s = s0 + (row >> 5);
+                const int q0 = b.slice_ptr[s] + (row & 31), width = (b.slice_ptr[s + 1] - b.slice_ptr[s]) >> 5;
                 double sx = 0.0, sy = 0.0;
                 int deg = 0;
                 for (int k = 0; k < width; ++k) {
                     const int q = q0 + 32 * k;
                     if (b.slot_edge[q] < 0) continue;
-                    const double2 w = U[v0 + b.slot_col[q]];
+                    const double2 w = U[v0 + b.row_vert[v0 + b.slot_col[q]]];
                     sx += w.x; sy += w.y; ++deg;
                 }
                 const double dd = deg > 0 ? static_cast<double>(deg) : 1.0;
@@ -106,14 +107,15 @@ __global__ void k_repair_serial(uva_batch b, int rounds) {
             for (int k = 0; k < 3; ++k) {
                 const int i = cs[k];
                 if (b.vflags[v0 + i] & 2) continue;
-                const int s = s0 + (i >> 5);
-                const int q0 = b.slice_ptr[s] + (i & 31), width = (b.slice_ptr[s + 1] - b.slice_ptr[s]) >> 5;
+                const int row = b.vert_row[v0 + i];   // neighbours in ascending vertex order
+                const int s = s0 + (row >> 5);
+                const int q0 = b.slice_ptr[s] + (row & 31), width = (b.slice_ptr[s + 1] - b.slice_ptr[s]) >> 5;
                 double sx = 0.0, sy = 0.0;
                 int cnt = 0;
                 for (int kk = 0; kk < width; ++kk) {
                     const int q = q0 + 32 * kk;
                     if (b.slot_edge[q] < 0) continue;
-                    const double2 w = U[v0 + b.slot_col[q]];
+                    const double2 w = U[v0 + b.row_vert[v0 + b.slot_col[q]]];
                     sx += w.x; sy += w.y; ++cnt;
                 }
                 if (cnt > 0) U[v0 + i] = make_double2(sx / cnt, sy / cnt);

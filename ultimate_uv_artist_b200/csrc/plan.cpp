@@ -32,7 +32,45 @@ struct IslandPlan {
     std::vector<int32_t> bverts;       // sorted unique boundary sources
     int32_t nedges = 0, nslices = 0, nslots = 0;
     std::vector<int32_t> slice_w;      // per slice width
+    std::vector<int32_t> row_vert;     // solver row -> vertex (BFS-blob order)
+    std::vector<int32_t> vert_row;     // vertex -> solver row
+    int32_t agg_rows = 0;              // rows per coarse aggregate (0: no coarse level)
+    int32_t ncoarse = 0;               // aggregates
 };
+
+// Rows of the island's solver are ordered so that every run of `agg` rows is
+// a compact blob of the mesh: each aggregate grows by breadth-first search
+// from the lowest unvisited vertex and continues from the next one when its
+// component runs out. Aggregates then match whole 32-row slices, so the
+// coarse restriction of a vector is a sum of warp reductions.
+void blob_order(const IslandPlan& ip, int32_t n, int32_t agg, std::vector<int32_t>& order) {
+    order.clear();
+    order.reserve(n);
+    std::vector<uint8_t> placed(n, 0), inq(n, 0);
+    std::vector<int32_t> queue;
+    queue.reserve(n);
+    int32_t seed = 0;
+    while (static_cast<int32_t>(order.size()) < n) {
+        const int32_t target = std::min<int32_t>(n, static_cast<int32_t>(order.size()) + agg);
+        while (static_cast<int32_t>(order.size()) < target) {
+            while (placed[seed]) ++seed;   // an unplaced vertex exists: order.size() < n
+            queue.clear();
+            queue.push_back(seed);
+            inq[seed] = 1;
+            size_t head = 0;
+            while (head < queue.size() && static_cast<int32_t>(order.size()) < target) {
+                const int32_t v = queue[head++];
+                placed[v] = 1;
+                order.push_back(v);
+                for (int32_t q = ip.row_ptr[v]; q < ip.row_ptr[v + 1]; ++q) {
+                    const int32_t w = ip.row_col[q];
+                    if (!placed[w] && !inq[w]) { inq[w] = 1; queue.push_back(w); }
+                }
+            }
+            for (const int32_t v : queue) inq[v] = 0;
+        }
+    }
+}
 
 void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& bad) {
     ip.n = n; ip.t = t;
@@ -116,13 +154,27 @@ void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& 
     }
     ip.bverts.clear();
     for (int32_t v = 0; v < n; ++v) if (isb[v]) ip.bverts.push_back(v);
-    // sliced ELL: 32 rows per slice
+    // solver row order and coarse aggregates (islands above one warp's rows)
+    if (n > 256) {
+        ip.agg_rows = 128;
+        while ((n + ip.agg_rows - 1) / ip.agg_rows > 256) ip.agg_rows += 128;
+        ip.ncoarse = (n + ip.agg_rows - 1) / ip.agg_rows;
+        blob_order(ip, n, ip.agg_rows, ip.row_vert);
+    } else {
+        ip.agg_rows = 0;
+        ip.ncoarse = 0;
+        ip.row_vert.resize(n);
+        for (int32_t v = 0; v < n; ++v) ip.row_vert[v] = v;
+    }
+    ip.vert_row.assign(n, 0);
+    for (int32_t r = 0; r < n; ++r) ip.vert_row[ip.row_vert[r]] = r;
+    // sliced ELL over solver rows: 32 rows per slice
     ip.nslices = (n + 31) / 32;
     ip.slice_w.assign(ip.nslices, 0);
     ip.nslots = 0;
     for (int32_t s = 0; s < ip.nslices; ++s) {
         int32_t w = 0;
-        for (int32_t r = s * 32; r < std::min(n, s * 32 + 32); ++r) w = std::max(w, deg[r]);
+        for (int32_t r = s * 32; r < std::min(n, s * 32 + 32); ++r) w = std::max(w, deg[ip.row_vert[r]]);
         w = (w + 3) & ~3;            // multiple of 4: the SpMV loads slots 4 at a time
         ip.slice_w[s] = w;
         ip.nslots += 32 * w;
@@ -136,7 +188,7 @@ struct uva_plan {
     int64_t n = 0, t = 0, E = 0, nslices = 0, nslots = 0, nbverts = 0, maxrows = 0;
     std::vector<int64_t> vofs, tofs;
     std::vector<IslandPlan> isl;
-    std::vector<int64_t> eofs, sofs, slotofs, bofs;
+    std::vector<int64_t> eofs, sofs, slotofs, bofs, cofs;
     const int64_t* tris = nullptr;   // not owned; only valid during create
     std::vector<int32_t> tri_local;  // 3t local ids (copied)
 };
@@ -189,15 +241,17 @@ extern "C" int uva_plan_create(const int64_t* tris, const int64_t* vofs, const i
     for (auto& th : pool) th.join();
     if (anybad) { delete p; uva_set_error("uva_plan_create: triangle index outside its island"); return UVA_E_ARG; }
     p->eofs.assign(nc + 1, 0); p->sofs.assign(nc + 1, 0); p->slotofs.assign(nc + 1, 0); p->bofs.assign(nc + 1, 0);
+    p->cofs.assign(nc + 1, 0);
     for (int32_t i = 0; i < nc; ++i) {
         p->eofs[i + 1] = p->eofs[i] + p->isl[i].nedges;
         p->sofs[i + 1] = p->sofs[i] + p->isl[i].nslices;
         p->slotofs[i + 1] = p->slotofs[i] + p->isl[i].nslots;
         p->bofs[i + 1] = p->bofs[i] + static_cast<int64_t>(p->isl[i].bverts.size());
+        p->cofs[i + 1] = p->cofs[i] + static_cast<int64_t>(p->isl[i].ncoarse) * p->isl[i].ncoarse;
         p->maxrows = std::max<int64_t>(p->maxrows, p->isl[i].n);
     }
     p->E = p->eofs[nc]; p->nslices = p->sofs[nc]; p->nslots = p->slotofs[nc]; p->nbverts = p->bofs[nc];
-    if (p->nslots > (int64_t(1) << 31) - 1 || p->E > (int64_t(1) << 31) - 1) {
+    if (p->nslots > (int64_t(1) << 31) - 1 || p->E > (int64_t(1) << 31) - 1 || 4 * p->cofs[nc] > (int64_t(1) << 31) - 1) {
         delete p; uva_set_error("uva_plan_create: plan too large for 32-bit offsets"); return UVA_E_TOOBIG;
     }
     *out = p;
@@ -209,6 +263,7 @@ extern "C" int uva_plan_sizes(const uva_plan* p, int64_t* s) {
     s[UVA_PLAN_NC] = p->nc; s[UVA_PLAN_N] = p->n; s[UVA_PLAN_T] = p->t; s[UVA_PLAN_E] = p->E;
     s[UVA_PLAN_NSLICES] = p->nslices; s[UVA_PLAN_NSLOTS] = p->nslots; s[UVA_PLAN_NBVERTS] = p->nbverts;
     s[UVA_PLAN_MAXROWS] = p->maxrows;
+    s[UVA_PLAN_NCOARSE] = p->cofs[p->nc];
     return UVA_OK;
 }
 
@@ -239,12 +294,13 @@ extern "C" int uva_plan_export(const uva_plan* p, int32_t* tri4, int32_t* tri_ed
                 const int32_t w = ip.slice_w[s];
                 for (int32_t k = 0; k < w; ++k) {
                     for (int32_t lane = 0; lane < 32; ++lane) {
-                        const int32_t r = s * 32 + lane;
+                        const int32_t row = s * 32 + lane;
                         const int64_t q = slot + static_cast<int64_t>(k) * 32 + lane;
-                        if (r < ip.n && k < ip.row_ptr[r + 1] - ip.row_ptr[r]) {
+                        const int32_t r = row < ip.n ? ip.row_vert[row] : 0;   // vertex of this row
+                        if (row < ip.n && k < ip.row_ptr[r + 1] - ip.row_ptr[r]) {
                             const int32_t j = ip.row_col[ip.row_ptr[r] + k];
                             const int32_t e = ip.row_edge[ip.row_ptr[r] + k];
-                            slot_col[q] = j;
+                            slot_col[q] = ip.vert_row[j];
                             slot_edge[q] = static_cast<int32_t>(eb + e);
                             const int32_t info = ip.edge_info[e];
                             const int32_t nf = (info >> 10) & 1023, nr = (info >> 20) & 1023;
@@ -253,7 +309,7 @@ extern "C" int uva_plan_export(const uva_plan* p, int32_t* tri4, int32_t* tri_ed
                             const int32_t b_rj = n_jr == 0 ? n_rj : 0, b_jr = n_rj == 0 ? n_jr : 0;
                             slot_c[q] = -0.5f * static_cast<float>(b_rj) + 0.5f * static_cast<float>(b_jr);
                         } else {
-                            slot_col[q] = r < ip.n ? r : 0;
+                            slot_col[q] = row < ip.n ? row : 0;
                             slot_edge[q] = -1;
                             slot_c[q] = 0.0f;
                         }
@@ -296,3 +352,19 @@ extern "C" int uva_plan_export(const uva_plan* p, int32_t* tri4, int32_t* tri_ed
 }
 
 extern "C" void uva_plan_destroy(uva_plan* p) { delete p; }
+
+extern "C" int uva_plan_export_rows(const uva_plan* p, int32_t* row_vert, int32_t* vert_row, int32_t* agg_rows,
+                                    int32_t* cofs) {
+    if (!p || !row_vert || !vert_row || !agg_rows || !cofs) { uva_set_error("uva_plan_export_rows: null argument"); return UVA_E_ARG; }
+    const int64_t v0 = p->vofs.empty() ? 0 : p->vofs[0];
+    for (int32_t i = 0; i < p->nc; ++i) {
+        const IslandPlan& ip = p->isl[i];
+        const int64_t vb = p->vofs[i] - v0;
+        std::memcpy(row_vert + vb, ip.row_vert.data(), sizeof(int32_t) * ip.n);
+        std::memcpy(vert_row + vb, ip.vert_row.data(), sizeof(int32_t) * ip.n);
+        agg_rows[i] = ip.agg_rows;
+        cofs[i] = static_cast<int32_t>(p->cofs[i]);
+    }
+    cofs[p->nc] = static_cast<int32_t>(p->cofs[p->nc]);
+    return UVA_OK;
+}

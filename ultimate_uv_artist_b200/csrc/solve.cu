@@ -211,6 +211,7 @@ struct Team {
     int* redi;
     int* slot;
     float2 *sp, *sr, *sd;   // CG vectors (shared memory, or null for class G)
+    float *cg, *cy;         // coarse restriction / coarse solution (shared memory)
     __device__ __forceinline__ void sync() { team_sync<NTT>(bar); }
 };
 
@@ -297,8 +298,27 @@ __device__ __forceinline__ void for_rows(int tid, int n, F&& f) {
     }
 }
 
+// Same rows as for_rows, but every lane of a warp runs every iteration (with
+// `valid` false past the island's last row), so warp shuffles are legal:
+// the 32 lanes of a warp hold the 32 consecutive rows of one slice.
+template <int NTT, int R, typename F>
+__device__ __forceinline__ void slice_loop(int tid, int n, F&& f) {
+    if constexpr (R > 0) {
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            const int i = tid + j * NTT;
+            f(i, j, i < n);
+        }
+    } else {
+        for (int base = 0; base < n; base += NTT) f(base + tid, 0, base + tid < n);
+    }
+}
+
 struct Isl {
-    int id, v0, n, f0, nt, s0, pin, p0, p1;
+    int id, v0, n, f0, nt, s0;
+    int pin, p0, p1;          // solver rows of the ARAP pin and the LSCM pins (-1: none)
+    int pinv;                 // ARAP pin vertex
+    int agg, M, co;           // rows per aggregate, aggregates (0: Jacobi only), coarse offset
     double wpin;
 };
 
@@ -308,9 +328,14 @@ __device__ __forceinline__ Isl load_island(const uva_batch& b, int isl) {
     I.v0 = b.vofs[isl]; I.n = b.vofs[isl + 1] - I.v0;
     I.f0 = b.tofs[isl]; I.nt = b.tofs[isl + 1] - I.f0;
     I.s0 = b.sofs[isl];
-    I.pin = b.pins[3 * isl];
-    I.p0 = b.pins[3 * isl + 1];
-    I.p1 = b.pins[3 * isl + 2];
+    I.pinv = b.pins[3 * isl];
+    I.pin = I.n > 0 ? b.vert_row[I.v0 + I.pinv] : -1;
+    const int p0 = b.pins[3 * isl + 1], p1 = b.pins[3 * isl + 2];
+    I.p0 = p0 >= 0 ? b.vert_row[I.v0 + p0] : -1;
+    I.p1 = p1 >= 0 ? b.vert_row[I.v0 + p1] : -1;
+    I.agg = b.agg_rows[isl];
+    I.M = I.agg > 0 ? (I.n + I.agg - 1) / I.agg : 0;
+    I.co = b.cofs[isl];
     I.wpin = b.wpin[isl];
     return I;
 }
@@ -395,10 +420,86 @@ __device__ __forceinline__ float jacobi(const uva_batch& b, const Isl& I, int i)
     return __ldg(b.dinv + I.v0 + i);
 }
 
-// Solves A x = rhs for one island. x64 (global, FP64) holds the start on entry
-// and the solution on exit. FP64 residual refinement around FP32 Jacobi-PCG
-// corrections; NCOL = 2 (ARAP: u and v separately) or 1 (LSCM: one vector of
-// 2n unknowns). Returns the inner CG iterations executed.
+// Two-level additive preconditioner z = D^-1 r + P Ac^-1 P^T r. P is the
+// piecewise-constant prolongation over aggregates of `agg` consecutive solver
+// rows (compact mesh blobs from the plan; agg is a multiple of 128, so an
+// aggregate is agg/32 whole slices), Ac = P^T A P is inverted once per batch
+// by the setup. Restriction is deterministic: each warp writes the sum of its
+// slice (one warp owns one slice in slice_loop) to b.cpart, and coarse_solve
+// adds the slices of each aggregate in slice order before the dense product
+// with Ac^-1 (one warp per output row).
+template <int NTT, Op OP>
+__device__ __forceinline__ void coarse_restrict(const uva_batch& b, Team<NTT>& tm, const Isl& I, int i, bool valid,
+                                                float2 r) {
+    float rx = valid ? r.x : 0.f, ry = valid ? r.y : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        rx += __shfl_xor_sync(0xffffffffu, rx, o);
+        ry += __shfl_xor_sync(0xffffffffu, ry, o);
+    }
+    if ((tm.tid & 31) == 0 && (i - (tm.tid & 31)) < I.n)
+        reinterpret_cast<float2*>(b.cpart)[I.s0 + (i >> 5)] = make_float2(rx, ry);
+}
+
+// y = Ac^-1 g, g gathered from the slice sums of the last restriction (which a
+// team barrier completed). Ends with a barrier: y complete, slice sums free.
+template <int NTT, Op OP>
+__device__ __forceinline__ void coarse_solve(const uva_batch& b, Team<NTT>& tm, const Isl& I) {
+    constexpr int NW = NTT / 32;
+    const int lane = tm.tid & 31, warp = tm.tid >> 5;
+    const float2* part = reinterpret_cast<const float2*>(b.cpart) + I.s0;
+    const int spa = I.agg >> 5, nsl = (I.n + 31) >> 5;
+    for (int a = tm.tid; a < I.M; a += NTT) {
+        float gx = 0.f, gy = 0.f;
+        for (int s = a * spa; s < min((a + 1) * spa, nsl); ++s) {
+            const float2 p = part[s];
+            gx += p.x; gy += p.y;
+        }
+        if (OP == OP_ARAP) { tm.cg[a] = gx; tm.cg[I.M + a] = gy; }
+        else { tm.cg[2 * a] = gx; tm.cg[2 * a + 1] = gy; }
+    }
+    tm.sync();   // g complete
+    if (OP == OP_ARAP) {
+        const float* A = b.coarse_a + I.co;
+        for (int o = warp; o < I.M; o += NW) {
+            float au = 0.f, av = 0.f;
+            for (int c = lane; c < I.M; c += 32) {
+                const float w = __ldg(A + static_cast<size_t>(o) * I.M + c);
+                au = fmaf(w, tm.cg[c], au);
+                av = fmaf(w, tm.cg[I.M + c], av);
+            }
+#pragma unroll
+            for (int k = 16; k > 0; k >>= 1) {
+                au += __shfl_xor_sync(0xffffffffu, au, k);
+                av += __shfl_xor_sync(0xffffffffu, av, k);
+            }
+            if (lane == 0) { tm.cy[o] = au; tm.cy[I.M + o] = av; }
+        }
+    } else {
+        const int N = 2 * I.M;
+        const float* A = b.coarse_l + 4 * static_cast<size_t>(I.co);
+        for (int o = warp; o < N; o += NW) {
+            float acc = 0.f;
+            for (int c = lane; c < N; c += 32) acc = fmaf(__ldg(A + static_cast<size_t>(o) * N + c), tm.cg[c], acc);
+#pragma unroll
+            for (int k = 16; k > 0; k >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, k);
+            if (lane == 0) tm.cy[o] = acc;
+        }
+    }
+    tm.sync();   // y complete
+}
+
+template <int NTT, Op OP>
+__device__ __forceinline__ float2 prolong(const Team<NTT>& tm, const Isl& I, int i) {
+    const int a = i / I.agg;
+    if (OP == OP_ARAP) return make_float2(tm.cy[a], tm.cy[I.M + a]);
+    return make_float2(tm.cy[2 * a], tm.cy[2 * a + 1]);
+}
+
+// Solves A x = rhs for one island. x64 (global, FP64, by solver row) holds the
+// start on entry and the solution on exit. FP64 residual refinement around
+// FP32 PCG corrections; NCOL = 2 (ARAP: u and v separately) or 1 (LSCM: one
+// vector of 2n unknowns). Returns the inner CG iterations executed.
 template <int NTT, int R, Op OP, int NCOL>
 __device__ int refine_solve(const uva_batch& b, const Isl& I, const uva_solve_params& prm, Team<NTT>& tm,
                             const double bb[2], double res_out[2], int& nref, bool& capped) {
@@ -410,23 +511,29 @@ __device__ int refine_solve(const uva_batch& b, const Isl& I, const uva_solve_pa
     float2* sq = reinterpret_cast<float2*>(b.q32) + I.v0;   // class G only
     const float wpin32 = static_cast<float>(I.wpin);
     const int tid = tm.tid, n = I.n;
+    const bool two_level = NTT > 32 && I.M > 0;
     float2 qreg[R > 0 ? R : 1];
     int total = 0;
     capped = false;
     nref = 0;
     for (int ref = 0;; ++ref) {
-        // ---- FP64 residual r = rhs - A x
+        // ---- FP64 residual r = rhs - A x; restriction of r for the coarse level
         double rr[2] = {0.0, 0.0};
-        for_rows<NTT, R>(tid, n, [&](int i, int) {
-            double2 r = make_double2(0.0, 0.0);
-            if (!is_pinned<OP>(I, i)) {
-                const double2 ax = apply64<OP>(b, I, i, x64);
-                const double2 rhs = OP == OP_ARAP ? b64[i] : make_double2(0.0, 0.0);
-                r = make_double2(rhs.x - ax.x, rhs.y - ax.y);
+        slice_loop<NTT, R>(tid, n, [&](int i, int, bool valid) {
+            float2 r32 = make_float2(0.f, 0.f);
+            if (valid) {
+                double2 r = make_double2(0.0, 0.0);
+                if (!is_pinned<OP>(I, i)) {
+                    const double2 ax = apply64<OP>(b, I, i, x64);
+                    const double2 rhs = OP == OP_ARAP ? b64[i] : make_double2(0.0, 0.0);
+                    r = make_double2(rhs.x - ax.x, rhs.y - ax.y);
+                }
+                r32 = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
+                sr[i] = r32;
+                rr[0] += r.x * r.x;
+                rr[1] += r.y * r.y;
             }
-            sr[i] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
-            rr[0] += r.x * r.x;
-            rr[1] += r.y * r.y;
+            if (two_level) coarse_restrict<NTT, OP>(b, tm, I, i, valid, r32);
         });
         team_sum<NTT, 2>(tm, rr, tm.redd);
         ++nref;
@@ -440,16 +547,21 @@ __device__ int refine_solve(const uva_batch& b, const Isl& I, const uva_solve_pa
             res_out[0] = res_out[1] = sqrt(s / fmax(bb[0], 1e-300));
             done = s <= prm.tol * prm.tol * fmax(bb[0], 1e-300);
         }
-        if (done) break;
-        if (ref >= prm.max_refine || !isfinite(rr[0] + rr[1])) { capped = true; break; }
+        if (done || ref >= prm.max_refine || !isfinite(rr[0] + rr[1])) {
+            if (!done) capped = true;
+            break;
+        }
+        if (two_level) coarse_solve<NTT, OP>(b, tm, I);
         // ---- inner FP32 PCG on A d = r, d0 = 0
         float red4[4] = {0.f, 0.f, 0.f, 0.f};   // r.z (2), r.r (2)
         for_rows<NTT, R>(tid, n, [&](int i, int) {
             const float2 r = sr[i];
             const float m = jacobi<OP>(b, I, i);
+            float2 z = make_float2(m * r.x, m * r.y);
+            if (two_level && !is_pinned<OP>(I, i)) { const float2 y = prolong<NTT, OP>(tm, I, i); z.x += y.x; z.y += y.y; }
             sd[i] = make_float2(0.f, 0.f);
-            sp[i] = make_float2(m * r.x, m * r.y);
-            red4[0] += m * r.x * r.x; red4[1] += m * r.y * r.y;
+            sp[i] = z;
+            red4[0] += r.x * z.x; red4[1] += r.y * z.y;
             red4[2] += r.x * r.x; red4[3] += r.y * r.y;
         });
         team_sum<NTT, 4>(tm, red4, tm.redf);
@@ -491,17 +603,32 @@ __device__ int refine_solve(const uva_batch& b, const Isl& I, const uva_solve_pa
                 const float s = pq[0] + pq[1];
                 alpha[0] = alpha[1] = (act[0] && s > 0.f) ? rz[0] / s : 0.f;
             }
+            // update d, r; restrict r
+            slice_loop<NTT, R>(tid, n, [&](int i, int j, bool valid) {
+                float2 r = make_float2(0.f, 0.f);
+                if (valid) {
+                    float2 q;
+                    if constexpr (R > 0) q = qreg[j]; else q = sq[i];
+                    const float2 p = sp[i];
+                    float2 d = sd[i];
+                    r = sr[i];
+                    d.x = fmaf(alpha[0], p.x, d.x); d.y = fmaf(alpha[1], p.y, d.y);
+                    r.x = fmaf(-alpha[0], q.x, r.x); r.y = fmaf(-alpha[1], q.y, r.y);
+                    sd[i] = d; sr[i] = r;
+                }
+                if (two_level) coarse_restrict<NTT, OP>(b, tm, I, i, valid, r);
+            });
+            if (two_level) {
+                tm.sync();   // slice sums complete
+                coarse_solve<NTT, OP>(b, tm, I);
+            }
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            for_rows<NTT, R>(tid, n, [&](int i, int j) {
-                float2 q;
-                if constexpr (R > 0) q = qreg[j]; else q = sq[i];
-                const float2 p = sp[i];
-                float2 d = sd[i], r = sr[i];
-                d.x = fmaf(alpha[0], p.x, d.x); d.y = fmaf(alpha[1], p.y, d.y);
-                r.x = fmaf(-alpha[0], q.x, r.x); r.y = fmaf(-alpha[1], q.y, r.y);
-                sd[i] = d; sr[i] = r;
+            for_rows<NTT, R>(tid, n, [&](int i, int) {
+                const float2 r = sr[i];
                 const float m = jacobi<OP>(b, I, i);
-                acc[0] += m * r.x * r.x; acc[1] += m * r.y * r.y;
+                float zx = m * r.x, zy = m * r.y;
+                if (two_level && !is_pinned<OP>(I, i)) { const float2 y = prolong<NTT, OP>(tm, I, i); zx += y.x; zy += y.y; }
+                acc[0] += r.x * zx; acc[1] += r.y * zy;
                 acc[2] += r.x * r.x; acc[3] += r.y * r.y;
             });
             team_sum<NTT, 4>(tm, acc, tm.redf);
@@ -524,7 +651,9 @@ __device__ int refine_solve(const uva_batch& b, const Isl& I, const uva_solve_pa
             for_rows<NTT, R>(tid, n, [&](int i, int) {
                 const float2 r = sr[i], p = sp[i];
                 const float m = jacobi<OP>(b, I, i);
-                sp[i] = make_float2(fmaf(beta[0], p.x, m * r.x), fmaf(beta[1], p.y, m * r.y));
+                float zx = m * r.x, zy = m * r.y;
+                if (two_level && !is_pinned<OP>(I, i)) { const float2 y = prolong<NTT, OP>(tm, I, i); zx += y.x; zy += y.y; }
+                sp[i] = make_float2(fmaf(beta[0], p.x, zx), fmaf(beta[1], p.y, zy));
             });
         }
         if (it >= prm.max_inner) capped = true;
@@ -607,7 +736,8 @@ __device__ __forceinline__ double step_bound(const uva_batch& b, const Isl& I, i
                                              bool batch) {
     const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
     const double2 u0 = U[I.v0 + tv.x], u1 = U[I.v0 + tv.y], u2 = U[I.v0 + tv.z];
-    const double2 x0 = X[I.v0 + tv.x], x1 = X[I.v0 + tv.y], x2 = X[I.v0 + tv.z];
+    const int* vr = b.vert_row + I.v0;
+    const double2 x0 = X[I.v0 + vr[tv.x]], x1 = X[I.v0 + vr[tv.y]], x2 = X[I.v0 + vr[tv.z]];
     const double2 d0 = make_double2(x0.x - u0.x, x0.y - u0.y), d1 = make_double2(x1.x - u1.x, x1.y - u1.y),
                   d2 = make_double2(x2.x - u2.x, x2.y - u2.y);
     const double ux1 = u1.x - u0.x, uy1 = u1.y - u0.y, ux2 = u2.x - u0.x, uy2 = u2.y - u0.y;
@@ -679,7 +809,7 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
         tm.sync();   // corner terms complete
         double bb[2] = {0.0, 0.0};
         for_rows<NTT, R>(tid, I.n, [&](int i, int) {
-            const int v = I.v0 + i;
+            const int v = I.v0 + __ldg(b.row_vert + I.v0 + i);   // vertex of solver row i
             double bx = 0.0, by = 0.0;
             const int pe = __ldg(b.vt_ptr + v + 1);
             for (int p = __ldg(b.vt_ptr + v); p < pe; ++p) {
@@ -688,8 +818,8 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
             }
             const double2 u = U[v];
             if (i == I.pin) { bx += I.wpin * u.x; by += I.wpin * u.y; }
-            b64[v] = make_double2(bx, by);
-            x64[v] = u;
+            b64[I.v0 + i] = make_double2(bx, by);
+            x64[I.v0 + i] = u;
             bb[0] += bx * bx; bb[1] += by * by;
         });
         team_sum<NTT, 2>(tm, bb, tm.redd);   // also publishes x64 / b64 to the team
@@ -716,8 +846,8 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
         st.step = step;
         tm.sync();   // all line-search reads of U done
         for_rows<NTT, R>(tid, I.n, [&](int i, int) {
-            const int v = I.v0 + i;
-            const double2 u = U[v], x = x64[v];
+            const int v = I.v0 + __ldg(b.row_vert + I.v0 + i);
+            const double2 u = U[v], x = x64[I.v0 + i];
             U[v] = use_ls ? make_double2(u.x + (x.x - u.x) * step, u.y + (x.y - u.y) * step) : x;
         });
         tm.sync();
@@ -754,8 +884,8 @@ __device__ void solve_lscm(const uva_batch& b, const uva_solve_params& prm, Team
         nrm[2] += e1x * e2y - e1y * e2x;
     }
     team_sum<NTT, 3>(tm, nrm, tm.redd);
-    const double* pp0 = P + 3 * (I.v0 + I.p0);
-    const double* pp1 = P + 3 * (I.v0 + I.p1);
+    const double* pp0 = P + 3 * (I.v0 + b.pins[3 * I.id + 1]);   // pin vertices
+    const double* pp1 = P + 3 * (I.v0 + b.pins[3 * I.id + 2]);
     // every thread derives the same basis from the same totals
     const double nl = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
     double nx = 0.0, ny = 0.0, nz = 1.0;
@@ -770,7 +900,7 @@ __device__ void solve_lscm(const uva_batch& b, const uva_solve_params& prm, Team
     else { ax = 1.0; ay = 0.0; az = 0.0; }
     const double bx = ny * az - nz * ay, by = nz * ax - nx * az, bz = nx * ay - ny * ax;
     for_rows<NTT, R>(tid, I.n, [&](int i, int) {
-        const double* pi = P + 3 * (I.v0 + i);
+        const double* pi = P + 3 * (I.v0 + __ldg(b.row_vert + I.v0 + i));
         const double dx = pi[0] - pp0[0], dy = pi[1] - pp0[1], dz = pi[2] - pp0[2];
         double2 x = make_double2(s * (dx * ax + dy * ay + dz * az), s * (dx * bx + dy * by + dz * bz));
         if (i == I.p0) x = make_double2(0.0, 0.0);
@@ -807,7 +937,7 @@ __device__ void solve_lscm(const uva_batch& b, const uva_solve_params& prm, Team
     for_rows<NTT, R>(tid, I.n, [&](int i, int) {
         const double2 x = x64[I.v0 + i];
         bad |= finite2(x) ? 0 : 1;
-        U[I.v0 + i] = x;
+        U[I.v0 + __ldg(b.row_vert + I.v0 + i)] = x;
     });
     bad = team_or(tm, bad);
     if (bad) st.flags |= UVA_ST_NONFINITE;
@@ -845,8 +975,10 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
     __shared__ float redf[2 * 4 * 32];
     __shared__ int redi[2 * 32];
     __shared__ int slots[8];
+    __shared__ float coarse_buf[1024];   // g and y of the coarse level (CTA: 512 each; sub-team: 128 each)
     {
-        Team<KB> tm{static_cast<int>(threadIdx.x), 0, 0, redd, redf, redi, &slots[0], nullptr, nullptr, nullptr};
+        Team<KB> tm{static_cast<int>(threadIdx.x), 0, 0, redd, redf, redi, &slots[0], nullptr, nullptr, nullptr,
+                    coarse_buf, coarse_buf + 512};
         run_class<KB, 0, OP>(b, prm, tm, 0);
         tm.sp = dyn; tm.sr = dyn + KB * RB; tm.sd = dyn + 2 * KB * RB;
         run_class<KB, RB, OP>(b, prm, tm, 1);
@@ -856,16 +988,131 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
     {
         float2* base = dyn + s * (3 * SUB * RB);
         Team<SUB> tm{static_cast<int>(threadIdx.x % SUB), 1 + s, 0, redd + s * 64, redf + s * 64, redi + s * 16,
-                     &slots[1 + s], base, base + SUB * RB, base + 2 * SUB * RB};
+                     &slots[1 + s], base, base + SUB * RB, base + 2 * SUB * RB, coarse_buf + 256 * s,
+                     coarse_buf + 256 * s + 128};
         run_class<SUB, RB, OP>(b, prm, tm, 2);
     }
     {
         const int w = threadIdx.x / 32;
         float2* base = dyn + w * (3 * 32 * RB);
         Team<32> tm{static_cast<int>(threadIdx.x % 32), 0, 0, nullptr, nullptr, nullptr, nullptr,
-                    base, base + 32 * RB, base + 2 * 32 * RB};
+                    base, base + 32 * RB, base + 2 * 32 * RB, nullptr, nullptr};
         run_class<32, RB, OP>(b, prm, tm, 3);
     }
+}
+
+// In-place Gauss-Jordan inverse of an SPD N x N FP64 matrix (no pivoting
+// needed), one CTA. A non-positive pivot (a singular coarse block, e.g. a
+// disconnected island) zeroes that row and column of the result.
+__device__ void gauss_jordan(double* W, int N, double* colk) {
+    for (int k = 0; k < N; ++k) {
+        __syncthreads();
+        const double piv = W[static_cast<size_t>(k) * N + k];
+        const double ip = (piv > 0.0 && isfinite(piv)) ? 1.0 / piv : 0.0;
+        for (int i = threadIdx.x; i < N; i += blockDim.x) colk[i] = i == k ? 0.0 : W[static_cast<size_t>(i) * N + k];
+        __syncthreads();
+        for (int j = threadIdx.x; j < N; j += blockDim.x)
+            W[static_cast<size_t>(k) * N + j] = j == k ? ip : W[static_cast<size_t>(k) * N + j] * ip;
+        __syncthreads();
+        for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+            const int i = e / N, j = e % N;
+            if (i == k) continue;
+            const double f = colk[i];
+            if (f == 0.0) continue;
+            const double base = j == k ? 0.0 : W[e];
+            W[e] = base - f * W[static_cast<size_t>(k) * N + j];
+        }
+    }
+    __syncthreads();
+}
+
+// Coarse operators of every island with aggregates: ARAP Ac = P^T A P (with
+// the soft pin) and LSCM Hc = P^T H P over free unknowns (u, v per aggregate),
+// accumulated from the FP32 slot weights in FP64, inverted, stored in FP32.
+__global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
+    __shared__ double colk[512];
+    const int isl = blockIdx.x;
+    if (isl >= b.nc) return;
+    const int agg = b.agg_rows[isl];
+    if (agg <= 0) return;
+    const int v0 = b.vofs[isl], n = b.vofs[isl + 1] - v0, s0 = b.sofs[isl];
+    const int M = (n + agg - 1) / agg;
+    const int co = b.cofs[isl];
+    double* W = b.coarse_work + 4 * static_cast<size_t>(co);
+    const int2* cw = reinterpret_cast<const int2*>(b.slot_cw);
+    auto row_slots_l = [&](int r, int& q0, int& width) {
+        const int s = s0 + (r >> 5);
+        q0 = b.slice_ptr[s] + (r & 31);
+        width = (b.slice_ptr[s + 1] - b.slice_ptr[s]) >> 5;
+    };
+    // ---- ARAP
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) W[e] = 0.0;
+    __syncthreads();
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        const int a = r / agg;
+        int q0, width;
+        row_slots_l(r, q0, width);
+        double dsum = 0.0;
+        for (int k = 0; k < width; ++k) {
+            const int2 sl = cw[q0 + 32 * k];
+            const double w = static_cast<double>(__int_as_float(sl.y));
+            if (w == 0.0) continue;
+            const int c = sl.x / agg;
+            dsum += w;
+            if (c != a) atomicAdd(W + static_cast<size_t>(a) * M + c, -w);
+            else dsum -= w;
+        }
+        if (dsum != 0.0) atomicAdd(W + static_cast<size_t>(a) * M + a, dsum);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int pr = b.vert_row[v0 + b.pins[3 * isl]];
+        const int a = pr / agg;
+        W[static_cast<size_t>(a) * M + a] += b.wpin[isl];
+    }
+    gauss_jordan(W, M, colk);
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) b.coarse_a[co + e] = static_cast<float>(W[e]);
+    __syncthreads();
+    // ---- LSCM (free unknowns only; the pins are fixed)
+    const int pv0 = b.pins[3 * isl + 1], pv1 = b.pins[3 * isl + 2];
+    if (pv0 < 0 || pv1 < 0) return;
+    const int p0 = b.vert_row[v0 + pv0], p1 = b.vert_row[v0 + pv1];
+    const int N = 2 * M;
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) W[e] = 0.0;
+    __syncthreads();
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        if (r == p0 || r == p1) continue;
+        const int a = r / agg;
+        int q0, width;
+        row_slots_l(r, q0, width);
+        double dsum = 0.0;
+        for (int k = 0; k < width; ++k) {
+            const int q = q0 + 32 * k;
+            const int2 sl = cw[q];
+            const double w = static_cast<double>(__int_as_float(sl.y));
+            const double cc = static_cast<double>(b.slot_c[q]);
+            if (w == 0.0 && cc == 0.0) continue;
+            dsum += w;
+            if (sl.x == p0 || sl.x == p1) continue;   // pinned neighbour: no coarse coupling
+            const int c = sl.x / agg;
+            if (c == a) {
+                dsum -= w;
+            } else {
+                atomicAdd(W + static_cast<size_t>(2 * a) * N + 2 * c, -w);
+                atomicAdd(W + static_cast<size_t>(2 * a + 1) * N + 2 * c + 1, -w);
+            }
+            if (cc != 0.0) {
+                atomicAdd(W + static_cast<size_t>(2 * a) * N + 2 * c + 1, cc);
+                atomicAdd(W + static_cast<size_t>(2 * a + 1) * N + 2 * c, -cc);
+            }
+        }
+        if (dsum != 0.0) {
+            atomicAdd(W + static_cast<size_t>(2 * a) * N + 2 * a, dsum);
+            atomicAdd(W + static_cast<size_t>(2 * a + 1) * N + 2 * a + 1, dsum);
+        }
+    }
+    gauss_jordan(W, N, colk);
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) b.coarse_l[4 * static_cast<size_t>(co) + e] = static_cast<float>(W[e]);
 }
 
 int sm_count() {
@@ -877,7 +1124,8 @@ int sm_count() {
 
 bool check_batch(const uva_batch* b) {
     return b && b->nc >= 0 && b->n >= 0 && b->t >= 0 &&
-           (b->nc == 0 || (b->vofs && b->tofs && b->sofs && b->order && b->work && b->slot_cw));
+           (b->nc == 0 || (b->vofs && b->tofs && b->sofs && b->order && b->work && b->slot_cw && b->row_vert &&
+                           b->vert_row && b->agg_rows && b->cofs && b->coarse_a && b->coarse_l && b->cpart));
 }
 
 bool check_classes(const uva_batch* b) {
@@ -928,6 +1176,10 @@ extern "C" int uva_batch_setup(uva_batch* b, void* stream) {
     UVA_CHECK_LAUNCH("uva_batch_setup/rows");
     k_far_pair<<<(b->nc + 127) / 128, 128, 0, s>>>(*b);
     UVA_CHECK_LAUNCH("uva_batch_setup/pins");
+    if (b->coarse_a && b->coarse_l && b->coarse_work) {
+        k_coarse<<<b->nc, 1024, 0, s>>>(*b);
+        UVA_CHECK_LAUNCH("uva_batch_setup/coarse");
+    }
     return UVA_OK;
 }
 
@@ -960,8 +1212,10 @@ constexpr size_t kNaX64 = kAlignUp(sizeof(double) * 2 * kNoAllocMaxVerts);      
 constexpr size_t kNaB64 = kAlignUp(sizeof(double) * 2 * kNoAllocMaxVerts);        // b64
 constexpr size_t kNaRc = kAlignUp(sizeof(double) * 6 * kNoAllocMaxTris);          // rc
 constexpr size_t kNaF32 = kAlignUp(sizeof(float) * 2 * kNoAllocMaxVerts);         // r32, d32, p32, q32
-constexpr size_t kNoAllocBytes = kNaWork + kNaX64 + kNaB64 + kNaRc + 4 * kNaF32;   // 5,243,136 bytes
+constexpr size_t kNaPart = kAlignUp(sizeof(float) * 2 * kNoAllocMaxVerts);        // cpart (nslices <= n)
+constexpr size_t kNoAllocBytes = kNaWork + kNaX64 + kNaB64 + kNaRc + 4 * kNaF32 + kNaPart;   // 5,505,280 bytes
 
+static_assert(kNoAllocBytes == 5505280, "documented size of the static scratch");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 // Device address of g_noalloc_scratch on the current device, looked up once
@@ -991,7 +1245,7 @@ extern "C" int uva_arap_noalloc(const uva_batch* b, const uva_solve_params* prm,
         uva_set_error("uva_arap_noalloc: bad arguments (status and U are required outputs)");
         return UVA_E_ARG;
     }
-    if (b->n > kNoAllocMaxVerts || b->t > kNoAllocMaxTris) {
+    if (b->n > kNoAllocMaxVerts || b->t > kNoAllocMaxTris || b->nslices > kNoAllocMaxVerts) {
         uva_set_error("uva_arap_noalloc: batch above the fixed scratch limit of 32768 vertices / 65536 triangles");
         return UVA_E_TOOBIG;
     }
@@ -1008,7 +1262,8 @@ extern "C" int uva_arap_noalloc(const uva_batch* b, const uva_solve_params* prm,
     w.r32 = reinterpret_cast<float*>(base + off); off += kNaF32;
     w.d32 = reinterpret_cast<float*>(base + off); off += kNaF32;
     w.p32 = reinterpret_cast<float*>(base + off); off += kNaF32;
-    w.q32 = reinterpret_cast<float*>(base + off);
+    w.q32 = reinterpret_cast<float*>(base + off); off += kNaF32;
+    w.cpart = reinterpret_cast<float*>(base + off);
     // the work counters are the only scratch that must start at zero;
     // launch_islands clears them on the stream before the launch
     return launch_islands<OP_ARAP>(&w, prm, static_cast<cudaStream_t>(stream));

@@ -6,9 +6,10 @@ and keeps every per-island array in HBM: frames, weights, the sliced-ELL
 Laplacian, UVs and solver scratch. All solver calls run on one CUDA stream and
 never synchronise the host.
 
-Memory: about 80 bytes per triangle plus about 170 bytes per vertex
-(UVs and solver vectors), so a 180 GB B200 holds batches of several hundred
-million triangles.
+Memory: about 80 bytes per triangle plus about 180 bytes per vertex
+(UVs, solver vectors, sliced-ELL slots) and 20 bytes per squared coarse
+aggregate, so a 180 GB B200 holds batches of several hundred million
+triangles.
 """
 from __future__ import annotations
 
@@ -53,6 +54,7 @@ class Plan:
             check(L.uva_plan_sizes(h, ptr(sz)), "uva_plan_sizes")
             self.nc, self.n, self.t, self.E = int(sz[0]), int(sz[1]), int(sz[2]), int(sz[3])
             self.nslices, self.nslots, self.nbverts, self.maxrows = int(sz[4]), int(sz[5]), int(sz[6]), int(sz[7])
+            self.ncoarse = int(sz[8])
             self.tri4 = np.empty((self.t, 4), np.int32)
             self.tri_edge = np.empty((self.t, 3), np.int32)
             self.sofs = np.empty(nc + 1, np.int32)
@@ -69,6 +71,12 @@ class Plan:
                                     ptr(self.slot_col), ptr(self.slot_edge), ptr(self.slot_c), ptr(self.vt_ptr),
                                     ptr(self.vt), ptr(self.vflags), ptr(self.bofs), ptr(self.bverts)),
                   "uva_plan_export")
+            self.row_vert = np.empty(max(self.n, 1), np.int32)
+            self.vert_row = np.empty(max(self.n, 1), np.int32)
+            self.agg_rows = np.empty(max(nc, 1), np.int32)
+            self.cofs = np.empty(nc + 1, np.int32)
+            check(L.uva_plan_export_rows(h, ptr(self.row_vert), ptr(self.vert_row), ptr(self.agg_rows), ptr(self.cofs)),
+                  "uva_plan_export_rows")
         finally:
             L.uva_plan_destroy(h)
         self.vofs = vofs.astype(np.int32)
@@ -126,6 +134,8 @@ class DeviceBatch:
         self.slot_edge = up(plan.slot_edge); self.slot_c = up(plan.slot_c)
         self.vt_ptr = up(plan.vt_ptr); self.vt = up(plan.vt); self.vflags = up(plan.vflags)
         self.bofs = up(plan.bofs); self.bverts = up(plan.bverts); self.order = up(plan.order)
+        self.row_vert = up(plan.row_vert); self.vert_row = up(plan.vert_row)
+        self.agg_rows = up(plan.agg_rows); self.cofs = up(plan.cofs)
         # geometry
         n, t, nc = max(self.n, 1), max(self.t, 1), max(self.nc, 1)
         f64, f32 = torch.float64, torch.float32
@@ -136,6 +146,11 @@ class DeviceBatch:
         self.wedge = torch.empty(max(plan.E, 1), dtype=f64, device=d)
         self.slot_cw = torch.empty((max(plan.nslots, 1), 2), dtype=torch.int32, device=d)
         self.wdiag = torch.empty(n, dtype=f64, device=d)
+        nco = max(plan.ncoarse, 1)
+        self.coarse_a = torch.empty(nco, dtype=f32, device=d)
+        self.coarse_l = torch.empty(4 * nco, dtype=f32, device=d)
+        self.coarse_work = torch.empty(4 * nco, dtype=f64, device=d)
+        self.cpart = torch.empty(2 * max(plan.nslices, 1), dtype=f32, device=d)
         self.dinv = torch.empty(n, dtype=f32, device=d)
         self.pins = torch.zeros((nc, 3), dtype=torch.int32, device=d)
         self.wpin = torch.empty(nc, dtype=f64, device=d)
@@ -165,7 +180,8 @@ class DeviceBatch:
         for c in range(5):
             D.class_ofs[c] = int(p.class_ofs[c])
         for name in ("vofs", "tofs", "sofs", "tri4", "tri_edge", "slice_ptr", "slot_col", "slot_edge", "slot_c",
-                     "vt_ptr", "vt", "vflags", "bofs", "bverts", "order", "P", "frame", "wtri", "tscale", "wedge",
+                     "vt_ptr", "vt", "vflags", "bofs", "bverts", "order", "row_vert", "vert_row", "agg_rows", "cofs",
+                     "coarse_a", "coarse_l", "coarse_work", "cpart", "P", "frame", "wtri", "tscale", "wedge",
                      "slot_cw", "wdiag", "dinv", "pins", "wpin", "U", "x64", "b64", "rc", "r32", "d32", "p32",
                      "q32", "status", "work"):
             setattr(D, name, getattr(self, name).data_ptr())

@@ -161,9 +161,16 @@ class Batch:
     def wpin(self):
         return self.db.wpin[0].to(self.dt) if self.nc else torch.tensor(1e-12, dtype=self.dt, device=self.dev)
 
+    def _wdiag_by_vertex(self):
+        """Row sums of the weights, reordered from solver rows to vertices."""
+        vr = self.db.vert_row[:self.n].to(torch.int64)
+        base = torch.repeat_interleave(self.db.vofs[:-1].to(torch.int64),
+                                       torch.as_tensor(np.diff(self.offsets), device=self.dev))
+        return self.db.wdiag[:self.n][base + vr]
+
     @property
     def dinv(self):
-        d = self.db.wdiag[:self.n].clone()
+        d = self._wdiag_by_vertex().clone()
         d[self.pins] += self.db.wpin[:self.nc]
         return (1.0 / d.clamp_min(1e-30)).to(self.dt)
 
@@ -174,7 +181,7 @@ class Batch:
         p = self.db.plan
         wsum = self.db.wedge[:p.E].to(self.dt)
         keep = ea != eb
-        diag = self.db.wdiag[:self.n].clone()
+        diag = self._wdiag_by_vertex().clone()
         diag[self.pins] += self.db.wpin[:self.nc]
         return sym_csr(self.n, ea[keep], eb[keep], -wsum[keep], diag.to(self.dt))
 
