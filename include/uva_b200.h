@@ -62,6 +62,10 @@ typedef struct uva_island_status {
     double  resid[2];      /* last FP64 relative residual per column        */
     double  energy;        /* last ARAP energy (param semantics)            */
     double  step;          /* last line-search step                         */
+    int64_t t_begin;       /* %globaltimer (ns) when the island's team took it */
+    int64_t t_end;         /* %globaltimer (ns) when the team finished it    */
+    int32_t sm;            /* SM that ran the island                        */
+    int32_t team;          /* team width that ran it (1024, 256 or 32)      */
 } uva_island_status;
 
 /* --------------------------------------------------------------------------
@@ -176,6 +180,22 @@ int uva_lscm(uva_batch* b, const uva_solve_params* prm, void* stream);
 /* ARAP local/global iterations of every island in one persistent launch
  * (gpu.py:230-249 with semantics BATCH, param.py:379-414 with PARAM).      */
 int uva_arap(uva_batch* b, const uva_solve_params* prm, void* stream);
+
+/* Step graphs. No counterpart in the reference, which launches every kernel
+ * of gpu.Batch.arap (gpu.py:230-249) from Python, one host sync per CG
+ * iteration. Captures any subset of setup + LSCM + ARAP of one batch into a CUDA graph
+ * (private stream, thread-local capture mode) and replays it with one
+ * launch. The graph holds the batch's pointers and the parameters given at
+ * creation: re-create it after changing either. Replays of one graph must
+ * not overlap (they share the batch scratch). */
+#define UVA_STEP_SETUP 1
+#define UVA_STEP_LSCM  2
+#define UVA_STEP_ARAP  4
+typedef struct uva_graph uva_graph;
+int uva_step_graph_create(uva_batch* b, int32_t parts, const uva_solve_params* lscm,
+                          const uva_solve_params* arap, uva_graph** out);
+int uva_graph_launch(uva_graph* g, void* stream);
+int uva_graph_destroy(uva_graph* g);
 
 /* No counterpart in the reference. The same ARAP iterations as uva_arap, for
  * callers that cannot allocate device memory while they run (for example a

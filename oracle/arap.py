@@ -52,7 +52,11 @@ def batch_frames(P, T):
 class BatchRef:
     """FP64 restatement of engine/gpu.py:66-299 with exact global solves."""
 
-    def __init__(self, charts):
+    def __init__(self, charts, wpin=None):
+        """``wpin`` overrides the soft-pin weight (the reference takes the max
+        |w| of the whole batch; a sub-batch checked against a larger batch
+        passes that batch's value)."""
+        self._wpin_override = wpin
         P, T, U, cv, ct = [], [], [], [], []
         off = 0
         for i, (p, t, u) in enumerate(charts):
@@ -91,6 +95,8 @@ class BatchRef:
         diag = np.bincount(ea, weights=wsum, minlength=n) + np.bincount(eb, weights=wsum, minlength=n)
         self.pins = self.offsets[:-1].copy()
         self.wpin = max(float(np.abs(W).max()) if len(W) else 0.0, 1e-12)
+        if self._wpin_override is not None:
+            self.wpin = float(self._wpin_override)
         diag[self.pins] += self.wpin
         rows = np.concatenate([ea, eb, np.arange(n)])
         cols = np.concatenate([eb, ea, np.arange(n)])

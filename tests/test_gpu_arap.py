@@ -119,3 +119,29 @@ def test_lscm_closed_chart_raises(cuda):
     b = gpu.Batch([(P, T, None)])
     with pytest.raises(ValueError):
         b.lscm()
+
+
+def test_step_graph_replays_the_direct_calls(cuda):
+    """setup + LSCM + 5 ARAP iterations captured once (uva_step_graph_create)
+    and replayed twice give the UVs of the same calls made directly: the
+    island solver is deterministic (fixed reduction orders, slice-ordered
+    coarse restriction), so the comparison is exact."""
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.engine import gpu
+    isl = synth.uneven_islands(seed=77, count=40, tmin=20, tmax=12000)
+    b = gpu.Batch([(p, t, None) for p, t in isl])
+    db = b.db
+    db.setup(); db.lscm(); db.arap(iters=5)
+    torch.cuda.synchronize()
+    direct = db.U.clone()
+    st_direct = db.island_status()
+    g = db.step_graph(setup=True, lscm=True, arap_iters=5)
+    for _ in range(2):
+        db.U.zero_()
+        g.launch()
+        torch.cuda.synchronize()
+        assert torch.equal(db.U, direct)
+    st = db.island_status()
+    assert np.array_equal(st["cg_iters"], st_direct["cg_iters"])
+    assert (st["resid"] <= 1e-6 + 1e-12).all()
+    g.close()

@@ -27,6 +27,7 @@ ST_ENERGYSTOP = 4
 ST_NOBOUNDARY = 8
 
 PLAN_NSIZES = 9
+STEP_SETUP, STEP_LSCM, STEP_ARAP = 1, 2, 4
 CLASS_BIG, CLASS_MID, CLASS_SMALL = 8192, 2048, 256
 (PLAN_NC, PLAN_N, PLAN_T, PLAN_E, PLAN_NSLICES, PLAN_NSLOTS, PLAN_NBVERTS, PLAN_MAXROWS, PLAN_NCOARSE) = range(9)
 
@@ -36,7 +37,8 @@ i32 = C.c_int32
 
 class IslandStatus(C.Structure):
     _fields_ = [("cg_iters", i32), ("refinements", i32), ("outer_iters", i32), ("flags", i32),
-                ("resid", C.c_double * 2), ("energy", C.c_double), ("step", C.c_double)]
+                ("resid", C.c_double * 2), ("energy", C.c_double), ("step", C.c_double),
+                ("t_begin", C.c_int64), ("t_end", C.c_int64), ("sm", i32), ("team", i32)]
 
 
 class BatchDesc(C.Structure):
@@ -71,6 +73,9 @@ _SIGS = {
     "uva_lscm": [vp, vp, vp],
     "uva_arap": [vp, vp, vp],
     "uva_arap_noalloc": [vp, vp, vp],
+    "uva_step_graph_create": [vp, i32, vp, vp, vp],
+    "uva_graph_launch": [vp, vp],
+    "uva_graph_destroy": [vp],
     "uva_orient_positive": [vp, vp],
     "uva_repair_flips": [vp, i32, vp],
     "uva_repair_flips_serial": [vp, i32, vp],

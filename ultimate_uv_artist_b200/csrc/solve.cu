@@ -945,6 +945,18 @@ __device__ void solve_lscm(const uva_batch& b, const uva_solve_params& prm, Team
     tm.sync();
 }
 
+__device__ __forceinline__ long long global_ns() {
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned sm_id() {
+    unsigned r;
+    asm("mov.u32 %0, %%smid;" : "=r"(r));
+    return r;
+}
+
 template <int NTT, int R, Op OP>
 __device__ void run_class(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, int cls) {
     const int lo = b.class_ofs[cls], hi = b.class_ofs[cls + 1];
@@ -963,8 +975,16 @@ __device__ void run_class(const uva_batch& b, const uva_solve_params& prm, Team<
         }
         if (lo + qi >= hi) break;
         const Isl I = load_island(b, b.order[lo + qi]);
+        const long long t0 = global_ns();
         if (OP == OP_ARAP) solve_arap<NTT, R>(b, prm, tm, I);
         else solve_lscm<NTT, R>(b, prm, tm, I);
+        if (tm.tid == 0) {   // the same thread wrote the rest of the status
+            uva_island_status& st = b.status[I.id];
+            st.t_begin = t0;
+            st.t_end = global_ns();
+            st.sm = static_cast<int32_t>(sm_id());
+            st.team = NTT;
+        }
     }
 }
 
@@ -1116,10 +1136,35 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
 }
 
 int sm_count() {
-    int dev = 0, n = 0;
+    static std::mutex mu;
+    static std::vector<int> cache;
+    int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    return n > 0 ? n : 148;
+    std::lock_guard<std::mutex> lk(mu);
+    if (static_cast<int>(cache.size()) <= dev) cache.resize(dev + 1, 0);
+    if (cache[dev] == 0) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cache[dev] = n > 0 ? n : 148;
+    }
+    return cache[dev];
+}
+
+// The island kernel's shared-memory opt-in, once per device and operator (so
+// that a launch inside a stream capture issues no attribute call).
+template <Op OP>
+cudaError_t ensure_islands_attr() {
+    static std::mutex mu;
+    static std::vector<char> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (static_cast<int>(done.size()) <= dev) done.resize(dev + 1, 0);
+    if (done[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_islands<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kDynSmem));
+    if (e == cudaSuccess) done[dev] = 1;
+    return e;
 }
 
 bool check_batch(const uva_batch* b) {
@@ -1141,8 +1186,7 @@ int launch_islands(const uva_batch* b, const uva_solve_params* prm, cudaStream_t
         uva_set_error("uva_arap/uva_lscm: class_ofs must be 0 <= ... <= nc, non-decreasing");
         return UVA_E_ARG;
     }
-    cudaError_t e = cudaFuncSetAttribute(k_islands<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(kDynSmem));
+    cudaError_t e = ensure_islands_attr<OP>();
     if (e != cudaSuccess) return uva_cuda_status(e, "uva_islands/cudaFuncSetAttribute");
     e = cudaMemsetAsync(b->work, 0, sizeof(int32_t) * 4, s);
     if (e != cudaSuccess) return uva_cuda_status(e, "uva_islands/memset");
@@ -1193,6 +1237,73 @@ extern "C" int uva_lscm(uva_batch* b, const uva_solve_params* prm, void* stream)
     if (!check_batch(b) || !prm) { uva_set_error("uva_lscm: bad arguments"); return UVA_E_ARG; }
     if (b->nc == 0) return UVA_OK;
     return launch_islands<OP_LSCM>(b, prm, static_cast<cudaStream_t>(stream));
+}
+
+// ------------------------------------------------------------------ step graphs
+// One batch step (setup, LSCM, ARAP: any subset) captured once into a CUDA
+// graph and replayed with one launch. The capture runs on a private stream in
+// thread-local mode; the kernels take the uva_batch by value, so the graph
+// holds the pointers and parameters given at creation.
+struct uva_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" int uva_step_graph_create(uva_batch* b, int32_t parts, const uva_solve_params* lscm,
+                                     const uva_solve_params* arap, uva_graph** out) {
+    if (!out || !check_batch(b) || (parts & ~7) || !parts || ((parts & UVA_STEP_LSCM) && !lscm) ||
+        ((parts & UVA_STEP_ARAP) && !arap)) {
+        uva_set_error("uva_step_graph_create: bad arguments");
+        return UVA_E_ARG;
+    }
+    *out = nullptr;
+    cudaError_t e = ensure_islands_attr<OP_ARAP>();
+    if (e == cudaSuccess) e = ensure_islands_attr<OP_LSCM>();
+    if (e != cudaSuccess) return uva_cuda_status(e, "uva_step_graph_create/attributes");
+    sm_count();
+    cudaStream_t cs = nullptr;
+    e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return uva_cuda_status(e, "uva_step_graph_create/stream");
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        return uva_cuda_status(e, "uva_step_graph_create/begin");
+    }
+    int rc = UVA_OK;
+    if ((parts & UVA_STEP_SETUP) && rc == UVA_OK) rc = uva_batch_setup(b, cs);
+    if ((parts & UVA_STEP_LSCM) && rc == UVA_OK) rc = uva_lscm(b, lscm, cs);
+    if ((parts & UVA_STEP_ARAP) && rc == UVA_OK) rc = uva_arap(b, arap, cs);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (rc != UVA_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return uva_cuda_status(e, "uva_step_graph_create/end");
+    cudaGraphExec_t x = nullptr;
+    e = cudaGraphInstantiate(&x, g, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return uva_cuda_status(e, "uva_step_graph_create/instantiate");
+    }
+    *out = new uva_graph{g, x};
+    return UVA_OK;
+}
+
+extern "C" int uva_graph_launch(uva_graph* g, void* stream) {
+    if (!g || !g->exec) { uva_set_error("uva_graph_launch: null graph"); return UVA_E_ARG; }
+    const cudaError_t e = cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return uva_cuda_status(e, "uva_graph_launch");
+    return UVA_OK;
+}
+
+extern "C" int uva_graph_destroy(uva_graph* g) {
+    if (!g) return UVA_OK;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return UVA_OK;
 }
 
 // ------------------------------------------------------------------ no-allocation ARAP

@@ -8,9 +8,9 @@ Same public surface as the reference module (engine/gpu.py:16-299):
 
 What changes underneath: every Batch computation runs in the uva_b200 CUDA
 kernels (sm_100a) on a device-resident batch. A global step is solved per
-island to ||b - L x|| <= 1e-6 ||b|| per column, checked in FP64 (FP32 CG with
-FP64 residual refinement), instead of 40 CG iterations with a global stop
-test and a host sync per iteration. UVs are kept in FP64 on the device;
+island to ||b - L x|| <= 2e-7 ||b|| per column, checked in FP64 (FP32 CG with
+FP64 residual refinement), instead of at most 40 CG iterations with a 1e-6
+stop test on the whole batch and a host sync per iteration. UVs are kept in FP64 on the device;
 ``U`` returns them in the Batch dtype. There is no CPU path: constructing a
 Batch without a CUDA device raises RuntimeError.
 """
@@ -223,7 +223,7 @@ class Batch:
         """ARAP local/global iterations (engine/gpu.py:230-249).
 
         ``cg_iters`` is accepted for signature compatibility; convergence is
-        decided per island by the FP64 residual test (``tol``, default 1e-6).
+        decided per island by the FP64 residual test (``tol``, default 2e-7).
         """
         self.db.arap(iters=iters, line_search=line_search, tol=tol)
         return self.U
