@@ -240,6 +240,19 @@ extern "C" int uva_plan_create(const int64_t* tris, const int64_t* vofs, const i
     worker();
     for (auto& th : pool) th.join();
     if (anybad) { delete p; uva_set_error("uva_plan_create: triangle index outside its island"); return UVA_E_ARG; }
+    for (int32_t i = 0; i < nc; ++i) {
+        // the solver packs an island row in 24 bits and twice the LSCM
+        // boundary coupling in 8 (signed)
+        const IslandPlan& ip = p->isl[i];
+        if (ip.n >= (1 << 24)) { delete p; uva_set_error("uva_plan_create: island above 16M vertices"); return UVA_E_TOOBIG; }
+        for (int32_t e = 0; e < ip.nedges; ++e) {
+            const int32_t info = ip.edge_info[e];
+            if (((info >> 10) & 1023) > 127 || ((info >> 20) & 1023) > 127) {
+                delete p; uva_set_error("uva_plan_create: an edge is used by more than 127 triangles in one direction");
+                return UVA_E_ARG;
+            }
+        }
+    }
     p->eofs.assign(nc + 1, 0); p->sofs.assign(nc + 1, 0); p->slotofs.assign(nc + 1, 0); p->bofs.assign(nc + 1, 0);
     p->cofs.assign(nc + 1, 0);
     for (int32_t i = 0; i < nc; ++i) {

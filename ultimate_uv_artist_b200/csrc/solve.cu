@@ -124,7 +124,8 @@ __global__ void k_rows(uva_batch b, const int32_t* vert_isl) {
         const int q = q0 + 32 * k;
         const int e = b.slot_edge[q];
         const float w32 = e >= 0 ? static_cast<float>(b.wedge[e]) : 0.0f;
-        reinterpret_cast<int2*>(b.slot_cw)[q] = make_int2(b.slot_col[q], __float_as_int(w32));
+        const int c2 = __float2int_rn(2.0f * b.slot_c[q]);   // |c2| <= 127 (checked by the plan)
+        reinterpret_cast<int2*>(b.slot_cw)[q] = make_int2((c2 << 24) | b.slot_col[q], __float_as_int(w32));
         sum += static_cast<double>(w32);
     }
     b.wdiag[v] = sum;
@@ -212,6 +213,8 @@ struct Team {
     int* slot;
     float2 *sp, *sr, *sd;   // CG vectors (shared memory, or null for class G)
     float *cg, *cy;         // coarse restriction / coarse solution (shared memory)
+    int* sc;                // slice-pointer cache of the current island (shared memory)
+    int sc_cap;             // its capacity (slices + 1)
     __device__ __forceinline__ void sync() { team_sync<NTT>(bar); }
 };
 
@@ -234,11 +237,12 @@ __device__ __forceinline__ void team_sum(Team<NTT>& tm, T (&v)[K], T* red) {
             for (int k = 0; k < K; ++k) buf[k * NW + warp] = v[k];
         }
         tm.sync();
+        // every warp folds the per-warp partials with the same butterfly
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            T s = T(0);
+            T s = lane < NW ? buf[k * NW + lane] : T(0);
 #pragma unroll
-            for (int w = 0; w < NW; ++w) s += buf[k * NW + w];
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             v[k] = s;
         }
     } else {
@@ -256,9 +260,9 @@ __device__ __forceinline__ double team_min(Team<NTT>& tm, double v) {
         tm.phase ^= 1;
         if ((tm.tid & 31) == 0) buf[tm.tid >> 5] = v;
         tm.sync();
-        v = buf[0];
+        v = (tm.tid & 31) < NW ? buf[tm.tid & 31] : 1e300;
 #pragma unroll
-        for (int w = 1; w < NW; ++w) v = fmin(v, buf[w]);
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
     } else {
         __syncwarp();
     }
@@ -274,9 +278,7 @@ __device__ __forceinline__ int team_or(Team<NTT>& tm, int v) {
         tm.phase ^= 1;
         if ((tm.tid & 31) == 0) buf[tm.tid >> 5] = v;
         tm.sync();
-        v = 0;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) v |= buf[w];
+        v = __any_sync(0xffffffffu, (tm.tid & 31) < NW && buf[tm.tid & 31] != 0) ? 1 : 0;
     } else {
         __syncwarp();
     }
@@ -319,6 +321,8 @@ struct Isl {
     int pin, p0, p1;          // solver rows of the ARAP pin and the LSCM pins (-1: none)
     int pinv;                 // ARAP pin vertex
     int agg, M, co;           // rows per aggregate, aggregates (0: Jacobi only), coarse offset
+    int aggsh;                // log2(agg) when agg is a power of two, else -1
+    const int* sptr;          // slot offsets of the island's slices (shared-memory cache or global)
     double wpin;
 };
 
@@ -336,15 +340,24 @@ __device__ __forceinline__ Isl load_island(const uva_batch& b, int isl) {
     I.agg = b.agg_rows[isl];
     I.M = I.agg > 0 ? (I.n + I.agg - 1) / I.agg : 0;
     I.co = b.cofs[isl];
+    I.aggsh = (I.agg > 0 && (I.agg & (I.agg - 1)) == 0) ? __ffs(I.agg) - 1 : -1;
+    I.sptr = b.slice_ptr + I.s0;
     I.wpin = b.wpin[isl];
     return I;
 }
 
-__device__ __forceinline__ void row_slots(const uva_batch& b, const Isl& I, int i, int& q0, int& width) {
-    const int s = I.s0 + (i >> 5);
-    const int p = __ldg(b.slice_ptr + s);
+__device__ __forceinline__ int agg_of(const Isl& I, int i) { return I.aggsh >= 0 ? (i >> I.aggsh) : i / I.agg; }
+
+// Packed slot column: island row in the low 24 bits, twice the LSCM
+// boundary coupling (a small integer) in the high 8 bits.
+__device__ __forceinline__ int slot_row(int x) { return x & 0xFFFFFF; }
+__device__ __forceinline__ float slot_c2(int x) { return static_cast<float>(x >> 24); }
+
+__device__ __forceinline__ void row_slots(const uva_batch&, const Isl& I, int i, int& q0, int& width) {
+    const int s = i >> 5;
+    const int p = I.sptr[s];
     q0 = p + (i & 31);
-    width = (__ldg(b.slice_ptr + s + 1) - p) >> 5;
+    width = (I.sptr[s + 1] - p) >> 5;
 }
 
 template <Op OP>
@@ -364,11 +377,11 @@ __device__ __forceinline__ double2 apply64(const uva_batch& b, const Isl& I, int
         const int q = q0 + 32 * k;
         const int2 s = __ldg(cw + q);
         const double w = static_cast<double>(__int_as_float(s.y));
-        const double2 xj = x[s.x];
+        const double2 xj = x[slot_row(s.x)];
         ax += w * (xi.x - xj.x);
         ay += w * (xi.y - xj.y);
         if (OP == OP_LSCM) {
-            const double c = static_cast<double>(__ldg(b.slot_c + q));
+            const double c = 0.5 * static_cast<double>(slot_c2(s.x));
             ax += c * xj.y;
             ay -= c * xj.x;
         }
@@ -389,20 +402,16 @@ __device__ __forceinline__ float2 apply32(const uva_batch& b, const Isl& I, int 
         int2 s[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) s[u] = __ldg(cw + q0 + 32 * (k + u));
-        float c[4];
-        if (OP == OP_LSCM) {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) c[u] = __ldg(b.slot_c + q0 + 32 * (k + u));
-        }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const float2 xj = p[s[u].x];
+            const float2 xj = p[slot_row(s[u].x)];
             const float w = __int_as_float(s[u].y);
             ax = fmaf(w, xi.x - xj.x, ax);
             ay = fmaf(w, xi.y - xj.y, ay);
             if (OP == OP_LSCM) {
-                ax = fmaf(c[u], xj.y, ax);
-                ay = fmaf(-c[u], xj.x, ay);
+                const float c = 0.5f * slot_c2(s[u].x);
+                ax = fmaf(c, xj.y, ax);
+                ay = fmaf(-c, xj.x, ay);
             }
         }
     }
@@ -491,7 +500,7 @@ __device__ __forceinline__ void coarse_solve(const uva_batch& b, Team<NTT>& tm, 
 
 template <int NTT, Op OP>
 __device__ __forceinline__ float2 prolong(const Team<NTT>& tm, const Isl& I, int i) {
-    const int a = i / I.agg;
+    const int a = agg_of(I, i);
     if (OP == OP_ARAP) return make_float2(tm.cy[a], tm.cy[I.M + a]);
     return make_float2(tm.cy[2 * a], tm.cy[2 * a + 1]);
 }
@@ -918,9 +927,9 @@ __device__ void solve_lscm(const uva_batch& b, const uva_solve_params& prm, Team
         for (int k = 0; k < width; ++k) {
             const int q = q0 + 32 * k;
             const int2 sl = __ldg(cw + q);
-            if (sl.x != I.p1) continue;   // p0 sits at the origin
+            if (slot_row(sl.x) != I.p1) continue;   // p0 sits at the origin
             const double w = static_cast<double>(__int_as_float(sl.y));
-            const double c = static_cast<double>(__ldg(b.slot_c + q));
+            const double c = 0.5 * static_cast<double>(slot_c2(sl.x));
             rx -= w * dpin;
             ry -= c * dpin;
         }
@@ -974,8 +983,14 @@ __device__ void run_class(const uva_batch& b, const uva_solve_params& prm, Team<
             tm.sync();
         }
         if (lo + qi >= hi) break;
-        const Isl I = load_island(b, b.order[lo + qi]);
+        Isl I = load_island(b, b.order[lo + qi]);
         const long long t0 = global_ns();
+        const int nsl1 = ((I.n + 31) >> 5) + 1;
+        if (tm.sc && nsl1 <= tm.sc_cap) {   // the previous island ended with a team barrier
+            for (int k = tm.tid; k < nsl1; k += NTT) tm.sc[k] = __ldg(b.slice_ptr + I.s0 + k);
+            tm.sync();
+            I.sptr = tm.sc;
+        }
         if (OP == OP_ARAP) solve_arap<NTT, R>(b, prm, tm, I);
         else solve_lscm<NTT, R>(b, prm, tm, I);
         if (tm.tid == 0) {   // the same thread wrote the rest of the status
@@ -988,36 +1003,56 @@ __device__ void run_class(const uva_batch& b, const uva_solve_params& prm, Team<
     }
 }
 
+// The first `nrev` CTAs take the classes in reverse order (warps first):
+// the many small islands are latency bound and long-lived for their size,
+// so starting some of them at once keeps them out of the launch's tail,
+// while the other CTAs start with the largest islands.
 template <Op OP>
-__global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params prm) {
+__global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params prm, int nrev) {
     extern __shared__ float2 dyn[];
     __shared__ double redd[2 * 4 * 32];
     __shared__ float redf[2 * 4 * 32];
     __shared__ int redi[2 * 32];
     __shared__ int slots[8];
     __shared__ float coarse_buf[1024];   // g and y of the coarse level (CTA: 512 each; sub-team: 128 each)
-    {
+    __shared__ int sc_buf[288];          // slice pointers (CTA: 288; sub-team: 72 each; warp: 9 each)
+    const bool rev = static_cast<int>(blockIdx.x) < nrev;
+    auto whole_cta = [&]() {
         Team<KB> tm{static_cast<int>(threadIdx.x), 0, 0, redd, redf, redi, &slots[0], nullptr, nullptr, nullptr,
-                    coarse_buf, coarse_buf + 512};
+                    coarse_buf, coarse_buf + 512, sc_buf, 288};
         run_class<KB, 0, OP>(b, prm, tm, 0);
         tm.sp = dyn; tm.sr = dyn + KB * RB; tm.sd = dyn + 2 * KB * RB;
         run_class<KB, RB, OP>(b, prm, tm, 1);
-    }
-    __syncthreads();
-    const int s = threadIdx.x / SUB;
-    {
+    };
+    // a sub-team reuses only its own quarter of the buffers, a warp only its
+    // own 1/32 (inside its sub-team's quarter)
+    auto sub_teams = [&]() {
+        const int s = threadIdx.x / SUB;
         float2* base = dyn + s * (3 * SUB * RB);
         Team<SUB> tm{static_cast<int>(threadIdx.x % SUB), 1 + s, 0, redd + s * 64, redf + s * 64, redi + s * 16,
                      &slots[1 + s], base, base + SUB * RB, base + 2 * SUB * RB, coarse_buf + 256 * s,
-                     coarse_buf + 256 * s + 128};
+                     coarse_buf + 256 * s + 128, sc_buf + 72 * s, 72};
         run_class<SUB, RB, OP>(b, prm, tm, 2);
-    }
-    {
+    };
+    auto warps = [&]() {
         const int w = threadIdx.x / 32;
         float2* base = dyn + w * (3 * 32 * RB);
         Team<32> tm{static_cast<int>(threadIdx.x % 32), 0, 0, nullptr, nullptr, nullptr, nullptr,
-                    base, base + 32 * RB, base + 2 * 32 * RB, nullptr, nullptr};
+                    base, base + 32 * RB, base + 2 * 32 * RB, nullptr, nullptr, sc_buf + 9 * w, 9};
         run_class<32, RB, OP>(b, prm, tm, 3);
+    };
+    // one copy of each phase in the code; the order is decided at run time
+    for (int step = 0; step < 3; ++step) {
+        const int ph = rev ? 2 - step : step;
+        if (ph == 0) {
+            if (step > 0) __syncthreads();   // every sub-team and warp is done
+            whole_cta();
+            if (step < 2) __syncthreads();
+        } else if (ph == 1) {
+            sub_teams();   // its first barrier waits for the team's 8 warps
+        } else {
+            warps();
+        }
     }
 }
 
@@ -1077,7 +1112,7 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
             const int2 sl = cw[q0 + 32 * k];
             const double w = static_cast<double>(__int_as_float(sl.y));
             if (w == 0.0) continue;
-            const int c = sl.x / agg;
+            const int c = slot_row(sl.x) / agg;
             dsum += w;
             if (c != a) atomicAdd(W + static_cast<size_t>(a) * M + c, -w);
             else dsum -= w;
@@ -1113,8 +1148,8 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
             const double cc = static_cast<double>(b.slot_c[q]);
             if (w == 0.0 && cc == 0.0) continue;
             dsum += w;
-            if (sl.x == p0 || sl.x == p1) continue;   // pinned neighbour: no coarse coupling
-            const int c = sl.x / agg;
+            if (slot_row(sl.x) == p0 || slot_row(sl.x) == p1) continue;   // pinned neighbour: no coarse coupling
+            const int c = slot_row(sl.x) / agg;
             if (c == a) {
                 dsum -= w;
             } else {
@@ -1194,7 +1229,10 @@ int launch_islands(const uva_batch* b, const uva_solve_params* prm, cudaStream_t
     const int small = b->class_ofs[4] - b->class_ofs[2];    // islands for sub-teams / warps
     const int want = big + (small + 3) / 4;
     const int grid = std::max(1, std::min(sm_count(), want));
-    k_islands<OP><<<grid, KB, kDynSmem, s>>>(*b, *prm);
+    // reverse-order CTAs: one per 128 warp-class islands, at most a quarter
+    const int nwarp = b->class_ofs[4] - b->class_ofs[3];
+    const int nrev = big > 0 ? std::min(grid / 4, (nwarp + 127) / 128) : 0;
+    k_islands<OP><<<grid, KB, kDynSmem, s>>>(*b, *prm, nrev);
     UVA_CHECK_LAUNCH(OP == OP_ARAP ? "uva_arap" : "uva_lscm");
     return UVA_OK;
 }
