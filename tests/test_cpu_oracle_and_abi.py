@@ -118,7 +118,7 @@ def test_plan_matches_numpy_topology():
         assert np.array_equal(np.sort(rv), np.arange(n)) and np.array_equal(rv[vr], np.arange(n))
         if n > 256:   # aggregates of agg_rows consecutive rows, at most 256 of them
             m = -(-n // pl.agg_rows[i])
-            assert pl.agg_rows[i] % 128 == 0 and m <= 256 and pl.cofs[i + 1] - pl.cofs[i] == m * m
+            assert pl.agg_rows[i] % 64 == 0 and m <= 256 and pl.cofs[i + 1] - pl.cofs[i] == m * m
         else:
             assert pl.agg_rows[i] == 0 and pl.cofs[i + 1] == pl.cofs[i] and np.array_equal(rv, np.arange(n))
         for v in range(n):

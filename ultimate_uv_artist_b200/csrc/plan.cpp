@@ -156,8 +156,8 @@ void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& 
     for (int32_t v = 0; v < n; ++v) if (isb[v]) ip.bverts.push_back(v);
     // solver row order and coarse aggregates (islands above one warp's rows)
     if (n > 256) {
-        ip.agg_rows = 128;
-        while ((n + ip.agg_rows - 1) / ip.agg_rows > 256) ip.agg_rows += 128;
+        ip.agg_rows = 64;
+        while ((n + ip.agg_rows - 1) / ip.agg_rows > 256) ip.agg_rows += 64;
         ip.ncoarse = (n + ip.agg_rows - 1) / ip.agg_rows;
         blob_order(ip, n, ip.agg_rows, ip.row_vert);
     } else {

@@ -19,6 +19,7 @@
 //  * Convergence is per island and per column, so small islands stop early
 //    and never wait for the largest one (the reference's test is global over
 //    the batch, engine/gpu.py:196).
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -215,6 +216,10 @@ struct Team {
     float *cg, *cy;         // coarse restriction / coarse solution (shared memory)
     int* sc;                // slice-pointer cache of the current island (shared memory)
     int sc_cap;             // its capacity (slices + 1)
+    float2* pc;             // per-slice residual sums (shared memory, or null)
+    int pc_cap;             // its capacity (slices)
+    __nv_bfloat16* dc;      // Jacobi diagonal of the current island (shared memory, or null)
+    int dc_cap;             // its capacity (rows)
     __device__ __forceinline__ void sync() { team_sync<NTT>(bar); }
 };
 
@@ -323,9 +328,12 @@ struct Isl {
     int agg, M, co;           // rows per aggregate, aggregates (0: Jacobi only), coarse offset
     int aggsh;                // log2(agg) when agg is a power of two, else -1
     const int* sptr;          // slot offsets of the island's slices (shared-memory cache or global)
+    float2* part;             // per-slice residual sums (shared memory or b.cpart)
+    const __nv_bfloat16* dv;  // Jacobi diagonal in shared memory (null: read b.dinv)
     double wpin;
 };
 
+template <Op OP>
 __device__ __forceinline__ Isl load_island(const uva_batch& b, int isl) {
     Isl I;
     I.id = isl;
@@ -342,6 +350,8 @@ __device__ __forceinline__ Isl load_island(const uva_batch& b, int isl) {
     I.co = b.cofs[isl];
     I.aggsh = (I.agg > 0 && (I.agg & (I.agg - 1)) == 0) ? __ffs(I.agg) - 1 : -1;
     I.sptr = b.slice_ptr + I.s0;
+    I.part = reinterpret_cast<float2*>(b.cpart) + I.s0;
+    I.dv = nullptr;
     I.wpin = b.wpin[isl];
     return I;
 }
@@ -373,6 +383,7 @@ __device__ __forceinline__ double2 apply64(const uva_batch& b, const Isl& I, int
     const int2* cw = reinterpret_cast<const int2*>(b.slot_cw);
     const double2 xi = x[i];
     double ax = 0.0, ay = 0.0;
+#pragma unroll 4
     for (int k = 0; k < width; ++k) {
         const int q = q0 + 32 * k;
         const int2 s = __ldg(cw + q);
@@ -419,8 +430,59 @@ __device__ __forceinline__ float2 apply32(const uva_batch& b, const Isl& I, int 
     return make_float2(ax, ay);
 }
 
+// Inverse Jacobi diagonal of row i: 0 on the LSCM hard pins, the ARAP pin
+// row includes the soft-pin weight.
+// (A p) for two rows of one thread at once (rows of different slices):
+// the slot loads of both rows are in flight together, which halves the
+// chain of dependent L2 round trips of the single-row product.
 template <Op OP>
-__device__ __forceinline__ float jacobi(const uva_batch& b, const Isl& I, int i) {
+__device__ __forceinline__ void apply32_pair(const uva_batch& b, const Isl& I, int ia, int ib, bool vb,
+                                             const float2* p, float wpin32, float2& qa, float2& qb) {
+    int q0a, wa, q0b = 0, wb = 0;
+    row_slots(b, I, ia, q0a, wa);
+    if (vb) row_slots(b, I, ib, q0b, wb);
+    const int2* cw = reinterpret_cast<const int2*>(b.slot_cw);
+    const float2 xa = p[ia], xb = vb ? p[ib] : make_float2(0.f, 0.f);
+    float ax = 0.f, ay = 0.f, bx = 0.f, by = 0.f;
+    const int wmax = max(wa, wb);
+    for (int k = 0; k < wmax; k += 4) {
+        int2 sa[4], sb[4];
+        const bool ha = k < wa, hb = k < wb;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            sa[u] = ha ? __ldg(cw + q0a + 32 * (k + u)) : make_int2(ia, 0);
+            sb[u] = hb ? __ldg(cw + q0b + 32 * (k + u)) : make_int2(ib, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float2 ya = p[slot_row(sa[u].x)];
+            const float wA = __int_as_float(sa[u].y);
+            ax = fmaf(wA, xa.x - ya.x, ax);
+            ay = fmaf(wA, xa.y - ya.y, ay);
+            if (OP == OP_LSCM) {
+                const float c = 0.5f * slot_c2(sa[u].x);
+                ax = fmaf(c, ya.y, ax);
+                ay = fmaf(-c, ya.x, ay);
+            }
+            const float2 yb = p[slot_row(sb[u].x)];
+            const float wB = __int_as_float(sb[u].y);
+            bx = fmaf(wB, xb.x - yb.x, bx);
+            by = fmaf(wB, xb.y - yb.y, by);
+            if (OP == OP_LSCM) {
+                const float c = 0.5f * slot_c2(sb[u].x);
+                bx = fmaf(c, yb.y, bx);
+                by = fmaf(-c, yb.x, by);
+            }
+        }
+    }
+    if (OP == OP_ARAP && ia == I.pin) { ax = fmaf(wpin32, xa.x, ax); ay = fmaf(wpin32, xa.y, ay); }
+    if (OP == OP_ARAP && ib == I.pin) { bx = fmaf(wpin32, xb.x, bx); by = fmaf(wpin32, xb.y, by); }
+    qa = is_pinned<OP>(I, ia) ? make_float2(0.f, 0.f) : make_float2(ax, ay);
+    qb = (vb && !is_pinned<OP>(I, ib)) ? make_float2(bx, by) : make_float2(0.f, 0.f);
+}
+
+template <Op OP>
+__device__ __forceinline__ float jacobi_global(const uva_batch& b, const Isl& I, int i) {
     if (is_pinned<OP>(I, i)) return 0.0f;
     if (OP == OP_ARAP && i == I.pin) {
         const double diag = b.wdiag[I.v0 + i] + I.wpin;
@@ -429,12 +491,21 @@ __device__ __forceinline__ float jacobi(const uva_batch& b, const Isl& I, int i)
     return __ldg(b.dinv + I.v0 + i);
 }
 
+// The preconditioner reads a bfloat16 copy from shared memory when the team
+// has room for it (a preconditioner may be approximate; CG stays exact).
+template <Op OP>
+__device__ __forceinline__ float jacobi(const uva_batch& b, const Isl& I, int i) {
+    if (I.dv) return __bfloat162float(I.dv[i]);
+    return jacobi_global<OP>(b, I, i);
+}
+
 // Two-level additive preconditioner z = D^-1 r + P Ac^-1 P^T r. P is the
 // piecewise-constant prolongation over aggregates of `agg` consecutive solver
 // rows (compact mesh blobs from the plan; agg is a multiple of 128, so an
 // aggregate is agg/32 whole slices), Ac = P^T A P is inverted once per batch
 // by the setup. Restriction is deterministic: each warp writes the sum of its
-// slice (one warp owns one slice in slice_loop) to b.cpart, and coarse_solve
+// slice (one warp owns one slice in slice_loop) to the slice sums (shared
+// memory when the team has room, else b.cpart), and coarse_solve
 // adds the slices of each aggregate in slice order before the dense product
 // with Ac^-1 (one warp per output row).
 template <int NTT, Op OP>
@@ -447,7 +518,7 @@ __device__ __forceinline__ void coarse_restrict(const uva_batch& b, Team<NTT>& t
         ry += __shfl_xor_sync(0xffffffffu, ry, o);
     }
     if ((tm.tid & 31) == 0 && (i - (tm.tid & 31)) < I.n)
-        reinterpret_cast<float2*>(b.cpart)[I.s0 + (i >> 5)] = make_float2(rx, ry);
+        I.part[i >> 5] = make_float2(rx, ry);
 }
 
 // y = Ac^-1 g, g gathered from the slice sums of the last restriction (which a
@@ -456,7 +527,7 @@ template <int NTT, Op OP>
 __device__ __forceinline__ void coarse_solve(const uva_batch& b, Team<NTT>& tm, const Isl& I) {
     constexpr int NW = NTT / 32;
     const int lane = tm.tid & 31, warp = tm.tid >> 5;
-    const float2* part = reinterpret_cast<const float2*>(b.cpart) + I.s0;
+    const float2* part = I.part;
     const int spa = I.agg >> 5, nsl = (I.n + 31) >> 5;
     for (int a = tm.tid; a < I.M; a += NTT) {
         float gx = 0.f, gy = 0.f;
@@ -596,13 +667,35 @@ __device__ int refine_solve(const uva_batch& b, const Isl& I, const uva_solve_pa
         while ((act[0] || act[1]) && it < prm.max_inner) {
             tm.sync();   // p complete
             float pq[2] = {0.f, 0.f};
-            for_rows<NTT, R>(tid, n, [&](int i, int j) {
-                float2 q = make_float2(0.f, 0.f);
-                if (!is_pinned<OP>(I, i)) q = apply32<OP>(b, I, i, sp, wpin32);
-                if constexpr (R > 0) qreg[j] = q; else sq[i] = q;
-                const float2 p = sp[i];
-                pq[0] += p.x * q.x; pq[1] += p.y * q.y;
-            });
+            if constexpr (R > 0) {
+#pragma unroll
+                for (int j = 0; j < R; j += 2) {
+                    const int ia = tid + j * NTT, ib = ia + NTT;
+                    if (ia < n) {
+                        const bool vb = j + 1 < R && ib < n;
+                        float2 qa, qb;
+                        apply32_pair<OP>(b, I, ia, ib, vb, sp, wpin32, qa, qb);
+                        qreg[j] = qa;
+                        const float2 pa = sp[ia];
+                        pq[0] += pa.x * qa.x; pq[1] += pa.y * qa.y;
+                        if (j + 1 < R) {
+                            qreg[j + 1] = qb;
+                            if (vb) {
+                                const float2 pb = sp[ib];
+                                pq[0] += pb.x * qb.x; pq[1] += pb.y * qb.y;
+                            }
+                        }
+                    }
+                }
+            } else {
+                for_rows<NTT, R>(tid, n, [&](int i, int) {
+                    float2 q = make_float2(0.f, 0.f);
+                    if (!is_pinned<OP>(I, i)) q = apply32<OP>(b, I, i, sp, wpin32);
+                    sq[i] = q;
+                    const float2 p = sp[i];
+                    pq[0] += p.x * q.x; pq[1] += p.y * q.y;
+                });
+            }
             team_sum<NTT, 2>(tm, pq, tm.redf);
             float alpha[2];
             if (NCOL == 2) {
@@ -791,7 +884,10 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
     double2* x64 = reinterpret_cast<double2*>(b.x64);
     double2* b64 = reinterpret_cast<double2*>(b.b64);
     const double2* rc = reinterpret_cast<const double2*>(b.rc);
-    uva_island_status st{};
+    // the status accumulates in global memory (thread 0 only): nothing of it
+    // stays live in registers across the CG loops
+    uva_island_status* gst = b.status + I.id;
+    if (tid == 0) *gst = uva_island_status{};
     bool use_ls = prm.line_search != 0;
     double prev_e = 0.0;
     for (int it = 0; it < prm.iters; ++it) {
@@ -807,13 +903,12 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
                 use_ls = prm.line_search != 0 && ev[1] == 0.0;
                 prev_e = ev[0];
             } else if (prm.energy_tol > 0.0 && fabs(prev_e - ev[0]) <= prm.energy_tol * fmax(prev_e, 1e-300)) {
-                st.flags |= UVA_ST_ENERGYSTOP;
-                st.energy = ev[0];
+                if (tid == 0) { gst->flags |= UVA_ST_ENERGYSTOP; gst->energy = ev[0]; }
                 break;
             } else {
                 prev_e = ev[0];
             }
-            st.energy = ev[0];
+            if (tid == 0) gst->energy = ev[0];
         }
         tm.sync();   // corner terms complete
         double bb[2] = {0.0, 0.0};
@@ -834,15 +929,20 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
         team_sum<NTT, 2>(tm, bb, tm.redd);   // also publishes x64 / b64 to the team
         int nref = 0;
         bool capped = false;
-        st.cg_iters += refine_solve<NTT, R, OP_ARAP, 2>(b, I, prm, tm, bb, st.resid, nref, capped);
-        st.refinements += nref;
-        if (capped) st.flags |= UVA_ST_MAXITER;
+        double res[2];
+        const int cgi = refine_solve<NTT, R, OP_ARAP, 2>(b, I, prm, tm, bb, res, nref, capped);
+        if (tid == 0) {
+            gst->cg_iters += cgi;
+            gst->refinements += nref;
+            gst->resid[0] = res[0]; gst->resid[1] = res[1];
+            if (capped) gst->flags |= UVA_ST_MAXITER;
+            gst->outer_iters = it + 1;
+        }
         int bad = 0;
         for_rows<NTT, R>(tid, I.n, [&](int i, int) { bad |= finite2(x64[I.v0 + i]) ? 0 : 1; });
         bad = team_or(tm, bad);
-        st.outer_iters = it + 1;
         if (bad) {   // non-finite charts keep their layout (gpu.py:235-240)
-            st.flags |= UVA_ST_NONFINITE;
+            if (tid == 0) gst->flags |= UVA_ST_NONFINITE;
             continue;
         }
         double step = 1.0;
@@ -852,7 +952,7 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
             tmin = team_min(tm, tmin);
             step = fmin(0.9 * tmin, 1.0);
         }
-        st.step = step;
+        if (tid == 0) gst->step = step;
         tm.sync();   // all line-search reads of U done
         for_rows<NTT, R>(tid, I.n, [&](int i, int) {
             const int v = I.v0 + __ldg(b.row_vert + I.v0 + i);
@@ -861,7 +961,6 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
         });
         tm.sync();
     }
-    if (tid == 0) b.status[I.id] = st;
 }
 
 // ---- LSCM of one island: hard pins p0 -> (0,0), p1 -> (|P[p1]-P[p0]|, 0);
@@ -983,14 +1082,25 @@ __device__ void run_class(const uva_batch& b, const uva_solve_params& prm, Team<
             tm.sync();
         }
         if (lo + qi >= hi) break;
-        Isl I = load_island(b, b.order[lo + qi]);
+        Isl I = load_island<OP>(b, b.order[lo + qi]);
         const long long t0 = global_ns();
+        // shared-memory copies of the island's slice pointers and Jacobi
+        // diagonal, and room for its slice sums (the previous island ended
+        // with a team barrier, so the buffers are free)
         const int nsl1 = ((I.n + 31) >> 5) + 1;
-        if (tm.sc && nsl1 <= tm.sc_cap) {   // the previous island ended with a team barrier
+        bool cached = false;
+        if (tm.sc && nsl1 <= tm.sc_cap) {
             for (int k = tm.tid; k < nsl1; k += NTT) tm.sc[k] = __ldg(b.slice_ptr + I.s0 + k);
-            tm.sync();
             I.sptr = tm.sc;
+            cached = true;
         }
+        if (tm.pc && nsl1 - 1 <= tm.pc_cap) I.part = tm.pc;
+        if (tm.dc && I.n <= tm.dc_cap) {
+            for (int i = tm.tid; i < I.n; i += NTT) tm.dc[i] = __float2bfloat16(jacobi_global<OP>(b, I, i));
+            I.dv = tm.dc;
+            cached = true;
+        }
+        if (cached) tm.sync();
         if (OP == OP_ARAP) solve_arap<NTT, R>(b, prm, tm, I);
         else solve_lscm<NTT, R>(b, prm, tm, I);
         if (tm.tid == 0) {   // the same thread wrote the rest of the status
@@ -1016,10 +1126,12 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
     __shared__ int slots[8];
     __shared__ float coarse_buf[1024];   // g and y of the coarse level (CTA: 512 each; sub-team: 128 each)
     __shared__ int sc_buf[288];          // slice pointers (CTA: 288; sub-team: 72 each; warp: 9 each)
+    __shared__ float2 part_buf[256];     // slice sums (CTA: 256; sub-team: 64 each)
+    __shared__ __nv_bfloat16 dinv_buf[KB * RB];   // Jacobi (CTA: 8192; sub-team: 2048; warp: 256)
     const bool rev = static_cast<int>(blockIdx.x) < nrev;
     auto whole_cta = [&]() {
         Team<KB> tm{static_cast<int>(threadIdx.x), 0, 0, redd, redf, redi, &slots[0], nullptr, nullptr, nullptr,
-                    coarse_buf, coarse_buf + 512, sc_buf, 288};
+                    coarse_buf, coarse_buf + 512, sc_buf, 288, part_buf, 256, dinv_buf, KB * RB};
         run_class<KB, 0, OP>(b, prm, tm, 0);
         tm.sp = dyn; tm.sr = dyn + KB * RB; tm.sd = dyn + 2 * KB * RB;
         run_class<KB, RB, OP>(b, prm, tm, 1);
@@ -1031,14 +1143,16 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
         float2* base = dyn + s * (3 * SUB * RB);
         Team<SUB> tm{static_cast<int>(threadIdx.x % SUB), 1 + s, 0, redd + s * 64, redf + s * 64, redi + s * 16,
                      &slots[1 + s], base, base + SUB * RB, base + 2 * SUB * RB, coarse_buf + 256 * s,
-                     coarse_buf + 256 * s + 128, sc_buf + 72 * s, 72};
+                     coarse_buf + 256 * s + 128, sc_buf + 72 * s, 72, part_buf + 64 * s, 64,
+                     dinv_buf + SUB * RB * s, SUB * RB};
         run_class<SUB, RB, OP>(b, prm, tm, 2);
     };
     auto warps = [&]() {
         const int w = threadIdx.x / 32;
         float2* base = dyn + w * (3 * 32 * RB);
         Team<32> tm{static_cast<int>(threadIdx.x % 32), 0, 0, nullptr, nullptr, nullptr, nullptr,
-                    base, base + 32 * RB, base + 2 * 32 * RB, nullptr, nullptr, sc_buf + 9 * w, 9};
+                    base, base + 32 * RB, base + 2 * 32 * RB, nullptr, nullptr, sc_buf + 9 * w, 9, nullptr, 0,
+                    dinv_buf + 32 * RB * w, 32 * RB};
         run_class<32, RB, OP>(b, prm, tm, 3);
     };
     // one copy of each phase in the code; the order is decided at run time
@@ -1082,9 +1196,16 @@ __device__ void gauss_jordan(double* W, int N, double* colk) {
 }
 
 // Coarse operators of every island with aggregates: ARAP Ac = P^T A P (with
-// the soft pin) and LSCM Hc = P^T H P over free unknowns (u, v per aggregate),
-// accumulated from the FP32 slot weights in FP64, inverted, stored in FP32.
+// the soft pin) and LSCM Hc = P^T H P over free unknowns (u, v per
+// aggregate), accumulated from the FP32 slot weights in FP64, inverted,
+// stored in FP32. One thread owns each coarse row and adds its terms in
+// slot order, so the operators are the same bits on every run. The
+// inversion works in shared memory when the block fits (kCoarseSmemN).
+constexpr int kCoarseSmemN = 128;
+constexpr size_t kCoarseSmem = sizeof(double) * kCoarseSmemN * kCoarseSmemN;   // 131,072 bytes
+
 __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
+    extern __shared__ double wsm[];
     __shared__ double colk[512];
     const int isl = blockIdx.x;
     if (isl >= b.nc) return;
@@ -1093,37 +1214,34 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
     const int v0 = b.vofs[isl], n = b.vofs[isl + 1] - v0, s0 = b.sofs[isl];
     const int M = (n + agg - 1) / agg;
     const int co = b.cofs[isl];
-    double* W = b.coarse_work + 4 * static_cast<size_t>(co);
     const int2* cw = reinterpret_cast<const int2*>(b.slot_cw);
     auto row_slots_l = [&](int r, int& q0, int& width) {
         const int s = s0 + (r >> 5);
         q0 = b.slice_ptr[s] + (r & 31);
         width = (b.slice_ptr[s + 1] - b.slice_ptr[s]) >> 5;
     };
+    auto work = [&](int N) { return N <= kCoarseSmemN ? wsm : b.coarse_work + 4 * static_cast<size_t>(co); };
     // ---- ARAP
+    double* W = work(M);
     for (int e = threadIdx.x; e < M * M; e += blockDim.x) W[e] = 0.0;
     __syncthreads();
-    for (int r = threadIdx.x; r < n; r += blockDim.x) {
-        const int a = r / agg;
-        int q0, width;
-        row_slots_l(r, q0, width);
+    const int pin_agg = b.vert_row[v0 + b.pins[3 * isl]] / agg;
+    for (int a = threadIdx.x; a < M; a += blockDim.x) {
+        double* Wa = W + static_cast<size_t>(a) * M;
         double dsum = 0.0;
-        for (int k = 0; k < width; ++k) {
-            const int2 sl = cw[q0 + 32 * k];
-            const double w = static_cast<double>(__int_as_float(sl.y));
-            if (w == 0.0) continue;
-            const int c = slot_row(sl.x) / agg;
-            dsum += w;
-            if (c != a) atomicAdd(W + static_cast<size_t>(a) * M + c, -w);
-            else dsum -= w;
+        for (int r = a * agg; r < min(n, (a + 1) * agg); ++r) {
+            int q0, width;
+            row_slots_l(r, q0, width);
+            for (int k = 0; k < width; ++k) {
+                const int2 sl = cw[q0 + 32 * k];
+                const double w = static_cast<double>(__int_as_float(sl.y));
+                if (w == 0.0) continue;
+                const int c = slot_row(sl.x) / agg;
+                if (c != a) { dsum += w; Wa[c] -= w; }
+            }
         }
-        if (dsum != 0.0) atomicAdd(W + static_cast<size_t>(a) * M + a, dsum);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const int pr = b.vert_row[v0 + b.pins[3 * isl]];
-        const int a = pr / agg;
-        W[static_cast<size_t>(a) * M + a] += b.wpin[isl];
+        if (a == pin_agg) dsum += b.wpin[isl];
+        Wa[a] += dsum;
     }
     gauss_jordan(W, M, colk);
     for (int e = threadIdx.x; e < M * M; e += blockDim.x) b.coarse_a[co + e] = static_cast<float>(W[e]);
@@ -1132,42 +1250,58 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
     const int pv0 = b.pins[3 * isl + 1], pv1 = b.pins[3 * isl + 2];
     if (pv0 < 0 || pv1 < 0) return;
     const int p0 = b.vert_row[v0 + pv0], p1 = b.vert_row[v0 + pv1];
-    const int N = 2 * M;
+    const int aggl = agg;
+    const int ML = M;
+    const int N = 2 * ML;
+    W = work(N);
     for (int e = threadIdx.x; e < N * N; e += blockDim.x) W[e] = 0.0;
     __syncthreads();
-    for (int r = threadIdx.x; r < n; r += blockDim.x) {
-        if (r == p0 || r == p1) continue;
-        const int a = r / agg;
-        int q0, width;
-        row_slots_l(r, q0, width);
-        double dsum = 0.0;
-        for (int k = 0; k < width; ++k) {
-            const int q = q0 + 32 * k;
-            const int2 sl = cw[q];
-            const double w = static_cast<double>(__int_as_float(sl.y));
-            const double cc = static_cast<double>(b.slot_c[q]);
-            if (w == 0.0 && cc == 0.0) continue;
-            dsum += w;
-            if (slot_row(sl.x) == p0 || slot_row(sl.x) == p1) continue;   // pinned neighbour: no coarse coupling
-            const int c = slot_row(sl.x) / agg;
-            if (c == a) {
-                dsum -= w;
-            } else {
-                atomicAdd(W + static_cast<size_t>(2 * a) * N + 2 * c, -w);
-                atomicAdd(W + static_cast<size_t>(2 * a + 1) * N + 2 * c + 1, -w);
-            }
-            if (cc != 0.0) {
-                atomicAdd(W + static_cast<size_t>(2 * a) * N + 2 * c + 1, cc);
-                atomicAdd(W + static_cast<size_t>(2 * a + 1) * N + 2 * c, -cc);
+    for (int a = threadIdx.x; a < ML; a += blockDim.x) {
+        double* Wu = W + static_cast<size_t>(2 * a) * N;      // row of u_a
+        double* Wv = W + static_cast<size_t>(2 * a + 1) * N;  // row of v_a
+        double dsum = 0.0, cuv = 0.0, cvu = 0.0;
+        for (int r = a * aggl; r < min(n, (a + 1) * aggl); ++r) {
+            if (r == p0 || r == p1) continue;
+            int q0, width;
+            row_slots_l(r, q0, width);
+            for (int k = 0; k < width; ++k) {
+                const int2 sl = cw[q0 + 32 * k];
+                const double w = static_cast<double>(__int_as_float(sl.y));
+                const double cc = 0.5 * static_cast<double>(slot_c2(sl.x));
+                if (w == 0.0 && cc == 0.0) continue;
+                const int col = slot_row(sl.x);
+                const bool pinned_nb = col == p0 || col == p1;   // no coarse coupling
+                const int c = col / aggl;
+                if (pinned_nb || c != a) dsum += w;
+                if (pinned_nb) continue;
+                if (c != a) { Wu[2 * c] -= w; Wv[2 * c + 1] -= w; }
+                if (cc != 0.0) {
+                    if (c == a) { cuv += cc; cvu -= cc; }
+                    else { Wu[2 * c + 1] += cc; Wv[2 * c] -= cc; }
+                }
             }
         }
-        if (dsum != 0.0) {
-            atomicAdd(W + static_cast<size_t>(2 * a) * N + 2 * a, dsum);
-            atomicAdd(W + static_cast<size_t>(2 * a + 1) * N + 2 * a + 1, dsum);
-        }
+        Wu[2 * a] += dsum;
+        Wv[2 * a + 1] += dsum;
+        Wu[2 * a + 1] += cuv;
+        Wv[2 * a] += cvu;
     }
     gauss_jordan(W, N, colk);
     for (int e = threadIdx.x; e < N * N; e += blockDim.x) b.coarse_l[4 * static_cast<size_t>(co) + e] = static_cast<float>(W[e]);
+}
+
+cudaError_t ensure_coarse_attr() {
+    static std::mutex mu;
+    static std::vector<char> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (static_cast<int>(done.size()) <= dev) done.resize(dev + 1, 0);
+    if (done[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kCoarseSmem));
+    if (e == cudaSuccess) done[dev] = 1;
+    return e;
 }
 
 int sm_count() {
@@ -1259,7 +1393,9 @@ extern "C" int uva_batch_setup(uva_batch* b, void* stream) {
     k_far_pair<<<(b->nc + 127) / 128, 128, 0, s>>>(*b);
     UVA_CHECK_LAUNCH("uva_batch_setup/pins");
     if (b->coarse_a && b->coarse_l && b->coarse_work) {
-        k_coarse<<<b->nc, 1024, 0, s>>>(*b);
+        const cudaError_t e = ensure_coarse_attr();   // 128 KB of dynamic shared memory
+        if (e != cudaSuccess) return uva_cuda_status(e, "uva_batch_setup/coarse attribute");
+        k_coarse<<<b->nc, 1024, kCoarseSmem, s>>>(*b);
         UVA_CHECK_LAUNCH("uva_batch_setup/coarse");
     }
     return UVA_OK;
@@ -1297,6 +1433,7 @@ extern "C" int uva_step_graph_create(uva_batch* b, int32_t parts, const uva_solv
     *out = nullptr;
     cudaError_t e = ensure_islands_attr<OP_ARAP>();
     if (e == cudaSuccess) e = ensure_islands_attr<OP_LSCM>();
+    if (e == cudaSuccess) e = ensure_coarse_attr();
     if (e != cudaSuccess) return uva_cuda_status(e, "uva_step_graph_create/attributes");
     sm_count();
     cudaStream_t cs = nullptr;
