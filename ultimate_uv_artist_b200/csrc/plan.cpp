@@ -74,38 +74,51 @@ void blob_order(const IslandPlan& ip, int32_t n, int32_t agg, std::vector<int32_
 
 void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& bad) {
     ip.n = n; ip.t = t;
-    struct HE { int64_t key; int32_t he; };
-    std::vector<HE> he(static_cast<size_t>(3) * t);
+    // half-edges grouped by (lo, hi, half-edge id): a stable counting sort by
+    // lo, then a stable insertion sort by hi inside each (short) bucket
+    const int32_t nh = 3 * t;
+    std::vector<int32_t> hlo(nh), hhi(nh);
     for (int32_t f = 0; f < t; ++f) {
         for (int k = 0; k < 3; ++k) {
-            int64_t a = T[3 * f + (k + 1) % 3], b = T[3 * f + (k + 2) % 3];
+            const int64_t a = T[3 * f + (k + 1) % 3], b = T[3 * f + (k + 2) % 3];
             if (a < 0 || a >= n || b < 0 || b >= n) { bad = true; return; }
-            int64_t lo = a < b ? a : b, hi = a < b ? b : a;
-            he[3 * f + k] = {lo * n + hi, 3 * f + k};
+            hlo[3 * f + k] = static_cast<int32_t>(a < b ? a : b);
+            hhi[3 * f + k] = static_cast<int32_t>(a < b ? b : a);
         }
     }
-    std::sort(he.begin(), he.end(), [](const HE& x, const HE& y) {
-        return x.key < y.key || (x.key == y.key && x.he < y.he);
-    });
+    std::vector<int32_t> bstart(n + 1, 0), hs(nh);
+    for (int32_t h = 0; h < nh; ++h) ++bstart[hlo[h] + 1];
+    for (int32_t v = 0; v < n; ++v) bstart[v + 1] += bstart[v];
+    {
+        std::vector<int32_t> fillb(bstart.begin(), bstart.end() - 1);
+        for (int32_t h = 0; h < nh; ++h) hs[fillb[hlo[h]]++] = h;
+    }
+    for (int32_t v = 0; v < n; ++v) {
+        for (int32_t q = bstart[v] + 1; q < bstart[v + 1]; ++q) {
+            const int32_t h = hs[q];
+            int32_t r = q - 1;
+            while (r >= bstart[v] && hhi[hs[r]] > hhi[h]) { hs[r + 1] = hs[r]; --r; }
+            hs[r + 1] = h;
+        }
+    }
     ip.tri_edge.assign(static_cast<size_t>(3) * t, -1);
     ip.edge_info.clear();
     std::vector<int64_t> ekey;
-    for (size_t s = 0; s < he.size();) {
-        size_t e = s;
+    for (int32_t s = 0; s < nh;) {
+        int32_t e = s;
         int32_t fwd = 0, rev = 0;
-        const int64_t key = he[s].key;
-        const int64_t lo = key / n;
-        while (e < he.size() && he[e].key == key) {
-            const int32_t h = he[e].he;
+        const int32_t lo = hlo[hs[s]], hi = hhi[hs[s]];
+        while (e < nh && hlo[hs[e]] == lo && hhi[hs[e]] == hi) {
+            const int32_t h = hs[e];
             const int32_t f = h / 3, k = h % 3;
             const int64_t a = T[3 * f + (k + 1) % 3];
             if (a == lo) ++fwd; else ++rev;
             ip.tri_edge[h] = static_cast<int32_t>(ekey.size());
             ++e;
         }
-        const int32_t cnt = static_cast<int32_t>(e - s);
+        const int32_t cnt = e - s;
         ip.edge_info.push_back(std::min(cnt, 1023) | (std::min(fwd, 1023) << 10) | (std::min(rev, 1023) << 20));
-        ekey.push_back(key);
+        ekey.push_back(static_cast<int64_t>(lo) * n + hi);
         s = e;
     }
     ip.nedges = static_cast<int32_t>(ekey.size());
@@ -346,21 +359,29 @@ extern "C" int uva_plan_export(const uva_plan* p, int32_t* tri4, int32_t* tri_ed
     if (sofs) sofs[nc] = static_cast<int32_t>(p->nslices);
     slice_ptr[p->nslices] = static_cast<int32_t>(p->nslots);
     if (bofs) bofs[nc] = static_cast<int32_t>(p->nbverts);
-    // vertex -> (triangle, corner) incidence, ascending by f*3+corner
-    std::vector<int32_t> cnt(p->n + 1, 0);
-    for (int32_t i = 0; i < nc; ++i) {
-        const int64_t fb = p->tofs[i] - t0, vb = p->vofs[i] - v0;
-        for (int32_t f = 0; f < p->isl[i].t; ++f)
-            for (int k = 0; k < 3; ++k) ++cnt[vb + p->tri_local[3 * (fb + f) + k] + 1];
+    // vertex -> (triangle, corner) incidence, ascending by f*3+corner. An
+    // island's corners are its own 3*t entries, so islands fill their part
+    // of vt independently (offset 3 * tofs[i]).
+    auto inc = [&](int32_t lo, int32_t hi) {
+        for (int32_t i = lo; i < hi; ++i) {
+            const int64_t fb = p->tofs[i] - t0, vb = p->vofs[i] - v0;
+            const int32_t n = p->isl[i].n, t = p->isl[i].t;
+            std::vector<int32_t> cnt(n + 1, 0);
+            for (int64_t c = 3 * fb; c < 3 * (fb + t); ++c) ++cnt[p->tri_local[c] + 1];
+            for (int32_t v = 0; v < n; ++v) cnt[v + 1] += cnt[v];
+            for (int32_t v = 0; v <= n; ++v) vt_ptr[vb + v] = static_cast<int32_t>(3 * fb + cnt[v]);
+            for (int64_t c = 3 * fb; c < 3 * (fb + t); ++c) vt[3 * fb + cnt[p->tri_local[c]]++] = static_cast<int32_t>(c);
+        }
+    };
+    {
+        std::vector<std::thread> pool2;
+        for (int32_t k = 0; k < nt; ++k) {
+            const int32_t lo = k * chunk, hi = std::min(nc, lo + chunk);
+            if (lo < hi) pool2.emplace_back(inc, lo, hi);
+        }
+        for (auto& th : pool2) th.join();
     }
-    for (int64_t v = 0; v < p->n; ++v) cnt[v + 1] += cnt[v];
-    for (int64_t v = 0; v <= p->n; ++v) vt_ptr[v] = cnt[v];
-    std::vector<int32_t> fillp(cnt.begin(), cnt.end() - 1);
-    for (int32_t i = 0; i < nc; ++i) {
-        const int64_t fb = p->tofs[i] - t0, vb = p->vofs[i] - v0;
-        for (int32_t f = 0; f < p->isl[i].t; ++f)
-            for (int k = 0; k < 3; ++k) vt[fillp[vb + p->tri_local[3 * (fb + f) + k]]++] = static_cast<int32_t>(3 * (fb + f) + k);
-    }
+    vt_ptr[p->n] = static_cast<int32_t>(3 * p->t);
     return UVA_OK;
 }
 
