@@ -508,7 +508,8 @@ def main():
         dbb = bb.db
         h2d = int(sum(getattr(dbb.plan, k).nbytes for k in ("tri4", "tri_edge", "sofs", "slice_ptr", "slot_col",
                                                               "slot_edge", "slot_c", "vt_ptr", "vt", "vflags",
-                                                              "bofs", "bverts", "order", "vofs", "tofs"))
+                                                              "bofs", "bverts", "order", "vofs", "tofs",
+                                                              "row_vert", "vert_row", "agg_rows", "cofs"))
                   + dbb.P.numel() * 8 + dbb.U.numel() * 8)
         d2h = int(sum(u.nbytes for u in Us))
         del bb

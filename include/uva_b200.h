@@ -197,6 +197,18 @@ int uva_step_graph_create(uva_batch* b, int32_t parts, const uva_solve_params* l
 int uva_graph_launch(uva_graph* g, void* stream);
 int uva_graph_destroy(uva_graph* g);
 
+/* SLIM iterations of every island (param.refine(method="slim"),
+ * param.py:415-454 with _arap_rotations mode 1 :206-256 and the normal
+ * equations of _assemble_weighted / _slim_system :341-377). PARAM semantics
+ * only. prm: iters, energy_tol (refine's tol), inner_eta and max_inner (the
+ * CG relative tolerance and iteration cap of each global step; the
+ * reference solves exactly when 2n <= 220,000, else CG rtol 1e-6, at most
+ * 500 iterations). A start with an inverted triangle is left unchanged
+ * (status flag UVA_ST_NONFINITE), as the reference returns early.
+ * scratch: uva_slim_scratch_bytes(b) bytes, 16-byte aligned.             */
+int uva_slim_scratch_bytes(const uva_batch* b, int64_t* bytes);
+int uva_slim(uva_batch* b, const uva_solve_params* prm, double* scratch, void* stream);
+
 /* No counterpart in the reference. The same ARAP iterations as uva_arap, for
  * callers that cannot allocate device memory while they run (for example a
  * host application that owns a fixed device pool, or code that must not call
@@ -343,6 +355,8 @@ enum {
     UVA_OP_MAX_STEP,        /* _max_step :259-291   U, D -> out (1)           */
     UVA_OP_ENERGY           /* _energy :294-319, kind = arg -> out (1)        */
 };
+/* UVA_OP_ROTATIONS: arg = mode; mode 1 writes the SLIM weight matrices
+ * (param.py:234-255) to out2 (t*4).                                      */
 int uva_chart_op(int32_t op, int32_t arg, const double* P, const int64_t* T, const double* U, const double* D,
                  const double* X, const double* cots, const double* R, const double* area, int32_t n, int32_t t,
                  double* out, double* out2, void* stream);

@@ -488,6 +488,95 @@ def refine_arap(P, T, U, iters=10, line_search=True, tol=1e-5, pin=None):
     return U
 
 
+def slim_local(U, T, X):
+    """engine/param.py:206-256 (mode 1): per triangle the signed SVD of the
+    Jacobian J = U_f M^-1 (numpy svd, last singular value negated when
+    det(U V^T) < 0), the rotation U V^T and the SLIM weights
+    W = U diag(w) U^T with w = sqrt((s - s^-3) / (s - 1)) of |s| clamped at
+    1e-8 (2 when |s - 1| < 1e-6). Frame-less triangles get R = W = I."""
+    t = len(T)
+    x1 = X[:, 1, 0]; x2 = X[:, 2, 0]; y2 = X[:, 2, 1]
+    good = np.abs(x1 * y2) >= 1e-300
+    x1s = np.where(good, x1, 1.0); y2s = np.where(good, y2, 1.0)
+    du1 = U[T[:, 1]] - U[T[:, 0]]
+    du2 = U[T[:, 2]] - U[T[:, 0]]
+    j00 = du1[:, 0] / x1s; j10 = du1[:, 1] / x1s
+    j01 = (du2[:, 0] - j00 * x2) / y2s; j11 = (du2[:, 1] - j10 * x2) / y2s
+    J = np.stack([np.stack([j00, j01], 1), np.stack([j10, j11], 1)], 1)
+    Us, S, Vt = np.linalg.svd(J)
+    neg = np.linalg.det(Us @ Vt) < 0
+    Us[neg, :, 1] *= -1.0
+    S[neg, 1] *= -1.0
+    R = Us @ Vt
+    s = np.maximum(np.abs(S), 1e-8)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        w = np.where(np.abs(s - 1.0) < 1e-6, 2.0, np.sqrt(np.maximum((s - s ** -3) / (s - 1.0), 1e-12)))
+    W = np.einsum("tij,tj,tkj->tik", Us, w, Us)
+    eye = np.broadcast_to(np.eye(2), (t, 2, 2))
+    R = np.where(good[:, None, None], R, eye)
+    W = np.where(good[:, None, None], W, eye)
+    return R, W
+
+
+def slim_system(n, T, X, area, R, W):
+    """engine/param.py:341-377: rows sqrt(area) (W (J - R)) over the 2n
+    unknowns [u; v]; returns A (4t x 2n) and b."""
+    t = len(T)
+    x1 = X[:, 1, 0]; x2 = X[:, 2, 0]; y2 = X[:, 2, 1]
+    G = np.zeros((t, 2, 3))
+    G[:, 0, 0] = -1 / x1; G[:, 0, 1] = 1 / x1
+    G[:, 1, 0] = (-1 + x2 / x1) / y2; G[:, 1, 1] = (-x2 / x1) / y2; G[:, 1, 2] = 1 / y2
+    sq = np.sqrt(area)
+    WR = W @ R
+    rows, cols, vals, rhs = [], [], [], []
+    for si in range(2):
+        for c in range(2):
+            r0 = (2 * si + c) * t + np.arange(t)
+            for comp in range(2):
+                for k in range(3):
+                    rows.append(r0); cols.append(T[:, k] + comp * n)
+                    vals.append(sq * W[:, si, comp] * G[:, c, k])
+            rhs.append(sq * WR[:, si, c])
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(4 * t, 2 * n))
+    return A, np.concatenate(rhs)
+
+
+def refine_slim(P, T, U, iters=10, tol=1e-5):
+    """engine/param.py:415-454 (method='slim'), exact solves: normal
+    equations (A^T A + 1e-12 sum(area) I) x = A^T b + 1e-12 sum(area) x0,
+    flip-safe step min(1, 0.9 tmax), halving up to 12 times while the
+    symmetric Dirichlet energy is not below the previous one, relative-energy
+    stop. A start with an inverted triangle is returned unchanged."""
+    P = np.asarray(P, np.float64); T = np.asarray(T, np.int64); U = np.asarray(U, np.float64).copy()
+    n = len(P)
+    X, area = local_frames(P, T)
+    prev = energy(U, T, X, area, 1)
+    if not np.isfinite(prev):
+        return U
+    reg = 1e-12 * area.sum()
+    for _ in range(iters):
+        R, W = slim_local(U, T, X)
+        A, b = slim_system(n, T, X, area, R, W)
+        M = (A.T @ A).tocsc() + sp.identity(2 * n, format="csc") * reg
+        x0 = np.r_[U[:, 0], U[:, 1]]
+        x = spla.spsolve(M, A.T @ b + reg * x0)
+        D = np.stack([x[:n], x[n:]], 1) - U
+        step = min(1.0, 0.9 * max_step_param(U, D, T))
+        e = energy(U + step * D, T, X, area, 1)
+        k = 0
+        while (not np.isfinite(e) or e > prev) and k < 12:
+            step *= 0.5
+            e = energy(U + step * D, T, X, area, 1)
+            k += 1
+        if not np.isfinite(e) or e > prev:
+            break
+        U = U + step * D
+        if abs(prev - e) <= tol * prev:
+            break
+        prev = e
+    return U
+
+
 def repair_flips_param(U, T, rounds=60):
     """engine/param.py:477-516: Gauss-Seidel 1-ring moves in triangle order."""
     U = np.array(U, np.float64, copy=True)

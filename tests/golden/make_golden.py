@@ -156,6 +156,21 @@ def main(ref_root):
                v_dist_keys=np.array(sorted(dist)), v_dist_vals=np.array([float(dist[k]) for k in sorted(dist)]),
                v_s1=s1, v_s2=s2, v_sa=sgn, v_A3=A3, v_good=good, v_counts=counts,
                v_cF=fchart, v_cU=uchart, v_cov=cov)
+    # ------------------------------------------------------------ SLIM (artist profile)
+    rng = np.random.default_rng(21)
+    Ps, Ts = synth.disk_patch(rng, 600, amp=0.3)
+    Ps = Ps.astype(np.float64)
+    Us0 = param.lscm(Ps, Ts)
+    Xs, areas = param.local_frames(Ps, Ts)
+    cotss = param.cot_weights(Xs)
+    assert np.isfinite(param._energy(Us0, Ts, Xs, areas, 1)), "SLIM fixture needs a flip-free start"
+    Rs1, Ws1 = param._arap_rotations(Us0, Ts, Xs, cotss, 1, np.empty(0))
+    Us5, _ = param.refine(Ps, Ts, Us0, iters=5, method="slim", tol=0.0)
+    Us20, _ = param.refine(Ps, Ts, Us0, iters=20, method="slim")
+    out.update(s_P=Ps, s_T=Ts, s_U0=Us0, s_R1=Rs1, s_W1=Ws1, s_U5=Us5, s_U20=Us20,
+               s_E0=np.array(param._energy(Us0, Ts, Xs, areas, 1)),
+               s_E5=np.array(param._energy(Us5, Ts, Xs, areas, 1)),
+               s_E20=np.array(param._energy(Us20, Ts, Xs, areas, 1)))
     path = os.path.join(HERE, "golden_small.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")

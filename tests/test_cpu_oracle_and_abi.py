@@ -33,6 +33,27 @@ def test_oracle_param_matches_reference(golden):
     assert np.array_equal(O.repair_flips_param(golden["p_Uf"], T), golden["p_Ur"])
 
 
+def _rel_modulo_translation(U, ref):
+    """Max |U - ref| over the UV extent after removing the mean shift. The
+    SLIM normal equations fix the translation only through a 1e-12 sum(area)
+    regulariser (engine/param.py:426-429), so the reference's own translation
+    moves by about 1e-5 of the extent with the sparse LU's round-off."""
+    d = U - ref
+    return float(np.abs(d - d.mean(0)).max() / np.ptp(ref, 0).max())
+
+
+def test_oracle_slim_matches_reference(golden):
+    P, T, U0 = golden["s_P"], golden["s_T"], golden["s_U0"]
+    X, area = O.local_frames(P, T)
+    R, W = O.slim_local(U0, T, X)
+    assert np.abs(R - golden["s_R1"]).max() < 1e-12 and np.abs(W - golden["s_W1"]).max() < 1e-11
+    U5 = O.refine_slim(P, T, U0, iters=5, tol=0.0)
+    assert _rel_modulo_translation(U5, golden["s_U5"]) < 1e-12
+    assert abs(O.energy(U5, T, X, area, 1) - float(golden["s_E5"])) <= 1e-12 * float(golden["s_E5"])
+    U20 = O.refine_slim(P, T, U0, iters=20)
+    assert _rel_modulo_translation(U20, golden["s_U20"]) < 1e-12
+
+
 def test_oracle_batch_matches_reference(golden):
     nc = int(golden["b_nc"])
     items = [(golden[f"b_P{k}"], golden[f"b_T{k}"], golden[f"b_U{k}"]) for k in range(nc)]

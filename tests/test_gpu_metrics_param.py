@@ -97,6 +97,33 @@ def test_param_solvers(golden, cuda):
     assert np.allclose(q["per_tri_area"], golden["p_q_area"], rtol=1e-9)
 
 
+def test_slim_rotations_and_refine(golden, cuda):
+    """SLIM (engine/param.py:206-256 mode 1, 415-454) against the reference's
+    outputs. UVs are compared after removing the mean shift: the SLIM normal
+    equations fix the translation only through a 1e-12 sum(area) regulariser,
+    so the reference's own translation moves with its LU round-off."""
+    from ultimate_uv_artist_b200.engine import param as Pm
+    P, T, U0 = golden["s_P"], golden["s_T"], golden["s_U0"]
+    X, area = O.local_frames(P, T)
+    R, W = Pm._arap_rotations(U0, T, X, None, 1, True)
+    assert np.abs(R - golden["s_R1"]).max() < 1e-12
+    assert np.abs(W - golden["s_W1"]).max() < 1e-10
+    ext = np.ptp(golden["s_U5"], 0).max()
+    for iters, tol, key in ((5, 0.0, "s_U5"), (20, 1e-5, "s_U20")):
+        U, solver = Pm.refine(P, T, U0, iters=iters, method="slim", tol=tol)
+        assert solver is None
+        d = U - golden[key]
+        assert np.abs(d - d.mean(0)).max() / ext < 1e-5, (key, np.abs(d - d.mean(0)).max() / ext)
+        assert np.abs(d.mean(0)).max() / ext < 1e-3
+    U5, _ = Pm.refine(P, T, U0, iters=5, method="slim", tol=0.0)
+    assert rel(Pm._energy(U5, T, X, area, 1), golden["s_E5"]) < 1e-8
+    # an inverted start is returned unchanged, as the reference does
+    Uf = U0.copy()
+    Uf[:, 0] *= -1.0
+    Ub, _ = Pm.refine(P, T, Uf, iters=3, method="slim")
+    assert np.array_equal(Ub, Uf)
+
+
 def test_spd_solver_and_tutte(cuda):
     import scipy.sparse as sp
     import scipy.sparse.linalg as spla

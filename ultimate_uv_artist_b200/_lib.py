@@ -73,6 +73,8 @@ _SIGS = {
     "uva_lscm": [vp, vp, vp],
     "uva_arap": [vp, vp, vp],
     "uva_arap_noalloc": [vp, vp, vp],
+    "uva_slim": [vp, vp, vp, vp],
+    "uva_slim_scratch_bytes": [vp, vp],
     "uva_step_graph_create": [vp, i32, vp, vp, vp],
     "uva_graph_launch": [vp, vp],
     "uva_graph_destroy": [vp],

@@ -5,7 +5,8 @@
 //   UVA_OP_FRAMES      local_frames (param.py:19-32): X (t,3,2), area (t)
 //   UVA_OP_COTS        cot_weights (param.py:35-44) from X
 //   UVA_OP_SIGNED_AREA signed_areas (param.py:97-99)
-//   UVA_OP_ROTATIONS   _arap_rotations mode 0 (param.py:206-233): R (t,2,2)
+//   UVA_OP_ROTATIONS   _arap_rotations (param.py:206-256), mode in `arg`: R (t,2,2);
+//                      mode 1 also the SLIM weight matrices W (t,2,2) in out2
 //   UVA_OP_RHS         _arap_rhs (param.py:457-474): b (n,2), FP64 atomics
 //   UVA_OP_MAX_STEP    _max_step (param.py:259-291): one scalar
 //   UVA_OP_ENERGY      _energy (param.py:294-319), kind in `arg`: one scalar
@@ -88,11 +89,20 @@ __global__ void k_chart_op(ChartArgs a) {
                 const double* U = a.U;
                 const double x1 = X[2], x2 = X[4], y2 = X[5];
                 double* R = a.out + 4 * static_cast<size_t>(f);
+                double* W = (a.arg == 1 && a.out2) ? a.out2 + 4 * static_cast<size_t>(f) : nullptr;
+                if (W) { W[0] = 1.0; W[1] = 0.0; W[2] = 0.0; W[3] = 1.0; }
                 if (fabs(x1 * y2) < 1e-300) { R[0] = 1.0; R[1] = 0.0; R[2] = 0.0; R[3] = 1.0; break; }
                 const double du1x = U[2 * i1] - U[2 * i0], du1y = U[2 * i1 + 1] - U[2 * i0 + 1];
                 const double du2x = U[2 * i2] - U[2 * i0], du2y = U[2 * i2 + 1] - U[2 * i0 + 1];
                 const double j00 = du1x / x1, j10 = du1y / x1;
                 const double j01 = (du2x - j00 * x2) / y2, j11 = (du2y - j10 * x2) / y2;
+                if (W) {   // SVD-based rotation and SLIM weights (param.py:234-255)
+                    double rc, rs, w00, w01, w11;
+                    slim_2x2(j00, j01, j10, j11, rc, rs, w00, w01, w11);
+                    R[0] = rc; R[1] = -rs; R[2] = rs; R[3] = rc;
+                    W[0] = w00; W[1] = w01; W[2] = w01; W[3] = w11;
+                    break;
+                }
                 double ca = j00 + j11, cb = j10 - j01;
                 double h = sqrt(ca * ca + cb * cb);
                 if (h < 1e-300) { ca = 1.0; cb = 0.0; h = 1.0; }

@@ -25,6 +25,33 @@ __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_fl
 
 __device__ __forceinline__ bool finite2(double2 v) { return isfinite(v.x) && isfinite(v.y); }
 
+// SLIM local step of one 2x2 Jacobian J = [[j00, j01], [j10, j11]]
+// (engine/param.py:234-255, mode 1): signed singular values s1 = Q + R,
+// s2 = Q - R and first left singular vector at angle phi (closed form),
+// weights w = sqrt((|s| - |s|^-3) / (|s| - 1)) (2 when |s| ~ 1, |s| clamped
+// at 1e-8), W = U diag(w) U^T (symmetric: w00, w01, w11), and the closest
+// rotation R = [[rc, -rs], [rs, rc]].
+__device__ __forceinline__ double slim_weight(double s) {
+    s = fmax(fabs(s), 1e-8);
+    if (fabs(s - 1.0) < 1e-6) return 2.0;
+    return sqrt(fmax((s - 1.0 / (s * s * s)) / (s - 1.0), 1e-12));
+}
+
+__device__ __forceinline__ void slim_2x2(double j00, double j01, double j10, double j11, double& rc, double& rs,
+                                         double& w00, double& w01, double& w11) {
+    const double E = 0.5 * (j00 + j11), F = 0.5 * (j00 - j11), G = 0.5 * (j10 + j01), H = 0.5 * (j10 - j01);
+    const double Q = sqrt(E * E + H * H), R = sqrt(F * F + G * G);
+    if (Q > 0.0) { rc = E / Q; rs = H / Q; } else { rc = 1.0; rs = 0.0; }
+    const double phi = 0.5 * (atan2(G, F) + atan2(H, E));
+    const double cp = cos(phi), sp = sin(phi);
+    const double w1 = slim_weight(Q + R), w2 = slim_weight(Q - R);
+    const double d = w1 - w2;
+    w00 = w2 + d * cp * cp;
+    w01 = d * cp * sp;
+    w11 = w2 + d * sp * sp;
+}
+
+
 // Block-wide all-reduce of K values (every thread gets the totals, summed in
 // the same order on every thread, so branch decisions stay uniform).
 // `red` holds 2 * K * NW slots; `phase` alternates between the two halves so

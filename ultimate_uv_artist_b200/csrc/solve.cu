@@ -1371,6 +1371,285 @@ int launch_islands(const uva_batch* b, const uva_solve_params* prm, cudaStream_t
     return UVA_OK;
 }
 
+// ------------------------------------------------------------------ SLIM
+// Symmetric-Dirichlet SLIM iterations (engine/param.py:206-256 mode 1,
+// 341-377 and 415-454), one 1024-thread CTA per island, FP64 throughout.
+//
+// Local step per triangle: J = U M^-1 in the triangle's frame, its signed
+// singular values s1 = q + r, s2 = q - r and left singular vector u1
+// (closed form), SLIM weights w_k = sqrt((|s| - |s|^-3) / (|s| - 1)) (2 at
+// |s| ~ 1), W = U diag(w) U^T and the closest rotation R. Global step: the
+// reference builds A (4t x 2n) with rows sqrt(area) W (J - R) and solves the
+// normal equations (A^T A + reg I) x = A^T b + reg x0, reg = 1e-12 sum(area).
+// Here A^T A is applied without forming it: per triangle
+//   (A^T A x)_{r,k} = area (W^2 J(x) G)_{r,k},   (A^T b)_{r,k} = area (W^2 R G)_{r,k},
+// with G the 2x3 gradient of the linear interpolant; each vertex gathers its
+// incident corners (vt), so no atomics and a fixed summation order. CG with
+// the diagonal of A^T A (the reference's Jacobi) from x0 = U; the reference
+// solves exactly (splu) when 2n <= 220,000 and runs CG to rtol 1e-6, at most
+// 500 iterations, above: prm.inner_eta and prm.max_inner carry that choice.
+// Then the flip-safe step min(1, 0.9 tmax) and halving while the symmetric
+// Dirichlet energy is not below the previous one (at most 12 times).
+struct SlimTri {
+    double x1, x2, y2, area;
+    double g0[3], g1[3];   // rows of G (gradient of the linear interpolant)
+    bool live;
+};
+
+__device__ __forceinline__ SlimTri slim_tri(const uva_batch& b, int f) {
+    const double4 fr = reinterpret_cast<const double4*>(b.frame)[f];
+    SlimTri t;
+    t.x1 = fr.x; t.x2 = fr.y; t.y2 = fr.z; t.area = fr.w;
+    t.live = fabs(t.x1 * t.y2) >= 1e-300;
+    const double ix1 = 1.0 / t.x1, iy2 = 1.0 / t.y2;
+    t.g0[0] = -ix1; t.g0[1] = ix1; t.g0[2] = 0.0;
+    t.g1[0] = (-1.0 + t.x2 * ix1) * iy2; t.g1[1] = (-t.x2 * ix1) * iy2; t.g1[2] = iy2;
+    return t;
+}
+
+// J (rows u, v; columns c) of corner values q_u, q_v
+__device__ __forceinline__ void slim_jac(const SlimTri& t, const double2 q[3], double J[2][2]) {
+    J[0][0] = t.g0[0] * q[0].x + t.g0[1] * q[1].x + t.g0[2] * q[2].x;
+    J[0][1] = t.g1[0] * q[0].x + t.g1[1] * q[1].x + t.g1[2] * q[2].x;
+    J[1][0] = t.g0[0] * q[0].y + t.g0[1] * q[1].y + t.g0[2] * q[2].y;
+    J[1][1] = t.g1[0] * q[0].y + t.g1[1] * q[1].y + t.g1[2] * q[2].y;
+}
+
+// symmetric Dirichlet energy of one triangle, inf if inverted (param.py:310-318)
+__device__ __forceinline__ double sd_energy_tri(const SlimTri& t, const double2 q[3]) {
+    if (!t.live) return 0.0;
+    const double j00 = (q[1].x - q[0].x) / t.x1, j10 = (q[1].y - q[0].y) / t.x1;
+    const double j01 = ((q[2].x - q[0].x) - j00 * t.x2) / t.y2, j11 = ((q[2].y - q[0].y) - j10 * t.x2) / t.y2;
+    const double dj = j00 * j11 - j01 * j10;
+    if (dj <= 0.0) return INFINITY;
+    const double fro = j00 * j00 + j01 * j01 + j10 * j10 + j11 * j11;
+    return t.area * (fro + fro / (dj * dj) - 4.0);
+}
+
+// local step of one triangle: S = W^2 (symmetric: s00, s01, s11) and the
+// closest rotation R = [[rc, -rs], [rs, rc]]
+__device__ __forceinline__ void slim_local(const SlimTri& t, const double2 q[3], double S[3], double& rc, double& rs) {
+    if (!t.live) { S[0] = 1.0; S[1] = 0.0; S[2] = 1.0; rc = 1.0; rs = 0.0; return; }
+    const double j00 = (q[1].x - q[0].x) / t.x1, j10 = (q[1].y - q[0].y) / t.x1;
+    const double j01 = ((q[2].x - q[0].x) - j00 * t.x2) / t.y2, j11 = ((q[2].y - q[0].y) - j10 * t.x2) / t.y2;
+    double w00, w01, w11;
+    slim_2x2(j00, j01, j10, j11, rc, rs, w00, w01, w11);
+    S[0] = w00 * w00 + w01 * w01;
+    S[1] = w00 * w01 + w01 * w11;
+    S[2] = w01 * w01 + w11 * w11;
+}
+
+template <Op OP>
+__global__ void __launch_bounds__(KB, 1) k_slim(uva_batch b, uva_solve_params prm, double* scratch) {
+    __shared__ double redd[2 * 4 * 32];
+    __shared__ float redf[2 * 4 * 32];
+    __shared__ int redi[2 * 32];
+    Team<KB> tm{static_cast<int>(threadIdx.x), 0, 0, redd, redf, redi, nullptr, nullptr, nullptr, nullptr,
+                nullptr, nullptr, nullptr, 0, nullptr, 0, nullptr, 0};
+    const int tid = tm.tid;
+    double2* U = reinterpret_cast<double2*>(b.U);
+    double2* X = reinterpret_cast<double2*>(b.x64);   // trial solution (by vertex)
+    double2* Bv = reinterpret_cast<double2*>(b.b64);  // right-hand side
+    double* Sbuf = scratch;                               // 3t: W^2 per triangle
+    double2* Rv = reinterpret_cast<double2*>(scratch + ((3 * static_cast<size_t>(b.t) + 1) & ~static_cast<size_t>(1)));   // residual
+    double2* Pv = Rv + b.n;
+    double2* Qv = Pv + b.n;
+    double2* RCS = Qv + b.n;                              // t: rotation (c, s) per triangle
+    for (int isl = blockIdx.x; isl < b.nc; isl += gridDim.x) {
+        const int v0 = b.vofs[isl], n = b.vofs[isl + 1] - v0, f0 = b.tofs[isl], nt = b.tofs[isl + 1] - f0;
+        uva_island_status st{};
+        // energy at the start; a non-finite start is returned unchanged (param.py:418-419)
+        double acc[2] = {0.0, 0.0};
+        for (int f = f0 + tid; f < f0 + nt; f += KB) {
+            const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
+            const double2 q[3] = {U[v0 + tv.x], U[v0 + tv.y], U[v0 + tv.z]};
+            const SlimTri t = slim_tri(b, f);
+            acc[0] += sd_energy_tri(t, q);
+            acc[1] += t.area;
+        }
+        team_sum<KB, 2>(tm, acc, tm.redd);
+        double prev = acc[0];
+        const double reg = 1e-12 * acc[1];
+        st.energy = prev;
+        if (!isfinite(prev)) {
+            st.flags |= UVA_ST_NONFINITE;
+            if (tid == 0) b.status[isl] = st;
+            __syncthreads();
+            continue;
+        }
+        for (int it = 0; it < prm.iters; ++it) {
+            // ---- local step
+            for (int f = f0 + tid; f < f0 + nt; f += KB) {
+                const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
+                const double2 q[3] = {U[v0 + tv.x], U[v0 + tv.y], U[v0 + tv.z]};
+                double S[3], rc, rs;
+                slim_local(slim_tri(b, f), q, S, rc, rs);
+                Sbuf[3 * f] = S[0]; Sbuf[3 * f + 1] = S[1]; Sbuf[3 * f + 2] = S[2];
+                RCS[f] = make_double2(rc, rs);
+            }
+            __syncthreads();
+            // ---- right-hand side A^T b + reg x0, Jacobi diagonal, r0 = rhs - M x0
+            // per vertex over its incident corners (vt), in corner order
+            auto apply = [&](int v, const double2* x, bool with_rhs, double2& mx, double2& rhs, double2& dg) {
+                mx = make_double2(0.0, 0.0); rhs = make_double2(0.0, 0.0); dg = make_double2(0.0, 0.0);
+                const int pe = __ldg(b.vt_ptr + v + 1);
+                for (int pq = __ldg(b.vt_ptr + v); pq < pe; ++pq) {
+                    const int c = __ldg(b.vt + pq);
+                    const int f = c / 3, k = c - 3 * f;
+                    const SlimTri t = slim_tri(b, f);
+                    if (!t.live) continue;
+                    const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
+                    const double2 q[3] = {x[v0 + tv.x], x[v0 + tv.y], x[v0 + tv.z]};
+                    double J[2][2];
+                    slim_jac(t, q, J);
+                    const double s00 = Sbuf[3 * f], s01 = Sbuf[3 * f + 1], s11 = Sbuf[3 * f + 2];
+                    const double gk0 = t.g0[k], gk1 = t.g1[k];
+                    // (S J G)_{r,k} = sum_c (S J)_{r,c} G_{c,k}
+                    const double sj00 = s00 * J[0][0] + s01 * J[1][0], sj01 = s00 * J[0][1] + s01 * J[1][1];
+                    const double sj10 = s01 * J[0][0] + s11 * J[1][0], sj11 = s01 * J[0][1] + s11 * J[1][1];
+                    mx.x += t.area * (sj00 * gk0 + sj01 * gk1);
+                    mx.y += t.area * (sj10 * gk0 + sj11 * gk1);
+                    if (with_rhs) {
+                        const double2 r = RCS[f];   // R = [[c, -s], [s, c]]
+                        const double sr00 = s00 * r.x + s01 * r.y, sr01 = -s00 * r.y + s01 * r.x;
+                        const double sr10 = s01 * r.x + s11 * r.y, sr11 = -s01 * r.y + s11 * r.x;
+                        rhs.x += t.area * (sr00 * gk0 + sr01 * gk1);
+                        rhs.y += t.area * (sr10 * gk0 + sr11 * gk1);
+                        const double gg = gk0 * gk0 + gk1 * gk1;
+                        dg.x += t.area * s00 * gg;
+                        dg.y += t.area * s11 * gg;
+                    }
+                }
+                mx.x += reg * x[v].x; mx.y += reg * x[v].y;
+            };
+            double bb[2] = {0.0, 0.0};   // ||rhs||^2, ||r0||^2
+            double rz = 0.0;
+            for (int i = tid; i < n; i += KB) {
+                const int v = v0 + i;
+                double2 mx, rhs, dg;
+                apply(v, U, true, mx, rhs, dg);
+                rhs.x += reg * U[v].x; rhs.y += reg * U[v].y;
+                dg.x += reg; dg.y += reg;
+                Bv[v] = make_double2(1.0 / dg.x, 1.0 / dg.y);   // Jacobi (inverse diagonal)
+                const double2 r = make_double2(rhs.x - mx.x, rhs.y - mx.y);
+                Rv[v] = r;
+                X[v] = U[v];
+                const double2 z = make_double2(r.x / dg.x, r.y / dg.y);
+                Pv[v] = z;
+                bb[0] += rhs.x * rhs.x + rhs.y * rhs.y;
+                bb[1] += r.x * r.x + r.y * r.y;
+                rz += r.x * z.x + r.y * z.y;
+            }
+            double tot[3] = {bb[0], bb[1], rz};
+            team_sum<KB, 3>(tm, tot, tm.redd);
+            const double thr2 = prm.inner_eta * prm.inner_eta * tot[0];
+            double rr = tot[1];
+            rz = tot[2];
+            int cg = 0;
+            while (rr >= thr2 && cg < prm.max_inner && rz > 0.0) {   // scipy: stop once ||r|| < rtol ||b||
+                double pq = 0.0;
+                for (int i = tid; i < n; i += KB) {
+                    const int v = v0 + i;
+                    double2 mx, rhs, dg;
+                    apply(v, Pv, false, mx, rhs, dg);
+                    Qv[v] = mx;
+                    pq += Pv[v].x * mx.x + Pv[v].y * mx.y;
+                }
+                double t1[1] = {pq};
+                team_sum<KB, 1>(tm, t1, tm.redd);
+                if (!(t1[0] > 0.0)) break;
+                const double alpha = rz / t1[0];
+                double t2[2] = {0.0, 0.0};
+                for (int i = tid; i < n; i += KB) {
+                    const int v = v0 + i;
+                    const double2 p = Pv[v], q = Qv[v], m = Bv[v];
+                    double2 x = X[v], r = Rv[v];
+                    x.x += alpha * p.x; x.y += alpha * p.y;
+                    r.x -= alpha * q.x; r.y -= alpha * q.y;
+                    X[v] = x; Rv[v] = r;
+                    t2[0] += r.x * r.x + r.y * r.y;
+                    t2[1] += r.x * r.x * m.x + r.y * r.y * m.y;
+                }
+                team_sum<KB, 2>(tm, t2, tm.redd);
+                ++cg;
+                rr = t2[0];
+                if (rr < thr2) break;
+                const double beta = t2[1] / rz;
+                rz = t2[1];
+                for (int i = tid; i < n; i += KB) {
+                    const int v = v0 + i;
+                    const double2 r = Rv[v], m = Bv[v], p = Pv[v];
+                    Pv[v] = make_double2(r.x * m.x + beta * p.x, r.y * m.y + beta * p.y);
+                }
+                __syncthreads();
+            }
+            st.cg_iters += cg;
+            st.resid[0] = st.resid[1] = sqrt(rr / fmax(tot[0], 1e-300));
+            if (cg >= prm.max_inner) st.flags |= UVA_ST_MAXITER;
+            __syncthreads();
+            // ---- flip-safe step and energy backtracking (param.py:436-454)
+            double tmin = 1e30;
+            for (int f = f0 + tid; f < f0 + nt; f += KB) {
+                const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
+                const double2 u0 = U[v0 + tv.x], u1 = U[v0 + tv.y], u2 = U[v0 + tv.z];
+                const double2 a0 = X[v0 + tv.x], a1 = X[v0 + tv.y], a2 = X[v0 + tv.z];
+                const double ux1 = u1.x - u0.x, uy1 = u1.y - u0.y, ux2 = u2.x - u0.x, uy2 = u2.y - u0.y;
+                const double dx1 = (a1.x - u1.x) - (a0.x - u0.x), dy1 = (a1.y - u1.y) - (a0.y - u0.y);
+                const double dx2 = (a2.x - u2.x) - (a0.x - u0.x), dy2 = (a2.y - u2.y) - (a0.y - u0.y);
+                const double C = ux1 * uy2 - ux2 * uy1;
+                const double B = ux1 * dy2 + dx1 * uy2 - ux2 * dy1 - dx2 * uy1;
+                const double A = dx1 * dy2 - dx2 * dy1;
+                if (!(C > 0.0)) continue;
+                if (A == 0.0 || fabs(A) < 1e-30 * fmax(fabs(B), 1e-300)) {
+                    if (B < 0.0) tmin = fmin(tmin, -C / B);
+                    continue;
+                }
+                const double disc = B * B - 4.0 * A * C;
+                if (disc < 0.0) continue;
+                const double sq = sqrt(disc);
+                const double r1 = (-B - sq) / (2.0 * A), r2 = (-B + sq) / (2.0 * A);
+                if (r1 > 0.0) tmin = fmin(tmin, r1);
+                if (r2 > 0.0) tmin = fmin(tmin, r2);
+            }
+            tmin = team_min(tm, tmin);
+            double step = fmin(1.0, 0.9 * tmin);
+            double e = 0.0;
+            for (int k = 0; k <= 12; ++k) {
+                double ev[1] = {0.0};
+                for (int f = f0 + tid; f < f0 + nt; f += KB) {
+                    const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
+                    const int vv[3] = {v0 + tv.x, v0 + tv.y, v0 + tv.z};
+                    double2 q[3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                        q[c] = make_double2(U[vv[c]].x + step * (X[vv[c]].x - U[vv[c]].x),
+                                            U[vv[c]].y + step * (X[vv[c]].y - U[vv[c]].y));
+                    ev[0] += sd_energy_tri(slim_tri(b, f), q);
+                }
+                team_sum<KB, 1>(tm, ev, tm.redd);
+                e = ev[0];
+                if ((isfinite(e) && e <= prev) || k == 12) break;
+                step *= 0.5;
+            }
+            st.outer_iters = it + 1;
+            if (!isfinite(e) || e > prev) break;   // no acceptable step: keep U
+            for (int i = tid; i < n; i += KB) {
+                const int v = v0 + i;
+                const double2 u = U[v], x = X[v];
+                U[v] = make_double2(u.x + step * (x.x - u.x), u.y + step * (x.y - u.y));
+            }
+            __syncthreads();
+            st.step = step;
+            const bool stop = fabs(prev - e) <= prm.energy_tol * prev;
+            prev = e;
+            st.energy = e;
+            if (stop) break;
+        }
+        if (tid == 0) b.status[isl] = st;
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 extern "C" int uva_batch_setup(uva_batch* b, void* stream) {
@@ -1405,6 +1684,25 @@ extern "C" int uva_arap(uva_batch* b, const uva_solve_params* prm, void* stream)
     if (!check_batch(b) || !prm) { uva_set_error("uva_arap: bad arguments"); return UVA_E_ARG; }
     if (b->nc == 0 || prm->iters <= 0) return UVA_OK;
     return launch_islands<OP_ARAP>(b, prm, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int uva_slim_scratch_bytes(const uva_batch* b, int64_t* bytes) {
+    if (!b || !bytes) { uva_set_error("uva_slim_scratch_bytes: null argument"); return UVA_E_ARG; }
+    *bytes = static_cast<int64_t>(sizeof(double)) *
+             (3 * static_cast<int64_t>(b->t) + 1 + 6 * static_cast<int64_t>(b->n) + 2 * static_cast<int64_t>(b->t));
+    return UVA_OK;
+}
+
+extern "C" int uva_slim(uva_batch* b, const uva_solve_params* prm, double* scratch, void* stream) {
+    if (!check_batch(b) || !prm || !scratch || !b->status || b->semantics != UVA_SEM_PARAM) {
+        uva_set_error("uva_slim: bad arguments (scratch, status and PARAM semantics are required)");
+        return UVA_E_ARG;
+    }
+    if (b->nc == 0 || prm->iters <= 0) return UVA_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_slim<OP_ARAP><<<std::min(sm_count(), b->nc), KB, 0, s>>>(*b, *prm, scratch);
+    UVA_CHECK_LAUNCH("uva_slim");
+    return UVA_OK;
 }
 
 extern "C" int uva_lscm(uva_batch* b, const uva_solve_params* prm, void* stream) {

@@ -223,6 +223,15 @@ class DeviceBatch:
         prm = self.params("arap", iters=iters, line_search=line_search, energy_tol=energy_tol, **kw)
         check(_lib.lib().uva_arap(C.byref(self.desc), C.byref(prm), self._stream()), "uva_arap")
 
+    def slim(self, iters=10, energy_tol=1e-5, cg_tol=1e-13, cg_max=50000):
+        """SLIM iterations of every island (uva_slim; PARAM semantics)."""
+        nb = C.c_int64()
+        check(_lib.lib().uva_slim_scratch_bytes(C.byref(self.desc), C.byref(nb)), "uva_slim_scratch_bytes")
+        scratch = torch.empty(max(int(nb.value) // 8, 2), dtype=torch.float64, device=self.dev)
+        prm = self.params("arap", iters=iters, line_search=True, energy_tol=energy_tol, inner_eta=cg_tol,
+                          max_inner=cg_max)
+        check(_lib.lib().uva_slim(C.byref(self.desc), C.byref(prm), ptr(scratch), self._stream()), "uva_slim")
+
     def step_graph(self, setup=True, lscm=True, arap_iters=20, line_search=True, lscm_kw=None, arap_kw=None):
         """Capture setup + LSCM + ARAP (any subset) into one CUDA graph."""
         return StepGraph(self, setup, lscm, arap_iters, line_search, lscm_kw or {}, arap_kw or {})

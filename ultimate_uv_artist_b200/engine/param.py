@@ -18,8 +18,9 @@ runs in the uva_b200 CUDA kernels:
 ``cot_laplacian`` returns a scipy matrix and ``boundary_edges_oriented`` /
 ``boundary_loops`` / ``_far_pair`` return host index arrays, as the reference
 does; they are topology bookkeeping. ``refine(method="slim")`` (symmetric
-Dirichlet SLIM, used by the "artist" profile) is not part of this build and
-raises NotImplementedError.
+Dirichlet SLIM, used by the "artist" profile) runs ``uva_slim``: the SLIM
+normal equations applied without forming them, FP64 CG, the reference's
+flip-safe step and energy backtracking.
 """
 from __future__ import annotations
 
@@ -277,11 +278,13 @@ def tutte(P, T):
 
 # ------------------------------------------------------------------ local step kernels
 def _arap_rotations(U, T, X, cots, mode, sd_weights):
-    """Per-triangle target rotation (engine/param.py:206-256, mode 0); the
-    weight matrices are identities."""
-    if mode != 0:
-        raise NotImplementedError("SLIM weights (mode 1) are not part of this build")
+    """Per-triangle target rotation and weight matrices (engine/param.py:206-256):
+    mode 0 the closest rotation and identity weights, mode 1 the SVD-based
+    rotation and the SLIM symmetric-Dirichlet weights."""
     T = np.asarray(T, np.int64).reshape(-1, 3)
+    if mode == 1:
+        R, Wm = _op(OP_ROTATIONS, T, len(U), (len(T), 2, 2), arg=1, U=U, X=X, out2_shape=(len(T), 2, 2))
+        return R.cpu().numpy(), Wm.cpu().numpy()
     R, _ = _op(OP_ROTATIONS, T, len(U), (len(T), 2, 2), U=U, X=X)
     Wm = np.broadcast_to(np.eye(2), (len(T), 2, 2)).copy()
     return R.cpu().numpy(), Wm
@@ -311,8 +314,18 @@ def _arap_rhs(n, T, X, cots, R):
 def refine(P, T, U, iters=10, method="arap", X=None, area=None, cots=None, solver=None, line_search=True, tol=1e-5,
            pin=None):
     """Local-global refinement (engine/param.py:379-454). Returns (U, solver)."""
+    if method == "slim":
+        # SLIM (param.py:415-454): the reference solves each global step
+        # exactly when 2n <= DIRECT_LIMIT, else CG rtol 1e-6, 500 iterations
+        ch = _chart(P, T, solver)
+        db = ch.db
+        db.U[:db.n].copy_(torch.from_numpy(np.asarray(U, np.float64).reshape(-1, 2)))
+        direct = 2 * db.n <= DIRECT_LIMIT
+        db.slim(iters=int(iters), energy_tol=float(tol), cg_tol=1e-12 if direct else 1e-6,
+                cg_max=50000 if direct else 500)
+        return db.uvs(), None
     if method != "arap":
-        raise NotImplementedError("refine(method='slim') is not part of this build")
+        raise ValueError(f"unknown refine method {method!r}")
     ch = _chart(P, T, solver)
     db = ch.db
     db.U[:db.n].copy_(torch.from_numpy(np.asarray(U, np.float64).reshape(-1, 2)))
