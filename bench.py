@@ -479,10 +479,8 @@ def main():
     full, comp = arap_bytes(n, t, nnz, st)
     units = float(tris * args.iters)
     if ws > 1:
-        tt = torch.tensor([ms, units], dtype=torch.float64, device=dev)
-        mx = tt.clone(); dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = tt.clone(); dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms_max, units_all = float(mx[0]), float(sm[1])
+        from ultimate_uv_artist_b200 import shard
+        ms_max, units_all = shard.reduce_step(ms, units, device=dev)
     else:
         ms_max, units_all = ms, units
     value = units_all / (ms_max / 1e3)
