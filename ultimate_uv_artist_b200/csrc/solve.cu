@@ -1207,8 +1207,8 @@ constexpr size_t kCoarseSmem = sizeof(double) * kCoarseSmemN * kCoarseSmemN;   /
 __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
     extern __shared__ double wsm[];
     __shared__ double colk[512];
-    const int isl = blockIdx.x;
-    if (isl >= b.nc) return;
+    if (static_cast<int>(blockIdx.x) >= b.nc) return;
+    const int isl = b.order[blockIdx.x];   // largest islands first (b.order is by size)
     const int agg = b.agg_rows[isl];
     if (agg <= 0) return;
     const int v0 = b.vofs[isl], n = b.vofs[isl + 1] - v0, s0 = b.sofs[isl];
@@ -1217,8 +1217,9 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
     const int2* cw = reinterpret_cast<const int2*>(b.slot_cw);
     auto row_slots_l = [&](int r, int& q0, int& width) {
         const int s = s0 + (r >> 5);
-        q0 = b.slice_ptr[s] + (r & 31);
-        width = (b.slice_ptr[s + 1] - b.slice_ptr[s]) >> 5;
+        const int p0s = __ldg(b.slice_ptr + s), p1s = __ldg(b.slice_ptr + s + 1);
+        q0 = p0s + (r & 31);
+        width = (p1s - p0s) >> 5;
     };
     auto work = [&](int N) { return N <= kCoarseSmemN ? wsm : b.coarse_work + 4 * static_cast<size_t>(co); };
     // ---- ARAP
@@ -1232,12 +1233,17 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
         for (int r = a * agg; r < min(n, (a + 1) * agg); ++r) {
             int q0, width;
             row_slots_l(r, q0, width);
-            for (int k = 0; k < width; ++k) {
-                const int2 sl = cw[q0 + 32 * k];
-                const double w = static_cast<double>(__int_as_float(sl.y));
-                if (w == 0.0) continue;
-                const int c = slot_row(sl.x) / agg;
-                if (c != a) { dsum += w; Wa[c] -= w; }
+            for (int k = 0; k < width; k += 4) {   // widths are multiples of 4
+                int2 s4[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) s4[u] = __ldg(cw + q0 + 32 * (k + u));
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const double w = static_cast<double>(__int_as_float(s4[u].y));
+                    if (w == 0.0) continue;
+                    const int c = slot_row(s4[u].x) / agg;
+                    if (c != a) { dsum += w; Wa[c] -= w; }
+                }
             }
         }
         if (a == pin_agg) dsum += b.wpin[isl];
@@ -1264,20 +1270,26 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
             if (r == p0 || r == p1) continue;
             int q0, width;
             row_slots_l(r, q0, width);
-            for (int k = 0; k < width; ++k) {
-                const int2 sl = cw[q0 + 32 * k];
-                const double w = static_cast<double>(__int_as_float(sl.y));
-                const double cc = 0.5 * static_cast<double>(slot_c2(sl.x));
-                if (w == 0.0 && cc == 0.0) continue;
-                const int col = slot_row(sl.x);
-                const bool pinned_nb = col == p0 || col == p1;   // no coarse coupling
-                const int c = col / aggl;
-                if (pinned_nb || c != a) dsum += w;
-                if (pinned_nb) continue;
-                if (c != a) { Wu[2 * c] -= w; Wv[2 * c + 1] -= w; }
-                if (cc != 0.0) {
-                    if (c == a) { cuv += cc; cvu -= cc; }
-                    else { Wu[2 * c + 1] += cc; Wv[2 * c] -= cc; }
+            for (int k = 0; k < width; k += 4) {
+                int2 s4[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) s4[u] = __ldg(cw + q0 + 32 * (k + u));
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int2 sl = s4[u];
+                    const double w = static_cast<double>(__int_as_float(sl.y));
+                    const double cc = 0.5 * static_cast<double>(slot_c2(sl.x));
+                    if (w == 0.0 && cc == 0.0) continue;
+                    const int col = slot_row(sl.x);
+                    const bool pinned_nb = col == p0 || col == p1;   // no coarse coupling
+                    const int c = col / aggl;
+                    if (pinned_nb || c != a) dsum += w;
+                    if (pinned_nb) continue;
+                    if (c != a) { Wu[2 * c] -= w; Wv[2 * c + 1] -= w; }
+                    if (cc != 0.0) {
+                        if (c == a) { cuv += cc; cvu -= cc; }
+                        else { Wu[2 * c + 1] += cc; Wv[2 * c] -= cc; }
+                    }
                 }
             }
         }
