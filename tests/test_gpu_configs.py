@@ -1,0 +1,78 @@
+"""The benchmark's other configurations as parity cases on the GPU path.
+
+* Config 1, full size: one 50x50-grid hemisphere patch (4,802 triangles,
+  N(0, 0.01) jitter), LSCM with the far-pair pins and 10 ARAP iterations
+  (param semantics), against the FP64 oracle; then the exact validation
+  report against the oracle's.
+* Config 5, reduced: a displaced sphere cut into k-means charts, the disk
+  charts kept, batched LSCM + 20 ARAP iterations (gpu.Batch semantics)
+  against the FP64 oracle, then the charts shelf-packed and validated
+  bit-exactly against the oracle (the full 5M-triangle case only changes
+  the sizes).
+"""
+import numpy as np
+import pytest
+
+from oracle import arap as O
+from oracle import validate as OV
+
+pytestmark = pytest.mark.gpu
+
+UV_TOL = 1e-5
+
+
+def _validate_both(V, F, UV, atlas, padding):
+    from ultimate_uv_artist_b200.engine import validate as GV
+    rep, problems = GV.validate_uvs(V, F, UV, atlas=atlas, padding=padding)
+    ref, rprob, _ = OV.validate_uvs(V, F, UV, atlas=atlas, padding=padding)
+    for k, v in ref.items():
+        if isinstance(v, (int, float, bool, np.integer, np.floating)) and k in rep:
+            a, b = float(rep[k]), float(v)
+            assert a == b or (np.isnan(a) and np.isnan(b)), (k, rep[k], v)
+    assert np.array_equal(problems, rprob)
+    return rep
+
+
+def test_config1_hemisphere_full_size(cuda):
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.engine import param as Pm
+    V, F = synth.hemisphere_patch(seed=1000, n=50, jitter=0.01)
+    P = V.astype(np.float64)
+    assert len(F) == 4802
+    U0 = Pm.lscm(P, F)
+    U0r = O.lscm(P, F)
+    ext = np.ptp(U0r, 0).max()
+    assert np.abs(U0 - U0r).max() / ext < UV_TOL
+    U1, _ = Pm.refine(P, F, U0r, iters=10, method="arap", line_search=True, tol=0.0)
+    U1r = O.refine_arap(P, F, U0r, iters=10, line_search=True, tol=0.0)
+    assert np.abs(U1 - U1r).max() / np.ptp(U1r, 0).max() < UV_TOL
+    # validation of the chart scaled into the unit square
+    lo, hi = U1r.min(0), U1r.max(0)
+    UV = ((U1 - lo) / (hi - lo).max() * 0.9 + 0.05).astype(np.float32)
+    _validate_both(V, F, UV, 1024, 4)
+
+
+def test_config5_dense_scan_reduced(cuda):
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.engine import gpu
+    V, F = synth.noisy_sphere(seed=5000, tris=60000)
+    charts = synth.disk_charts(V, F, synth.kmeans_charts(V, F, k=60, seed=5001), min_tris=30)
+    assert len(charts) >= 20
+    b = gpu.Batch([(p, t, None) for p, t in charts])
+    b.lscm()
+    b.arap(20, line_search=True)
+    st = b.status()
+    assert (st["resid"] <= 2e-7 * 1.001).all() and (st["flags"] & 3 == 0).all()
+    U = b.chart_uvs()
+    items = [(p.astype(np.float64), t, O.lscm(p.astype(np.float64), t)) for p, t in charts]
+    ref = O.BatchRef(items)
+    ref.arap(20, line_search=True)
+    assert O.uv_rel_error(np.concatenate(U), ref.U, ref.offsets) < UV_TOL
+    # shelf-pack the charts and validate the atlas bit-exactly
+    packed = synth.shelf_pack(U, atlas=2048, padding=4)
+    offs = np.cumsum([0] + [len(p) for p, _ in charts])
+    Vall = np.concatenate([p for p, _ in charts]).astype(np.float32)
+    Fall = np.concatenate([t + o for (_, t), o in zip(charts, offs[:-1])])
+    UVall = np.concatenate(packed).astype(np.float32)
+    rep = _validate_both(Vall, Fall, UVall, 2048, 4)
+    assert rep["islands"] == len(charts)

@@ -314,3 +314,58 @@ def kmeans_charts(V, F, k=3000, seed=5001, iters=8):
     order = np.argsort(comp, kind="stable")
     cuts = np.flatnonzero(np.diff(comp[order])) + 1
     return np.split(order, cuts)
+
+
+def disk_charts(V, F, charts, min_tris=20):
+    """(P, T) of every chart (face-index array) that is a topological disk:
+    one boundary loop and Euler characteristic 1, at least ``min_tris``
+    triangles (the dense-scan workload keeps disks only)."""
+    out = []
+    for fidx in charts:
+        if len(fidx) < min_tris:
+            continue
+        P, T = _compact(V, F[fidx])
+        a = np.concatenate([T[:, 0], T[:, 1], T[:, 2]]); b = np.concatenate([T[:, 1], T[:, 2], T[:, 0]])
+        key = np.minimum(a, b) * len(P) + np.maximum(a, b)
+        uk, cnt = np.unique(key, return_counts=True)
+        if len(P) - len(uk) + len(T) != 1 or (cnt > 2).any():
+            continue
+        # boundary half-edges (edges used once) must form a single loop
+        once = np.isin(key, uk[cnt == 1])
+        ba, bb = a[once], b[once]
+        if len(ba) == 0:
+            continue
+        nxt = dict(zip(ba.tolist(), bb.tolist()))
+        if len(nxt) != len(ba):
+            continue
+        start = int(ba[0]); v = start; steps = 0
+        while True:
+            v = nxt.get(v, -1); steps += 1
+            if v == start or v < 0 or steps > len(ba):
+                break
+        if v == start and steps == len(ba):
+            out.append((P.astype(np.float32), T))
+    return out
+
+
+def shelf_pack(uvs, atlas=4096, padding=4, fill=0.6):
+    """Shelf packing of per-chart UV arrays into [0, 1]^2 with ``padding``
+    texels between charts (test data for validation; not a product packer)."""
+    lo = [u.min(0) for u in uvs]
+    ext = np.array([u.max(0) - l for u, l in zip(uvs, lo)])
+    pad = padding / atlas
+    total = float(((ext[:, 0] + pad) * (ext[:, 1] + pad)).sum())
+    scale = np.sqrt(fill / max(total, 1e-30))
+    for _ in range(20):
+        x = pad; y = pad; row_h = 0.0
+        place = np.zeros((len(uvs), 2))
+        for i in np.argsort(-ext[:, 1], kind="stable"):
+            w, h = ext[i] * scale
+            if x + w + pad > 1.0:
+                x = pad; y += row_h + pad; row_h = 0.0
+            place[i] = (x, y)
+            x += w + pad; row_h = max(row_h, h)
+        if y + row_h + pad <= 1.0:
+            return [(u - l) * scale + place[i] for i, (u, l) in enumerate(zip(uvs, lo))]
+        scale *= 0.9
+    raise RuntimeError("shelf_pack: charts do not fit")
