@@ -42,6 +42,21 @@ def require_cuda(dev=None):
     return d
 
 
+def host_empty(shape, dtype):
+    """numpy array in page-locked host memory when CUDA is present (torch's
+    caching host allocator: reused across batches), so uploads are plain
+    asynchronous DMA; ordinary memory otherwise."""
+    if torch.cuda.is_available():
+        n = int(np.prod(shape)) if np.ndim(shape) else int(shape)
+        t = torch.empty(max(n, 1), dtype=_TORCH_OF[np.dtype(dtype)], pin_memory=True)
+        return t.numpy()[:n].reshape(shape)
+    return np.empty(shape, dtype)
+
+
+_TORCH_OF = {np.dtype(np.int32): torch.int32, np.dtype(np.int64): torch.int64, np.dtype(np.float32): torch.float32,
+             np.dtype(np.float64): torch.float64, np.dtype(np.uint8): torch.uint8}
+
+
 class Plan:
     """Host topology plan (wraps uva_plan_create / uva_plan_export)."""
 
@@ -60,15 +75,15 @@ class Plan:
             self.nc, self.n, self.t, self.E = int(sz[0]), int(sz[1]), int(sz[2]), int(sz[3])
             self.nslices, self.nslots, self.nbverts, self.maxrows = int(sz[4]), int(sz[5]), int(sz[6]), int(sz[7])
             self.ncoarse = int(sz[8])
-            self.tri4 = np.empty((self.t, 4), np.int32)
-            self.tri_edge = np.empty((self.t, 3), np.int32)
+            self.tri4 = host_empty((self.t, 4), np.int32)
+            self.tri_edge = host_empty((self.t, 3), np.int32)
             self.sofs = np.empty(nc + 1, np.int32)
-            self.slice_ptr = np.empty(self.nslices + 1, np.int32)
-            self.slot_col = np.empty(self.nslots, np.int32)
-            self.slot_edge = np.empty(self.nslots, np.int32)
-            self.slot_c = np.empty(self.nslots, np.float32)
-            self.vt_ptr = np.empty(self.n + 1, np.int32)
-            self.vt = np.empty(3 * self.t, np.int32)
+            self.slice_ptr = host_empty(self.nslices + 1, np.int32)
+            self.slot_col = host_empty(self.nslots, np.int32)
+            self.slot_edge = host_empty(self.nslots, np.int32)
+            self.slot_c = host_empty(self.nslots, np.float32)
+            self.vt_ptr = host_empty(self.n + 1, np.int32)
+            self.vt = host_empty(3 * self.t, np.int32)
             self.vflags = np.empty(self.n, np.uint8)
             self.bofs = np.empty(nc + 1, np.int32)
             self.bverts = np.empty(max(self.nbverts, 1), np.int32)
@@ -102,9 +117,10 @@ def concat_charts(charts, with_uv=True):
     for i, ch in enumerate(charts):
         vofs[i + 1] = vofs[i] + len(ch[0])
         tofs[i + 1] = tofs[i] + len(ch[1])
-    P = np.empty((int(vofs[-1]), 3), np.float64)
+    P = host_empty((int(vofs[-1]), 3), np.float64)
     T = np.empty((int(tofs[-1]), 3), np.int64)
-    U = np.zeros((int(vofs[-1]), 2), np.float64)
+    U = host_empty((int(vofs[-1]), 2), np.float64)
+    U[:] = 0.0
     for i, ch in enumerate(charts):
         P[vofs[i]:vofs[i + 1]] = np.asarray(ch[0], np.float64).reshape(-1, 3)
         T[tofs[i]:tofs[i + 1]] = np.asarray(ch[1], np.int64).reshape(-1, 3)
@@ -130,7 +146,10 @@ class DeviceBatch:
             t = torch.from_numpy(np.ascontiguousarray(a))
             if t.numel() == 0:
                 t = torch.zeros(1, dtype=t.dtype)
-            return t.to(d, non_blocking=False) if dtype is None else t.to(d, dtype)
+            # page-locked sources (the plan's arrays) copy asynchronously on
+            # the current stream; the plan keeps them alive
+            nb = t.is_pinned()
+            return t.to(d, non_blocking=nb) if dtype is None else t.to(d, dtype, non_blocking=nb)
 
         # topology
         self.vofs = up(plan.vofs); self.tofs = up(plan.tofs); self.sofs = up(plan.sofs)
@@ -144,6 +163,9 @@ class DeviceBatch:
         # geometry
         n, t, nc = max(self.n, 1), max(self.t, 1), max(self.nc, 1)
         f64, f32 = torch.float64, torch.float32
+        # asynchronous uploads read page-locked host memory until they finish:
+        # the batch keeps its host sources alive (the plan holds the rest)
+        self._host_src = (P, U)
         self.P = up(np.asarray(P, np.float64).reshape(-1, 3)) if self.n else torch.zeros((1, 3), dtype=f64, device=d)
         self.frame = torch.empty((t, 4), dtype=f64, device=d)
         self.wtri = torch.empty((t, 4), dtype=f64, device=d)
