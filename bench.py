@@ -548,6 +548,16 @@ def main():
                "sample": f"{len(sample)} size-stratified islands of {len(islands)} ({stris} triangles), "
                          f"LSCM + {args.iters} ARAP iterations per island (param.lscm + param.refine, "
                          f"exact LU), {dt:.1f} s"}
+        if val is not None:   # the validation workload's CPU time (oracle port, one thread)
+            from ultimate_uv_artist_b200 import synth as _synth
+            Vv, Fv, UVv, _ = _synth.validation_atlas(seed=3000)
+            vs, vrep = cpu_baseline.time_validation(Vv, Fv, UVv)
+            cpu["validation"] = {"seconds": vs, "cores": 1, "kind": "port",
+                                 "pairs_per_s": val["pairs_aabb"] / vs,
+                                 "same_report": all(float(vrep[k]) == float(val[k2]) for k, k2 in
+                                                    (("overlapping_triangles_exact", "overlapping_triangles"),
+                                                     ("flipped_triangles", "flipped"),
+                                                     ("mirrored_islands", "mirrored")))}
         err, ni, nt_ = cpu_baseline.uv_error_batch(islands, our_uvs, args.iters)
         cpu["uv_error_check"] = {"max_rel_uv_error": err, "islands": ni, "triangles": nt_,
                                  "against": "FP64 oracle of LSCM + gpu.Batch.arap with exact solves"}

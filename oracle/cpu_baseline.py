@@ -87,3 +87,12 @@ def uv_error_batch(islands, uvs, iters, count=12):
     U = np.concatenate([uvs[i] for i in pick])
     off = np.cumsum([0] + [len(c[0]) for c in charts])
     return O.uv_rel_error(U, Uref, off), len(pick), int(sum(len(c[1]) for c in charts))
+
+
+def time_validation(V, F, UV, atlas=4096, padding=4):
+    """Seconds of the oracle's validate_uvs (numpy + the C restatement of the
+    reference's serial loops, one thread) on an atlas, and its report."""
+    from oracle import validate as OV
+    t0 = time.perf_counter()
+    rep, _, _ = OV.validate_uvs(V, F, UV, atlas=atlas, padding=padding)
+    return time.perf_counter() - t0, rep
