@@ -495,8 +495,8 @@ def main():
             bb.db.arap(iters=args.iters, line_search=True)
             return bb, bb.chart_uvs()
 
-        for _ in range(2):   # untimed warm-up (page-locked host allocator caches, first touch)
-            e2e_step()
+        for _ in range(2):   # untimed warm-up, same pattern as the timed loop (the previous
+            bb, Us = e2e_step()   # batch is alive while the next is built): page-locked host caches
         torch.cuda.synchronize()
         w0 = time.perf_counter()
         for _ in range(args.e2e_steps):
