@@ -145,3 +145,59 @@ def test_step_graph_replays_the_direct_calls(cuda):
     assert np.array_equal(st["cg_iters"], st_direct["cg_iters"])
     assert (st["resid"] <= 1e-6 + 1e-12).all()
     g.close()
+
+
+def test_large_island_global_memory_class_vs_oracle(cuda):
+    """An island above the shared-memory classes (n > 8192 rows: CG vectors
+    in L2, 128-row or larger aggregates) next to small ones: LSCM and 4 ARAP
+    iterations against the FP64 oracle."""
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.engine import gpu
+    rng = np.random.default_rng(8)
+    isl = [synth.disk_patch(rng, 60000, amp=0.3), synth.disk_patch(rng, 300), synth.disk_patch(rng, 3000)]
+    assert len(isl[0][0]) > 8192
+    b = gpu.Batch([(p, t, None) for p, t in isl])
+    assert int(b.db.plan.class_ofs[1]) == 1          # one island in the global-memory class
+    b.lscm()
+    items = [(p.astype(np.float64), t, O.lscm(p.astype(np.float64), t)) for p, t in isl]
+    off = _offsets(items)
+    assert O.uv_rel_error(np.concatenate(b.chart_uvs()), np.concatenate([u for _, _, u in items]), off) < UV_TOL
+    ref = O.BatchRef(items)
+    b.U = torch.from_numpy(ref.U)
+    b.arap(4, line_search=True)
+    ref.arap(4, line_search=True)
+    assert (b.status()["resid"] <= 2e-7 * 1.001).all()
+    assert O.uv_rel_error(np.concatenate(b.chart_uvs()), ref.U, off) < UV_TOL
+
+
+def test_batch_edge_cases(cuda):
+    """Empty batch; one-triangle and degenerate charts; a chart with
+    non-finite UVs keeps them while its neighbours solve normally
+    (gpu.py:235-240)."""
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.engine import gpu
+    e = gpu.Batch([])
+    e.arap(3)
+    assert e.chart_uvs() == []
+    rng = np.random.default_rng(9)
+    P1 = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], float)
+    T1 = np.array([[0, 1, 2]])
+    Pd = np.array([[0, 0, 0], [1, 0, 0], [2, 0, 0], [0, 1, 0]], float)   # one zero-area triangle
+    Td = np.array([[0, 1, 2], [0, 1, 3]])
+    Pg, Tg = synth.disk_patch(rng, 400)
+    Pn, Tn = synth.disk_patch(rng, 200)
+    Ug = Pg[:, :2].astype(np.float64)
+    Un = np.full((len(Pn), 2), np.nan)
+    items = [(P1, T1, P1[:, :2].copy()), (Pd, Td, Pd[:, :2].copy()), (Pg, Tg, Ug), (Pn, Tn, Un)]
+    b = gpu.Batch(items)
+    b.arap(3, line_search=True)
+    st = b.status()
+    U = b.chart_uvs()
+    assert np.isnan(U[3]).all() and st["flags"][3] & 2
+    # the degenerate chart's lone vertex has an all-zero row: it keeps its UV
+    assert np.isfinite(U[1]).all() and np.array_equal(U[1][2], Pd[2, :2])
+    # the oracle's exact LU needs non-singular blocks: compare the other two
+    sel = [items[0], items[2]]
+    ref = O.BatchRef([(np.asarray(p, np.float64), t, u) for p, t, u in sel])
+    ref.arap(3, line_search=True)
+    assert O.uv_rel_error(np.concatenate([U[0], U[2]]), ref.U, _offsets(sel)) < UV_TOL
