@@ -890,6 +890,11 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
     if (tid == 0) *gst = uva_island_status{};
     bool use_ls = prm.line_search != 0;
     double prev_e = 0.0;
+    // CG start of each global step: the outer iterates converge about
+    // linearly, so the next solution is near U_k + theta (U_k - U_{k-1}),
+    // theta = |U_k - U_{k-1}| / |U_{k-1} - U_{k-2}| (clamped to [0, 1]);
+    // only the work of the solve changes, not its tolerance
+    double dn2 = 0.0, dn2_prev = 0.0;
     for (int it = 0; it < prm.iters; ++it) {
         double ev[2] = {0.0, 0.0};
         for (int f = I.f0 + tid; f < I.f0 + I.nt; f += NTT) {
@@ -911,6 +916,7 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
             if (tid == 0) gst->energy = ev[0];
         }
         tm.sync();   // corner terms complete
+        const double theta = (it >= 2 && dn2_prev > 0.0) ? fmin(1.0, sqrt(dn2 / dn2_prev)) : 0.0;
         double bb[2] = {0.0, 0.0};
         for_rows<NTT, R>(tid, I.n, [&](int i, int) {
             const int v = I.v0 + __ldg(b.row_vert + I.v0 + i);   // vertex of solver row i
@@ -923,7 +929,16 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
             const double2 u = U[v];
             if (i == I.pin) { bx += I.wpin * u.x; by += I.wpin * u.y; }
             b64[I.v0 + i] = make_double2(bx, by);
-            x64[I.v0 + i] = u;
+            double2 x0 = u;
+            if constexpr (R > 0) {   // previous iterate, FP32, in the class-G CG buffer
+                float2* prev = reinterpret_cast<float2*>(b.r32) + I.v0;
+                if (theta > 0.0) {
+                    const float2 pu = prev[i];
+                    x0 = make_double2(u.x + theta * (u.x - pu.x), u.y + theta * (u.y - pu.y));
+                }
+                prev[i] = make_float2(static_cast<float>(u.x), static_cast<float>(u.y));
+            }
+            x64[I.v0 + i] = x0;
             bb[0] += bx * bx; bb[1] += by * by;
         });
         team_sum<NTT, 2>(tm, bb, tm.redd);   // also publishes x64 / b64 to the team
@@ -954,12 +969,17 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
         }
         if (tid == 0) gst->step = step;
         tm.sync();   // all line-search reads of U done
+        double dd[1] = {0.0};
         for_rows<NTT, R>(tid, I.n, [&](int i, int) {
             const int v = I.v0 + __ldg(b.row_vert + I.v0 + i);
             const double2 u = U[v], x = x64[I.v0 + i];
-            U[v] = use_ls ? make_double2(u.x + (x.x - u.x) * step, u.y + (x.y - u.y) * step) : x;
+            const double2 un = use_ls ? make_double2(u.x + (x.x - u.x) * step, u.y + (x.y - u.y) * step) : x;
+            U[v] = un;
+            dd[0] += (un.x - u.x) * (un.x - u.x) + (un.y - u.y) * (un.y - u.y);
         });
-        tm.sync();
+        team_sum<NTT, 1>(tm, dd, tm.redd);   // also the barrier before the next local step
+        dn2_prev = dn2;
+        dn2 = dd[0];
     }
 }
 
