@@ -103,7 +103,10 @@ void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& 
     }
     ip.tri_edge.assign(static_cast<size_t>(3) * t, -1);
     ip.edge_info.clear();
-    std::vector<int64_t> ekey;
+    ip.edge_info.reserve(nh / 2 + n + 4);
+    std::vector<int32_t> elo, ehi;   // endpoints of each unique edge (lo <= hi)
+    elo.reserve(nh / 2 + n + 4);
+    ehi.reserve(nh / 2 + n + 4);
     for (int32_t s = 0; s < nh;) {
         int32_t e = s;
         int32_t fwd = 0, rev = 0;
@@ -113,19 +116,20 @@ void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& 
             const int32_t f = h / 3, k = h % 3;
             const int64_t a = T[3 * f + (k + 1) % 3];
             if (a == lo) ++fwd; else ++rev;
-            ip.tri_edge[h] = static_cast<int32_t>(ekey.size());
+            ip.tri_edge[h] = static_cast<int32_t>(elo.size());
             ++e;
         }
         const int32_t cnt = e - s;
         ip.edge_info.push_back(std::min(cnt, 1023) | (std::min(fwd, 1023) << 10) | (std::min(rev, 1023) << 20));
-        ekey.push_back(static_cast<int64_t>(lo) * n + hi);
+        elo.push_back(lo);
+        ehi.push_back(hi);
         s = e;
     }
-    ip.nedges = static_cast<int32_t>(ekey.size());
+    ip.nedges = static_cast<int32_t>(elo.size());
     // rows: appending in key order keeps each row sorted (see file comment)
     std::vector<int32_t> deg(n, 0);
-    for (int64_t key : ekey) {
-        const int64_t lo = key / n, hi = key % n;
+    for (int32_t e = 0; e < ip.nedges; ++e) {
+        const int32_t lo = elo[e], hi = ehi[e];
         if (lo == hi) continue;
         ++deg[lo]; ++deg[hi];
     }
@@ -135,10 +139,10 @@ void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& 
     ip.row_edge.assign(ip.row_ptr[n], 0);
     std::vector<int32_t> fill(ip.row_ptr.begin(), ip.row_ptr.end() - 1);
     for (int32_t e = 0; e < ip.nedges; ++e) {
-        const int64_t lo = ekey[e] / n, hi = ekey[e] % n;
+        const int32_t lo = elo[e], hi = ehi[e];
         if (lo == hi) continue;
-        ip.row_col[fill[lo]] = static_cast<int32_t>(hi); ip.row_edge[fill[lo]++] = e;
-        ip.row_col[fill[hi]] = static_cast<int32_t>(lo); ip.row_edge[fill[hi]++] = e;
+        ip.row_col[fill[lo]] = hi; ip.row_edge[fill[lo]++] = e;
+        ip.row_col[fill[hi]] = lo; ip.row_edge[fill[hi]++] = e;
     }
     // the fill above appends hi-entries of row `lo` before lo-entries of rows
     // met later; restore ascending column order per row
@@ -159,7 +163,7 @@ void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& 
     for (int32_t e = 0; e < ip.nedges; ++e) {
         const int32_t info = ip.edge_info[e];
         const int32_t cnt = info & 1023, fwd = (info >> 10) & 1023, rev = (info >> 20) & 1023;
-        const int64_t lo = ekey[e] / n, hi = ekey[e] % n;
+        const int32_t lo = elo[e], hi = ehi[e];
         if (cnt == 1) { ip.vflags[lo] |= 1; ip.vflags[hi] |= 1; }
         if (lo == hi) continue;
         if (fwd > 0 && rev == 0) { ip.vflags[lo] |= 2; ip.vflags[hi] |= 2; isb[lo] = 1; }
