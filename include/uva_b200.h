@@ -168,7 +168,8 @@ typedef struct uva_solve_params {
     int32_t max_inner;        /* inner CG iteration cap per refinement          */
     int32_t max_refine;       /* refinement cap per global step                 */
     int32_t threads;          /* threads per island team (0: autotuned)         */
-    int32_t reserved;
+    int32_t rev_ctas;         /* CTAs that start with the small-island classes
+                                 (0: automatic, < 0: none)                      */
 } uva_solve_params;
 
 /* Frames, weights, matrix values, Jacobi diagonal, pins and pin weights.

@@ -1397,7 +1397,8 @@ int launch_islands(const uva_batch* b, const uva_solve_params* prm, cudaStream_t
     const int grid = std::max(1, std::min(sm_count(), want));
     // reverse-order CTAs: one per 128 warp-class islands, at most a quarter
     const int nwarp = b->class_ofs[4] - b->class_ofs[3];
-    const int nrev = big > 0 ? std::min(grid / 4, (nwarp + 127) / 128) : 0;
+    int nrev = big > 0 ? std::min(grid / 4, (nwarp + 127) / 128) : 0;
+    if (prm->rev_ctas != 0) nrev = std::max(0, std::min(grid, prm->rev_ctas));
     k_islands<OP><<<grid, KB, kDynSmem, s>>>(*b, *prm, nrev);
     UVA_CHECK_LAUNCH(OP == OP_ARAP ? "uva_arap" : "uva_lscm");
     return UVA_OK;

@@ -234,6 +234,7 @@ class DeviceBatch:
         P.tol = float(base["tol"]); P.energy_tol = float(energy_tol)
         P.inner_eta = float(base["inner_eta"]); P.max_inner = int(base["max_inner"])
         P.max_refine = int(base["max_refine"]); P.threads = int(threads)
+        P.rev_ctas = int(over.get("rev_ctas") or 0)
         return P
 
     # ------------------------------------------------------------ solvers
