@@ -201,3 +201,26 @@ def test_batch_edge_cases(cuda):
     ref = O.BatchRef([(np.asarray(p, np.float64), t, u) for p, t, u in sel])
     ref.arap(3, line_search=True)
     assert O.uv_rel_error(np.concatenate([U[0], U[2]]), ref.U, _offsets(sel)) < UV_TOL
+
+
+def test_schedule_autotuner(cuda):
+    """The autotuner times the candidate team schedules on the batch and
+    applies the fastest; the schedule changes which team solves an island,
+    not the solution (every island still reaches the tolerance)."""
+    from ultimate_uv_artist_b200 import autotune, synth
+    from ultimate_uv_artist_b200.engine import gpu
+    isl = synth.uneven_islands(seed=78, count=60, tmin=20, tmax=6000)
+    b = gpu.Batch([(p, t, None) for p, t in isl])
+    db = b.db
+    db.lscm()
+    db.arap(iters=4)
+    ref = db.U.clone()
+    db.lscm()
+    best, res = autotune.tune(db, arap_iters=2)
+    assert len(res) == 12 and best == autotune.tune(db)[0]      # second call: cached
+    assert (best["mid"], best["small"]) == db.plan.classes
+    db.lscm()
+    db.arap(iters=4)
+    assert (db.island_status()["resid"] <= 2e-7 * 1.001).all()
+    ext = float((ref.max(0).values - ref.min(0).values).max())
+    assert float((db.U - ref).abs().max()) / ext < 1e-7

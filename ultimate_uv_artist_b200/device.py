@@ -103,10 +103,20 @@ class Plan:
         self.tofs = tofs.astype(np.int32)
         # island work order: grouped by size class (whole CTA with global or
         # shared-memory vectors, 256-thread sub-team, warp), largest first
-        nv = np.diff(vofs)
-        cls = np.where(nv > _lib.CLASS_BIG, 0, np.where(nv > _lib.CLASS_MID, 1, np.where(nv > _lib.CLASS_SMALL, 2, 3)))
+        self.set_classes(_lib.CLASS_MID, _lib.CLASS_SMALL)
+
+    def set_classes(self, mid, small):
+        """Island work order for team thresholds ``mid`` (whole CTA above) and
+        ``small`` (sub-team above, warp at or below); islands above
+        CLASS_BIG vertices keep global-memory vectors. The kernels' team
+        capacities bound them: mid <= CLASS_MID, small <= CLASS_SMALL."""
+        mid = int(min(mid, _lib.CLASS_MID))
+        small = int(min(small, _lib.CLASS_SMALL, mid))
+        nv = np.diff(self.vofs.astype(np.int64))
+        cls = np.where(nv > _lib.CLASS_BIG, 0, np.where(nv > mid, 1, np.where(nv > small, 2, 3)))
         self.order = np.lexsort((-nv, cls)).astype(np.int32)
         self.class_ofs = np.searchsorted(cls[self.order], np.arange(5)).astype(np.int32)
+        self.classes = (mid, small)
 
 
 def concat_charts(charts, with_uv=True):
@@ -195,6 +205,7 @@ class DeviceBatch:
         self.q32 = torch.empty((n, 2), dtype=f32, device=d)
         self.status = torch.zeros((nc, C.sizeof(_lib.IslandStatus)), dtype=torch.uint8, device=d)
         self.work = torch.zeros(8, dtype=torch.int32, device=d)
+        self.rev_ctas = 0   # schedule knob (autotune.tune)
         self.desc = self._make_desc()
         self.setup()
 
@@ -239,10 +250,12 @@ class DeviceBatch:
 
     # ------------------------------------------------------------ solvers
     def lscm(self, **kw):
+        kw.setdefault("rev_ctas", self.rev_ctas)
         prm = self.params("lscm", **kw)
         check(_lib.lib().uva_lscm(C.byref(self.desc), C.byref(prm), self._stream()), "uva_lscm")
 
     def arap(self, iters=8, line_search=True, energy_tol=0.0, **kw):
+        kw.setdefault("rev_ctas", self.rev_ctas)
         prm = self.params("arap", iters=iters, line_search=line_search, energy_tol=energy_tol, **kw)
         check(_lib.lib().uva_arap(C.byref(self.desc), C.byref(prm), self._stream()), "uva_arap")
 
@@ -254,6 +267,16 @@ class DeviceBatch:
         prm = self.params("arap", iters=iters, line_search=True, energy_tol=energy_tol, inner_eta=cg_tol,
                           max_inner=cg_max)
         check(_lib.lib().uva_slim(C.byref(self.desc), C.byref(prm), ptr(scratch), self._stream()), "uva_slim")
+
+    def set_classes(self, mid, small):
+        """Re-assign islands to team classes (see Plan.set_classes); only the
+        work order changes, not the islands' data."""
+        self.plan.set_classes(mid, small)
+        if self.nc == 0:
+            return
+        self.order.copy_(torch.from_numpy(self.plan.order).to(self.dev))
+        for c in range(5):
+            self.desc.class_ofs[c] = int(self.plan.class_ofs[c])
 
     def step_graph(self, setup=True, lscm=True, arap_iters=20, line_search=True, lscm_kw=None, arap_kw=None):
         """Capture setup + LSCM + ARAP (any subset) into one CUDA graph."""
@@ -311,6 +334,9 @@ class StepGraph:
         self.db = db
         parts = (_lib.STEP_SETUP if setup else 0) | (_lib.STEP_LSCM if lscm else 0) | \
                 (_lib.STEP_ARAP if arap_iters > 0 else 0)
+        lscm_kw = dict(lscm_kw); arap_kw = dict(arap_kw)
+        lscm_kw.setdefault("rev_ctas", db.rev_ctas)
+        arap_kw.setdefault("rev_ctas", db.rev_ctas)
         self._lp = db.params("lscm", **lscm_kw)
         self._ap = db.params("arap", iters=max(arap_iters, 1), line_search=line_search, **arap_kw)
         h = C.c_void_p()
