@@ -36,6 +36,7 @@ METRIC = "ARAP tris/sec @1e-6 resid, batched-FP32+FP64-refine"
 UNIT = "tri-iters/s"
 ITERS = 20
 ISLANDS = 2000
+TRAFFIC_ARAP = 34.69e9   # bytes per ARAP launch of the default workload (ncu dram__bytes_read + write)
 
 
 def _args():
@@ -581,7 +582,9 @@ def main():
                        "schedule": tuned},
             "roofline": {"kernel": "k_islands<OP_ARAP>", "bound": "hbm", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_source": peak_src,
-                         "traffic": None, "kernel_ms": arap_ms, "algorithmic_bytes": full,
+                         # DRAM read + write of one full-size ARAP launch, measured by
+                         # an ncu capture of this workload (summary under profiles/)
+                         "traffic": TRAFFIC_ARAP if args.islands == ISLANDS else None, "kernel_ms": arap_ms, "algorithmic_bytes": full,
                          "compulsory_bytes": comp, "compulsory_frac": achieved_c / hbm,
                          "cg_iters_total": int(st["cg_iters"].sum()),
                          "refinements_total": int(st["refinements"].sum()),
