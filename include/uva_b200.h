@@ -126,8 +126,10 @@ typedef struct uva_batch {
     const int32_t* vert_row;  /* n: vertex -> solver row (island-local)       */
     const int32_t* agg_rows;  /* nc: rows per coarse aggregate (0: none)      */
     const int32_t* cofs;      /* nc+1: offset of the island's m*m coarse block */
-    float*  coarse_a;         /* cofs[nc]: inverse coarse ARAP operators (FP32) */
-    float*  coarse_l;         /* 4*cofs[nc]: inverse coarse LSCM operators     */
+    float*  coarse_a;         /* cofs[nc] floats: inverse coarse ARAP operators,
+                                 FP16 scaled to a largest entry of 1024, then
+                                 the inverse scale (FP32)                      */
+    float*  coarse_l;         /* 4*cofs[nc] floats: the same for LSCM          */
     double* coarse_work;      /* 4*cofs[nc]: FP64 workspace of the setup        */
     float*  cpart;            /* 2*nslices: per-slice residual sums (solve scratch) */
     int32_t class_ofs[5];     /* host values: class c owns order[ofs[c]..ofs[c+1]) */

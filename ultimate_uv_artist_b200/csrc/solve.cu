@@ -20,6 +20,7 @@
 //    and never wait for the largest one (the reference's test is global over
 //    the batch, engine/gpu.py:196).
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -499,6 +500,14 @@ __device__ __forceinline__ float jacobi(const uva_batch& b, const Isl& I, int i)
     return jacobi_global<OP>(b, I, i);
 }
 
+// Inverse coarse operators are stored as FP16, scaled so that the largest
+// entry is 1024 (a CPU probe on LSCM islands: same PCG iterations as FP32,
+// still positive definite), in the first half of the island's FP32 block;
+// the float after the halves holds the inverse of the scale.
+__host__ __device__ __forceinline__ const float* coarse_scale(const float* block, int nhalf) {
+    return block + (nhalf + 1) / 2;
+}
+
 // Two-level additive preconditioner z = D^-1 r + P Ac^-1 P^T r. P is the
 // piecewise-constant prolongation over aggregates of `agg` consecutive solver
 // rows (compact mesh blobs from the plan; agg is a multiple of 128, so an
@@ -540,11 +549,12 @@ __device__ __forceinline__ void coarse_solve(const uva_batch& b, Team<NTT>& tm, 
     }
     tm.sync();   // g complete
     if (OP == OP_ARAP) {
-        const float* A = b.coarse_a + I.co;
+        const __half* A = reinterpret_cast<const __half*>(b.coarse_a + I.co);
+        const float isc = __ldg(coarse_scale(b.coarse_a + I.co, I.M * I.M));
         for (int o = warp; o < I.M; o += NW) {
             float au = 0.f, av = 0.f;
             for (int c = lane; c < I.M; c += 32) {
-                const float w = __ldg(A + static_cast<size_t>(o) * I.M + c);
+                const float w = __half2float(A[static_cast<size_t>(o) * I.M + c]);
                 au = fmaf(w, tm.cg[c], au);
                 av = fmaf(w, tm.cg[I.M + c], av);
             }
@@ -553,17 +563,18 @@ __device__ __forceinline__ void coarse_solve(const uva_batch& b, Team<NTT>& tm, 
                 au += __shfl_xor_sync(0xffffffffu, au, k);
                 av += __shfl_xor_sync(0xffffffffu, av, k);
             }
-            if (lane == 0) { tm.cy[o] = au; tm.cy[I.M + o] = av; }
+            if (lane == 0) { tm.cy[o] = au * isc; tm.cy[I.M + o] = av * isc; }
         }
     } else {
         const int N = 2 * I.M;
-        const float* A = b.coarse_l + 4 * static_cast<size_t>(I.co);
+        const __half* A = reinterpret_cast<const __half*>(b.coarse_l + 4 * static_cast<size_t>(I.co));
+        const float isc = __ldg(coarse_scale(b.coarse_l + 4 * static_cast<size_t>(I.co), N * N));
         for (int o = warp; o < N; o += NW) {
             float acc = 0.f;
-            for (int c = lane; c < N; c += 32) acc = fmaf(__ldg(A + static_cast<size_t>(o) * N + c), tm.cg[c], acc);
+            for (int c = lane; c < N; c += 32) acc = fmaf(__half2float(A[static_cast<size_t>(o) * N + c]), tm.cg[c], acc);
 #pragma unroll
             for (int k = 16; k > 0; k >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, k);
-            if (lane == 0) tm.cy[o] = acc;
+            if (lane == 0) tm.cy[o] = acc * isc;
         }
     }
     tm.sync();   // y complete
@@ -1221,6 +1232,26 @@ __device__ void gauss_jordan(double* W, int N, double* colk) {
 // stored in FP32. One thread owns each coarse row and adds its terms in
 // slot order, so the operators are the same bits on every run. The
 // inversion works in shared memory when the block fits (kCoarseSmemN).
+// W (FP64) -> FP16 halves scaled to a largest entry of 1024, plus the
+// inverse scale after them (coarse_scale); `red` is >= 32 doubles of
+// shared memory. Whole CTA.
+__device__ void store_half_scaled(const double* W, int cnt, float* block, double* red) {
+    double m = 0.0;
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) m = fmax(m, fabs(W[e]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __syncthreads();   // red may still be read by the caller's last step
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+    const double sc = (m > 0.0 && isfinite(m)) ? 1024.0 / m : 1.0;
+    __half* h = reinterpret_cast<__half*>(block);
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) h[e] = __double2half(W[e] * sc);
+    if (threadIdx.x == 0) *const_cast<float*>(coarse_scale(block, cnt)) = static_cast<float>(1.0 / sc);
+    __syncthreads();
+}
+
 constexpr int kCoarseSmemN = 128;
 constexpr size_t kCoarseSmem = sizeof(double) * kCoarseSmemN * kCoarseSmemN;   // 131,072 bytes
 
@@ -1270,7 +1301,7 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
         Wa[a] += dsum;
     }
     gauss_jordan(W, M, colk);
-    for (int e = threadIdx.x; e < M * M; e += blockDim.x) b.coarse_a[co + e] = static_cast<float>(W[e]);
+    store_half_scaled(W, M * M, b.coarse_a + co, colk);
     __syncthreads();
     // ---- LSCM (free unknowns only; the pins are fixed)
     const int pv0 = b.pins[3 * isl + 1], pv1 = b.pins[3 * isl + 2];
@@ -1319,7 +1350,7 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
         Wv[2 * a] += cvu;
     }
     gauss_jordan(W, N, colk);
-    for (int e = threadIdx.x; e < N * N; e += blockDim.x) b.coarse_l[4 * static_cast<size_t>(co) + e] = static_cast<float>(W[e]);
+    store_half_scaled(W, N * N, b.coarse_l + 4 * static_cast<size_t>(co), colk);
 }
 
 cudaError_t ensure_coarse_attr() {
