@@ -111,6 +111,15 @@ int uva_plan_export(const uva_plan* plan, int32_t* tri4, int32_t* tri_edge, int3
 int uva_plan_export_rows(const uva_plan* plan, int32_t* row_vert, int32_t* vert_row, int32_t* agg_rows,
                          int32_t* cofs);
 void uva_plan_destroy(uva_plan* plan);
+/* Batch concatenation (host, parallel over charts). Replaces the per-chart
+ * copies of gpu.Batch.__init__ (gpu.py:69-87): chart i's P (rows of 3,
+ * float32/float64: pdt 0/1), T (rows of 3 local ids, int32/int64: tdt 0/1)
+ * and optional U (rows of 2, udt -1: none -> zeros, 0: float32, 1: float64;
+ * U or udt may be null: all zeros) land in P_out (n*3 FP64), T_out (t*3
+ * int64) and U_out (n*2 FP64, may be null) at vofs/tofs (nc+1 offsets).     */
+int uva_concat_charts(int32_t nc, const void* const* P, const int8_t* pdt, const void* const* T,
+                      const int8_t* tdt, const void* const* U, const int8_t* udt, const int64_t* vofs,
+                      const int64_t* tofs, double* P_out, int64_t* T_out, double* U_out, int32_t nthreads);
 
 /* --------------------------------------------------------------------------
  * Device batch descriptor: plain device pointers, filled by the host layer.
@@ -154,6 +163,14 @@ typedef struct uva_batch {
     float*  r32;  float*  d32;  float*  p32;  float* q32;
     uva_island_status* status;                  /* nc                         */
     int32_t* work;            /* >= 4 ints, zeroed by the callee per launch     */
+    /* Block-Jacobi smoother of the PCG (optional: all three null -> point
+     * Jacobi). uva_batch_setup writes, per 32-row slice, the inverse of the
+     * slice's diagonal block as FP16 scaled to a largest entry of 1024, in
+     * the fragment order of the warp-level MMA that applies it.             */
+    uint16_t* bj_a;           /* nslices*1024: ARAP block inverses (real)       */
+    uint16_t* bj_l;           /* nslices*2048: LSCM block inverses, real part
+                                 then imaginary part of the complex block     */
+    float*  bj_s;             /* nslices*2: inverse scales (ARAP, LSCM)         */
 } uva_batch;
 
 /* Island size classes of one persistent launch (see uva_arap): islands are
@@ -185,6 +202,11 @@ int uva_lscm(uva_batch* b, const uva_solve_params* prm, void* stream);
 /* ARAP local/global iterations of every island in one persistent launch
  * (gpu.py:230-249 with semantics BATCH, param.py:379-414 with PARAM).      */
 int uva_arap(uva_batch* b, const uva_solve_params* prm, void* stream);
+/* Block-Jacobi smoother applied to one vector: z = C r per 32-row slice of
+ * every island (op 0: ARAP blocks, 1: LSCM blocks), r and z FP32 (u, v) per
+ * solver row (n*2). No counterpart in the reference (its CG is point
+ * Jacobi, gpu.py:184-202); exported so tests can check the block inverses. */
+int uva_bjac_apply(const uva_batch* b, int32_t op, const float* r, float* z, void* stream);
 
 /* Step graphs. No counterpart in the reference, which launches every kernel
  * of gpu.Batch.arap (gpu.py:230-249) from Python, one host sync per CG

@@ -187,3 +187,26 @@ def test_uneven_islands_sizes():
     isl = synth.uneven_islands(seed=7, count=50)
     t = np.array([len(T) for _, T in isl])
     assert t.min() >= 8 and t.max() <= 20000
+
+
+def test_concat_charts_matches_numpy():
+    """uva_concat_charts widens and places every chart like numpy's
+    concatenation (gpu.Batch.__init__'s copies), for mixed input dtypes."""
+    from ultimate_uv_artist_b200.device import concat_charts
+    rng = np.random.default_rng(4)
+    charts = []
+    for k in range(40):
+        nv, nt = int(rng.integers(3, 60)), int(rng.integers(1, 90))
+        P = rng.standard_normal((nv, 3)).astype(np.float32 if k % 2 else np.float64)
+        T = rng.integers(0, nv, (nt, 3)).astype(np.int32 if k % 3 else np.int64)
+        U = None if k % 4 == 0 else rng.standard_normal((nv, 2)).astype(np.float32 if k % 5 else np.float64)
+        charts.append((P, T, U))
+    charts.append((np.zeros((0, 3)), np.zeros((0, 3), np.int64), None))   # empty chart
+    P, T, U, vofs, tofs = concat_charts(charts)
+    assert np.array_equal(P, np.concatenate([c[0].astype(np.float64) for c in charts]))
+    assert np.array_equal(T, np.concatenate([c[1].astype(np.int64) for c in charts]))
+    assert np.array_equal(U, np.concatenate([np.zeros((len(c[0]), 2)) if c[2] is None else c[2].astype(np.float64)
+                                             for c in charts]))
+    assert np.array_equal(np.diff(vofs), [len(c[0]) for c in charts])
+    with pytest.raises(ValueError):
+        concat_charts([(np.zeros((4, 3)), np.zeros((1, 3), np.int64), np.zeros((3, 2)))])

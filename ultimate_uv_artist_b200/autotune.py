@@ -30,11 +30,23 @@ _cache = {}
 
 def signature(db):
     """Device name and a coarse histogram of island sizes (log2 buckets)."""
-    nv = np.diff(db.plan.vofs.astype(np.int64))
+    return _signature(db.plan, db.dev)
+
+
+def _signature(plan, dev):
+    nv = np.diff(plan.vofs.astype(np.int64))
     hist = np.bincount(np.minimum(np.log2(np.maximum(nv, 1)).astype(int), 24), minlength=25)
     # bucket counts rounded to 2 significant bits so near-identical batches share a key
     key = tuple(int(2 ** np.floor(np.log2(h))) if h else 0 for h in hist)
-    return torch.cuda.get_device_name(db.dev), key
+    return torch.cuda.get_device_name(dev), key
+
+
+def lookup(plan, dev):
+    """The schedule ``tune`` chose earlier for batches of this signature on
+    this device, or None. DeviceBatch applies it to every new batch."""
+    if not _cache:
+        return None
+    return _cache.get(_signature(plan, dev))
 
 
 def _time(fn, dev):

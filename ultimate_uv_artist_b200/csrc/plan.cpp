@@ -406,3 +406,65 @@ extern "C" int uva_plan_export_rows(const uva_plan* p, int32_t* row_vert, int32_
     cofs[p->nc] = static_cast<int32_t>(p->cofs[p->nc]);
     return UVA_OK;
 }
+
+// ------------------------------------------------------------------ batch concatenation
+// Per-chart host arrays (numpy inputs of any supported dtype) into the batch
+// layout, charts in parallel: positions and UVs widened to FP64, triangles to
+// int64. Replaces the per-chart copies of engine/gpu.py:69-87.
+namespace {
+
+template <typename S, typename D>
+void widen(const void* src, D* dst, int64_t count) {
+    const S* s = static_cast<const S*>(src);
+    for (int64_t k = 0; k < count; ++k) dst[k] = static_cast<D>(s[k]);
+}
+
+}  // namespace
+
+extern "C" int uva_concat_charts(int32_t nc, const void* const* P, const int8_t* pdt, const void* const* T,
+                                 const int8_t* tdt, const void* const* U, const int8_t* udt, const int64_t* vofs,
+                                 const int64_t* tofs, double* P_out, int64_t* T_out, double* U_out,
+                                 int32_t nthreads) {
+    if (nc < 0 || (nc > 0 && (!P || !pdt || !T || !tdt || !vofs || !tofs || !P_out || !T_out))) {
+        uva_set_error("uva_concat_charts: bad arguments");
+        return UVA_E_ARG;
+    }
+    for (int32_t i = 0; i < nc; ++i) {
+        if (vofs[i + 1] < vofs[i] || tofs[i + 1] < tofs[i] || pdt[i] < 0 || pdt[i] > 1 || tdt[i] < 0 || tdt[i] > 1 ||
+            (U && udt && (udt[i] < -1 || udt[i] > 1))) {
+            uva_set_error("uva_concat_charts: offsets must be non-decreasing, dtype codes 0/1 (U: -1/0/1)");
+            return UVA_E_ARG;
+        }
+        if ((vofs[i + 1] > vofs[i] && !P[i]) || (tofs[i + 1] > tofs[i] && !T[i])) {
+            uva_set_error("uva_concat_charts: null chart array");
+            return UVA_E_ARG;
+        }
+    }
+    std::atomic<int32_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const int32_t i = next.fetch_add(1);
+            if (i >= nc) break;
+            // sizes were checked non-negative above
+            const int64_t nv = std::max<int64_t>(vofs[i + 1] - vofs[i], 0), nt = std::max<int64_t>(tofs[i + 1] - tofs[i], 0);
+            double* po = P_out + 3 * (vofs[i] - vofs[0]);
+            if (pdt[i] == 0) widen<float>(P[i], po, 3 * nv); else std::memcpy(po, P[i], sizeof(double) * 3 * nv);
+            int64_t* to = T_out + 3 * (tofs[i] - tofs[0]);
+            if (tdt[i] == 0) widen<int32_t>(T[i], to, 3 * nt); else std::memcpy(to, T[i], sizeof(int64_t) * 3 * nt);
+            if (U_out) {
+                double* uo = U_out + 2 * (vofs[i] - vofs[0]);
+                const int8_t d = (U && udt) ? udt[i] : -1;
+                if (d < 0 || !U[i]) std::memset(uo, 0, sizeof(double) * 2 * nv);
+                else if (d == 0) widen<float>(U[i], uo, 2 * nv);
+                else std::memcpy(uo, U[i], sizeof(double) * 2 * nv);
+            }
+        }
+    };
+    int32_t nt = nthreads > 0 ? nthreads : static_cast<int32_t>(std::thread::hardware_concurrency());
+    nt = std::max(1, std::min(nt, std::max(nc, 1)));
+    std::vector<std::thread> pool;
+    for (int32_t k = 1; k < nt; ++k) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    return UVA_OK;
+}

@@ -77,24 +77,24 @@ class Plan:
             self.ncoarse = int(sz[8])
             self.tri4 = host_empty((self.t, 4), np.int32)
             self.tri_edge = host_empty((self.t, 3), np.int32)
-            self.sofs = np.empty(nc + 1, np.int32)
+            self.sofs = host_empty(nc + 1, np.int32)
             self.slice_ptr = host_empty(self.nslices + 1, np.int32)
             self.slot_col = host_empty(self.nslots, np.int32)
             self.slot_edge = host_empty(self.nslots, np.int32)
             self.slot_c = host_empty(self.nslots, np.float32)
             self.vt_ptr = host_empty(self.n + 1, np.int32)
             self.vt = host_empty(3 * self.t, np.int32)
-            self.vflags = np.empty(self.n, np.uint8)
-            self.bofs = np.empty(nc + 1, np.int32)
-            self.bverts = np.empty(max(self.nbverts, 1), np.int32)
+            self.vflags = host_empty(self.n, np.uint8)
+            self.bofs = host_empty(nc + 1, np.int32)
+            self.bverts = host_empty(max(self.nbverts, 1), np.int32)
             check(L.uva_plan_export(h, ptr(self.tri4), ptr(self.tri_edge), ptr(self.sofs), ptr(self.slice_ptr),
                                     ptr(self.slot_col), ptr(self.slot_edge), ptr(self.slot_c), ptr(self.vt_ptr),
                                     ptr(self.vt), ptr(self.vflags), ptr(self.bofs), ptr(self.bverts)),
                   "uva_plan_export")
-            self.row_vert = np.empty(max(self.n, 1), np.int32)
-            self.vert_row = np.empty(max(self.n, 1), np.int32)
-            self.agg_rows = np.empty(max(nc, 1), np.int32)
-            self.cofs = np.empty(nc + 1, np.int32)
+            self.row_vert = host_empty(max(self.n, 1), np.int32)
+            self.vert_row = host_empty(max(self.n, 1), np.int32)
+            self.agg_rows = host_empty(max(nc, 1), np.int32)
+            self.cofs = host_empty(nc + 1, np.int32)
             check(L.uva_plan_export_rows(h, ptr(self.row_vert), ptr(self.vert_row), ptr(self.agg_rows), ptr(self.cofs)),
                   "uva_plan_export_rows")
         finally:
@@ -119,23 +119,53 @@ class Plan:
         self.classes = (mid, small)
 
 
+_FLOAT_CODE = {np.dtype(np.float32): 0, np.dtype(np.float64): 1}
+_INT_CODE = {np.dtype(np.int32): 0, np.dtype(np.int64): 1}
+
+
+def _chart_array(a, width, codes, fallback):
+    """(C-contiguous array of `width` columns, dtype code) without a copy
+    when the dtype is one the concatenation reads directly."""
+    a = np.asarray(a)
+    if a.dtype not in codes:
+        a = a.astype(fallback)
+    a = np.ascontiguousarray(a).reshape(-1, width)
+    return a, codes[a.dtype]
+
+
 def concat_charts(charts, with_uv=True):
-    """(P, T, U) per chart -> concatenated FP64 P, local int64 T, FP64 U, offsets."""
+    """(P, T, U) per chart -> concatenated FP64 P, local int64 T, FP64 U, offsets
+    (uva_concat_charts copies the charts in parallel; P and U in page-locked
+    memory for the uploads)."""
     nc = len(charts)
+    Ps, Ts, Us = [], [], []
+    pdt = np.empty(max(nc, 1), np.int8)
+    tdt = np.empty(max(nc, 1), np.int8)
+    udt = np.full(max(nc, 1), -1, np.int8)
     vofs = np.zeros(nc + 1, np.int64)
     tofs = np.zeros(nc + 1, np.int64)
     for i, ch in enumerate(charts):
-        vofs[i + 1] = vofs[i] + len(ch[0])
-        tofs[i + 1] = tofs[i] + len(ch[1])
+        a, pdt[i] = _chart_array(ch[0], 3, _FLOAT_CODE, np.float64)
+        t, tdt[i] = _chart_array(ch[1], 3, _INT_CODE, np.int64)
+        Ps.append(a)
+        Ts.append(t)
+        vofs[i + 1] = vofs[i] + len(a)
+        tofs[i + 1] = tofs[i] + len(t)
+        u = None
+        if with_uv and len(ch) > 2 and ch[2] is not None:
+            u, udt[i] = _chart_array(ch[2], 2, _FLOAT_CODE, np.float64)
+            if len(u) != len(a):
+                raise ValueError(f"chart {i}: U has {len(u)} rows for {len(a)} vertices")
+        Us.append(u)
     P = host_empty((int(vofs[-1]), 3), np.float64)
     T = np.empty((int(tofs[-1]), 3), np.int64)
     U = host_empty((int(vofs[-1]), 2), np.float64)
-    U[:] = 0.0
-    for i, ch in enumerate(charts):
-        P[vofs[i]:vofs[i + 1]] = np.asarray(ch[0], np.float64).reshape(-1, 3)
-        T[tofs[i]:tofs[i + 1]] = np.asarray(ch[1], np.int64).reshape(-1, 3)
-        if with_uv and len(ch) > 2 and ch[2] is not None:
-            U[vofs[i]:vofs[i + 1]] = np.asarray(ch[2], np.float64).reshape(-1, 2)
+    if nc:
+        pp = np.array([x.ctypes.data for x in Ps], np.uintp)
+        tp = np.array([x.ctypes.data for x in Ts], np.uintp)
+        up_ = np.array([0 if x is None else x.ctypes.data for x in Us], np.uintp)
+        check(_lib.lib().uva_concat_charts(nc, ptr(pp), ptr(pdt), ptr(tp), ptr(tdt), ptr(up_), ptr(udt), ptr(vofs),
+                                           ptr(tofs), ptr(P), ptr(T), ptr(U), 0), "uva_concat_charts")
     return P, T, U, vofs, tofs
 
 
@@ -143,12 +173,17 @@ class DeviceBatch:
     """Islands resident on one CUDA device, ready for the uva_* kernels."""
 
     def __init__(self, P, T_local, vofs, tofs, U=None, semantics=_lib.SEM_BATCH, device=None, stream=None,
-                 plan=None):
+                 plan=None, block_jacobi=True):
         self.dev = require_cuda(device)
         self.stream = stream
         self.semantics = int(semantics)
         plan = plan if plan is not None else Plan(T_local, vofs, tofs)
         self.plan = plan
+        # a schedule tuned earlier for batches of this size signature (autotune)
+        from . import autotune
+        tuned = autotune.lookup(plan, self.dev)
+        if tuned is not None:
+            plan.set_classes(tuned["mid"], tuned["small"])
         self.nc, self.n, self.t = plan.nc, plan.n, plan.t
         d = self.dev
 
@@ -205,7 +240,15 @@ class DeviceBatch:
         self.q32 = torch.empty((n, 2), dtype=f32, device=d)
         self.status = torch.zeros((nc, C.sizeof(_lib.IslandStatus)), dtype=torch.uint8, device=d)
         self.work = torch.zeros(8, dtype=torch.int32, device=d)
-        self.rev_ctas = 0   # schedule knob (autotune.tune)
+        # block-Jacobi smoother: FP16 inverses of the 32-row diagonal blocks
+        # (6 KB per slice for ARAP + LSCM); block_jacobi=False keeps point Jacobi
+        ns = max(plan.nslices, 1)
+        self.block_jacobi = bool(block_jacobi)
+        if self.block_jacobi:
+            self.bj_a = torch.empty(1024 * ns, dtype=torch.int16, device=d)
+            self.bj_l = torch.empty(2048 * ns, dtype=torch.int16, device=d)
+            self.bj_s = torch.empty(2 * ns, dtype=f32, device=d)
+        self.rev_ctas = tuned["rev_ctas"] if tuned is not None else 0   # schedule knob (autotune.tune)
         self.desc = self._make_desc()
         self.setup()
 
@@ -223,6 +266,8 @@ class DeviceBatch:
                      "slot_cw", "wdiag", "dinv", "pins", "wpin", "U", "x64", "b64", "rc", "r32", "d32", "p32",
                      "q32", "status", "work"):
             setattr(D, name, getattr(self, name).data_ptr())
+        if self.block_jacobi:
+            D.bj_a, D.bj_l, D.bj_s = self.bj_a.data_ptr(), self.bj_l.data_ptr(), self.bj_s.data_ptr()
         return D
 
     def _refresh_u(self):
@@ -322,7 +367,15 @@ class DeviceBatch:
         return raw.view(dt).reshape(-1)
 
     def uvs(self):
-        return self.U[:self.n].double().cpu().numpy()
+        """UVs (n, 2) FP64 on the host: one asynchronous copy into
+        page-locked memory on the batch's stream, then a wait for it."""
+        out = host_empty((self.n, 2), np.float64)
+        if self.n:
+            s = self.stream if self.stream is not None else torch.cuda.current_stream(self.dev)
+            with torch.cuda.stream(s):
+                torch.from_numpy(out).copy_(self.U[:self.n], non_blocking=True)
+            s.synchronize()
+        return out
 
 
 class StepGraph:
