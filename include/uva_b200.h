@@ -163,14 +163,6 @@ typedef struct uva_batch {
     float*  r32;  float*  d32;  float*  p32;  float* q32;
     uva_island_status* status;                  /* nc                         */
     int32_t* work;            /* >= 4 ints, zeroed by the callee per launch     */
-    /* Block-Jacobi smoother of the PCG (optional: all three null -> point
-     * Jacobi). uva_batch_setup writes, per 32-row slice, the inverse of the
-     * slice's diagonal block as FP16 scaled to a largest entry of 1024, in
-     * the fragment order of the warp-level MMA that applies it.             */
-    uint16_t* bj_a;           /* nslices*1024: ARAP block inverses (real)       */
-    uint16_t* bj_l;           /* nslices*2048: LSCM block inverses, real part
-                                 then imaginary part of the complex block     */
-    float*  bj_s;             /* nslices*2: inverse scales (ARAP, LSCM)         */
 } uva_batch;
 
 /* Island size classes of one persistent launch (see uva_arap): islands are
@@ -202,11 +194,6 @@ int uva_lscm(uva_batch* b, const uva_solve_params* prm, void* stream);
 /* ARAP local/global iterations of every island in one persistent launch
  * (gpu.py:230-249 with semantics BATCH, param.py:379-414 with PARAM).      */
 int uva_arap(uva_batch* b, const uva_solve_params* prm, void* stream);
-/* Block-Jacobi smoother applied to one vector: z = C r per 32-row slice of
- * every island (op 0: ARAP blocks, 1: LSCM blocks), r and z FP32 (u, v) per
- * solver row (n*2). No counterpart in the reference (its CG is point
- * Jacobi, gpu.py:184-202); exported so tests can check the block inverses. */
-int uva_bjac_apply(const uva_batch* b, int32_t op, const float* r, float* z, void* stream);
 
 /* Step graphs. No counterpart in the reference, which launches every kernel
  * of gpu.Batch.arap (gpu.py:230-249) from Python, one host sync per CG

@@ -55,7 +55,7 @@ class BatchDesc(C.Structure):
                 ("P", vp), ("frame", vp), ("wtri", vp), ("tscale", vp), ("wedge", vp), ("slot_cw", vp),
                 ("wdiag", vp), ("dinv", vp), ("pins", vp), ("wpin", vp), ("U", vp),
                 ("x64", vp), ("b64", vp), ("rc", vp), ("r32", vp), ("d32", vp), ("p32", vp), ("q32", vp),
-                ("status", vp), ("work", vp), ("bj_a", vp), ("bj_l", vp), ("bj_s", vp)]
+                ("status", vp), ("work", vp)]
 
 
 class SolveParams(C.Structure):
@@ -75,7 +75,6 @@ _SIGS = {
     "uva_lscm": [vp, vp, vp],
     "uva_arap": [vp, vp, vp],
     "uva_arap_noalloc": [vp, vp, vp],
-    "uva_bjac_apply": [vp, i32, vp, vp, vp],
     "uva_slim": [vp, vp, vp, vp],
     "uva_slim_scratch_bytes": [vp, vp],
     "uva_step_graph_create": [vp, i32, vp, vp, vp],

@@ -503,105 +503,6 @@ __device__ __forceinline__ float jacobi(const uva_batch& b, const Isl& I, int i)
     return jacobi_global<OP>(b, I, i);
 }
 
-// ---- block-Jacobi smoother: z = C r over the 32 rows of one slice, C the
-// inverse of the slice's diagonal block (FP16, scaled; k_bjac writes it in
-// the fragment order used here). One warp per slice: lane l owns row l, as
-// everywhere in the solver. The product runs on the tensor cores as
-// m16n8k16 MMAs (FP16 operands, FP32 accumulation): the 32x32 block is 2x2
-// A tiles; the B operand carries the slice's residual, scaled by a power of
-// two per slice and split into FP16 high and low parts, as its columns
-// (u_hi, u_lo, v_hi, v_lo), so the product keeps about 22 bits of r.
-// LSCM blocks are complex (C = Cr + i Ci acting on u + i v): a second MMA per
-// tile applies Ci to the columns (-v_hi, -v_lo, u_hi, u_lo).
-__device__ __forceinline__ void mma16816(float (&d)[4], const uint4& a, uint32_t b0, uint32_t b1) {
-    asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b0), "r"(b1));
-}
-
-__device__ __forceinline__ uint32_t half2_bits(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
-
-// High or low FP16 part of two scaled values.
-__device__ __forceinline__ uint32_t split_pair(float a, float c, bool lo) {
-    const __half2 h = __floats2half2_rn(a, c);
-    const float2 f = __half22float2(h);
-    const __half2 l = __floats2half2_rn(a - f.x, c - f.y);
-    return half2_bits(lo ? l : h);
-}
-
-// All 32 lanes of the warp call this with their row i (island-local solver
-// row; the slice must hold at least one row < n). r: island-local vector,
-// read only below n.
-template <Op OP>
-__device__ __forceinline__ float2 bj_apply(const uva_batch& b, int s0, int n, int i, const float2* r) {
-    constexpr int NT = OP == OP_ARAP ? 4 : 8;   // A tiles per slice
-    const int lane = i & 31, row0 = i - lane;
-    const int gs = s0 + (i >> 5);
-    const uint4* blk = reinterpret_cast<const uint4*>(OP == OP_ARAP ? b.bj_a : b.bj_l) +
-                       static_cast<size_t>(gs) * (NT * 32) + lane;
-    uint4 a[NT];
-#pragma unroll
-    for (int t = 0; t < NT; ++t) a[t] = __ldg(blk + 32 * t);
-    const float bsc = __ldg(b.bj_s + 2 * gs + (OP == OP_ARAP ? 0 : 1));
-    // power-of-two scale: the slice's largest |r| maps into [2^13, 2^14)
-    const float2 ri = i < n ? r[i] : make_float2(0.f, 0.f);
-    const unsigned m = __reduce_max_sync(0xffffffffu, max(__float_as_uint(fabsf(ri.x)), __float_as_uint(fabsf(ri.y))));
-    if (m == 0u) return make_float2(0.f, 0.f);
-    const int ex = min(max(140 - static_cast<int>(m >> 23), -126), 126);
-    const float sc = __int_as_float((ex + 127) << 23), isc = __int_as_float((127 - ex) << 23);
-    const int g = lane >> 2, tq = lane & 3;
-    const bool use_v = (g & 2) != 0, lo = (g & 1) != 0, live = g < 4;
-    uint32_t b1[2][2], b2[2][2];
-#pragma unroll
-    for (int kt = 0; kt < 2; ++kt) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {   // rows 16 kt + 2 tq + 8 h + {0, 1}
-            const int k = row0 + 16 * kt + 2 * tq + 8 * h;
-            const float2 x0 = k < n ? r[k] : make_float2(0.f, 0.f);
-            const float2 x1 = k + 1 < n ? r[k + 1] : make_float2(0.f, 0.f);
-            const uint32_t v = split_pair((use_v ? x0.y : x0.x) * sc, (use_v ? x1.y : x1.x) * sc, lo);
-            b1[kt][h] = live ? v : 0u;
-        }
-    }
-    float d[2][4];
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) d[mt][e] = 0.f;
-    }
-    if constexpr (OP == OP_LSCM) {
-        // (-v_hi, -v_lo, u_hi, u_lo): column g of B2 is column g ^ 2 of B1
-        const uint32_t neg = g < 2 ? 0x80008000u : 0u;
-#pragma unroll
-        for (int kt = 0; kt < 2; ++kt) {
-#pragma unroll
-            for (int h = 0; h < 2; ++h) b2[kt][h] = __shfl_xor_sync(0xffffffffu, b1[kt][h], 8) ^ neg;
-        }
-    }
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-#pragma unroll
-        for (int kt = 0; kt < 2; ++kt) {
-            mma16816(d[mt], a[2 * mt + kt], b1[kt][0], b1[kt][1]);
-            if constexpr (OP == OP_LSCM) mma16816(d[mt], a[4 + 2 * mt + kt], b2[kt][0], b2[kt][1]);
-        }
-    }
-    // lane (g, tq): tq 0 holds u of rows g and g + 8 of each 16-row half as
-    // column pairs (hi, lo), tq 1 holds v; row i takes them from lanes 4 g'
-    // and 4 g' + 1
-    const int mt = lane >> 4, up = (lane >> 3) & 1, src = 4 * (lane & 7);
-    float zu = 0.f, zv = 0.f;
-#pragma unroll
-    for (int t = 0; t < 2; ++t) {
-        const float s_lo = d[t][0] + d[t][1], s_hi = d[t][2] + d[t][3];
-        const float ul = __shfl_sync(0xffffffffu, s_lo, src), uh = __shfl_sync(0xffffffffu, s_hi, src);
-        const float vl = __shfl_sync(0xffffffffu, s_lo, src + 1), vh = __shfl_sync(0xffffffffu, s_hi, src + 1);
-        if (t == mt) { zu = up ? uh : ul; zv = up ? vh : vl; }
-    }
-    const float f = bsc * isc;
-    return make_float2(zu * f, zv * f);
-}
-
 // Inverse coarse operators are stored as FP16, scaled so that the largest
 // entry is 1024 (a CPU probe on LSCM islands: same PCG iterations as FP32,
 // still positive definite), in the first half of the island's FP32 block;
@@ -707,26 +608,7 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
     const float wpin32 = static_cast<float>(I.wpin);
     const int tid = tm.tid, n = I.n;
     const bool two_level = NTT > 32 && I.M > 0;
-    const bool use_bj = (OP == OP_ARAP ? b.bj_a : b.bj_l) != nullptr;
-    const int nsl = (n + 31) >> 5;
-    float2 qreg[R > 0 ? R : 1];   // A p of the thread's rows, then M r
-    // z = M r for row i: block-Jacobi (whole warps: every lane of a slice
-    // calls it) or point Jacobi, plus the coarse correction
-    auto precond = [&](int i, bool valid) {
-        float2 z = make_float2(0.f, 0.f);
-        if (use_bj) {
-            if ((i >> 5) < nsl) z = bj_apply<OP>(b, I.s0, n, i, sr);
-        } else if (valid) {
-            const float2 r = sr[i];
-            const float m = jacobi<OP>(b, I, i);
-            z = make_float2(m * r.x, m * r.y);
-        }
-        if (valid && two_level && !is_pinned<OP>(I, i)) {
-            const float2 y = prolong<NTT, OP>(tm, I, i);
-            z.x += y.x; z.y += y.y;
-        }
-        return z;
-    };
+    float2 qreg[R > 0 ? R : 1];
     int total = 0;
     capped = false;
     nref = 0;
@@ -768,15 +650,15 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
         if (two_level) coarse_solve<NTT, OP>(b, tm, I);
         // ---- inner FP32 PCG on A d = r, d0 = 0
         float red4[4] = {0.f, 0.f, 0.f, 0.f};   // r.z (2), r.r (2)
-        slice_loop<NTT, R>(tid, n, [&](int i, int, bool valid) {
-            const float2 z = precond(i, valid);
-            if (valid) {
-                const float2 r = sr[i];
-                sd[i] = make_float2(0.f, 0.f);
-                sp[i] = z;
-                red4[0] += r.x * z.x; red4[1] += r.y * z.y;
-                red4[2] += r.x * r.x; red4[3] += r.y * r.y;
-            }
+        for_rows<NTT, R>(tid, n, [&](int i, int) {
+            const float2 r = sr[i];
+            const float m = jacobi<OP>(b, I, i);
+            float2 z = make_float2(m * r.x, m * r.y);
+            if (two_level && !is_pinned<OP>(I, i)) { const float2 y = prolong<NTT, OP>(tm, I, i); z.x += y.x; z.y += y.y; }
+            sd[i] = make_float2(0.f, 0.f);
+            sp[i] = z;
+            red4[0] += r.x * z.x; red4[1] += r.y * z.y;
+            red4[2] += r.x * r.x; red4[3] += r.y * r.y;
         });
         team_sum<NTT, 4>(tm, red4, tm.redf);
         float rz[2], thr2[2];
@@ -857,18 +739,15 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
             if (two_level) {
                 tm.sync();   // slice sums complete
                 coarse_solve<NTT, OP>(b, tm, I);
-            } else {
-                __syncwarp();   // a slice's residuals (one warp wrote them) for the block product
             }
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            slice_loop<NTT, R>(tid, n, [&](int i, int j, bool valid) {
-                const float2 z = precond(i, valid);
-                if (valid) {
-                    const float2 r = sr[i];
-                    if constexpr (R > 0) qreg[j] = z; else sq[i] = z;
-                    acc[0] += r.x * z.x; acc[1] += r.y * z.y;
-                    acc[2] += r.x * r.x; acc[3] += r.y * r.y;
-                }
+            for_rows<NTT, R>(tid, n, [&](int i, int) {
+                const float2 r = sr[i];
+                const float m = jacobi<OP>(b, I, i);
+                float zx = m * r.x, zy = m * r.y;
+                if (two_level && !is_pinned<OP>(I, i)) { const float2 y = prolong<NTT, OP>(tm, I, i); zx += y.x; zy += y.y; }
+                acc[0] += r.x * zx; acc[1] += r.y * zy;
+                acc[2] += r.x * r.x; acc[3] += r.y * r.y;
             });
             team_sum<NTT, 4>(tm, acc, tm.redf);
             ++it;
@@ -887,11 +766,12 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
                 if (acc[2] + acc[3] <= thr2[0] || !(s > 0.f)) act[0] = act[1] = false;
             }
             if (!(act[0] || act[1])) break;
-            for_rows<NTT, R>(tid, n, [&](int i, int j) {
-                const float2 p = sp[i];
-                float2 z;
-                if constexpr (R > 0) z = qreg[j]; else z = sq[i];
-                sp[i] = make_float2(fmaf(beta[0], p.x, z.x), fmaf(beta[1], p.y, z.y));
+            for_rows<NTT, R>(tid, n, [&](int i, int) {
+                const float2 r = sr[i], p = sp[i];
+                const float m = jacobi<OP>(b, I, i);
+                float zx = m * r.x, zy = m * r.y;
+                if (two_level && !is_pinned<OP>(I, i)) { const float2 y = prolong<NTT, OP>(tm, I, i); zx += y.x; zy += y.y; }
+                sp[i] = make_float2(fmaf(beta[0], p.x, zx), fmaf(beta[1], p.y, zy));
             });
         }
         if (it >= prm.max_inner) capped = true;
@@ -1387,173 +1267,6 @@ __device__ void store_half_scaled(const double* W, int cnt, float* block, double
     __syncthreads();
 }
 
-// Block-Jacobi inverses for bj_apply: per 32-row slice the diagonal block
-// of the ARAP operator (Laplacian with the soft pin) and of the LSCM
-// operator (complex: -w - i c off the diagonal, the row sum of w on it,
-// hard pins removed), assembled in FP64 from the FP32 slot weights (the
-// matrix the FP32 products apply), inverted by Gauss-Jordan without
-// pivoting (principal blocks of positive (semi)definite operators),
-// made exactly (skew-)symmetric and stored as scaled FP16 MMA fragments.
-// Rows past the island's end, hard-pinned rows and rows whose diagonal is
-// not positive are identity rows; a block whose elimination meets a
-// non-positive pivot keeps its point-Jacobi diagonal instead. One warp per
-// slice, FP64 work matrices in shared memory.
-constexpr int kBjWarps = 2;
-
-template <bool CPLX>
-__device__ void bj_invert(double (*R)[33], double (*Im)[33], int lane, const double* dg, unsigned dead) {
-    // identity rows and columns
-    const bool me_dead = (dead >> lane) & 1u;
-    for (int j = 0; j < 32; ++j) {
-        if (me_dead || ((dead >> j) & 1u)) { R[lane][j] = 0.0; if (CPLX) Im[lane][j] = 0.0; }
-    }
-    R[lane][lane] = me_dead ? 1.0 : dg[lane];
-    if (CPLX) Im[lane][lane] = 0.0;
-    bool ok = true;
-    for (int k = 0; k < 32; ++k) {
-        __syncwarp();
-        const double pr = R[k][k], pi = CPLX ? Im[k][k] : 0.0;
-        ok = ok && pr > 0.0 && isfinite(pr) && isfinite(pi);
-        const double den = pr * pr + pi * pi;
-        const double ir = den > 0.0 ? pr / den : 0.0, ii = den > 0.0 ? -pi / den : 0.0;
-        __syncwarp();
-        {   // row k times 1/p, its diagonal replaced by 1/p
-            const double xr = lane == k ? 1.0 : R[k][lane];
-            const double xi = (lane == k || !CPLX) ? 0.0 : Im[k][lane];
-            R[k][lane] = xr * ir - xi * ii;
-            if (CPLX) Im[k][lane] = xr * ii + xi * ir;
-        }
-        __syncwarp();
-        if (lane != k) {
-            const double fr = R[lane][k], fi = CPLX ? Im[lane][k] : 0.0;
-            for (int j = 0; j < 32; ++j) {
-                const double akr = R[k][j], aki = CPLX ? Im[k][j] : 0.0;
-                const double br = j == k ? 0.0 : R[lane][j];
-                R[lane][j] = br - (fr * akr - fi * aki);
-                if (CPLX) {
-                    const double bi = j == k ? 0.0 : Im[lane][j];
-                    Im[lane][j] = bi - (fr * aki + fi * akr);
-                }
-            }
-        }
-    }
-    __syncwarp();
-    if (!__all_sync(0xffffffffu, ok)) {   // point-Jacobi diagonal instead
-        for (int j = 0; j < 32; ++j) { R[lane][j] = 0.0; if (CPLX) Im[lane][j] = 0.0; }
-        R[lane][lane] = me_dead ? 1.0 : (dg[lane] > 0.0 ? 1.0 / dg[lane] : 1.0);
-    }
-    __syncwarp();
-}
-
-// FP16 fragments of the (skew-)symmetric part of the inverse: tiles (mt, kt)
-// of the real part at out[(2 mt + kt) * 32 + lane], the imaginary part after
-// them; returns the inverse scale.
-template <bool CPLX>
-__device__ float bj_store(double (*R)[33], double (*Im)[33], int lane, uint4* out) {
-    double m = 0.0;
-    for (int j = 0; j < 32; ++j) {
-        m = fmax(m, fabs(0.5 * (R[lane][j] + R[j][lane])));
-        if (CPLX) m = fmax(m, fabs(0.5 * (Im[lane][j] - Im[j][lane])));
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    const double sc = (m > 0.0 && isfinite(m)) ? 1024.0 / m : 1.0;
-    const int g = lane >> 2, tq = lane & 3;
-    auto re = [&](int i, int j) { return static_cast<float>(0.5 * (R[i][j] + R[j][i]) * sc); };
-    auto im = [&](int i, int j) { return static_cast<float>(0.5 * (Im[i][j] - Im[j][i]) * sc); };
-    for (int part = 0; part < (CPLX ? 2 : 1); ++part) {
-        for (int mt = 0; mt < 2; ++mt) {
-            for (int kt = 0; kt < 2; ++kt) {
-                const int ra = 16 * mt + g, rb = ra + 8, ca = 16 * kt + 2 * tq, cb = ca + 8;
-                auto h2 = [&](int i, int j) {
-                    const float x = part ? im(i, j) : re(i, j), y = part ? im(i, j + 1) : re(i, j + 1);
-                    return half2_bits(__floats2half2_rn(x, y));
-                };
-                out[(part * 4 + 2 * mt + kt) * 32 + lane] = make_uint4(h2(ra, ca), h2(rb, ca), h2(ra, cb), h2(rb, cb));
-            }
-        }
-    }
-    return static_cast<float>(1.0 / sc);
-}
-
-__global__ void __launch_bounds__(32 * kBjWarps) k_bjac(uva_batch b) {
-    __shared__ double sre[kBjWarps][32][33], sim[kBjWarps][32][33];
-    __shared__ double sdg[kBjWarps][32];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int gs = blockIdx.x * kBjWarps + warp;
-    if (gs >= b.nslices) return;   // whole warp
-    int lo = 0, hi = b.nc - 1;     // island: the last one whose slices start at or before gs
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (b.sofs[mid] <= gs) lo = mid; else hi = mid - 1;
-    }
-    const int isl = lo;
-    const int v0 = b.vofs[isl], n = b.vofs[isl + 1] - v0, ls = gs - b.sofs[isl], r = 32 * ls + lane;
-    const bool live = r < n;
-    const int pin = b.vert_row[v0 + b.pins[3 * isl]];
-    const int p0v = b.pins[3 * isl + 1], p1v = b.pins[3 * isl + 2];
-    const int p0 = p0v >= 0 ? b.vert_row[v0 + p0v] : -1, p1 = p1v >= 0 ? b.vert_row[v0 + p1v] : -1;
-    double (*R)[33] = sre[warp];
-    double (*Im)[33] = sim[warp];
-    double* dg = sdg[warp];
-    const int2* cw = reinterpret_cast<const int2*>(b.slot_cw);
-    const int q0 = b.slice_ptr[gs] + lane, width = (b.slice_ptr[gs + 1] - b.slice_ptr[gs]) >> 5;
-    auto assemble = [&](bool cplx) {
-        for (int j = 0; j < 32; ++j) { R[lane][j] = 0.0; if (cplx) Im[lane][j] = 0.0; }
-        double d = 0.0;
-        if (live) {
-            for (int k = 0; k < width; ++k) {
-                const int2 sl = __ldg(cw + q0 + 32 * k);
-                const int col = slot_row(sl.x);
-                if (col == r) continue;
-                const double w = static_cast<double>(__int_as_float(sl.y));
-                d += w;
-                if ((col >> 5) == ls) {
-                    R[lane][col & 31] -= w;
-                    if (cplx) Im[lane][col & 31] -= 0.5 * static_cast<double>(slot_c2(sl.x));
-                }
-            }
-        }
-        return d;
-    };
-    // ARAP: Laplacian + soft pin
-    double d = assemble(false);
-    if (r == pin) d += b.wpin[isl];
-    dg[lane] = d;
-    unsigned dead = __ballot_sync(0xffffffffu, !live || !(d > 0.0));
-    __syncwarp();
-    bj_invert<false>(R, Im, lane, dg, dead);
-    uint4* outa = reinterpret_cast<uint4*>(b.bj_a) + static_cast<size_t>(gs) * 128;
-    const float sa = bj_store<false>(R, Im, lane, outa);
-    __syncwarp();
-    // LSCM: complex block over the free unknowns
-    d = assemble(true);
-    dg[lane] = d;
-    dead = __ballot_sync(0xffffffffu, !live || r == p0 || r == p1 || !(d > 0.0));
-    __syncwarp();
-    bj_invert<true>(R, Im, lane, dg, dead);
-    uint4* outl = reinterpret_cast<uint4*>(b.bj_l) + static_cast<size_t>(gs) * 256;
-    const float sl = bj_store<true>(R, Im, lane, outl);
-    if (lane == 0) { b.bj_s[2 * gs] = sa; b.bj_s[2 * gs + 1] = sl; }
-}
-
-// z = C r of every slice (bj_apply over the whole batch); r and z by solver
-// row (n * 2 floats). A test hook of the block inverses.
-template <Op OP>
-__global__ void k_bjac_apply(uva_batch b, const float2* r, float2* z) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= b.nslices) return;
-    int lo = 0, hi = b.nc - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (b.sofs[mid] <= warp) lo = mid; else hi = mid - 1;
-    }
-    const int v0 = b.vofs[lo], n = b.vofs[lo + 1] - v0, s0 = b.sofs[lo];
-    const int i = 32 * (warp - s0) + lane;
-    const float2 zi = bj_apply<OP>(b, s0, n, i, r + v0);
-    if (i < n) z[v0 + i] = zi;
-}
-
 constexpr int kCoarseSmemN = 128;
 constexpr size_t kCoarseSmem = sizeof(double) * kCoarseSmemN * kCoarseSmemN;   // 131,072 bytes
 
@@ -2043,26 +1756,6 @@ extern "C" int uva_batch_setup(uva_batch* b, void* stream) {
         k_coarse<<<b->nc, 1024, kCoarseSmem, s>>>(*b);
         UVA_CHECK_LAUNCH("uva_batch_setup/coarse");
     }
-    if (b->bj_a && b->bj_l && b->bj_s && b->nslices > 0) {
-        k_bjac<<<(b->nslices + kBjWarps - 1) / kBjWarps, 32 * kBjWarps, 0, s>>>(*b);
-        UVA_CHECK_LAUNCH("uva_batch_setup/block jacobi");
-    }
-    return UVA_OK;
-}
-
-extern "C" int uva_bjac_apply(const uva_batch* b, int32_t op, const float* r, float* z, void* stream) {
-    if (!check_batch(b) || !b->bj_a || !b->bj_l || !b->bj_s || !r || !z || (op != 0 && op != 1)) {
-        uva_set_error("uva_bjac_apply: bad arguments (block inverses, r and z are required)");
-        return UVA_E_ARG;
-    }
-    if (b->nslices == 0) return UVA_OK;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int grid = (b->nslices + 7) / 8;
-    const float2* r2 = reinterpret_cast<const float2*>(r);
-    float2* z2 = reinterpret_cast<float2*>(z);
-    if (op == 0) k_bjac_apply<OP_ARAP><<<grid, 256, 0, s>>>(*b, r2, z2);
-    else k_bjac_apply<OP_LSCM><<<grid, 256, 0, s>>>(*b, r2, z2);
-    UVA_CHECK_LAUNCH("uva_bjac_apply");
     return UVA_OK;
 }
 

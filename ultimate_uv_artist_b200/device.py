@@ -173,7 +173,7 @@ class DeviceBatch:
     """Islands resident on one CUDA device, ready for the uva_* kernels."""
 
     def __init__(self, P, T_local, vofs, tofs, U=None, semantics=_lib.SEM_BATCH, device=None, stream=None,
-                 plan=None, block_jacobi=True):
+                 plan=None):
         self.dev = require_cuda(device)
         self.stream = stream
         self.semantics = int(semantics)
@@ -240,14 +240,6 @@ class DeviceBatch:
         self.q32 = torch.empty((n, 2), dtype=f32, device=d)
         self.status = torch.zeros((nc, C.sizeof(_lib.IslandStatus)), dtype=torch.uint8, device=d)
         self.work = torch.zeros(8, dtype=torch.int32, device=d)
-        # block-Jacobi smoother: FP16 inverses of the 32-row diagonal blocks
-        # (6 KB per slice for ARAP + LSCM); block_jacobi=False keeps point Jacobi
-        ns = max(plan.nslices, 1)
-        self.block_jacobi = bool(block_jacobi)
-        if self.block_jacobi:
-            self.bj_a = torch.empty(1024 * ns, dtype=torch.int16, device=d)
-            self.bj_l = torch.empty(2048 * ns, dtype=torch.int16, device=d)
-            self.bj_s = torch.empty(2 * ns, dtype=f32, device=d)
         self.rev_ctas = tuned["rev_ctas"] if tuned is not None else 0   # schedule knob (autotune.tune)
         self.desc = self._make_desc()
         self.setup()
@@ -266,8 +258,6 @@ class DeviceBatch:
                      "slot_cw", "wdiag", "dinv", "pins", "wpin", "U", "x64", "b64", "rc", "r32", "d32", "p32",
                      "q32", "status", "work"):
             setattr(D, name, getattr(self, name).data_ptr())
-        if self.block_jacobi:
-            D.bj_a, D.bj_l, D.bj_s = self.bj_a.data_ptr(), self.bj_l.data_ptr(), self.bj_s.data_ptr()
         return D
 
     def _refresh_u(self):
