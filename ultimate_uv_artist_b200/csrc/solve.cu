@@ -132,6 +132,16 @@ __global__ void k_rows(uva_batch b, const int32_t* vert_isl) {
     }
     b.wdiag[v] = sum;
     b.dinv[v] = sum > 1e-30 ? static_cast<float>(1.0 / sum) : 1.0f;
+    // the island's last row also fills the padding rows of its slice (the
+    // plan's zero-weight slots): the solver's slice-wide products read them
+    const int n = b.vofs[isl + 1] - b.vofs[isl];
+    if (i == n - 1) {
+        for (int r = i + 1; r < ((n + 31) & ~31); ++r) {
+            const int qr = b.slice_ptr[s] + (r & 31);
+            for (int k = 0; k < width; ++k)
+                reinterpret_cast<int2*>(b.slot_cw)[qr + 32 * k] = make_int2(b.slot_col[qr + 32 * k], 0);
+        }
+    }
 }
 
 // LSCM pins: the far boundary pair of engine/param.py:172-179, evaluated in
@@ -440,28 +450,44 @@ __device__ __forceinline__ float2 apply32(const uva_batch& b, const Isl& I, int 
     return make_float2(ax, ay);
 }
 
-// Inverse Jacobi diagonal of row i: 0 on the LSCM hard pins, the ARAP pin
-// row includes the soft-pin weight.
+// Four slots of one row of (A p), accumulated into (ax, ay).
+template <Op OP>
+__device__ __forceinline__ void row_group4(const int2* cw, int q, const float2* p, float2 x, float& ax, float& ay) {
+    int2 s[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) s[u] = __ldg(cw + q + 32 * u);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const float2 y = p[slot_row(s[u].x)];
+        const float w = __int_as_float(s[u].y);
+        ax = fmaf(w, x.x - y.x, ax);
+        ay = fmaf(w, x.y - y.y, ay);
+    }
+    if (OP == OP_LSCM && ((s[0].x | s[1].x | s[2].x | s[3].x) >> 24) != 0) lscm_coupling(s, p, ax, ay);
+}
+
 // (A p) for two rows of one thread at once (rows of different slices):
 // the slot loads of both rows are in flight together, which halves the
-// chain of dependent L2 round trips of the single-row product.
+// chain of dependent L2 round trips of the single-row product. Row ib is
+// used only when hb (its slice exists); widths are per slice, so every loop
+// bound is the same on all lanes of the warp.
 template <Op OP>
-__device__ __forceinline__ void apply32_pair(const uva_batch& b, const Isl& I, int ia, int ib, bool vb,
+__device__ __forceinline__ void apply32_pair(const uva_batch& b, const Isl& I, int ia, int ib, bool hb,
                                              const float2* p, float wpin32, float2& qa, float2& qb) {
     int q0a, wa, q0b = 0, wb = 0;
     row_slots(b, I, ia, q0a, wa);
-    if (vb) row_slots(b, I, ib, q0b, wb);
+    if (hb) row_slots(b, I, ib, q0b, wb);
     const int2* cw = reinterpret_cast<const int2*>(b.slot_cw);
-    const float2 xa = p[ia], xb = vb ? p[ib] : make_float2(0.f, 0.f);
+    const float2 xa = p[ia], xb = hb ? p[ib] : make_float2(0.f, 0.f);
     float ax = 0.f, ay = 0.f, bx = 0.f, by = 0.f;
-    const int wmax = max(wa, wb);
-    for (int k = 0; k < wmax; k += 4) {
+    const int wmin = min(wa, wb);
+    int k = 0;
+    for (; k < wmin; k += 4) {
         int2 sa[4], sb[4];
-        const bool ha = k < wa, hb = k < wb;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            sa[u] = ha ? __ldg(cw + q0a + 32 * (k + u)) : make_int2(ia, 0);
-            sb[u] = hb ? __ldg(cw + q0b + 32 * (k + u)) : make_int2(ib, 0);
+            sa[u] = __ldg(cw + q0a + 32 * (k + u));
+            sb[u] = __ldg(cw + q0b + 32 * (k + u));
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -479,12 +505,16 @@ __device__ __forceinline__ void apply32_pair(const uva_batch& b, const Isl& I, i
             if (((sb[0].x | sb[1].x | sb[2].x | sb[3].x) >> 24) != 0) lscm_coupling(sb, p, bx, by);
         }
     }
+    for (int ka = k; ka < wa; ka += 4) row_group4<OP>(cw, q0a + 32 * ka, p, xa, ax, ay);
+    for (int kb = k; kb < wb; kb += 4) row_group4<OP>(cw, q0b + 32 * kb, p, xb, bx, by);
     if (OP == OP_ARAP && ia == I.pin) { ax = fmaf(wpin32, xa.x, ax); ay = fmaf(wpin32, xa.y, ay); }
     if (OP == OP_ARAP && ib == I.pin) { bx = fmaf(wpin32, xb.x, bx); by = fmaf(wpin32, xb.y, by); }
     qa = is_pinned<OP>(I, ia) ? make_float2(0.f, 0.f) : make_float2(ax, ay);
-    qb = (vb && !is_pinned<OP>(I, ib)) ? make_float2(bx, by) : make_float2(0.f, 0.f);
+    qb = (hb && !is_pinned<OP>(I, ib)) ? make_float2(bx, by) : make_float2(0.f, 0.f);
 }
 
+// Inverse Jacobi diagonal of row i: 0 on the LSCM hard pins, the ARAP pin
+// row includes the soft-pin weight.
 template <Op OP>
 __device__ __forceinline__ float jacobi_global(const uva_batch& b, const Isl& I, int i) {
     if (is_pinned<OP>(I, i)) return 0.0f;
@@ -506,10 +536,15 @@ __device__ __forceinline__ float jacobi(const uva_batch& b, const Isl& I, int i)
 // Inverse coarse operators are stored as FP16, scaled so that the largest
 // entry is 1024 (a CPU probe on LSCM islands: same PCG iterations as FP32,
 // still positive definite), in the first half of the island's FP32 block;
-// the float after the halves holds the inverse of the scale.
+// the float after the halves holds the inverse of the scale. Rows are padded
+// (zeros) to a stride of a whole number of vector loads: 2 halves for ARAP
+// (4-byte aligned blocks), 4 for LSCM (16-byte aligned blocks).
 __host__ __device__ __forceinline__ const float* coarse_scale(const float* block, int nhalf) {
     return block + (nhalf + 1) / 2;
 }
+template <Op OP>
+__host__ __device__ constexpr int coarse_vec() { return OP == OP_ARAP ? 2 : 4; }
+__host__ __device__ constexpr int coarse_stride(int N, int vec) { return (N + vec - 1) / vec * vec; }
 
 // Two-level additive preconditioner z = D^-1 r + P Ac^-1 P^T r. P is the
 // piecewise-constant prolongation over aggregates of `agg` consecutive solver
@@ -551,33 +586,62 @@ __device__ __forceinline__ void coarse_solve(const uva_batch& b, Team<NTT>& tm, 
         else { tm.cg[2 * a] = gx; tm.cg[2 * a + 1] = gy; }
     }
     tm.sync();   // g complete
-    if (OP == OP_ARAP) {
-        const __half* A = reinterpret_cast<const __half*>(b.coarse_a + I.co);
-        const float isc = __ldg(coarse_scale(b.coarse_a + I.co, I.M * I.M));
-        for (int o = warp; o < I.M; o += NW) {
-            float au = 0.f, av = 0.f;
-            for (int c = lane; c < I.M; c += 32) {
-                const float w = __half2float(A[static_cast<size_t>(o) * I.M + c]);
-                au = fmaf(w, tm.cg[c], au);
-                av = fmaf(w, tm.cg[I.M + c], av);
-            }
+    // y = Ac^-1 g, one warp per coarse row. A lane takes VEC consecutive
+    // columns of every (32 VEC)-column chunk with one vector load per row and
+    // keeps its part of g in registers for all the rows it visits.
+    constexpr int VEC = coarse_vec<OP>();
+    constexpr int NR = OP == OP_ARAP ? 2 : 1;   // right-hand sides (ARAP: u and v)
+    constexpr int CH = 4;                        // chunks: N <= 256 (ARAP), 512 (LSCM)
+    const int N = OP == OP_ARAP ? I.M : 2 * I.M;
+    const int S = coarse_stride(N, VEC);
+    const float* blockf = OP == OP_ARAP ? b.coarse_a + I.co : b.coarse_l + 4 * static_cast<size_t>(I.co);
+    const __half* A = reinterpret_cast<const __half*>(blockf);
+    const float isc = __ldg(coarse_scale(blockf, N * S));
+    float gr[NR][CH][VEC];
 #pragma unroll
-            for (int k = 16; k > 0; k >>= 1) {
-                au += __shfl_xor_sync(0xffffffffu, au, k);
-                av += __shfl_xor_sync(0xffffffffu, av, k);
-            }
-            if (lane == 0) { tm.cy[o] = au * isc; tm.cy[I.M + o] = av * isc; }
+    for (int ch = 0; ch < CH; ++ch) {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) {
+            const int c = 32 * VEC * ch + VEC * lane + e;
+#pragma unroll
+            for (int r = 0; r < NR; ++r) gr[r][ch][e] = c < N ? tm.cg[r * N + c] : 0.f;
         }
-    } else {
-        const int N = 2 * I.M;
-        const __half* A = reinterpret_cast<const __half*>(b.coarse_l + 4 * static_cast<size_t>(I.co));
-        const float isc = __ldg(coarse_scale(b.coarse_l + 4 * static_cast<size_t>(I.co), N * N));
-        for (int o = warp; o < N; o += NW) {
-            float acc = 0.f;
-            for (int c = lane; c < N; c += 32) acc = fmaf(__half2float(A[static_cast<size_t>(o) * N + c]), tm.cg[c], acc);
+    }
+    for (int o = warp; o < N; o += NW) {
+        const __half* row = A + static_cast<size_t>(o) * S;
+        float acc[NR];
 #pragma unroll
-            for (int k = 16; k > 0; k >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, k);
-            if (lane == 0) tm.cy[o] = acc * isc;
+        for (int r = 0; r < NR; ++r) acc[r] = 0.f;
+#pragma unroll
+        for (int ch = 0; ch < CH; ++ch) {
+            const int c0 = 32 * VEC * ch + VEC * lane;
+            if (c0 < S) {
+                float a[VEC];
+                if constexpr (VEC == 4) {
+                    const uint2 raw = __ldg(reinterpret_cast<const uint2*>(row + c0));
+                    const float2 f01 = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
+                    const float2 f23 = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
+                    a[0] = f01.x; a[1] = f01.y; a[2] = f23.x; a[3] = f23.y;
+                } else {
+                    const unsigned raw = __ldg(reinterpret_cast<const unsigned*>(row + c0));
+                    const float2 f01 = __half22float2(*reinterpret_cast<const __half2*>(&raw));
+                    a[0] = f01.x; a[1] = f01.y;
+                }
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) {
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) acc[r] = fmaf(a[e], gr[r][ch][e], acc[r]);
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+#pragma unroll
+            for (int k = 16; k > 0; k >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], k);
+        }
+        if (lane == 0) {
+            if (OP == OP_ARAP) { tm.cy[o] = acc[0] * isc; tm.cy[I.M + o] = acc[NR - 1] * isc; }
+            else tm.cy[o] = acc[0] * isc;
         }
     }
     tm.sync();   // y complete
@@ -685,18 +749,24 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
             float pq[2] = {0.f, 0.f};
             if constexpr (R > 0) {
 #pragma unroll
+                // whole slices at a time (a warp's lanes are one slice, so the
+                // branch and the widths are the same on every lane); rows past
+                // the island's end compute zero-weight padding and are dropped
+                const int nsl = (n + 31) >> 5;
                 for (int j = 0; j < R; j += 2) {
                     const int ia = tid + j * NTT, ib = ia + NTT;
-                    if (ia < n) {
-                        const bool vb = j + 1 < R && ib < n;
+                    if ((ia >> 5) < nsl) {
+                        const bool sb = j + 1 < R && (ib >> 5) < nsl;
                         float2 qa, qb;
-                        apply32_pair<OP>(b, I, ia, ib, vb, sp, wpin32, qa, qb);
+                        apply32_pair<OP>(b, I, ia, ib, sb, sp, wpin32, qa, qb);
                         qreg[j] = qa;
-                        const float2 pa = sp[ia];
-                        pq[0] += pa.x * qa.x; pq[1] += pa.y * qa.y;
+                        if (ia < n) {
+                            const float2 pa = sp[ia];
+                            pq[0] += pa.x * qa.x; pq[1] += pa.y * qa.y;
+                        }
                         if (j + 1 < R) {
                             qreg[j + 1] = qb;
-                            if (vb) {
+                            if (sb && ib < n) {
                                 const float2 pb = sp[ib];
                                 pq[0] += pb.x * qb.x; pq[1] += pb.y * qb.y;
                             }
@@ -1247,10 +1317,11 @@ __device__ void gauss_jordan(double* W, int N, double* colk) {
 // stored in FP32. One thread owns each coarse row and adds its terms in
 // slot order, so the operators are the same bits on every run. The
 // inversion works in shared memory when the block fits (kCoarseSmemN).
-// W (FP64) -> FP16 halves scaled to a largest entry of 1024, plus the
-// inverse scale after them (coarse_scale); `red` is >= 32 doubles of
-// shared memory. Whole CTA.
-__device__ void store_half_scaled(const double* W, int cnt, float* block, double* red) {
+// W (FP64, N x N) -> FP16 halves scaled to a largest entry of 1024, in rows
+// of stride S (zero padding), plus the inverse scale after them
+// (coarse_scale); `red` is >= 32 doubles of shared memory. Whole CTA.
+__device__ void store_half_scaled(const double* W, int N, int S, float* block, double* red) {
+    const int cnt = N * N;
     double m = 0.0;
     for (int e = threadIdx.x; e < cnt; e += blockDim.x) m = fmax(m, fabs(W[e]));
 #pragma unroll
@@ -1262,8 +1333,11 @@ __device__ void store_half_scaled(const double* W, int cnt, float* block, double
     for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
     const double sc = (m > 0.0 && isfinite(m)) ? 1024.0 / m : 1.0;
     __half* h = reinterpret_cast<__half*>(block);
-    for (int e = threadIdx.x; e < cnt; e += blockDim.x) h[e] = __double2half(W[e] * sc);
-    if (threadIdx.x == 0) *const_cast<float*>(coarse_scale(block, cnt)) = static_cast<float>(1.0 / sc);
+    for (int e = threadIdx.x; e < N * S; e += blockDim.x) {   // rows padded to the stride S
+        const int r = e / S, c = e - r * S;
+        h[e] = c < N ? __double2half(W[static_cast<size_t>(r) * N + c] * sc) : __double2half(0.0);
+    }
+    if (threadIdx.x == 0) *const_cast<float*>(coarse_scale(block, N * S)) = static_cast<float>(1.0 / sc);
     __syncthreads();
 }
 
@@ -1316,7 +1390,7 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
         Wa[a] += dsum;
     }
     gauss_jordan(W, M, colk);
-    store_half_scaled(W, M * M, b.coarse_a + co, colk);
+    store_half_scaled(W, M, coarse_stride(M, coarse_vec<OP_ARAP>()), b.coarse_a + co, colk);
     __syncthreads();
     // ---- LSCM (free unknowns only; the pins are fixed)
     const int pv0 = b.pins[3 * isl + 1], pv1 = b.pins[3 * isl + 2];
@@ -1365,7 +1439,7 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
         Wv[2 * a] += cvu;
     }
     gauss_jordan(W, N, colk);
-    store_half_scaled(W, N * N, b.coarse_l + 4 * static_cast<size_t>(co), colk);
+    store_half_scaled(W, N, coarse_stride(N, coarse_vec<OP_LSCM>()), b.coarse_l + 4 * static_cast<size_t>(co), colk);
 }
 
 cudaError_t ensure_coarse_attr() {
