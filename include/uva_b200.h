@@ -142,7 +142,7 @@ typedef struct uva_batch {
                                  the inverse scale (FP32)                      */
     float*  coarse_l;         /* 4*cofs[nc] floats: the same for LSCM          */
     double* coarse_work;      /* 4*cofs[nc]: FP64 workspace of the setup        */
-    float*  cpart;            /* 2*nslices: per-slice residual sums (solve scratch) */
+    float*  cpart;            /* 2*nslices floats of solve scratch (reserved)   */
     int32_t class_ofs[5];     /* host values: class c owns order[ofs[c]..ofs[c+1]) */
     /* geometry, written by uva_batch_setup */
     const double*  P;         /* n*3 positions (FP64)                          */

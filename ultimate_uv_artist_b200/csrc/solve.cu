@@ -227,8 +227,6 @@ struct Team {
     float *cg, *cy;         // coarse restriction / coarse solution (shared memory)
     int* sc;                // slice-pointer cache of the current island (shared memory)
     int sc_cap;             // its capacity (slices + 1)
-    float2* pc;             // per-slice residual sums (shared memory, or null)
-    int pc_cap;             // its capacity (slices)
     __nv_bfloat16* dc;      // Jacobi diagonal of the current island (shared memory, or null)
     int dc_cap;             // its capacity (rows)
     __device__ __forceinline__ void sync() { team_sync<NTT>(bar); }
@@ -339,7 +337,6 @@ struct Isl {
     int agg, M, co;           // rows per aggregate, aggregates (0: Jacobi only), coarse offset
     int aggsh;                // log2(agg) when agg is a power of two, else -1
     const int* sptr;          // slot offsets of the island's slices (shared-memory cache or global)
-    float2* part;             // per-slice residual sums (shared memory or b.cpart)
     const __nv_bfloat16* dv;  // Jacobi diagonal in shared memory (null: read b.dinv)
     double wpin;
 };
@@ -361,7 +358,6 @@ __device__ __forceinline__ Isl load_island(const uva_batch& b, int isl) {
     I.co = b.cofs[isl];
     I.aggsh = (I.agg > 0 && (I.agg & (I.agg - 1)) == 0) ? __ffs(I.agg) - 1 : -1;
     I.sptr = b.slice_ptr + I.s0;
-    I.part = reinterpret_cast<float2*>(b.cpart) + I.s0;
     I.dv = nullptr;
     I.wpin = b.wpin[isl];
     return I;
@@ -548,42 +544,38 @@ __host__ __device__ constexpr int coarse_stride(int N, int vec) { return (N + ve
 
 // Two-level additive preconditioner z = D^-1 r + P Ac^-1 P^T r. P is the
 // piecewise-constant prolongation over aggregates of `agg` consecutive solver
-// rows (compact mesh blobs from the plan; agg is a multiple of 128, so an
+// rows (compact mesh blobs from the plan; agg is a multiple of 64, so an
 // aggregate is agg/32 whole slices), Ac = P^T A P is inverted once per batch
-// by the setup. Restriction is deterministic: each warp writes the sum of its
-// slice (one warp owns one slice in slice_loop) to the slice sums (shared
-// memory when the team has room, else b.cpart), and coarse_solve
-// adds the slices of each aggregate in slice order before the dense product
-// with Ac^-1 (one warp per output row).
+// by the setup.
+// y = Ac^-1 P^T r for the residual r (complete: a team barrier precedes the
+// call). The restriction g = P^T r is deterministic: T threads per aggregate
+// (a power of two, T * M <= NTT where possible) add rows a*agg + t, + T, ...
+// and fold with xor shuffles in a fixed order. Ends with a barrier: y complete.
 template <int NTT, Op OP>
-__device__ __forceinline__ void coarse_restrict(const uva_batch& b, Team<NTT>& tm, const Isl& I, int i, bool valid,
-                                                float2 r) {
-    float rx = valid ? r.x : 0.f, ry = valid ? r.y : 0.f;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        rx += __shfl_xor_sync(0xffffffffu, rx, o);
-        ry += __shfl_xor_sync(0xffffffffu, ry, o);
-    }
-    if ((tm.tid & 31) == 0 && (i - (tm.tid & 31)) < I.n)
-        I.part[i >> 5] = make_float2(rx, ry);
-}
-
-// y = Ac^-1 g, g gathered from the slice sums of the last restriction (which a
-// team barrier completed). Ends with a barrier: y complete, slice sums free.
-template <int NTT, Op OP>
-__device__ __forceinline__ void coarse_solve(const uva_batch& b, Team<NTT>& tm, const Isl& I) {
+__device__ __forceinline__ void coarse_solve(const uva_batch& b, Team<NTT>& tm, const Isl& I, const float2* r) {
     constexpr int NW = NTT / 32;
     const int lane = tm.tid & 31, warp = tm.tid >> 5;
-    const float2* part = I.part;
-    const int spa = I.agg >> 5, nsl = (I.n + 31) >> 5;
-    for (int a = tm.tid; a < I.M; a += NTT) {
+    int lt = 5;   // log2 T
+    while (lt > 0 && (I.M << lt) > NTT) --lt;
+    const int T = 1 << lt, groups = NTT >> lt;
+    for (int base = 0; base < I.M; base += groups) {   // the same trip count on every thread
+        const int a = base + (tm.tid >> lt), t = tm.tid & (T - 1);
         float gx = 0.f, gy = 0.f;
-        for (int s = a * spa; s < min((a + 1) * spa, nsl); ++s) {
-            const float2 p = part[s];
-            gx += p.x; gy += p.y;
+        if (a < I.M) {
+            const int r1 = min((a + 1) * I.agg, I.n);
+            for (int i = a * I.agg + t; i < r1; i += T) {
+                const float2 v = r[i];
+                gx += v.x; gy += v.y;
+            }
         }
-        if (OP == OP_ARAP) { tm.cg[a] = gx; tm.cg[I.M + a] = gy; }
-        else { tm.cg[2 * a] = gx; tm.cg[2 * a + 1] = gy; }
+        for (int o = T >> 1; o > 0; o >>= 1) {
+            gx += __shfl_xor_sync(0xffffffffu, gx, o);
+            gy += __shfl_xor_sync(0xffffffffu, gy, o);
+        }
+        if (t == 0 && a < I.M) {
+            if (OP == OP_ARAP) { tm.cg[a] = gx; tm.cg[I.M + a] = gy; }
+            else { tm.cg[2 * a] = gx; tm.cg[2 * a + 1] = gy; }
+        }
     }
     tm.sync();   // g complete
     // y = Ac^-1 g, one warp per coarse row. A lane takes VEC consecutive
@@ -679,21 +671,16 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
     for (int ref = 0;; ++ref) {
         // ---- FP64 residual r = rhs - A x; restriction of r for the coarse level
         double rr[2] = {0.0, 0.0};
-        slice_loop<NTT, R>(tid, n, [&](int i, int, bool valid) {
-            float2 r32 = make_float2(0.f, 0.f);
-            if (valid) {
-                double2 r = make_double2(0.0, 0.0);
-                if (!is_pinned<OP>(I, i)) {
-                    const double2 ax = apply64<OP>(b, I, i, x64);
-                    const double2 rhs = OP == OP_ARAP ? b64[i] : make_double2(0.0, 0.0);
-                    r = make_double2(rhs.x - ax.x, rhs.y - ax.y);
-                }
-                r32 = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
-                sr[i] = r32;
-                rr[0] += r.x * r.x;
-                rr[1] += r.y * r.y;
+        for_rows<NTT, R>(tid, n, [&](int i, int) {
+            double2 r = make_double2(0.0, 0.0);
+            if (!is_pinned<OP>(I, i)) {
+                const double2 ax = apply64<OP>(b, I, i, x64);
+                const double2 rhs = OP == OP_ARAP ? b64[i] : make_double2(0.0, 0.0);
+                r = make_double2(rhs.x - ax.x, rhs.y - ax.y);
             }
-            if (two_level) coarse_restrict<NTT, OP>(b, tm, I, i, valid, r32);
+            sr[i] = make_float2(static_cast<float>(r.x), static_cast<float>(r.y));
+            rr[0] += r.x * r.x;
+            rr[1] += r.y * r.y;
         });
         team_sum<NTT, 2>(tm, rr, tm.redd);
         ++nref;
@@ -711,7 +698,7 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
             if (!done) capped = true;
             break;
         }
-        if (two_level) coarse_solve<NTT, OP>(b, tm, I);
+        if (two_level) coarse_solve<NTT, OP>(b, tm, I, sr);
         // ---- inner FP32 PCG on A d = r, d0 = 0
         float red4[4] = {0.f, 0.f, 0.f, 0.f};   // r.z (2), r.r (2)
         for_rows<NTT, R>(tid, n, [&](int i, int) {
@@ -748,7 +735,6 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
             tm.sync();   // p complete
             float pq[2] = {0.f, 0.f};
             if constexpr (R > 0) {
-#pragma unroll
                 // whole slices at a time (a warp's lanes are one slice, so the
                 // branch and the widths are the same on every lane); rows past
                 // the island's end compute zero-weight padding and are dropped
@@ -791,24 +777,19 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
                 const float s = pq[0] + pq[1];
                 alpha[0] = alpha[1] = (act[0] && s > 0.f) ? rz[0] / s : 0.f;
             }
-            // update d, r; restrict r
-            slice_loop<NTT, R>(tid, n, [&](int i, int j, bool valid) {
-                float2 r = make_float2(0.f, 0.f);
-                if (valid) {
-                    float2 q;
-                    if constexpr (R > 0) q = qreg[j]; else q = sq[i];
-                    const float2 p = sp[i];
-                    float2 d = sd[i];
-                    r = sr[i];
-                    d.x = fmaf(alpha[0], p.x, d.x); d.y = fmaf(alpha[1], p.y, d.y);
-                    r.x = fmaf(-alpha[0], q.x, r.x); r.y = fmaf(-alpha[1], q.y, r.y);
-                    sd[i] = d; sr[i] = r;
-                }
-                if (two_level) coarse_restrict<NTT, OP>(b, tm, I, i, valid, r);
+            // update d, r
+            for_rows<NTT, R>(tid, n, [&](int i, int j) {
+                float2 q;
+                if constexpr (R > 0) q = qreg[j]; else q = sq[i];
+                const float2 p = sp[i];
+                float2 d = sd[i], r = sr[i];
+                d.x = fmaf(alpha[0], p.x, d.x); d.y = fmaf(alpha[1], p.y, d.y);
+                r.x = fmaf(-alpha[0], q.x, r.x); r.y = fmaf(-alpha[1], q.y, r.y);
+                sd[i] = d; sr[i] = r;
             });
             if (two_level) {
-                tm.sync();   // slice sums complete
-                coarse_solve<NTT, OP>(b, tm, I);
+                tm.sync();   // residual complete
+                coarse_solve<NTT, OP>(b, tm, I, sr);
             }
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
             for_rows<NTT, R>(tid, n, [&](int i, int) {
@@ -1199,8 +1180,8 @@ __device__ __forceinline__ void run_class(const uva_batch& b, const uva_solve_pa
         }
         const long long t0 = global_ns();
         // shared-memory copies of the island's slice pointers and Jacobi
-        // diagonal, and room for its slice sums (the previous island ended
-        // with a team barrier, so the buffers are free)
+        // diagonal (the previous island ended with a team barrier, so the
+        // buffers are free)
         // (classes with R > 0 always fit the caches: their islands have at
         // most NTT * R rows; the choice is then fixed at compile time)
         const int nsl1 = ((I.n + 31) >> 5) + 1;
@@ -1210,7 +1191,6 @@ __device__ __forceinline__ void run_class(const uva_batch& b, const uva_solve_pa
             I.sptr = tm.sc;
             cached = true;
         }
-        if ((R > 0 && NTT > 32) || (tm.pc && nsl1 - 1 <= tm.pc_cap)) I.part = tm.pc;
         if (R > 0 || (tm.dc && I.n <= tm.dc_cap)) {
             for (int i = tm.tid; i < I.n; i += NTT) tm.dc[i] = __float2bfloat16(jacobi_global<OP>(b, I, i));
             I.dv = tm.dc;
@@ -1242,12 +1222,11 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
     __shared__ int slots[8];
     __shared__ float coarse_buf[1024];   // g and y of the coarse level (CTA: 512 each; sub-team: 128 each)
     __shared__ int sc_buf[288];          // slice pointers (CTA: 288; sub-team: 72 each; warp: 9 each)
-    __shared__ float2 part_buf[256];     // slice sums (CTA: 256; sub-team: 64 each)
     __shared__ __nv_bfloat16 dinv_buf[KB * RB];   // Jacobi (CTA: 8192; sub-team: 2048; warp: 256)
     const bool rev = static_cast<int>(blockIdx.x) < nrev;
     auto whole_cta = [&]() {
         Team<KB> tm{static_cast<int>(threadIdx.x), 0, 0, redd, redf, redi, &slots[0], nullptr, nullptr, nullptr,
-                    coarse_buf, coarse_buf + 512, sc_buf, 288, part_buf, 256, dinv_buf, KB * RB};
+                    coarse_buf, coarse_buf + 512, sc_buf, 288, dinv_buf, KB * RB};
         run_class<KB, 0, OP>(b, prm, tm, 0);
         tm.sp = dyn; tm.sr = dyn + KB * RB; tm.sd = dyn + 2 * KB * RB;
         run_class<KB, RB, OP>(b, prm, tm, 1);
@@ -1259,7 +1238,7 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
         float2* base = dyn + s * (3 * SUB * RB);
         Team<SUB> tm{static_cast<int>(threadIdx.x % SUB), 1 + s, 0, redd + s * 64, redf + s * 64, redi + s * 16,
                      &slots[1 + s], base, base + SUB * RB, base + 2 * SUB * RB, coarse_buf + 256 * s,
-                     coarse_buf + 256 * s + 128, sc_buf + 72 * s, 72, part_buf + 64 * s, 64,
+                     coarse_buf + 256 * s + 128, sc_buf + 72 * s, 72,
                      dinv_buf + SUB * RB * s, SUB * RB};
         run_class<SUB, RB, OP>(b, prm, tm, 2);
     };
@@ -1267,7 +1246,7 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
         const int w = threadIdx.x / 32;
         float2* base = dyn + w * (3 * 32 * RB);
         Team<32> tm{static_cast<int>(threadIdx.x % 32), 0, 0, nullptr, nullptr, nullptr, nullptr,
-                    base, base + 32 * RB, base + 2 * 32 * RB, nullptr, nullptr, sc_buf + 9 * w, 9, nullptr, 0,
+                    base, base + 32 * RB, base + 2 * 32 * RB, nullptr, nullptr, sc_buf + 9 * w, 9,
                     dinv_buf + 32 * RB * w, 32 * RB};
         run_class<32, RB, OP>(b, prm, tm, 3);
     };
@@ -1598,7 +1577,7 @@ __global__ void __launch_bounds__(KB, 1) k_slim(uva_batch b, uva_solve_params pr
     __shared__ float redf[2 * 4 * 32];
     __shared__ int redi[2 * 32];
     Team<KB> tm{static_cast<int>(threadIdx.x), 0, 0, redd, redf, redi, nullptr, nullptr, nullptr, nullptr,
-                nullptr, nullptr, nullptr, 0, nullptr, 0, nullptr, 0};
+                nullptr, nullptr, nullptr, 0, nullptr, 0};
     const int tid = tm.tid;
     double2* U = reinterpret_cast<double2*>(b.U);
     double2* X = reinterpret_cast<double2*>(b.x64);   // trial solution (by vertex)
