@@ -669,12 +669,22 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
     capped = false;
     nref = 0;
     for (int ref = 0;; ++ref) {
-        // ---- FP64 residual r = rhs - A x; restriction of r for the coarse level
+        // ---- FP64 residual r = rhs - A x. The shared-memory classes stage x
+        // in the p and d buffers first (adjacent: NTT * R FP64 pairs; both are
+        // rewritten before the inner CG reads them), so the product gathers
+        // from shared memory instead of L2.
+        const double2* xr = x64;
+        if constexpr (R > 0) {
+            double2* xs = reinterpret_cast<double2*>(sp);
+            for_rows<NTT, R>(tid, n, [&](int i, int) { xs[i] = x64[i]; });
+            tm.sync();
+            xr = xs;
+        }
         double rr[2] = {0.0, 0.0};
         for_rows<NTT, R>(tid, n, [&](int i, int) {
             double2 r = make_double2(0.0, 0.0);
             if (!is_pinned<OP>(I, i)) {
-                const double2 ax = apply64<OP>(b, I, i, x64);
+                const double2 ax = apply64<OP>(b, I, i, xr);
                 const double2 rhs = OP == OP_ARAP ? b64[i] : make_double2(0.0, 0.0);
                 r = make_double2(rhs.x - ax.x, rhs.y - ax.y);
             }
@@ -1215,7 +1225,7 @@ __device__ __forceinline__ void run_class(const uva_batch& b, const uva_solve_pa
 // while the other CTAs start with the largest islands.
 template <Op OP>
 __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params prm, int nrev) {
-    extern __shared__ float2 dyn[];
+    extern __shared__ __align__(16) float2 dyn[];   // 16-byte aligned: refine_solve stages FP64 pairs here
     __shared__ double redd[2 * 4 * 32];
     __shared__ float redf[2 * 4 * 32];
     __shared__ int redi[2 * 32];
@@ -1228,7 +1238,7 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
         Team<KB> tm{static_cast<int>(threadIdx.x), 0, 0, redd, redf, redi, &slots[0], nullptr, nullptr, nullptr,
                     coarse_buf, coarse_buf + 512, sc_buf, 288, dinv_buf, KB * RB};
         run_class<KB, 0, OP>(b, prm, tm, 0);
-        tm.sp = dyn; tm.sr = dyn + KB * RB; tm.sd = dyn + 2 * KB * RB;
+        tm.sp = dyn; tm.sd = dyn + KB * RB; tm.sr = dyn + 2 * KB * RB;   // sp, sd adjacent (see refine_solve)
         run_class<KB, RB, OP>(b, prm, tm, 1);
     };
     // a sub-team reuses only its own quarter of the buffers, a warp only its
@@ -1237,7 +1247,7 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
         const int s = threadIdx.x / SUB;
         float2* base = dyn + s * (3 * SUB * RB);
         Team<SUB> tm{static_cast<int>(threadIdx.x % SUB), 1 + s, 0, redd + s * 64, redf + s * 64, redi + s * 16,
-                     &slots[1 + s], base, base + SUB * RB, base + 2 * SUB * RB, coarse_buf + 256 * s,
+                     &slots[1 + s], base, base + 2 * SUB * RB, base + SUB * RB, coarse_buf + 256 * s,
                      coarse_buf + 256 * s + 128, sc_buf + 72 * s, 72,
                      dinv_buf + SUB * RB * s, SUB * RB};
         run_class<SUB, RB, OP>(b, prm, tm, 2);
@@ -1246,7 +1256,7 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
         const int w = threadIdx.x / 32;
         float2* base = dyn + w * (3 * 32 * RB);
         Team<32> tm{static_cast<int>(threadIdx.x % 32), 0, 0, nullptr, nullptr, nullptr, nullptr,
-                    base, base + 32 * RB, base + 2 * 32 * RB, nullptr, nullptr, sc_buf + 9 * w, 9,
+                    base, base + 2 * 32 * RB, base + 32 * RB, nullptr, nullptr, sc_buf + 9 * w, 9,
                     dinv_buf + 32 * RB * w, 32 * RB};
         run_class<32, RB, OP>(b, prm, tm, 3);
     };
