@@ -729,14 +729,14 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
             for (int c = 0; c < 2; ++c) {
                 rz[c] = red4[c];
                 const float t = fmaxf(static_cast<float>(prm.inner_eta) * sqrtf(red4[2 + c]),
-                                      static_cast<float>(0.5 * prm.tol * sqrt(bb[c])));
+                                      static_cast<float>(0.8 * prm.tol * sqrt(bb[c])));
                 thr2[c] = t * t;
                 act[c] = red4[2 + c] > thr2[c] && rz[c] > 0.f;
             }
         } else {
             rz[0] = rz[1] = red4[0] + red4[1];
             const float t = fmaxf(static_cast<float>(prm.inner_eta) * sqrtf(red4[2] + red4[3]),
-                                  static_cast<float>(0.5 * prm.tol * sqrt(bb[0])));
+                                  static_cast<float>(0.8 * prm.tol * sqrt(bb[0])));
             thr2[0] = thr2[1] = t * t;
             act[0] = act[1] = (red4[2] + red4[3]) > thr2[0] && rz[0] > 0.f;
         }

@@ -28,7 +28,7 @@ from ._lib import check, ptr
 # 1e-5 reduction (or the final tolerance): fewer FP64 restarts than 1e-3.
 DEFAULTS = {
     "arap": {"tol": 2e-7, "inner_eta": 1e-5, "max_inner": 4000, "max_refine": 12},
-    "lscm": {"tol": 1e-9, "inner_eta": 1e-4, "max_inner": 20000, "max_refine": 16},
+    "lscm": {"tol": 1e-9, "inner_eta": 1e-3, "max_inner": 20000, "max_refine": 16},
 }
 
 
