@@ -234,8 +234,11 @@ struct Team {
 
 // All-reduce of K values over the team; every thread gets bitwise-identical
 // totals (xor butterflies are symmetric; the cross-warp sum runs in one order).
+// The reduction buffers hold 2 * kRedMax values per warp.
+constexpr int kRedMax = 10;
 template <int NTT, int K, typename T>
 __device__ __forceinline__ void team_sum(Team<NTT>& tm, T (&v)[K], T* red) {
+    static_assert(K <= kRedMax, "team_sum: more values than the reduction buffers hold");
 #pragma unroll
     for (int k = 0; k < K; ++k) {
 #pragma unroll
@@ -646,13 +649,24 @@ __device__ __forceinline__ float2 prolong(const Team<NTT>& tm, const Isl& I, int
     return make_float2(tm.cy[2 * a], tm.cy[2 * a + 1]);
 }
 
+// The last two updates of the ARAP iterate and their images under A (FP32,
+// by solver row) for the Galerkin start of the next global step; d1 null:
+// start from the given x.
+struct StartSpace {
+    const float2* d1 = nullptr;
+    const float2* d0 = nullptr;
+    const float2* a1 = nullptr;
+    const float2* a0 = nullptr;
+};
+
 // Solves A x = rhs for one island. x64 (global, FP64, by solver row) holds the
 // start on entry and the solution on exit. FP64 residual refinement around
 // FP32 PCG corrections; NCOL = 2 (ARAP: u and v separately) or 1 (LSCM: one
 // vector of 2n unknowns). Returns the inner CG iterations executed.
 template <int NTT, int R, Op OP, int NCOL>
 __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, const uva_solve_params& prm, Team<NTT>& tm,
-                            const double bb[2], double res_out[2], int& nref, bool& capped) {
+                            const double bb[2], double res_out[2], int& nref, bool& capped,
+                            const StartSpace& gsp = StartSpace{}) {
     double2* x64 = reinterpret_cast<double2*>(b.x64) + I.v0;
     const double2* b64 = reinterpret_cast<const double2*>(b.b64) + I.v0;
     // classes with R > 0 always hold the vectors in shared memory; keeping
@@ -707,6 +721,50 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
         if (done || ref >= prm.max_refine || !isfinite(rr[0] + rr[1])) {
             if (!done) capped = true;
             break;
+        }
+        if (ref == 0 && gsp.d1) {
+            // Galerkin start: x += D t with D = [d1 d0] (the last two updates of
+            // the outer iteration) and t minimising the energy norm of the
+            // error over x + span(D): (D^T A D) t = D^T r, per column. A D is
+            // kept from the updates; r -= A D t follows without a product.
+            double gs[10] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            for_rows<NTT, R>(tid, n, [&](int i, int) {
+                const float2 r = sr[i], d1 = gsp.d1[i], d0 = gsp.d0[i], a1 = gsp.a1[i], a0 = gsp.a0[i];
+                gs[0] += static_cast<double>(d1.x) * r.x;  gs[1] += static_cast<double>(d0.x) * r.x;
+                gs[2] += static_cast<double>(d1.x) * a1.x; gs[3] += static_cast<double>(d1.x) * a0.x;
+                gs[4] += static_cast<double>(d0.x) * a0.x;
+                gs[5] += static_cast<double>(d1.y) * r.y;  gs[6] += static_cast<double>(d0.y) * r.y;
+                gs[7] += static_cast<double>(d1.y) * a1.y; gs[8] += static_cast<double>(d1.y) * a0.y;
+                gs[9] += static_cast<double>(d0.y) * a0.y;
+            });
+            team_sum<NTT, 10>(tm, gs, tm.redd);
+            double t1[2], t0[2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const double g1 = gs[5 * c], g0 = gs[5 * c + 1];
+                const double m11 = gs[5 * c + 2], m10 = gs[5 * c + 3], m00 = gs[5 * c + 4];
+                const double det = m11 * m00 - m10 * m10;
+                t1[c] = 0.0; t0[c] = 0.0;
+                if (m11 > 0.0 && m00 > 0.0 && det > 1e-8 * m11 * m00) {
+                    t1[c] = (m00 * g1 - m10 * g0) / det;
+                    t0[c] = (m11 * g0 - m10 * g1) / det;
+                } else if (m11 > 0.0) {   // collinear updates or no second one: along d1 only
+                    t1[c] = g1 / m11;
+                }
+                if (!isfinite(t1[c]) || !isfinite(t0[c])) { t1[c] = 0.0; t0[c] = 0.0; }
+            }
+            for_rows<NTT, R>(tid, n, [&](int i, int) {
+                const float2 d1 = gsp.d1[i], d0 = gsp.d0[i], a1 = gsp.a1[i], a0 = gsp.a0[i];
+                double2 x = x64[i];
+                x.x += t1[0] * d1.x + t0[0] * d0.x;
+                x.y += t1[1] * d1.y + t0[1] * d0.y;
+                x64[i] = x;
+                float2 r = sr[i];
+                r.x -= static_cast<float>(t1[0] * a1.x + t0[0] * a0.x);
+                r.y -= static_cast<float>(t1[1] * a1.y + t0[1] * a0.y);
+                sr[i] = r;
+            });
+            tm.sync();   // corrected residual complete (the coarse restriction reads all rows)
         }
         if (two_level) coarse_solve<NTT, OP>(b, tm, I, sr);
         // ---- inner FP32 PCG on A d = r, d0 = 0
@@ -967,11 +1025,19 @@ __device__ __forceinline__ void solve_arap(const uva_batch& b, const uva_solve_p
     if (tid == 0) *gst = uva_island_status{};
     bool use_ls = prm.line_search != 0;
     double prev_e = 0.0;
-    // CG start of each global step: the outer iterates converge about
-    // linearly, so the next solution is near U_k + theta (U_k - U_{k-1}),
-    // theta = |U_k - U_{k-1}| / |U_{k-1} - U_{k-2}| (clamped to [0, 1]);
-    // only the work of the solve changes, not its tolerance
-    double dn2 = 0.0, dn2_prev = 0.0;
+    // CG start of each global step (shared-memory classes): the outer
+    // iterates converge about linearly, so the next solution lies close to
+    // U_k + span(U_k - U_{k-1}, U_{k-1} - U_{k-2}); refine_solve takes the
+    // best point of that plane in the energy norm (StartSpace). The updates
+    // and their images under A live in the class-G CG buffers (FP32, by
+    // row), which these classes do not use. Only the work of the solve
+    // changes, not its tolerance.
+    StartSpace gsp;
+    float2* hd1 = reinterpret_cast<float2*>(b.p32) + I.v0;
+    float2* hd0 = reinterpret_cast<float2*>(b.d32) + I.v0;
+    float2* ha1 = reinterpret_cast<float2*>(b.q32) + I.v0;
+    float2* ha0 = reinterpret_cast<float2*>(b.r32) + I.v0;
+    const float wpin32 = static_cast<float>(I.wpin);
     for (int it = 0; it < prm.iters; ++it) {
         double ev[2] = {0.0, 0.0};
         for (int f = I.f0 + tid; f < I.f0 + I.nt; f += NTT) {
@@ -993,7 +1059,6 @@ __device__ __forceinline__ void solve_arap(const uva_batch& b, const uva_solve_p
             if (tid == 0) gst->energy = ev[0];
         }
         tm.sync();   // corner terms complete
-        const double theta = (it >= 2 && dn2_prev > 0.0) ? fmin(1.0, sqrt(dn2 / dn2_prev)) : 0.0;
         double bb[2] = {0.0, 0.0};
         for_rows<NTT, R>(tid, I.n, [&](int i, int) {
             const int v = I.v0 + __ldg(b.row_vert + I.v0 + i);   // vertex of solver row i
@@ -1006,23 +1071,15 @@ __device__ __forceinline__ void solve_arap(const uva_batch& b, const uva_solve_p
             const double2 u = U[v];
             if (i == I.pin) { bx += I.wpin * u.x; by += I.wpin * u.y; }
             b64[I.v0 + i] = make_double2(bx, by);
-            double2 x0 = u;
-            if constexpr (R > 0) {   // previous iterate, FP32, in the class-G CG buffer
-                float2* prev = reinterpret_cast<float2*>(b.r32) + I.v0;
-                if (theta > 0.0) {
-                    const float2 pu = prev[i];
-                    x0 = make_double2(u.x + theta * (u.x - pu.x), u.y + theta * (u.y - pu.y));
-                }
-                prev[i] = make_float2(static_cast<float>(u.x), static_cast<float>(u.y));
-            }
-            x64[I.v0 + i] = x0;
+            x64[I.v0 + i] = u;
             bb[0] += bx * bx; bb[1] += by * by;
         });
         team_sum<NTT, 2>(tm, bb, tm.redd);   // also publishes x64 / b64 to the team
         int nref = 0;
         bool capped = false;
         double res[2];
-        const int cgi = refine_solve<NTT, R, OP_ARAP, 2>(b, I, prm, tm, bb, res, nref, capped);
+        if (R > 0 && it >= 1) gsp = StartSpace{hd1, hd0, ha1, ha0};
+        const int cgi = refine_solve<NTT, R, OP_ARAP, 2>(b, I, prm, tm, bb, res, nref, capped, gsp);
         if (tid == 0) {
             gst->cg_iters += cgi;
             gst->refinements += nref;
@@ -1046,17 +1103,33 @@ __device__ __forceinline__ void solve_arap(const uva_batch& b, const uva_solve_p
         }
         if (tid == 0) gst->step = step;
         tm.sync();   // all line-search reads of U done
-        double dd[1] = {0.0};
         for_rows<NTT, R>(tid, I.n, [&](int i, int) {
             const int v = I.v0 + __ldg(b.row_vert + I.v0 + i);
             const double2 u = U[v], x = x64[I.v0 + i];
             const double2 un = use_ls ? make_double2(u.x + (x.x - u.x) * step, u.y + (x.y - u.y) * step) : x;
             U[v] = un;
-            dd[0] += (un.x - u.x) * (un.x - u.x) + (un.y - u.y) * (un.y - u.y);
+            if constexpr (R > 0) {   // update history for the next start
+                const float2 d = make_float2(static_cast<float>(un.x - u.x), static_cast<float>(un.y - u.y));
+                hd0[i] = it > 0 ? hd1[i] : make_float2(0.f, 0.f);
+                ha0[i] = it > 0 ? ha1[i] : make_float2(0.f, 0.f);
+                hd1[i] = d;
+                tm.sp[i] = d;
+            }
         });
-        team_sum<NTT, 1>(tm, dd, tm.redd);   // also the barrier before the next local step
-        dn2_prev = dn2;
-        dn2 = dd[0];
+        tm.sync();   // U and the update complete; also the barrier before the next local step
+        if (R > 0 && it + 1 < prm.iters) {   // A d of the update, the solver's own FP32 product
+            const int nsl = (I.n + 31) >> 5;
+            for (int j = 0; j < R; j += 2) {
+                const int ia = tid + j * NTT, ib = ia + NTT;
+                if ((ia >> 5) < nsl) {
+                    const bool sb = j + 1 < R && (ib >> 5) < nsl;
+                    float2 qa, qb;
+                    apply32_pair<OP_ARAP>(b, I, ia, ib, sb, tm.sp, wpin32, qa, qb);
+                    if (ia < I.n) ha1[ia] = qa;
+                    if (sb && ib < I.n) ha1[ib] = qb;
+                }
+            }
+        }
     }
 }
 
@@ -1226,8 +1299,8 @@ __device__ __forceinline__ void run_class(const uva_batch& b, const uva_solve_pa
 template <Op OP>
 __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params prm, int nrev) {
     extern __shared__ __align__(16) float2 dyn[];   // 16-byte aligned: refine_solve stages FP64 pairs here
-    __shared__ double redd[2 * 4 * 32];
-    __shared__ float redf[2 * 4 * 32];
+    __shared__ double redd[2 * kRedMax * 32];
+    __shared__ float redf[2 * kRedMax * 32];
     __shared__ int redi[2 * 32];
     __shared__ int slots[8];
     __shared__ float coarse_buf[1024];   // g and y of the coarse level (CTA: 512 each; sub-team: 128 each)
@@ -1246,7 +1319,8 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
     auto sub_teams = [&]() {
         const int s = threadIdx.x / SUB;
         float2* base = dyn + s * (3 * SUB * RB);
-        Team<SUB> tm{static_cast<int>(threadIdx.x % SUB), 1 + s, 0, redd + s * 64, redf + s * 64, redi + s * 16,
+        Team<SUB> tm{static_cast<int>(threadIdx.x % SUB), 1 + s, 0, redd + s * (2 * kRedMax * 8),
+                     redf + s * (2 * kRedMax * 8), redi + s * 16,
                      &slots[1 + s], base, base + 2 * SUB * RB, base + SUB * RB, coarse_buf + 256 * s,
                      coarse_buf + 256 * s + 128, sc_buf + 72 * s, 72,
                      dinv_buf + SUB * RB * s, SUB * RB};
@@ -1583,8 +1657,8 @@ __device__ __forceinline__ void slim_local(const SlimTri& t, const double2 q[3],
 
 template <Op OP>
 __global__ void __launch_bounds__(KB, 1) k_slim(uva_batch b, uva_solve_params prm, double* scratch) {
-    __shared__ double redd[2 * 4 * 32];
-    __shared__ float redf[2 * 4 * 32];
+    __shared__ double redd[2 * kRedMax * 32];
+    __shared__ float redf[2 * kRedMax * 32];
     __shared__ int redi[2 * 32];
     Team<KB> tm{static_cast<int>(threadIdx.x), 0, 0, redd, redf, redi, nullptr, nullptr, nullptr, nullptr,
                 nullptr, nullptr, nullptr, 0, nullptr, 0};
