@@ -163,6 +163,10 @@ typedef struct uva_batch {
     float*  r32;  float*  d32;  float*  p32;  float* q32;
     uva_island_status* status;                  /* nc                         */
     int32_t* work;            /* >= 4 ints, zeroed by the callee per launch     */
+    float*  hist;             /* 16*n floats (optional): the last 4 ARAP updates
+                                 and their images under the operator, FP32 by
+                                 solver row, for the start of each global step;
+                                 null: 2 updates kept in p32/d32/q32/r32        */
 } uva_batch;
 
 /* Island size classes of one persistent launch (see uva_arap): islands are
@@ -227,8 +231,8 @@ int uva_slim(uva_batch* b, const uva_solve_params* prm, double* scratch, void* s
  * callers that cannot allocate device memory while they run (for example a
  * host application that owns a fixed device pool, or code that must not call
  * cudaMalloc between frames). It allocates nothing: the solver scratch of `b`
- * (x64, b64, rc, r32, d32, p32, q32, cpart, work) is ignored and replaced by one
- * static device array of 5,505,280 bytes that every GPU loading the library
+ * (x64, b64, rc, r32, d32, p32, q32, cpart, work, hist) is ignored and replaced by one
+ * static device array of 7,602,432 bytes that every GPU loading the library
  * holds until exit. The caller still passes the inputs (topology, geometry,
  * pins, order) and the outputs (U, status). Limits: at most 32768 vertices
  * and 65536 triangles per call, else UVA_E_TOOBIG. The first call on a device

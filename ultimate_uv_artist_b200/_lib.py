@@ -55,7 +55,7 @@ class BatchDesc(C.Structure):
                 ("P", vp), ("frame", vp), ("wtri", vp), ("tscale", vp), ("wedge", vp), ("slot_cw", vp),
                 ("wdiag", vp), ("dinv", vp), ("pins", vp), ("wpin", vp), ("U", vp),
                 ("x64", vp), ("b64", vp), ("rc", vp), ("r32", vp), ("d32", vp), ("p32", vp), ("q32", vp),
-                ("status", vp), ("work", vp)]
+                ("status", vp), ("work", vp), ("hist", vp)]
 
 
 class SolveParams(C.Structure):

@@ -649,15 +649,69 @@ __device__ __forceinline__ float2 prolong(const Team<NTT>& tm, const Isl& I, int
     return make_float2(tm.cy[2 * a], tm.cy[2 * a + 1]);
 }
 
-// The last two updates of the ARAP iterate and their images under A (FP32,
-// by solver row) for the Galerkin start of the next global step; d1 null:
-// start from the given x.
+// The last m updates of the ARAP iterate and their images under A (FP32,
+// by solver row, most recent first) for the Galerkin start of the next
+// global step; m == 0: start from the given x.
+constexpr int kStartMax = 4;
 struct StartSpace {
-    const float2* d1 = nullptr;
-    const float2* d0 = nullptr;
-    const float2* a1 = nullptr;
-    const float2* a0 = nullptr;
+    int m = 0;
+    const float2* d[kStartMax] = {nullptr, nullptr, nullptr, nullptr};
+    const float2* a[kStartMax] = {nullptr, nullptr, nullptr, nullptr};
 };
+
+// t = M^+ g for the m x m Gram matrix M (lower triangle, row-major packed:
+// M[k(k+1)/2 + l], l <= k) of one column: LDL^T in FP64 that skips a vector
+// whose A-norm is below 1e-8 of its own after the earlier ones are removed
+// (near-parallel updates); skipped vectors get t = 0.
+__device__ __forceinline__ void start_coeffs(int m, const double* M, const double* g, double* t) {
+    double L[kStartMax][kStartMax], Dg[kStartMax], y[kStartMax];
+    bool on[kStartMax];
+#pragma unroll
+    for (int k = 0; k < kStartMax; ++k) {
+        on[k] = false; Dg[k] = 0.0; y[k] = 0.0; t[k] = 0.0;
+#pragma unroll
+        for (int l = 0; l < kStartMax; ++l) L[k][l] = 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < kStartMax; ++k) {
+        if (k >= m) break;
+        const double mkk = M[k * (k + 1) / 2 + k];
+        double v = mkk;
+#pragma unroll
+        for (int j = 0; j < kStartMax; ++j)
+            if (j < k && on[j]) v -= L[k][j] * L[k][j] * Dg[j];
+        if (!(mkk > 0.0) || !(v > 1e-8 * mkk) || !isfinite(v)) continue;
+        on[k] = true;
+        Dg[k] = v;
+#pragma unroll
+        for (int i = 0; i < kStartMax; ++i) {
+            if (i <= k || i >= m) continue;
+            double x = M[i * (i + 1) / 2 + k];
+#pragma unroll
+            for (int j = 0; j < kStartMax; ++j)
+                if (j < k && on[j]) x -= L[i][j] * L[k][j] * Dg[j];
+            L[i][k] = x / v;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kStartMax; ++k) {   // L y = g
+        if (k >= m || !on[k]) continue;
+        double x = g[k];
+#pragma unroll
+        for (int j = 0; j < kStartMax; ++j)
+            if (j < k && on[j]) x -= L[k][j] * y[j];
+        y[k] = x;
+    }
+#pragma unroll
+    for (int k = kStartMax - 1; k >= 0; --k) {   // D L^T t = y
+        if (k >= m || !on[k]) continue;
+        double x = y[k] / Dg[k];
+#pragma unroll
+        for (int i = 0; i < kStartMax; ++i)
+            if (i > k && i < m && on[i]) x -= L[i][k] * t[i];
+        t[k] = isfinite(x) ? x : 0.0;
+    }
+}
 
 // Solves A x = rhs for one island. x64 (global, FP64, by solver row) holds the
 // start on entry and the solution on exit. FP64 residual refinement around
@@ -722,46 +776,56 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
             if (!done) capped = true;
             break;
         }
-        if (ref == 0 && gsp.d1) {
-            // Galerkin start: x += D t with D = [d1 d0] (the last two updates of
-            // the outer iteration) and t minimising the energy norm of the
-            // error over x + span(D): (D^T A D) t = D^T r, per column. A D is
-            // kept from the updates; r -= A D t follows without a product.
-            double gs[10] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-            for_rows<NTT, R>(tid, n, [&](int i, int) {
-                const float2 r = sr[i], d1 = gsp.d1[i], d0 = gsp.d0[i], a1 = gsp.a1[i], a0 = gsp.a0[i];
-                gs[0] += static_cast<double>(d1.x) * r.x;  gs[1] += static_cast<double>(d0.x) * r.x;
-                gs[2] += static_cast<double>(d1.x) * a1.x; gs[3] += static_cast<double>(d1.x) * a0.x;
-                gs[4] += static_cast<double>(d0.x) * a0.x;
-                gs[5] += static_cast<double>(d1.y) * r.y;  gs[6] += static_cast<double>(d0.y) * r.y;
-                gs[7] += static_cast<double>(d1.y) * a1.y; gs[8] += static_cast<double>(d1.y) * a0.y;
-                gs[9] += static_cast<double>(d0.y) * a0.y;
-            });
-            team_sum<NTT, 10>(tm, gs, tm.redd);
-            double t1[2], t0[2];
+        if (ref == 0 && gsp.m > 0) {
+            // Galerkin start: x += D t with D the last m updates of the outer
+            // iteration and t minimising the energy norm of the error over
+            // x + span(D): (D^T A D) t = D^T r, per column. A D is kept from
+            // the updates; r -= A D t follows without a product.
+            // one pass per update k: d_k . r and d_k . A d_l (l <= k), per column
+            constexpr int NM = kStartMax * (kStartMax + 1) / 2;
+            double g[2][kStartMax], M[2][NM];
+            const int m = gsp.m;
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const double g1 = gs[5 * c], g0 = gs[5 * c + 1];
-                const double m11 = gs[5 * c + 2], m10 = gs[5 * c + 3], m00 = gs[5 * c + 4];
-                const double det = m11 * m00 - m10 * m10;
-                t1[c] = 0.0; t0[c] = 0.0;
-                if (m11 > 0.0 && m00 > 0.0 && det > 1e-8 * m11 * m00) {
-                    t1[c] = (m00 * g1 - m10 * g0) / det;
-                    t0[c] = (m11 * g0 - m10 * g1) / det;
-                } else if (m11 > 0.0) {   // collinear updates or no second one: along d1 only
-                    t1[c] = g1 / m11;
+            for (int k = 0; k < kStartMax; ++k) {
+                if (k >= m) break;
+                double acc[2 * (kStartMax + 1)];
+#pragma unroll
+                for (int e = 0; e < 2 * (kStartMax + 1); ++e) acc[e] = 0.0;
+                for_rows<NTT, R>(tid, n, [&](int i, int) {
+                    const float2 d = gsp.d[k][i], r = sr[i];
+                    acc[0] += static_cast<double>(d.x) * r.x;
+                    acc[1] += static_cast<double>(d.y) * r.y;
+#pragma unroll
+                    for (int l = 0; l <= k; ++l) {
+                        const float2 a = gsp.a[l][i];
+                        acc[2 + 2 * l] += static_cast<double>(d.x) * a.x;
+                        acc[3 + 2 * l] += static_cast<double>(d.y) * a.y;
+                    }
+                });
+                team_sum<NTT, 2 * (kStartMax + 1)>(tm, acc, tm.redd);
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    g[c][k] = acc[c];
+#pragma unroll
+                    for (int l = 0; l <= k; ++l) M[c][k * (k + 1) / 2 + l] = acc[2 + 2 * l + c];
                 }
-                if (!isfinite(t1[c]) || !isfinite(t0[c])) { t1[c] = 0.0; t0[c] = 0.0; }
             }
+            double t[2][kStartMax];
+            start_coeffs(m, M[0], g[0], t[0]);
+            start_coeffs(m, M[1], g[1], t[1]);
             for_rows<NTT, R>(tid, n, [&](int i, int) {
-                const float2 d1 = gsp.d1[i], d0 = gsp.d0[i], a1 = gsp.a1[i], a0 = gsp.a0[i];
                 double2 x = x64[i];
-                x.x += t1[0] * d1.x + t0[0] * d0.x;
-                x.y += t1[1] * d1.y + t0[1] * d0.y;
-                x64[i] = x;
                 float2 r = sr[i];
-                r.x -= static_cast<float>(t1[0] * a1.x + t0[0] * a0.x);
-                r.y -= static_cast<float>(t1[1] * a1.y + t0[1] * a0.y);
+                double ax = 0.0, ay = 0.0;
+#pragma unroll
+                for (int k = 0; k < kStartMax; ++k) {
+                    if (k >= m) break;
+                    const float2 d = gsp.d[k][i], a = gsp.a[k][i];
+                    x.x += t[0][k] * d.x; x.y += t[1][k] * d.y;
+                    ax += t[0][k] * a.x; ay += t[1][k] * a.y;
+                }
+                x64[i] = x;
+                r.x -= static_cast<float>(ax); r.y -= static_cast<float>(ay);
                 sr[i] = r;
             });
             tm.sync();   // corrected residual complete (the coarse restriction reads all rows)
@@ -1032,11 +1096,18 @@ __device__ __forceinline__ void solve_arap(const uva_batch& b, const uva_solve_p
     // and their images under A live in the class-G CG buffers (FP32, by
     // row), which these classes do not use. Only the work of the solve
     // changes, not its tolerance.
-    StartSpace gsp;
-    float2* hd1 = reinterpret_cast<float2*>(b.p32) + I.v0;
-    float2* hd0 = reinterpret_cast<float2*>(b.d32) + I.v0;
-    float2* ha1 = reinterpret_cast<float2*>(b.q32) + I.v0;
-    float2* ha0 = reinterpret_cast<float2*>(b.r32) + I.v0;
+    // History ring: slot k holds an update and its image under A. With the
+    // batch's history buffer (b.hist) kStartMax slots, else 2 slots in the
+    // class-G CG buffers (the no-allocation entry point's case).
+    const int depth = b.hist ? kStartMax : 2;
+    auto hist_d = [&](int k) -> float2* {
+        if (b.hist) return reinterpret_cast<float2*>(b.hist) + static_cast<size_t>(2 * k) * b.n + I.v0;
+        return reinterpret_cast<float2*>(k == 0 ? b.p32 : b.d32) + I.v0;
+    };
+    auto hist_a = [&](int k) -> float2* {
+        if (b.hist) return reinterpret_cast<float2*>(b.hist) + static_cast<size_t>(2 * k + 1) * b.n + I.v0;
+        return reinterpret_cast<float2*>(k == 0 ? b.q32 : b.r32) + I.v0;
+    };
     const float wpin32 = static_cast<float>(I.wpin);
     for (int it = 0; it < prm.iters; ++it) {
         double ev[2] = {0.0, 0.0};
@@ -1078,7 +1149,15 @@ __device__ __forceinline__ void solve_arap(const uva_batch& b, const uva_solve_p
         int nref = 0;
         bool capped = false;
         double res[2];
-        if (R > 0 && it >= 1) gsp = StartSpace{hd1, hd0, ha1, ha0};
+        StartSpace gsp;
+        if (R > 0) {
+            gsp.m = min(it, depth);
+            for (int k = 0; k < gsp.m; ++k) {   // most recent update first
+                const int slot = (it - 1 - k) % depth;
+                gsp.d[k] = hist_d(slot);
+                gsp.a[k] = hist_a(slot);
+            }
+        }
         const int cgi = refine_solve<NTT, R, OP_ARAP, 2>(b, I, prm, tm, bb, res, nref, capped, gsp);
         if (tid == 0) {
             gst->cg_iters += cgi;
@@ -1108,16 +1187,15 @@ __device__ __forceinline__ void solve_arap(const uva_batch& b, const uva_solve_p
             const double2 u = U[v], x = x64[I.v0 + i];
             const double2 un = use_ls ? make_double2(u.x + (x.x - u.x) * step, u.y + (x.y - u.y) * step) : x;
             U[v] = un;
-            if constexpr (R > 0) {   // update history for the next start
+            if constexpr (R > 0) {   // update history for the next starts
                 const float2 d = make_float2(static_cast<float>(un.x - u.x), static_cast<float>(un.y - u.y));
-                hd0[i] = it > 0 ? hd1[i] : make_float2(0.f, 0.f);
-                ha0[i] = it > 0 ? ha1[i] : make_float2(0.f, 0.f);
-                hd1[i] = d;
+                hist_d(it % depth)[i] = d;
                 tm.sp[i] = d;
             }
         });
         tm.sync();   // U and the update complete; also the barrier before the next local step
         if (R > 0 && it + 1 < prm.iters) {   // A d of the update, the solver's own FP32 product
+            float2* ha1 = hist_a(it % depth);
             const int nsl = (I.n + 31) >> 5;
             for (int j = 0; j < R; j += 2) {
                 const int ia = tid + j * NTT, ib = ia + NTT;
@@ -2013,9 +2091,10 @@ constexpr size_t kNaB64 = kAlignUp(sizeof(double) * 2 * kNoAllocMaxVerts);      
 constexpr size_t kNaRc = kAlignUp(sizeof(double) * 6 * kNoAllocMaxTris);          // rc
 constexpr size_t kNaF32 = kAlignUp(sizeof(float) * 2 * kNoAllocMaxVerts);         // r32, d32, p32, q32
 constexpr size_t kNaPart = kAlignUp(sizeof(float) * 2 * kNoAllocMaxVerts);        // cpart (nslices <= n)
-constexpr size_t kNoAllocBytes = kNaWork + kNaX64 + kNaB64 + kNaRc + 4 * kNaF32 + kNaPart;   // 5,505,280 bytes
+constexpr size_t kNaHist = kAlignUp(sizeof(float) * 16 * kNoAllocMaxVerts);      // ARAP start history
+constexpr size_t kNoAllocBytes = kNaWork + kNaX64 + kNaB64 + kNaRc + 4 * kNaF32 + kNaPart + kNaHist;   // 7,602,432 bytes
 
-static_assert(kNoAllocBytes == 5505280, "documented size of the static scratch");
+static_assert(kNoAllocBytes == 7602432, "documented size of the static scratch");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 // Device address of g_noalloc_scratch on the current device, looked up once
@@ -2063,7 +2142,8 @@ extern "C" int uva_arap_noalloc(const uva_batch* b, const uva_solve_params* prm,
     w.d32 = reinterpret_cast<float*>(base + off); off += kNaF32;
     w.p32 = reinterpret_cast<float*>(base + off); off += kNaF32;
     w.q32 = reinterpret_cast<float*>(base + off); off += kNaF32;
-    w.cpart = reinterpret_cast<float*>(base + off);
+    w.cpart = reinterpret_cast<float*>(base + off); off += kNaPart;
+    w.hist = reinterpret_cast<float*>(base + off);
     // the work counters are the only scratch that must start at zero;
     // launch_islands clears them on the stream before the launch
     return launch_islands<OP_ARAP>(&w, prm, static_cast<cudaStream_t>(stream));

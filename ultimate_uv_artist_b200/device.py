@@ -238,6 +238,7 @@ class DeviceBatch:
         self.d32 = torch.empty((n, 2), dtype=f32, device=d)
         self.p32 = torch.empty((n, 2), dtype=f32, device=d)
         self.q32 = torch.empty((n, 2), dtype=f32, device=d)
+        self.hist = torch.empty((8, n, 2), dtype=f32, device=d)   # ARAP start history (4 updates, A d)
         self.status = torch.zeros((nc, C.sizeof(_lib.IslandStatus)), dtype=torch.uint8, device=d)
         self.work = torch.zeros(8, dtype=torch.int32, device=d)
         self.rev_ctas = tuned["rev_ctas"] if tuned is not None else 0   # schedule knob (autotune.tune)
@@ -256,7 +257,7 @@ class DeviceBatch:
                      "vt_ptr", "vt", "vflags", "bofs", "bverts", "order", "row_vert", "vert_row", "agg_rows", "cofs",
                      "coarse_a", "coarse_l", "coarse_work", "cpart", "P", "frame", "wtri", "tscale", "wedge",
                      "slot_cw", "wdiag", "dinv", "pins", "wpin", "U", "x64", "b64", "rc", "r32", "d32", "p32",
-                     "q32", "status", "work"):
+                     "q32", "status", "work", "hist"):
             setattr(D, name, getattr(self, name).data_ptr())
         return D
 
