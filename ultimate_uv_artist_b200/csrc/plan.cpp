@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <memory>
 #include <numeric>
 #include <thread>
 #include <vector>
@@ -74,65 +75,68 @@ void blob_order(const IslandPlan& ip, int32_t n, int32_t agg, std::vector<int32_
 
 void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& bad) {
     ip.n = n; ip.t = t;
-    // half-edges grouped by (lo, hi, half-edge id): a stable counting sort by
-    // lo, then a stable insertion sort by hi inside each (short) bucket
+    // half-edges grouped by (lo, hi, half-edge id): a counting sort by lo
+    // into contiguous (hi, 2 h + dir) pairs (dir 1: the half-edge runs lo ->
+    // hi, or is a self-loop), then a stable insertion sort by hi inside each
+    // (short) bucket; everything after reads the buckets sequentially
     const int32_t nh = 3 * t;
-    std::vector<int32_t> hlo(nh), hhi(nh);
+    std::vector<int32_t> bstart(n + 1, 0);
     for (int32_t f = 0; f < t; ++f) {
         for (int k = 0; k < 3; ++k) {
             const int64_t a = T[3 * f + (k + 1) % 3], b = T[3 * f + (k + 2) % 3];
             if (a < 0 || a >= n || b < 0 || b >= n) { bad = true; return; }
-            hlo[3 * f + k] = static_cast<int32_t>(a < b ? a : b);
-            hhi[3 * f + k] = static_cast<int32_t>(a < b ? b : a);
+            ++bstart[(a < b ? a : b) + 1];
         }
     }
-    std::vector<int32_t> bstart(n + 1, 0), hs(nh);
-    for (int32_t h = 0; h < nh; ++h) ++bstart[hlo[h] + 1];
     for (int32_t v = 0; v < n; ++v) bstart[v + 1] += bstart[v];
+    std::vector<int32_t> bhi(nh), bhd(nh);
     {
         std::vector<int32_t> fillb(bstart.begin(), bstart.end() - 1);
-        for (int32_t h = 0; h < nh; ++h) hs[fillb[hlo[h]]++] = h;
+        for (int32_t f = 0; f < t; ++f) {
+            for (int k = 0; k < 3; ++k) {
+                const int32_t a = static_cast<int32_t>(T[3 * f + (k + 1) % 3]), b = static_cast<int32_t>(T[3 * f + (k + 2) % 3]);
+                const int32_t lo = a < b ? a : b;
+                const int32_t q = fillb[lo]++;
+                bhi[q] = a < b ? b : a;
+                bhd[q] = 2 * (3 * f + k) + (a == lo ? 1 : 0);
+            }
+        }
     }
     for (int32_t v = 0; v < n; ++v) {
         for (int32_t q = bstart[v] + 1; q < bstart[v + 1]; ++q) {
-            const int32_t h = hs[q];
+            const int32_t hi = bhi[q], hd = bhd[q];
             int32_t r = q - 1;
-            while (r >= bstart[v] && hhi[hs[r]] > hhi[h]) { hs[r + 1] = hs[r]; --r; }
-            hs[r + 1] = h;
+            while (r >= bstart[v] && bhi[r] > hi) { bhi[r + 1] = bhi[r]; bhd[r + 1] = bhd[r]; --r; }
+            bhi[r + 1] = hi; bhd[r + 1] = hd;
         }
     }
     ip.tri_edge.assign(static_cast<size_t>(3) * t, -1);
+    std::vector<int32_t> deg(n, 0);   // neighbours per vertex (self-loops excluded)
     ip.edge_info.clear();
     ip.edge_info.reserve(nh / 2 + n + 4);
     std::vector<int32_t> elo, ehi;   // endpoints of each unique edge (lo <= hi)
     elo.reserve(nh / 2 + n + 4);
     ehi.reserve(nh / 2 + n + 4);
-    for (int32_t s = 0; s < nh;) {
-        int32_t e = s;
-        int32_t fwd = 0, rev = 0;
-        const int32_t lo = hlo[hs[s]], hi = hhi[hs[s]];
-        while (e < nh && hlo[hs[e]] == lo && hhi[hs[e]] == hi) {
-            const int32_t h = hs[e];
-            const int32_t f = h / 3, k = h % 3;
-            const int64_t a = T[3 * f + (k + 1) % 3];
-            if (a == lo) ++fwd; else ++rev;
-            ip.tri_edge[h] = static_cast<int32_t>(elo.size());
-            ++e;
+    for (int32_t lo = 0; lo < n; ++lo) {
+        const int32_t qe = bstart[lo + 1];
+        for (int32_t q = bstart[lo]; q < qe;) {
+            const int32_t hi = bhi[q];
+            int32_t fwd = 0, rev = 0, e = q;
+            for (; e < qe && bhi[e] == hi; ++e) {
+                const int32_t hd = bhd[e];
+                if (hd & 1) ++fwd; else ++rev;
+                ip.tri_edge[hd >> 1] = static_cast<int32_t>(elo.size());
+            }
+            const int32_t cnt = e - q;
+            ip.edge_info.push_back(std::min(cnt, 1023) | (std::min(fwd, 1023) << 10) | (std::min(rev, 1023) << 20));
+            elo.push_back(lo);
+            ehi.push_back(hi);
+            if (lo != hi) { ++deg[lo]; ++deg[hi]; }
+            q = e;
         }
-        const int32_t cnt = e - s;
-        ip.edge_info.push_back(std::min(cnt, 1023) | (std::min(fwd, 1023) << 10) | (std::min(rev, 1023) << 20));
-        elo.push_back(lo);
-        ehi.push_back(hi);
-        s = e;
     }
     ip.nedges = static_cast<int32_t>(elo.size());
     // rows: appending in key order keeps each row sorted (see file comment)
-    std::vector<int32_t> deg(n, 0);
-    for (int32_t e = 0; e < ip.nedges; ++e) {
-        const int32_t lo = elo[e], hi = ehi[e];
-        if (lo == hi) continue;
-        ++deg[lo]; ++deg[hi];
-    }
     ip.row_ptr.assign(n + 1, 0);
     for (int32_t v = 0; v < n; ++v) ip.row_ptr[v + 1] = ip.row_ptr[v] + deg[v];
     ip.row_col.assign(ip.row_ptr[n], 0);
@@ -207,7 +211,7 @@ struct uva_plan {
     std::vector<IslandPlan> isl;
     std::vector<int64_t> eofs, sofs, slotofs, bofs, cofs;
     const int64_t* tris = nullptr;   // not owned; only valid during create
-    std::vector<int32_t> tri_local;  // 3t local ids (copied)
+    std::unique_ptr<int32_t[]> tri_local;   // 3t local ids (copied by the island workers)
 };
 
 extern "C" int uva_plan_create(const int64_t* tris, const int64_t* vofs, const int64_t* tofs, int32_t nc,
@@ -230,7 +234,7 @@ extern "C" int uva_plan_create(const int64_t* tris, const int64_t* vofs, const i
     }
     if (p->t > 0 && !tris) { delete p; uva_set_error("uva_plan_create: null triangles"); return UVA_E_ARG; }
     p->isl.resize(nc);
-    p->tri_local.assign(tris, tris + 3 * p->t);
+    p->tri_local.reset(new int32_t[static_cast<size_t>(3 * p->t) + 1]);   // uninitialised; filled per island
     // largest islands first for load balance
     std::vector<int32_t> order(nc);
     std::iota(order.begin(), order.end(), 0);
@@ -245,9 +249,11 @@ extern "C" int uva_plan_create(const int64_t* tris, const int64_t* vofs, const i
             if (q >= nc) break;
             const int32_t i = order[q];
             bool bad = false;
-            build_island(tris + 3 * (p->tofs[i] - p->tofs[0]), static_cast<int32_t>(p->vofs[i + 1] - p->vofs[i]),
+            const int64_t t0 = 3 * (p->tofs[i] - p->tofs[0]), tn = 3 * (p->tofs[i + 1] - p->tofs[i]);
+            build_island(tris + t0, static_cast<int32_t>(p->vofs[i + 1] - p->vofs[i]),
                          static_cast<int32_t>(p->tofs[i + 1] - p->tofs[i]), p->isl[i], bad);
             if (bad) anybad = true;
+            else for (int64_t c = 0; c < tn; ++c) p->tri_local[t0 + c] = static_cast<int32_t>(tris[t0 + c]);
         }
     };
     int32_t nt = nthreads > 0 ? nthreads : static_cast<int32_t>(std::thread::hardware_concurrency());
@@ -304,87 +310,88 @@ extern "C" int uva_plan_export(const uva_plan* p, int32_t* tri4, int32_t* tri_ed
     const int32_t nc = p->nc;
     const int64_t v0 = p->vofs.empty() ? 0 : p->vofs[0];
     const int64_t t0 = p->tofs.empty() ? 0 : p->tofs[0];
-    auto worker = [&](int32_t lo, int32_t hi) {
-        for (int32_t i = lo; i < hi; ++i) {
-            const IslandPlan& ip = p->isl[i];
-            const int64_t fb = p->tofs[i] - t0, vb = p->vofs[i] - v0;
-            const int64_t eb = p->eofs[i], sb = p->sofs[i], slb = p->slotofs[i];
-            for (int32_t f = 0; f < ip.t; ++f) {
-                for (int k = 0; k < 3; ++k) {
-                    tri4[4 * (fb + f) + k] = static_cast<int32_t>(p->tri_local[3 * (fb + f) + k]);
-                    const int32_t e = ip.tri_edge[3 * f + k];
-                    tri_edge[3 * (fb + f) + k] = e < 0 ? -1 : static_cast<int32_t>(eb + e);
-                }
-                tri4[4 * (fb + f) + 3] = i;
+    // islands are independent: every array of island i lands in its own
+    // range, so workers take islands from a shared counter, largest first
+    std::vector<int32_t> order(nc);
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return p->isl[a].t > p->isl[b].t; });
+    std::atomic<int32_t> next{0};
+    auto one = [&](int32_t i) {
+        const IslandPlan& ip = p->isl[i];
+        const int64_t fb = p->tofs[i] - t0, vb = p->vofs[i] - v0;
+        const int64_t eb = p->eofs[i], sb = p->sofs[i], slb = p->slotofs[i];
+        const int32_t* tl = p->tri_local.get() + 3 * fb;
+        for (int32_t f = 0; f < ip.t; ++f) {
+            for (int k = 0; k < 3; ++k) {
+                tri4[4 * (fb + f) + k] = tl[3 * f + k];
+                const int32_t e = ip.tri_edge[3 * f + k];
+                tri_edge[3 * (fb + f) + k] = e < 0 ? -1 : static_cast<int32_t>(eb + e);
             }
-            if (sofs) sofs[i] = static_cast<int32_t>(sb);
-            int64_t slot = slb;
-            for (int32_t s = 0; s < ip.nslices; ++s) {
-                slice_ptr[sb + s] = static_cast<int32_t>(slot);
-                const int32_t w = ip.slice_w[s];
-                for (int32_t k = 0; k < w; ++k) {
-                    for (int32_t lane = 0; lane < 32; ++lane) {
-                        const int32_t row = s * 32 + lane;
+            tri4[4 * (fb + f) + 3] = i;
+        }
+        if (sofs) sofs[i] = static_cast<int32_t>(sb);
+        // sliced ELL: row by row (its slots sit 32 apart inside the slice)
+        int64_t slot = slb;
+        for (int32_t s = 0; s < ip.nslices; ++s) {
+            slice_ptr[sb + s] = static_cast<int32_t>(slot);
+            const int32_t w = ip.slice_w[s];
+            for (int32_t lane = 0; lane < 32; ++lane) {
+                const int32_t row = s * 32 + lane;
+                int32_t k = 0;
+                if (row < ip.n) {
+                    const int32_t r = ip.row_vert[row];   // vertex of this row
+                    const int32_t a = ip.row_ptr[r], deg = ip.row_ptr[r + 1] - a;
+                    for (; k < deg; ++k) {
                         const int64_t q = slot + static_cast<int64_t>(k) * 32 + lane;
-                        const int32_t r = row < ip.n ? ip.row_vert[row] : 0;   // vertex of this row
-                        if (row < ip.n && k < ip.row_ptr[r + 1] - ip.row_ptr[r]) {
-                            const int32_t j = ip.row_col[ip.row_ptr[r] + k];
-                            const int32_t e = ip.row_edge[ip.row_ptr[r] + k];
-                            slot_col[q] = ip.vert_row[j];
-                            slot_edge[q] = static_cast<int32_t>(eb + e);
-                            const int32_t info = ip.edge_info[e];
-                            const int32_t nf = (info >> 10) & 1023, nr = (info >> 20) & 1023;
-                            // half-edges r->j and j->r (fwd is lo->hi)
-                            const int32_t n_rj = r < j ? nf : nr, n_jr = r < j ? nr : nf;
-                            const int32_t b_rj = n_jr == 0 ? n_rj : 0, b_jr = n_rj == 0 ? n_jr : 0;
-                            slot_c[q] = -0.5f * static_cast<float>(b_rj) + 0.5f * static_cast<float>(b_jr);
-                        } else {
-                            slot_col[q] = row < ip.n ? row : 0;
-                            slot_edge[q] = -1;
-                            slot_c[q] = 0.0f;
-                        }
+                        const int32_t j = ip.row_col[a + k];
+                        const int32_t e = ip.row_edge[a + k];
+                        slot_col[q] = ip.vert_row[j];
+                        slot_edge[q] = static_cast<int32_t>(eb + e);
+                        const int32_t info = ip.edge_info[e];
+                        const int32_t nf = (info >> 10) & 1023, nr = (info >> 20) & 1023;
+                        // half-edges r->j and j->r (fwd is lo->hi)
+                        const int32_t n_rj = r < j ? nf : nr, n_jr = r < j ? nr : nf;
+                        const int32_t b_rj = n_jr == 0 ? n_rj : 0, b_jr = n_rj == 0 ? n_jr : 0;
+                        slot_c[q] = -0.5f * static_cast<float>(b_rj) + 0.5f * static_cast<float>(b_jr);
                     }
                 }
-                slot += static_cast<int64_t>(w) * 32;
+                for (; k < w; ++k) {   // padding: zero weight, the row itself (0 past the island's end)
+                    const int64_t q = slot + static_cast<int64_t>(k) * 32 + lane;
+                    slot_col[q] = row < ip.n ? row : 0;
+                    slot_edge[q] = -1;
+                    slot_c[q] = 0.0f;
+                }
             }
-            for (int32_t v = 0; v < ip.n; ++v) vflags[vb + v] = ip.vflags[v];
-            if (bofs) bofs[i] = static_cast<int32_t>(p->bofs[i]);
-            for (size_t q = 0; q < ip.bverts.size(); ++q) bverts[p->bofs[i] + q] = ip.bverts[q];
+            slot += static_cast<int64_t>(w) * 32;
+        }
+        for (int32_t v = 0; v < ip.n; ++v) vflags[vb + v] = ip.vflags[v];
+        if (bofs) bofs[i] = static_cast<int32_t>(p->bofs[i]);
+        for (size_t q = 0; q < ip.bverts.size(); ++q) bverts[p->bofs[i] + q] = ip.bverts[q];
+        // vertex -> (triangle, corner) incidence, ascending by f*3+corner; an
+        // island's corners are its own 3*t entries (offset 3 * tofs[i])
+        const int32_t n = ip.n, t = ip.t;
+        std::vector<int32_t> cnt(n + 1, 0);
+        for (int32_t c = 0; c < 3 * t; ++c) ++cnt[tl[c] + 1];
+        for (int32_t v = 0; v < n; ++v) cnt[v + 1] += cnt[v];
+        for (int32_t v = 0; v <= n; ++v) vt_ptr[vb + v] = static_cast<int32_t>(3 * fb + cnt[v]);
+        for (int32_t c = 0; c < 3 * t; ++c) vt[3 * fb + cnt[tl[c]]++] = static_cast<int32_t>(3 * fb + c);
+    };
+    auto worker = [&]() {
+        for (;;) {
+            const int32_t q = next.fetch_add(1);
+            if (q >= nc) break;
+            one(order[q]);
         }
     };
-    const int32_t nt = std::max(1, std::min<int32_t>(static_cast<int32_t>(std::thread::hardware_concurrency()), nc));
+    int32_t nt = static_cast<int32_t>(std::thread::hardware_concurrency());
+    nt = std::max(1, std::min(nt, std::max(nc, 1)));
     std::vector<std::thread> pool;
-    const int32_t chunk = (nc + nt - 1) / std::max(nt, 1);
-    for (int32_t k = 0; k < nt; ++k) {
-        const int32_t lo = k * chunk, hi = std::min(nc, lo + chunk);
-        if (lo < hi) pool.emplace_back(worker, lo, hi);
-    }
+    for (int32_t k = 1; k < nt; ++k) pool.emplace_back(worker);
+    worker();
     for (auto& th : pool) th.join();
     if (sofs) sofs[nc] = static_cast<int32_t>(p->nslices);
     slice_ptr[p->nslices] = static_cast<int32_t>(p->nslots);
     if (bofs) bofs[nc] = static_cast<int32_t>(p->nbverts);
-    // vertex -> (triangle, corner) incidence, ascending by f*3+corner. An
-    // island's corners are its own 3*t entries, so islands fill their part
-    // of vt independently (offset 3 * tofs[i]).
-    auto inc = [&](int32_t lo, int32_t hi) {
-        for (int32_t i = lo; i < hi; ++i) {
-            const int64_t fb = p->tofs[i] - t0, vb = p->vofs[i] - v0;
-            const int32_t n = p->isl[i].n, t = p->isl[i].t;
-            std::vector<int32_t> cnt(n + 1, 0);
-            for (int64_t c = 3 * fb; c < 3 * (fb + t); ++c) ++cnt[p->tri_local[c] + 1];
-            for (int32_t v = 0; v < n; ++v) cnt[v + 1] += cnt[v];
-            for (int32_t v = 0; v <= n; ++v) vt_ptr[vb + v] = static_cast<int32_t>(3 * fb + cnt[v]);
-            for (int64_t c = 3 * fb; c < 3 * (fb + t); ++c) vt[3 * fb + cnt[p->tri_local[c]]++] = static_cast<int32_t>(c);
-        }
-    };
-    {
-        std::vector<std::thread> pool2;
-        for (int32_t k = 0; k < nt; ++k) {
-            const int32_t lo = k * chunk, hi = std::min(nc, lo + chunk);
-            if (lo < hi) pool2.emplace_back(inc, lo, hi);
-        }
-        for (auto& th : pool2) th.join();
-    }
     vt_ptr[p->n] = static_cast<int32_t>(3 * p->t);
     return UVA_OK;
 }
