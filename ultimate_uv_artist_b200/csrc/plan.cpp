@@ -402,14 +402,24 @@ extern "C" int uva_plan_export_rows(const uva_plan* p, int32_t* row_vert, int32_
                                     int32_t* cofs) {
     if (!p || !row_vert || !vert_row || !agg_rows || !cofs) { uva_set_error("uva_plan_export_rows: null argument"); return UVA_E_ARG; }
     const int64_t v0 = p->vofs.empty() ? 0 : p->vofs[0];
-    for (int32_t i = 0; i < p->nc; ++i) {
-        const IslandPlan& ip = p->isl[i];
-        const int64_t vb = p->vofs[i] - v0;
-        std::memcpy(row_vert + vb, ip.row_vert.data(), sizeof(int32_t) * ip.n);
-        std::memcpy(vert_row + vb, ip.vert_row.data(), sizeof(int32_t) * ip.n);
-        agg_rows[i] = ip.agg_rows;
-        cofs[i] = static_cast<int32_t>(p->cofs[i]);
-    }
+    std::atomic<int32_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const int32_t i = next.fetch_add(1);
+            if (i >= p->nc) break;
+            const IslandPlan& ip = p->isl[i];
+            const int64_t vb = p->vofs[i] - v0;
+            std::memcpy(row_vert + vb, ip.row_vert.data(), sizeof(int32_t) * ip.n);
+            std::memcpy(vert_row + vb, ip.vert_row.data(), sizeof(int32_t) * ip.n);
+            agg_rows[i] = ip.agg_rows;
+            cofs[i] = static_cast<int32_t>(p->cofs[i]);
+        }
+    };
+    int32_t nt = std::max(1, std::min<int32_t>(static_cast<int32_t>(std::thread::hardware_concurrency()), std::max(p->nc, 1)));
+    std::vector<std::thread> pool;
+    for (int32_t k = 1; k < nt; ++k) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
     cofs[p->nc] = static_cast<int32_t>(p->cofs[p->nc]);
     return UVA_OK;
 }

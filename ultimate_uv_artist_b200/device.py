@@ -14,6 +14,7 @@ triangles.
 from __future__ import annotations
 
 import ctypes as C
+import threading
 
 import numpy as np
 import torch
@@ -98,7 +99,9 @@ class Plan:
             check(L.uva_plan_export_rows(h, ptr(self.row_vert), ptr(self.vert_row), ptr(self.agg_rows), ptr(self.cofs)),
                   "uva_plan_export_rows")
         finally:
-            L.uva_plan_destroy(h)
+            # freeing the plan's per-island buffers takes a few ms: off the
+            # caller's path (ctypes releases the GIL during the call)
+            threading.Thread(target=L.uva_plan_destroy, args=(h,), daemon=True).start()
         self.vofs = vofs.astype(np.int32)
         self.tofs = tofs.astype(np.int32)
         # island work order: grouped by size class (whole CTA with global or
