@@ -535,14 +535,15 @@ __device__ __forceinline__ float jacobi(const uva_batch& b, const Isl& I, int i)
 // Inverse coarse operators are stored as FP16, scaled so that the largest
 // entry is 1024 (a CPU probe on LSCM islands: same PCG iterations as FP32,
 // still positive definite), in the first half of the island's FP32 block;
-// the float after the halves holds the inverse of the scale. Rows are padded
-// (zeros) to a stride of a whole number of vector loads: 2 halves for ARAP
-// (4-byte aligned blocks), 4 for LSCM (16-byte aligned blocks).
+// the float after the halves holds the inverse of the scale. ARAP: the real
+// M x M inverse; LSCM: the complex M x M inverse of the complex Hermitian
+// operator whose real representation is the (u, v) system, as (re, im)
+// half pairs. Rows are padded (zeros) to an even number of entries: one
+// vector load takes 2 entries (4-byte aligned ARAP blocks, 16-byte aligned
+// LSCM blocks).
 __host__ __device__ __forceinline__ const float* coarse_scale(const float* block, int nhalf) {
     return block + (nhalf + 1) / 2;
 }
-template <Op OP>
-__host__ __device__ constexpr int coarse_vec() { return OP == OP_ARAP ? 2 : 4; }
 __host__ __device__ constexpr int coarse_stride(int N, int vec) { return (N + vec - 1) / vec * vec; }
 
 // Two-level additive preconditioner z = D^-1 r + P Ac^-1 P^T r. P is the
@@ -581,62 +582,59 @@ __device__ __forceinline__ void coarse_solve(const uva_batch& b, Team<NTT>& tm, 
         }
     }
     tm.sync();   // g complete
-    // y = Ac^-1 g, one warp per coarse row. A lane takes VEC consecutive
-    // columns of every (32 VEC)-column chunk with one vector load per row and
-    // keeps its part of g in registers for all the rows it visits.
-    constexpr int VEC = coarse_vec<OP>();
-    constexpr int NR = OP == OP_ARAP ? 2 : 1;   // right-hand sides (ARAP: u and v)
-    constexpr int CH = 4;                        // chunks: N <= 256 (ARAP), 512 (LSCM)
-    const int N = OP == OP_ARAP ? I.M : 2 * I.M;
-    const int S = coarse_stride(N, VEC);
+    // y = Ac^-1 g, one warp per coarse row. ARAP: a real M x M inverse
+    // applied to the u and v columns; LSCM: a complex M x M inverse (the
+    // real (u, v) operator is the representation of a complex Hermitian one)
+    // applied to g_u + i g_v. A lane takes 2 consecutive entries of every
+    // 64-entry chunk with one vector load per row and keeps its part of g in
+    // registers for all the rows it visits.
+    constexpr int CH = 4;   // chunks: M <= 256
+    const int M = I.M;
+    const int S = coarse_stride(M, 2);
     const float* blockf = OP == OP_ARAP ? b.coarse_a + I.co : b.coarse_l + 4 * static_cast<size_t>(I.co);
     const __half* A = reinterpret_cast<const __half*>(blockf);
-    const float isc = __ldg(coarse_scale(blockf, N * S));
-    float gr[NR][CH][VEC];
+    const float isc = __ldg(coarse_scale(blockf, (OP == OP_ARAP ? 1 : 2) * M * S));
+    float gu[CH][2], gv[CH][2];
 #pragma unroll
     for (int ch = 0; ch < CH; ++ch) {
 #pragma unroll
-        for (int e = 0; e < VEC; ++e) {
-            const int c = 32 * VEC * ch + VEC * lane + e;
-#pragma unroll
-            for (int r = 0; r < NR; ++r) gr[r][ch][e] = c < N ? tm.cg[r * N + c] : 0.f;
+        for (int e = 0; e < 2; ++e) {
+            const int c = 64 * ch + 2 * lane + e;
+            const bool in = c < M;
+            gu[ch][e] = in ? (OP == OP_ARAP ? tm.cg[c] : tm.cg[2 * c]) : 0.f;
+            gv[ch][e] = in ? (OP == OP_ARAP ? tm.cg[M + c] : tm.cg[2 * c + 1]) : 0.f;
         }
     }
-    for (int o = warp; o < N; o += NW) {
-        const __half* row = A + static_cast<size_t>(o) * S;
-        float acc[NR];
-#pragma unroll
-        for (int r = 0; r < NR; ++r) acc[r] = 0.f;
+    for (int o = warp; o < M; o += NW) {
+        float au = 0.f, av = 0.f;
 #pragma unroll
         for (int ch = 0; ch < CH; ++ch) {
-            const int c0 = 32 * VEC * ch + VEC * lane;
+            const int c0 = 64 * ch + 2 * lane;
             if (c0 < S) {
-                float a[VEC];
-                if constexpr (VEC == 4) {
-                    const uint2 raw = __ldg(reinterpret_cast<const uint2*>(row + c0));
-                    const float2 f01 = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
-                    const float2 f23 = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
-                    a[0] = f01.x; a[1] = f01.y; a[2] = f23.x; a[3] = f23.y;
-                } else {
-                    const unsigned raw = __ldg(reinterpret_cast<const unsigned*>(row + c0));
-                    const float2 f01 = __half22float2(*reinterpret_cast<const __half2*>(&raw));
-                    a[0] = f01.x; a[1] = f01.y;
-                }
-#pragma unroll
-                for (int e = 0; e < VEC; ++e) {
-#pragma unroll
-                    for (int r = 0; r < NR; ++r) acc[r] = fmaf(a[e], gr[r][ch][e], acc[r]);
+                if constexpr (OP == OP_ARAP) {
+                    const unsigned raw = __ldg(reinterpret_cast<const unsigned*>(A + static_cast<size_t>(o) * S + c0));
+                    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw));
+                    au = fmaf(a.x, gu[ch][0], au); av = fmaf(a.x, gv[ch][0], av);
+                    au = fmaf(a.y, gu[ch][1], au); av = fmaf(a.y, gv[ch][1], av);
+                } else {   // two complex entries (re, im)
+                    const uint2 raw = __ldg(reinterpret_cast<const uint2*>(A + 2 * (static_cast<size_t>(o) * S + c0)));
+                    const float2 z0 = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
+                    const float2 z1 = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
+                    au = fmaf(z0.x, gu[ch][0], au); au = fmaf(-z0.y, gv[ch][0], au);
+                    av = fmaf(z0.y, gu[ch][0], av); av = fmaf(z0.x, gv[ch][0], av);
+                    au = fmaf(z1.x, gu[ch][1], au); au = fmaf(-z1.y, gv[ch][1], au);
+                    av = fmaf(z1.y, gu[ch][1], av); av = fmaf(z1.x, gv[ch][1], av);
                 }
             }
         }
 #pragma unroll
-        for (int r = 0; r < NR; ++r) {
-#pragma unroll
-            for (int k = 16; k > 0; k >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], k);
+        for (int k = 16; k > 0; k >>= 1) {
+            au += __shfl_xor_sync(0xffffffffu, au, k);
+            av += __shfl_xor_sync(0xffffffffu, av, k);
         }
         if (lane == 0) {
-            if (OP == OP_ARAP) { tm.cy[o] = acc[0] * isc; tm.cy[I.M + o] = acc[NR - 1] * isc; }
-            else tm.cy[o] = acc[0] * isc;
+            if (OP == OP_ARAP) { tm.cy[o] = au * isc; tm.cy[M + o] = av * isc; }
+            else { tm.cy[2 * o] = au * isc; tm.cy[2 * o + 1] = av * isc; }
         }
     }
     tm.sync();   // y complete
@@ -1482,6 +1480,42 @@ __device__ void store_half_scaled(const double* W, int N, int S, float* block, d
     __syncthreads();
 }
 
+// The LSCM inverse W (FP64, 2M x 2M, unknowns (u_a, v_a) interleaved) is
+// the real representation [[Cr, -Ci], [Ci, Cr]] of a complex M x M matrix
+// (per 2 x 2 block): Cr and Ci (the two copies averaged) -> (re, im) FP16
+// pairs scaled to a largest entry of 1024, rows of stride S (zero padding),
+// plus the inverse scale after them. Whole CTA.
+__device__ void store_complex_scaled(const double* W, int M, int S, float* block, double* red) {
+    const int N = 2 * M;
+    auto cre = [&](int o, int c) {
+        return 0.5 * (W[static_cast<size_t>(2 * o) * N + 2 * c] + W[static_cast<size_t>(2 * o + 1) * N + 2 * c + 1]);
+    };
+    auto cim = [&](int o, int c) {
+        return 0.5 * (W[static_cast<size_t>(2 * o + 1) * N + 2 * c] - W[static_cast<size_t>(2 * o) * N + 2 * c + 1]);
+    };
+    double m = 0.0;
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
+        const int o = e / M, c = e - o * M;
+        m = fmax(m, fmax(fabs(cre(o, c)), fabs(cim(o, c))));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __syncthreads();   // red may still be read by the caller's last step
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+    const double sc = (m > 0.0 && isfinite(m)) ? 1024.0 / m : 1.0;
+    __half2* h = reinterpret_cast<__half2*>(block);
+    for (int e = threadIdx.x; e < M * S; e += blockDim.x) {
+        const int o = e / S, c = e - o * S;
+        h[e] = c < M ? __floats2half2_rn(static_cast<float>(cre(o, c) * sc), static_cast<float>(cim(o, c) * sc))
+                     : __floats2half2_rn(0.f, 0.f);
+    }
+    if (threadIdx.x == 0) *const_cast<float*>(coarse_scale(block, 2 * M * S)) = static_cast<float>(1.0 / sc);
+    __syncthreads();
+}
+
 constexpr int kCoarseSmemN = 128;
 constexpr size_t kCoarseSmem = sizeof(double) * kCoarseSmemN * kCoarseSmemN;   // 131,072 bytes
 
@@ -1531,7 +1565,7 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
         Wa[a] += dsum;
     }
     gauss_jordan(W, M, colk);
-    store_half_scaled(W, M, coarse_stride(M, coarse_vec<OP_ARAP>()), b.coarse_a + co, colk);
+    store_half_scaled(W, M, coarse_stride(M, 2), b.coarse_a + co, colk);
     __syncthreads();
     // ---- LSCM (free unknowns only; the pins are fixed)
     const int pv0 = b.pins[3 * isl + 1], pv1 = b.pins[3 * isl + 2];
@@ -1580,7 +1614,7 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
         Wv[2 * a] += cvu;
     }
     gauss_jordan(W, N, colk);
-    store_half_scaled(W, N, coarse_stride(N, coarse_vec<OP_LSCM>()), b.coarse_l + 4 * static_cast<size_t>(co), colk);
+    store_complex_scaled(W, ML, coarse_stride(ML, 2), b.coarse_l + 4 * static_cast<size_t>(co), colk);
 }
 
 cudaError_t ensure_coarse_attr() {
