@@ -82,10 +82,19 @@ class Clocks:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.index)], stdout=self.fh,
+                                          "-lms", "50", "-i", str(self.index)], stdout=self.fh,
                                          stderr=subprocess.DEVNULL)
         except Exception:  # noqa: BLE001 - clocks are best effort
             self.proc = None
+            return
+        # the timed region starts only once the sampler is running (its start
+        # takes a few hundred ms; a short region would otherwise get no sample)
+        t_end = time.time() + 5.0
+        while time.time() < t_end and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+            time.sleep(0.02)
+        self.fh.flush()
+        with open(self.path) as fh:   # samples before this point are not the timed region's
+            self.skip = sum(1 for _ in fh)
 
     def stop(self):
         if self.proc is None:
@@ -99,7 +108,9 @@ class Clocks:
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         with open(self.path) as fh:
-            for line in fh:
+            for k, line in enumerate(fh):
+                if k < getattr(self, "skip", 0):
+                    continue
                 parts = [p.strip() for p in line.split(",")]
                 if len(parts) < 9:
                     continue
