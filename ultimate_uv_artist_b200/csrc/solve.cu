@@ -557,8 +557,6 @@ __host__ __device__ constexpr int coarse_stride(int N, int vec) { return (N + ve
 // and fold with xor shuffles in a fixed order. Ends with a barrier: y complete.
 template <int NTT, Op OP>
 __device__ __forceinline__ void coarse_solve(const uva_batch& b, Team<NTT>& tm, const Isl& I, const float2* r) {
-    constexpr int NW = NTT / 32;
-    const int lane = tm.tid & 31, warp = tm.tid >> 5;
     int lt = 5;   // log2 T
     while (lt > 0 && (I.M << lt) > NTT) --lt;
     const int T = 1 << lt, groups = NTT >> lt;
@@ -581,58 +579,53 @@ __device__ __forceinline__ void coarse_solve(const uva_batch& b, Team<NTT>& tm, 
             else { tm.cg[2 * a] = gx; tm.cg[2 * a + 1] = gy; }
         }
     }
+    // odd M: the product's last pair reads g one entry past the end (against a
+    // zero matrix entry), which must hold a finite value
+    if ((I.M & 1) && tm.tid == 0) { tm.cg[2 * I.M] = 0.f; tm.cg[2 * I.M + 1] = 0.f; }
     tm.sync();   // g complete
-    // y = Ac^-1 g, one warp per coarse row. ARAP: a real M x M inverse
-    // applied to the u and v columns; LSCM: a complex M x M inverse (the
-    // real (u, v) operator is the representation of a complex Hermitian one)
-    // applied to g_u + i g_v. A lane takes 2 consecutive entries of every
-    // 64-entry chunk with one vector load per row and keeps its part of g in
-    // registers for all the rows it visits.
-    constexpr int CH = 4;   // chunks: M <= 256
+    // y = Ac^-1 g. ARAP: a real M x M inverse applied to the u and v
+    // columns; LSCM: a complex M x M inverse (the real (u, v) operator is the
+    // representation of a complex Hermitian one) applied to g_u + i g_v.
+    // Eight lanes per coarse row, every row of the team in flight at once: a
+    // lane takes a run of consecutive entries (two per load) and the group
+    // folds with three xor shuffles.
+    constexpr int G = 8;
     const int M = I.M;
     const int S = coarse_stride(M, 2);
     const float* blockf = OP == OP_ARAP ? b.coarse_a + I.co : b.coarse_l + 4 * static_cast<size_t>(I.co);
     const __half* A = reinterpret_cast<const __half*>(blockf);
     const float isc = __ldg(coarse_scale(blockf, (OP == OP_ARAP ? 1 : 2) * M * S));
-    float gu[CH][2], gv[CH][2];
-#pragma unroll
-    for (int ch = 0; ch < CH; ++ch) {
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-            const int c = 64 * ch + 2 * lane + e;
-            const bool in = c < M;
-            gu[ch][e] = in ? (OP == OP_ARAP ? tm.cg[c] : tm.cg[2 * c]) : 0.f;
-            gv[ch][e] = in ? (OP == OP_ARAP ? tm.cg[M + c] : tm.cg[2 * c + 1]) : 0.f;
-        }
-    }
-    for (int o = warp; o < M; o += NW) {
+    const int gl = tm.tid & (G - 1), grow = tm.tid / G;
+    const int cpl = ((M + G - 1) / G + 1) & ~1;   // entries per lane, even
+    const int c_beg = gl * cpl, c_end = min(c_beg + cpl, M);
+    for (int base = 0; base < M; base += NTT / G) {   // the same trip count on every thread
+        const int o = base + grow;
         float au = 0.f, av = 0.f;
-#pragma unroll
-        for (int ch = 0; ch < CH; ++ch) {
-            const int c0 = 64 * ch + 2 * lane;
-            if (c0 < S) {
+        if (o < M) {
+            for (int c = c_beg; c < c_end; c += 2) {   // c even: entry c + 1 < S (zero past M)
                 if constexpr (OP == OP_ARAP) {
-                    const unsigned raw = __ldg(reinterpret_cast<const unsigned*>(A + static_cast<size_t>(o) * S + c0));
+                    const unsigned raw = __ldg(reinterpret_cast<const unsigned*>(A + static_cast<size_t>(o) * S + c));
                     const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw));
-                    au = fmaf(a.x, gu[ch][0], au); av = fmaf(a.x, gv[ch][0], av);
-                    au = fmaf(a.y, gu[ch][1], au); av = fmaf(a.y, gv[ch][1], av);
-                } else {   // two complex entries (re, im)
-                    const uint2 raw = __ldg(reinterpret_cast<const uint2*>(A + 2 * (static_cast<size_t>(o) * S + c0)));
+                    au = fmaf(a.x, tm.cg[c], au); au = fmaf(a.y, tm.cg[c + 1], au);
+                    av = fmaf(a.x, tm.cg[M + c], av); av = fmaf(a.y, tm.cg[M + c + 1], av);
+                } else {   // two complex entries (re, im) against (g_u, g_v) pairs
+                    const uint2 raw = __ldg(reinterpret_cast<const uint2*>(A + 2 * (static_cast<size_t>(o) * S + c)));
                     const float2 z0 = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
                     const float2 z1 = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
-                    au = fmaf(z0.x, gu[ch][0], au); au = fmaf(-z0.y, gv[ch][0], au);
-                    av = fmaf(z0.y, gu[ch][0], av); av = fmaf(z0.x, gv[ch][0], av);
-                    au = fmaf(z1.x, gu[ch][1], au); au = fmaf(-z1.y, gv[ch][1], au);
-                    av = fmaf(z1.y, gu[ch][1], av); av = fmaf(z1.x, gv[ch][1], av);
+                    const float4 g = *reinterpret_cast<const float4*>(tm.cg + 2 * c);
+                    au = fmaf(z0.x, g.x, au); au = fmaf(-z0.y, g.y, au);
+                    av = fmaf(z0.y, g.x, av); av = fmaf(z0.x, g.y, av);
+                    au = fmaf(z1.x, g.z, au); au = fmaf(-z1.y, g.w, au);
+                    av = fmaf(z1.y, g.z, av); av = fmaf(z1.x, g.w, av);
                 }
             }
         }
 #pragma unroll
-        for (int k = 16; k > 0; k >>= 1) {
+        for (int k = G / 2; k > 0; k >>= 1) {
             au += __shfl_xor_sync(0xffffffffu, au, k);
             av += __shfl_xor_sync(0xffffffffu, av, k);
         }
-        if (lane == 0) {
+        if (gl == 0 && o < M) {
             if (OP == OP_ARAP) { tm.cy[o] = au * isc; tm.cy[M + o] = av * isc; }
             else { tm.cy[2 * o] = au * isc; tm.cy[2 * o + 1] = av * isc; }
         }
@@ -1379,7 +1372,7 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
     __shared__ float redf[2 * kRedMax * 32];
     __shared__ int redi[2 * 32];
     __shared__ int slots[8];
-    __shared__ float coarse_buf[1024];   // g and y of the coarse level (CTA: 512 each; sub-team: 128 each)
+    __shared__ __align__(16) float coarse_buf[1024];   // g and y of the coarse level (CTA: 512 each; sub-team: 128 each)
     __shared__ int sc_buf[288];          // slice pointers (CTA: 288; sub-team: 72 each; warp: 9 each)
     __shared__ __nv_bfloat16 dinv_buf[KB * RB];   // Jacobi (CTA: 8192; sub-team: 2048; warp: 256)
     const bool rev = static_cast<int>(blockIdx.x) < nrev;
