@@ -1421,23 +1421,65 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
 // In-place Gauss-Jordan inverse of an SPD N x N FP64 matrix (no pivoting
 // needed), one CTA. A non-positive pivot (a singular coarse block, e.g. a
 // disconnected island) zeroes that row and column of the result.
-__device__ void gauss_jordan(double* W, int N, double* colk) {
+__device__ void gauss_jordan(double* W, int N, double* colk, double* rowk) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int k = 0; k < N; ++k) {
-        __syncthreads();
+        __syncthreads();   // the previous step's updates are complete
         const double piv = W[static_cast<size_t>(k) * N + k];
         const double ip = (piv > 0.0 && isfinite(piv)) ? 1.0 / piv : 0.0;
-        for (int i = threadIdx.x; i < N; i += blockDim.x) colk[i] = i == k ? 0.0 : W[static_cast<size_t>(i) * N + k];
+        for (int i = threadIdx.x; i < N; i += blockDim.x) {
+            colk[i] = i == k ? 0.0 : W[static_cast<size_t>(i) * N + k];
+            rowk[i] = i == k ? ip : W[static_cast<size_t>(k) * N + i] * ip;   // scaled pivot row
+        }
         __syncthreads();
-        for (int j = threadIdx.x; j < N; j += blockDim.x)
-            W[static_cast<size_t>(k) * N + j] = j == k ? ip : W[static_cast<size_t>(k) * N + j] * ip;
-        __syncthreads();
-        for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
-            const int i = e / N, j = e % N;
-            if (i == k) continue;
+        // one warp per row, lanes along the row: row k becomes the scaled
+        // pivot row, row i loses colk[i] times it (its column k becomes
+        // -colk[i] / piv)
+        for (int i = warp; i < N; i += nw) {
+            double* Wi = W + static_cast<size_t>(i) * N;
+            if (i == k) {
+                for (int j = lane; j < N; j += 32) Wi[j] = rowk[j];
+                continue;
+            }
             const double f = colk[i];
             if (f == 0.0) continue;
-            const double base = j == k ? 0.0 : W[e];
-            W[e] = base - f * W[static_cast<size_t>(k) * N + j];
+            for (int j = lane; j < N; j += 32) Wi[j] = (j == k ? 0.0 : Wi[j]) - f * rowk[j];
+        }
+    }
+    __syncthreads();
+}
+
+// The same for a complex Hermitian positive definite M x M matrix (pivots
+// real and positive); W row-major (re, im) pairs.
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ void gauss_jordan_c(double2* W, int M, double2* colk, double2* rowk) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = 0; k < M; ++k) {
+        __syncthreads();
+        const double2 piv = W[static_cast<size_t>(k) * M + k];
+        const double den = piv.x * piv.x + piv.y * piv.y;
+        const double2 ip = (piv.x > 0.0 && isfinite(den) && den > 0.0) ? make_double2(piv.x / den, -piv.y / den)
+                                                                        : make_double2(0.0, 0.0);
+        for (int i = threadIdx.x; i < M; i += blockDim.x) {
+            colk[i] = i == k ? make_double2(0.0, 0.0) : W[static_cast<size_t>(i) * M + k];
+            rowk[i] = i == k ? ip : cmul(W[static_cast<size_t>(k) * M + i], ip);
+        }
+        __syncthreads();
+        for (int i = warp; i < M; i += nw) {
+            double2* Wi = W + static_cast<size_t>(i) * M;
+            if (i == k) {
+                for (int j = lane; j < M; j += 32) Wi[j] = rowk[j];
+                continue;
+            }
+            const double2 f = colk[i];
+            if (f.x == 0.0 && f.y == 0.0) continue;
+            for (int j = lane; j < M; j += 32) {
+                const double2 base = j == k ? make_double2(0.0, 0.0) : Wi[j];
+                const double2 d = cmul(f, rowk[j]);
+                Wi[j] = make_double2(base.x - d.x, base.y - d.y);
+            }
         }
     }
     __syncthreads();
@@ -1473,19 +1515,12 @@ __device__ void store_half_scaled(const double* W, int N, int S, float* block, d
     __syncthreads();
 }
 
-// The LSCM inverse W (FP64, 2M x 2M, unknowns (u_a, v_a) interleaved) is
-// the real representation [[Cr, -Ci], [Ci, Cr]] of a complex M x M matrix
-// (per 2 x 2 block): Cr and Ci (the two copies averaged) -> (re, im) FP16
-// pairs scaled to a largest entry of 1024, rows of stride S (zero padding),
-// plus the inverse scale after them. Whole CTA.
-__device__ void store_complex_scaled(const double* W, int M, int S, float* block, double* red) {
-    const int N = 2 * M;
-    auto cre = [&](int o, int c) {
-        return 0.5 * (W[static_cast<size_t>(2 * o) * N + 2 * c] + W[static_cast<size_t>(2 * o + 1) * N + 2 * c + 1]);
-    };
-    auto cim = [&](int o, int c) {
-        return 0.5 * (W[static_cast<size_t>(2 * o + 1) * N + 2 * c] - W[static_cast<size_t>(2 * o) * N + 2 * c + 1]);
-    };
+// The LSCM inverse (complex M x M, FP64) -> its Hermitian part as (re, im)
+// FP16 pairs scaled to a largest entry of 1024, rows of stride S (zero
+// padding), plus the inverse scale after them. Whole CTA.
+__device__ void store_complex_scaled(const double2* W, int M, int S, float* block, double* red) {
+    auto cre = [&](int o, int c) { return 0.5 * (W[static_cast<size_t>(o) * M + c].x + W[static_cast<size_t>(c) * M + o].x); };
+    auto cim = [&](int o, int c) { return 0.5 * (W[static_cast<size_t>(o) * M + c].y - W[static_cast<size_t>(c) * M + o].y); };
     double m = 0.0;
     for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
         const int o = e / M, c = e - o * M;
@@ -1509,12 +1544,18 @@ __device__ void store_complex_scaled(const double* W, int M, int S, float* block
     __syncthreads();
 }
 
-constexpr int kCoarseSmemN = 128;
-constexpr size_t kCoarseSmem = sizeof(double) * kCoarseSmemN * kCoarseSmemN;   // 131,072 bytes
+// shared-memory work matrix: complex LSCM operators up to 118 x 118, real
+// ARAP operators up to 166 x 166 (larger ones work in b.coarse_work)
+constexpr int kCoarseSmemC = 118;
+constexpr size_t kCoarseSmem = sizeof(double2) * kCoarseSmemC * kCoarseSmemC;   // 222,784 bytes
+constexpr int kCoarseSmemN = 166;   // sizeof(double) * 166 * 166 <= kCoarseSmem
+static_assert(sizeof(double) * kCoarseSmemN * kCoarseSmemN <= kCoarseSmem, "real work matrix must fit");
 
 __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
-    extern __shared__ double wsm[];
-    __shared__ double colk[512];
+    extern __shared__ __align__(16) double wsm[];
+    __shared__ double2 colk2[256], rowk2[256];   // pivot column / row (complex; the real pass uses 256 doubles of each)
+    double* colk = reinterpret_cast<double*>(colk2);
+    double* rowk = reinterpret_cast<double*>(rowk2);
     if (static_cast<int>(blockIdx.x) >= b.nc) return;
     const int isl = b.order[blockIdx.x];   // largest islands first (b.order is by size)
     const int agg = b.agg_rows[isl];
@@ -1557,24 +1598,23 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
         if (a == pin_agg) dsum += b.wpin[isl];
         Wa[a] += dsum;
     }
-    gauss_jordan(W, M, colk);
+    gauss_jordan(W, M, colk, rowk);
     store_half_scaled(W, M, coarse_stride(M, 2), b.coarse_a + co, colk);
     __syncthreads();
     // ---- LSCM (free unknowns only; the pins are fixed)
     const int pv0 = b.pins[3 * isl + 1], pv1 = b.pins[3 * isl + 2];
     if (pv0 < 0 || pv1 < 0) return;
     const int p0 = b.vert_row[v0 + pv0], p1 = b.vert_row[v0 + pv1];
-    const int aggl = agg;
-    const int ML = M;
-    const int N = 2 * ML;
-    W = work(N);
-    for (int e = threadIdx.x; e < N * N; e += blockDim.x) W[e] = 0.0;
+    // the (u, v) operator per aggregate is the real form [[P, -Q], [Q, P]] of
+    // the complex Hermitian Hc = P + i Q: assembled and inverted as complex
+    double2* Wc = M <= kCoarseSmemC ? reinterpret_cast<double2*>(wsm)
+                                    : reinterpret_cast<double2*>(b.coarse_work + 4 * static_cast<size_t>(co));
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) Wc[e] = make_double2(0.0, 0.0);
     __syncthreads();
-    for (int a = threadIdx.x; a < ML; a += blockDim.x) {
-        double* Wu = W + static_cast<size_t>(2 * a) * N;      // row of u_a
-        double* Wv = W + static_cast<size_t>(2 * a + 1) * N;  // row of v_a
-        double dsum = 0.0, cuv = 0.0, cvu = 0.0;
-        for (int r = a * aggl; r < min(n, (a + 1) * aggl); ++r) {
+    for (int a = threadIdx.x; a < M; a += blockDim.x) {
+        double2* Wa = Wc + static_cast<size_t>(a) * M;
+        double dsum = 0.0, qaa = 0.0;
+        for (int r = a * agg; r < min(n, (a + 1) * agg); ++r) {
             if (r == p0 || r == p1) continue;
             int q0, width;
             row_slots_l(r, q0, width);
@@ -1590,24 +1630,22 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
                     if (w == 0.0 && cc == 0.0) continue;
                     const int col = slot_row(sl.x);
                     const bool pinned_nb = col == p0 || col == p1;   // no coarse coupling
-                    const int c = col / aggl;
+                    const int c = col / agg;
                     if (pinned_nb || c != a) dsum += w;
                     if (pinned_nb) continue;
-                    if (c != a) { Wu[2 * c] -= w; Wv[2 * c + 1] -= w; }
+                    if (c != a) Wa[c].x -= w;
                     if (cc != 0.0) {
-                        if (c == a) { cuv += cc; cvu -= cc; }
-                        else { Wu[2 * c + 1] += cc; Wv[2 * c] -= cc; }
+                        if (c == a) qaa -= cc;
+                        else Wa[c].y -= cc;
                     }
                 }
             }
         }
-        Wu[2 * a] += dsum;
-        Wv[2 * a + 1] += dsum;
-        Wu[2 * a + 1] += cuv;
-        Wv[2 * a] += cvu;
+        Wa[a].x += dsum;
+        Wa[a].y += qaa;
     }
-    gauss_jordan(W, N, colk);
-    store_complex_scaled(W, ML, coarse_stride(ML, 2), b.coarse_l + 4 * static_cast<size_t>(co), colk);
+    gauss_jordan_c(Wc, M, colk2, rowk2);
+    store_complex_scaled(Wc, M, coarse_stride(M, 2), b.coarse_l + 4 * static_cast<size_t>(co), colk);
 }
 
 cudaError_t ensure_coarse_attr() {
