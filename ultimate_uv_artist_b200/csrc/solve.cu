@@ -854,6 +854,7 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
             act[0] = act[1] = (red4[2] + red4[3]) > thr2[0] && rz[0] > 0.f;
         }
         int it = 0;
+        float apend[2] = {0.f, 0.f};   // alpha of the last step not yet added to d
         while ((act[0] || act[1]) && it < prm.max_inner) {
             tm.sync();   // p complete
             float pq[2] = {0.f, 0.f};
@@ -900,16 +901,15 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
                 const float s = pq[0] + pq[1];
                 alpha[0] = alpha[1] = (act[0] && s > 0.f) ? rz[0] / s : 0.f;
             }
-            // update d, r
+            // update r (d takes alpha p in the p update below, which reads p anyway)
             for_rows<NTT, R>(tid, n, [&](int i, int j) {
                 float2 q;
                 if constexpr (R > 0) q = qreg[j]; else q = sq[i];
-                const float2 p = sp[i];
-                float2 d = sd[i], r = sr[i];
-                d.x = fmaf(alpha[0], p.x, d.x); d.y = fmaf(alpha[1], p.y, d.y);
+                float2 r = sr[i];
                 r.x = fmaf(-alpha[0], q.x, r.x); r.y = fmaf(-alpha[1], q.y, r.y);
-                sd[i] = d; sr[i] = r;
+                sr[i] = r;
             });
+            apend[0] = alpha[0]; apend[1] = alpha[1];
             if (two_level) {
                 tm.sync();   // residual complete
                 coarse_solve<NTT, OP>(b, tm, I, sr);
@@ -942,17 +942,23 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
             if (!(act[0] || act[1])) break;
             for_rows<NTT, R>(tid, n, [&](int i, int) {
                 const float2 r = sr[i], p = sp[i];
+                float2 d = sd[i];
+                d.x = fmaf(apend[0], p.x, d.x); d.y = fmaf(apend[1], p.y, d.y);
+                sd[i] = d;
                 const float m = jacobi<OP>(b, I, i);
                 float zx = m * r.x, zy = m * r.y;
                 if (two_level && !is_pinned<OP>(I, i)) { const float2 y = prolong<NTT, OP>(tm, I, i); zx += y.x; zy += y.y; }
                 sp[i] = make_float2(fmaf(beta[0], p.x, zx), fmaf(beta[1], p.y, zy));
             });
+            apend[0] = 0.f; apend[1] = 0.f;
         }
         if (it >= prm.max_inner) capped = true;
         total += it;
         tm.sync();
-        for_rows<NTT, R>(tid, n, [&](int i, int) {
-            const float2 d = sd[i];
+        for_rows<NTT, R>(tid, n, [&](int i, int) {   // x += d (+ the last step's alpha p)
+            const float2 p = sp[i];
+            float2 d = sd[i];
+            d.x = fmaf(apend[0], p.x, d.x); d.y = fmaf(apend[1], p.y, d.y);
             double2 x = x64[i];
             x.x += static_cast<double>(d.x); x.y += static_cast<double>(d.y);
             x64[i] = x;
