@@ -644,11 +644,21 @@ __device__ __forceinline__ float2 prolong(const Team<NTT>& tm, const Isl& I, int
 // by solver row, most recent first) for the Galerkin start of the next
 // global step; m == 0: start from the given x.
 constexpr int kStartMax = 4;
+// Kept compact (two ints) because it stays live across the refinement loop:
+// the vectors are found from the batch (b.hist, or the class-G buffers).
 struct StartSpace {
-    int m = 0;
-    const float2* d[kStartMax] = {nullptr, nullptr, nullptr, nullptr};
-    const float2* a[kStartMax] = {nullptr, nullptr, nullptr, nullptr};
+    int m = 0;       // updates in use
+    int slots = 0;   // ring slot of update k (most recent first) in bits 2k..2k+1
+    __device__ __forceinline__ int slot(int k) const { return (slots >> (2 * k)) & 3; }
 };
+
+// Ring slot k of the ARAP update history of island rows [v0, v0 + n): the
+// update (part 0) or its image under A (part 1).
+__device__ __forceinline__ float2* start_vec(const uva_batch& b, int v0, int k, int part) {
+    if (b.hist) return reinterpret_cast<float2*>(b.hist) + static_cast<size_t>(2 * k + part) * b.n + v0;
+    float* base = part == 0 ? (k == 0 ? b.p32 : b.d32) : (k == 0 ? b.q32 : b.r32);
+    return reinterpret_cast<float2*>(base) + v0;
+}
 
 // t = M^+ g for the m x m Gram matrix M (lower triangle, row-major packed:
 // M[k(k+1)/2 + l], l <= k) of one column: LDL^T in FP64 that skips a vector
@@ -783,12 +793,12 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
 #pragma unroll
                 for (int e = 0; e < 2 * (kStartMax + 1); ++e) acc[e] = 0.0;
                 for_rows<NTT, R>(tid, n, [&](int i, int) {
-                    const float2 d = gsp.d[k][i], r = sr[i];
+                    const float2 d = start_vec(b, I.v0, gsp.slot(k), 0)[i], r = sr[i];
                     acc[0] += static_cast<double>(d.x) * r.x;
                     acc[1] += static_cast<double>(d.y) * r.y;
 #pragma unroll
                     for (int l = 0; l <= k; ++l) {
-                        const float2 a = gsp.a[l][i];
+                        const float2 a = start_vec(b, I.v0, gsp.slot(l), 1)[i];
                         acc[2 + 2 * l] += static_cast<double>(d.x) * a.x;
                         acc[3 + 2 * l] += static_cast<double>(d.y) * a.y;
                     }
@@ -811,7 +821,7 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
 #pragma unroll
                 for (int k = 0; k < kStartMax; ++k) {
                     if (k >= m) break;
-                    const float2 d = gsp.d[k][i], a = gsp.a[k][i];
+                    const float2 d = start_vec(b, I.v0, gsp.slot(k), 0)[i], a = start_vec(b, I.v0, gsp.slot(k), 1)[i];
                     x.x += t[0][k] * d.x; x.y += t[1][k] * d.y;
                     ax += t[0][k] * a.x; ay += t[1][k] * a.y;
                 }
@@ -1097,14 +1107,8 @@ __device__ __forceinline__ void solve_arap(const uva_batch& b, const uva_solve_p
     // batch's history buffer (b.hist) kStartMax slots, else 2 slots in the
     // class-G CG buffers (the no-allocation entry point's case).
     const int depth = b.hist ? kStartMax : 2;
-    auto hist_d = [&](int k) -> float2* {
-        if (b.hist) return reinterpret_cast<float2*>(b.hist) + static_cast<size_t>(2 * k) * b.n + I.v0;
-        return reinterpret_cast<float2*>(k == 0 ? b.p32 : b.d32) + I.v0;
-    };
-    auto hist_a = [&](int k) -> float2* {
-        if (b.hist) return reinterpret_cast<float2*>(b.hist) + static_cast<size_t>(2 * k + 1) * b.n + I.v0;
-        return reinterpret_cast<float2*>(k == 0 ? b.q32 : b.r32) + I.v0;
-    };
+    auto hist_d = [&](int k) -> float2* { return start_vec(b, I.v0, k, 0); };
+    auto hist_a = [&](int k) -> float2* { return start_vec(b, I.v0, k, 1); };
     const float wpin32 = static_cast<float>(I.wpin);
     for (int it = 0; it < prm.iters; ++it) {
         double ev[2] = {0.0, 0.0};
@@ -1149,11 +1153,7 @@ __device__ __forceinline__ void solve_arap(const uva_batch& b, const uva_solve_p
         StartSpace gsp;
         if (R > 0) {
             gsp.m = min(it, depth);
-            for (int k = 0; k < gsp.m; ++k) {   // most recent update first
-                const int slot = (it - 1 - k) % depth;
-                gsp.d[k] = hist_d(slot);
-                gsp.a[k] = hist_a(slot);
-            }
+            for (int k = 0; k < gsp.m; ++k) gsp.slots |= ((it - 1 - k) % depth) << (2 * k);   // most recent first
         }
         const int cgi = refine_solve<NTT, R, OP_ARAP, 2>(b, I, prm, tm, bb, res, nref, capped, gsp);
         if (tid == 0) {
