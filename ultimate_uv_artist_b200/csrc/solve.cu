@@ -925,11 +925,14 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
                 coarse_solve<NTT, OP>(b, tm, I, sr);
             }
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            for_rows<NTT, R>(tid, n, [&](int i, int) {
+            for_rows<NTT, R>(tid, n, [&](int i, int j) {
                 const float2 r = sr[i];
                 const float m = jacobi<OP>(b, I, i);
                 float zx = m * r.x, zy = m * r.y;
                 if (two_level && !is_pinned<OP>(I, i)) { const float2 y = prolong<NTT, OP>(tm, I, i); zx += y.x; zy += y.y; }
+                // LSCM keeps z for the p update in the A p registers (ARAP: its
+                // register budget is tighter, z is recomputed)
+                if constexpr (R > 0 && OP == OP_LSCM) qreg[j] = make_float2(zx, zy);
                 acc[0] += r.x * zx; acc[1] += r.y * zy;
                 acc[2] += r.x * r.x; acc[3] += r.y * r.y;
             });
@@ -950,14 +953,20 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
                 if (acc[2] + acc[3] <= thr2[0] || !(s > 0.f)) act[0] = act[1] = false;
             }
             if (!(act[0] || act[1])) break;
-            for_rows<NTT, R>(tid, n, [&](int i, int) {
-                const float2 r = sr[i], p = sp[i];
+            for_rows<NTT, R>(tid, n, [&](int i, int j) {
+                const float2 p = sp[i];
                 float2 d = sd[i];
                 d.x = fmaf(apend[0], p.x, d.x); d.y = fmaf(apend[1], p.y, d.y);
                 sd[i] = d;
-                const float m = jacobi<OP>(b, I, i);
-                float zx = m * r.x, zy = m * r.y;
-                if (two_level && !is_pinned<OP>(I, i)) { const float2 y = prolong<NTT, OP>(tm, I, i); zx += y.x; zy += y.y; }
+                float zx, zy;
+                if constexpr (R > 0 && OP == OP_LSCM) {
+                    zx = qreg[j].x; zy = qreg[j].y;
+                } else {
+                    const float2 r = sr[i];
+                    const float m = jacobi<OP>(b, I, i);
+                    zx = m * r.x; zy = m * r.y;
+                    if (two_level && !is_pinned<OP>(I, i)) { const float2 y = prolong<NTT, OP>(tm, I, i); zx += y.x; zy += y.y; }
+                }
                 sp[i] = make_float2(fmaf(beta[0], p.x, zx), fmaf(beta[1], p.y, zy));
             });
             apend[0] = 0.f; apend[1] = 0.f;
