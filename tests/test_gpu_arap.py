@@ -226,3 +226,61 @@ def test_schedule_autotuner(cuda):
     # the 2e-7 residual, so they agree to about that level, not bitwise
     ext = float((ref.max(0).values - ref.min(0).values).max())
     assert float((db.U - ref).abs().max()) / ext < 1e-6
+
+
+def test_start_history_buffer_optional(cuda):
+    """Without the batch's history buffer (uva_batch.hist null, as a C caller
+    may leave it) the ARAP starts use two updates kept in the class-G CG
+    buffers: same tolerance, the same UVs to the solver's accuracy."""
+    import ctypes as C
+    from ultimate_uv_artist_b200 import _lib, synth
+    from ultimate_uv_artist_b200.engine import gpu
+    isl = synth.uneven_islands(seed=311, count=30, tmin=20, tmax=6000)
+    b = gpu.Batch([(p, t, None) for p, t in isl])
+    db = b.db
+    db.lscm()
+    U0 = db.U.clone()
+    db.arap(iters=8)
+    ref = db.U.clone()
+    ext = float((ref.max(0).values - ref.min(0).values).max())
+    db.U.copy_(U0)
+    desc = _lib.BatchDesc.from_buffer_copy(db.desc)
+    desc.hist = None
+    prm = db.params("arap", iters=8, line_search=True)
+    _lib.check(_lib.lib().uva_arap(C.byref(desc), C.byref(prm), db._stream()), "uva_arap")
+    torch.cuda.synchronize()
+    assert (db.island_status()["resid"] <= 2e-7 * 1.001).all()
+    assert float((db.U - ref).abs().max()) / ext < 1e-5
+
+
+def test_class_capacity_guard(cuda):
+    """An island listed in a team class too small for it (a C caller's
+    inconsistent class_ofs) is refused with UVA_ST_BADCLASS and left
+    untouched; the islands that fit are solved."""
+    import ctypes as C
+    from ultimate_uv_artist_b200 import _lib, synth
+    from ultimate_uv_artist_b200.engine import gpu
+    isl = synth.uneven_islands(seed=312, count=12, tmin=20, tmax=2000)
+    b = gpu.Batch([(p, t, None) for p, t in isl])
+    db = b.db
+    db.lscm()
+    U0 = db.U.clone()
+    desc = _lib.BatchDesc.from_buffer_copy(db.desc)
+    for c in range(3):   # every island to the one-warp class (256 rows at most)
+        desc.class_ofs[c] = 0
+    desc.class_ofs[3] = 0
+    desc.class_ofs[4] = db.nc
+    prm = db.params("arap", iters=3, line_search=True)
+    _lib.check(_lib.lib().uva_arap(C.byref(desc), C.byref(prm), db._stream()), "uva_arap")
+    torch.cuda.synchronize()
+    st = db.island_status()
+    n = np.diff(db.plan.vofs)
+    big = n > 256
+    assert big.any() and (~big).any()
+    assert ((st["flags"][big] & _lib.ST_BADCLASS) != 0).all()
+    assert ((st["flags"][~big] & _lib.ST_BADCLASS) == 0).all()
+    assert (st["resid"][~big] <= 2e-7 * 1.001).all()
+    vofs = db.plan.vofs.astype(np.int64)
+    for i in np.where(big)[0]:
+        a, e = vofs[i], vofs[i + 1]
+        assert torch.equal(db.U[a:e], U0[a:e])
