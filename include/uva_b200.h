@@ -402,6 +402,47 @@ int uva_energy_bwd(const uva_batch* b, const double* P, const double* U, int32_t
 int uva_sd_refine(uva_batch* b, int32_t steps, int32_t halvings, double cap, double* e_isl, void* scratch,
                   void* stream);
 
+/* --------------------------------------------------------------------------
+ * Boundary self-intersection checks of UV charts, batched over charts.
+ * UVA_SEG_COUNT replaces engine/charts.py:547-608 (boundary_intersections /
+ * _seg_intersections): the number of crossing segment pairs counted once per
+ * grid cell the pair shares, with the reference's grid (lo and extent over
+ * the chart's UV rows, cell = max(4 median length, extent / 512, 1e-30)),
+ * capped at max(max_report, 1). UVA_SEG_ANY replaces engine/hier.py:183-266
+ * (_hit) as called by chart_checks (:270-353): 1 if any two segments
+ * cross, also when the endpoints' extent is not below 1e300.
+ * UVA_SEG_ANY_ALL is the same test as called by charts_collide (:183-225),
+ * which has no extent check.
+ * A crossing: the endpoints share no coordinates exactly and each segment's
+ * endpoints lie strictly on both sides of the other, beyond 1e-9 times its
+ * squared length (FP64, no fused multiply-add).
+ * ------------------------------------------------------------------------ */
+#define UVA_SEG_COUNT 0
+#define UVA_SEG_ANY   1
+#define UVA_SEG_ANY_ALL 2
+
+typedef struct uva_seg_desc {
+    int32_t nc;             /* charts                                         */
+    int32_t nseg;           /* boundary segments of all charts                */
+    int32_t n;              /* rows of U                                      */
+    int32_t mode;           /* UVA_SEG_COUNT, UVA_SEG_ANY or UVA_SEG_ANY_ALL  */
+    int32_t max_report;     /* UVA_SEG_COUNT: cap of the count                */
+    int32_t reserved;
+    const double* U;        /* n*2 FP64 UVs                                   */
+    const int32_t* vofs;    /* nc+1: UV rows of chart c (UVA_SEG_COUNT grid)  */
+    const int32_t* seg_ofs; /* nc+1: segments of chart c                      */
+    const int32_t* seg;     /* nseg*2: rows (a, b) of U, segment a -> b       */
+    int64_t* out;           /* out, nc. COUNT: the capped count, -1 for a
+                               chart with >= 3 segments and non-finite UVs
+                               (the reference raises), -2 for rows outside the
+                               chart; ANY: 0 or 1 (-2 for rows outside U)     */
+    void* scratch;          /* device scratch of uva_seg_scratch_bytes        */
+    int64_t scratch_bytes;
+} uva_seg_desc;
+
+int uva_seg_scratch_bytes(int32_t nc, int32_t nseg, int64_t* bytes);
+int uva_boundary_hits(const uva_seg_desc* d, void* stream);
+
 /* Library info. */
 const char* uva_last_error(void);
 int uva_version(void);

@@ -64,6 +64,15 @@ class SolveParams(C.Structure):
                 ("rev_ctas", i32)]
 
 
+class SegDesc(C.Structure):
+    """Mirror of ``uva_seg_desc``."""
+    _fields_ = [("nc", i32), ("nseg", i32), ("n", i32), ("mode", i32), ("max_report", i32), ("reserved", i32),
+                ("U", vp), ("vofs", vp), ("seg_ofs", vp), ("seg", vp), ("out", vp), ("scratch", vp),
+                ("scratch_bytes", C.c_int64)]
+
+
+SEG_COUNT, SEG_ANY, SEG_ANY_ALL = 0, 1, 2
+
 _SIGS = {
     "uva_plan_create": [vp, vp, vp, i32, i32, vp],
     "uva_plan_sizes": [vp, vp],
@@ -87,6 +96,8 @@ _SIGS = {
     "uva_signed_area": [vp, vp, vp, vp],
     "uva_jacobians": [vp, vp, vp, vp],
     "uva_shrink": [vp, vp, vp, i32, C.c_float, C.c_float, vp],
+    "uva_seg_scratch_bytes": [i32, i32, vp],
+    "uva_boundary_hits": [vp, vp],
     "uva_last_error": [],
     "uva_version": [],
 }
