@@ -390,6 +390,36 @@ def bench_validation(dev, steps=3):
             "min_gutter_texels": float(g)}
 
 
+def bench_boundary(b, reps=5):
+    """Boundary self-intersection counts (charts.boundary_intersections,
+    max_report 1000) of every chart of the batch at its current UVs, on the
+    device (uva_boundary_hits; the boundary half-edges are found once per
+    batch and kept)."""
+    import torch
+    from ultimate_uv_artist_b200 import _lib
+    db = b.db
+    seg, _, sofs = db.boundary_segments()
+    hits = db.boundary_hits(_lib.SEG_COUNT, 1000)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(db.dev)
+    out = {}
+    for name, mode in (("count", _lib.SEG_COUNT), ("any", _lib.SEG_ANY)):
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            db.boundary_hits(mode, 1000)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[f"{name}_ms"] = e0.elapsed_time(e1) / reps
+    m = np.diff(sofs)
+    pairs = int((m * (m - 1) // 2).sum())
+    h = hits.cpu().numpy()
+    out.update({"charts": int(len(m)), "segments": int(m.sum()), "pairs": pairs,
+                "pairs_per_s": pairs / (out["count_ms"] / 1e3), "charts_with_crossings": int((h > 0).sum()),
+                "hits": h})
+    return out
+
+
 def run_reference(args):
     """CPU reference arm: the oracle port of param.lscm + param.refine per
     island over all host cores, on a bounded sample of the same workload."""
@@ -557,6 +587,10 @@ def main():
         plain["speedup_vs_per_island"] = value / plain["per_island"]["value"]
         plain["speedup_vs_one_batch"] = value / plain["one_batch"]["value"]
 
+    bnd = None
+    if rank == 0 and not args.no_validate:
+        bnd = bench_boundary(b)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import cpu_baseline
@@ -576,6 +610,10 @@ def main():
                                                     (("overlapping_triangles_exact", "overlapping_triangles"),
                                                      ("flipped_triangles", "flipped"),
                                                      ("mirrored_islands", "mirrored")))}
+        if bnd is not None:   # the boundary checks' CPU time on a sample (oracle port, one thread)
+            bs, bsel, bwant = cpu_baseline.time_boundary(islands, our_uvs, args.cpu_budget_tris)
+            cpu["boundary_checks"] = {"seconds": bs, "cores": 1, "kind": "port", "charts": len(bsel),
+                                      "same_counts": bool(all(int(bnd["hits"][i]) == w for i, w in zip(bsel, bwant)))}
         err, ni, nt_ = cpu_baseline.uv_error_batch(islands, our_uvs, args.iters)
         cpu["uv_error_check"] = {"max_rel_uv_error": err, "islands": ni, "triangles": nt_,
                                  "against": "FP64 oracle of LSCM + gpu.Batch.arap with exact solves"}
@@ -607,6 +645,7 @@ def main():
             "plain_gpu": plain,
             "clocks": ck,
             "validate": val,
+            "boundary_checks": None if bnd is None else {k: v for k, v in bnd.items() if k != "hits"},
         }
         print(json.dumps(line), flush=True)
     if graphs:

@@ -442,6 +442,14 @@ typedef struct uva_seg_desc {
 
 int uva_seg_scratch_bytes(int32_t nc, int32_t nseg, int64_t* bytes);
 int uva_boundary_hits(const uva_seg_desc* d, void* stream);
+/* Directed boundary half-edges of every island of a device batch
+ * (engine/param.py:59-68 per island): seg_ofs (device, nc+1) and seg
+ * (device, capacity 3t*2: rows of U, island by island; the order inside an
+ * island is unspecified, which no check depends on). Scratch:
+ * uva_batch_boundary_scratch_bytes.                                        */
+int uva_batch_boundary_scratch_bytes(const uva_batch* b, int64_t* bytes);
+int uva_batch_boundary(const uva_batch* b, int32_t* seg_ofs, int32_t* seg, void* scratch, int64_t scratch_bytes,
+                       void* stream);
 
 /* Library info. */
 const char* uva_last_error(void);

@@ -89,6 +89,17 @@ def uv_error_batch(islands, uvs, iters, count=12):
     return O.uv_rel_error(U, Uref, off), len(pick), int(sum(len(c[1]) for c in charts))
 
 
+def time_boundary(islands, uvs, budget_tris):
+    """Seconds of the oracle's boundary_intersections (max_report 1000, one
+    thread) over a size-stratified sample of the charts at the given UVs;
+    returns (seconds, sampled chart indices, their counts)."""
+    from oracle import segments as OS
+    pick = sample_indices(islands, budget_tris)
+    t0 = time.perf_counter()
+    want = [OS.boundary_intersections(uvs[i], islands[i][1], 1000) for i in pick]
+    return time.perf_counter() - t0, [int(i) for i in pick], want
+
+
 def time_validation(V, F, UV, atlas=4096, padding=4):
     """Seconds of the oracle's validate_uvs (numpy + the C restatement of the
     reference's serial loops, one thread) on an atlas, and its report."""

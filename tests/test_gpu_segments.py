@@ -117,3 +117,23 @@ def test_any_modes_extent(cuda):
         want_all = o._chart_hit(UV, seg[:, 0], seg[:, 1], ext_check=False)
         assert segments.boundary_hits(UV, [0, 4], seg, segments.ANY)[0] == int(want_any)
         assert segments.boundary_hits(UV, [0, 4], seg, segments.ANY_ALL)[0] == int(want_all)
+
+
+def test_batch_boundary_intersections(cuda):
+    """gpu.Batch.boundary_intersections: boundary half-edges found on the
+    device from the batch topology, counts at the batch's current UVs equal
+    the oracle on (chart_uvs()[i], T_i), before and after the UVs change."""
+    from oracle import segments as o
+    from ultimate_uv_artist_b200.engine import gpu
+    ch = _random_charts(33, 24)
+    ch.append((np.array([[0, 0], [1, 0], [0, 1]], np.float64), np.array([[0, 1, 2], [0, 2, 1]], np.int64)))
+    P = [np.concatenate([U, np.zeros((len(U), 1))], 1) for U, _ in ch]
+    b = gpu.Batch([(p, T, U) for p, (U, T) in zip(P, ch)])
+    for r in (1, 1000):
+        want = [o.boundary_intersections(U, T, r) for U, T in ch]
+        assert b.boundary_intersections(max_report=r).tolist() == want
+    rng = np.random.default_rng(4)
+    b.U = np.concatenate([U for U, _ in ch]) + rng.normal(0, 0.05, (b.n, 2))
+    Us = b.chart_uvs()
+    want = [o.boundary_intersections(Us[i], ch[i][1], 1000) for i in range(len(ch))]
+    assert b.boundary_intersections().tolist() == want

@@ -98,6 +98,8 @@ _SIGS = {
     "uva_shrink": [vp, vp, vp, i32, C.c_float, C.c_float, vp],
     "uva_seg_scratch_bytes": [i32, i32, vp],
     "uva_boundary_hits": [vp, vp],
+    "uva_batch_boundary_scratch_bytes": [vp, vp],
+    "uva_batch_boundary": [vp, vp, vp, vp, C.c_int64, vp],
     "uva_last_error": [],
     "uva_version": [],
 }

@@ -362,7 +362,104 @@ __global__ void k_seg_final(uva_seg_desc d, const ChartGrid* grid, const unsigne
     d.out[c] = r;
 }
 
+// ------------------------------------------------------------------ batch boundary
+// Directed boundary half-edges of a device batch (engine/param.py:59-68 per
+// island): corner edge k of triangle f runs c[k+1] -> c[k+2] on unique edge
+// tri_edge[3f + k]; it is a boundary half-edge when no half-edge of the same
+// edge runs the other way (self-loops never are).
+__device__ __forceinline__ bool half_edge(const uva_batch& b, int f, int k, int& e, int& a, int& c, int& dir) {
+    e = b.tri_edge[3 * f + k];
+    const int4 t = reinterpret_cast<const int4*>(b.tri4)[f];
+    const int v[3] = {t.x, t.y, t.z};
+    a = v[(k + 1) % 3];
+    c = v[(k + 2) % 3];
+    dir = a < c ? 0 : 1;
+    return e >= 0 && a != c;
+}
+
+__global__ void k_bnd_count(uva_batch b, int* ecnt) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= b.t) return;
+    for (int k = 0; k < 3; ++k) {
+        int e, a, c, dir;
+        if (half_edge(b, f, k, e, a, c, dir)) atomicAdd(ecnt + 2 * e + dir, 1);
+    }
+}
+
+// pass 0: boundary half-edges per island; pass 1: write them (rows of U)
+__global__ void k_bnd_emit(uva_batch b, const int* ecnt, int* icnt, const int32_t* seg_ofs, int* cursor,
+                           int32_t* seg, int pass) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= b.t) return;
+    const int isl = b.tri4[4 * f + 3];
+    for (int k = 0; k < 3; ++k) {
+        int e, a, c, dir;
+        if (!half_edge(b, f, k, e, a, c, dir) || ecnt[2 * e + (dir ^ 1)] != 0) continue;
+        if (pass == 0) {
+            atomicAdd(icnt + isl, 1);
+        } else {
+            const int q = seg_ofs[isl] + atomicAdd(cursor + isl, 1);
+            seg[2 * q] = b.vofs[isl] + a;
+            seg[2 * q + 1] = b.vofs[isl] + c;
+        }
+    }
+}
+
+// seg_ofs = exclusive prefix of icnt (one CTA)
+__global__ void __launch_bounds__(kScan) k_bnd_scan(int nc, const int* icnt, int32_t* seg_ofs) {
+    __shared__ long long part[kScan];
+    const int per = (nc + kScan - 1) / kScan;
+    const int c0 = threadIdx.x * per, c1 = min(nc, c0 + per);
+    long long s = 0;
+    for (int c = c0; c < c1; ++c) s += icnt[c];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 1; o < kScan; o <<= 1) {
+        const long long add = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += add;
+        __syncthreads();
+    }
+    long long run = part[threadIdx.x] - s;
+    for (int c = c0; c < c1; ++c) {
+        seg_ofs[c] = static_cast<int32_t>(run);
+        run += icnt[c];
+    }
+    if (threadIdx.x == kScan - 1) seg_ofs[nc] = static_cast<int32_t>(part[kScan - 1]);
+}
+
 }  // namespace
+
+extern "C" int uva_batch_boundary_scratch_bytes(const uva_batch* b, int64_t* bytes) {
+    if (!b || !bytes || b->nc < 0 || b->E < 0) { uva_set_error("uva_batch_boundary_scratch_bytes: bad arguments"); return UVA_E_ARG; }
+    *bytes = 4 * (2 * static_cast<int64_t>(std::max(b->E, 1)) + 2 * static_cast<int64_t>(std::max(b->nc, 1)));
+    return UVA_OK;
+}
+
+extern "C" int uva_batch_boundary(const uva_batch* b, int32_t* seg_ofs, int32_t* seg, void* scratch,
+                                  int64_t scratch_bytes, void* stream) {
+    if (!b || b->nc < 0 || b->t < 0 || !seg_ofs || (b->nc > 0 && (!b->tri4 || !b->vofs || !scratch)) ||
+        (b->t > 0 && (!b->tri_edge || !seg))) {
+        uva_set_error("uva_batch_boundary: bad arguments");
+        return UVA_E_ARG;
+    }
+    if (b->nc == 0) return UVA_OK;
+    const int64_t need = 4 * (2 * static_cast<int64_t>(std::max(b->E, 1)) + 2 * static_cast<int64_t>(b->nc));
+    if (scratch_bytes < need) { uva_set_error("uva_batch_boundary: scratch too small"); return UVA_E_ARG; }
+    if (3 * static_cast<int64_t>(b->t) >= (int64_t(1) << 31)) { uva_set_error("uva_batch_boundary: too many triangles"); return UVA_E_TOOBIG; }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int* ecnt = static_cast<int*>(scratch);
+    int* icnt = ecnt + 2 * static_cast<size_t>(std::max(b->E, 1));
+    int* cursor = icnt + b->nc;
+    cudaMemsetAsync(scratch, 0, static_cast<size_t>(need), s);
+    const int blocks = std::max(1, (b->t + 255) / 256);
+    k_bnd_count<<<blocks, 256, 0, s>>>(*b, ecnt);
+    k_bnd_emit<<<blocks, 256, 0, s>>>(*b, ecnt, icnt, seg_ofs, cursor, seg, 0);
+    k_bnd_scan<<<1, kScan, 0, s>>>(b->nc, icnt, seg_ofs);
+    k_bnd_emit<<<blocks, 256, 0, s>>>(*b, ecnt, icnt, seg_ofs, cursor, seg, 1);
+    UVA_CHECK_LAUNCH("uva_batch_boundary");
+    return UVA_OK;
+}
 
 extern "C" int uva_seg_scratch_bytes(int32_t nc, int32_t nseg, int64_t* bytes) {
     if (nc < 0 || nseg < 0 || !bytes) { uva_set_error("uva_seg_scratch_bytes: bad arguments"); return UVA_E_ARG; }

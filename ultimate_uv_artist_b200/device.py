@@ -352,6 +352,45 @@ class DeviceBatch:
         check(_lib.lib().uva_shrink(C.byref(self.desc), ptr(sel), ptr(vmark), int(rings), float(factor),
                                     float(floor), self._stream()), "uva_shrink")
 
+    def boundary_segments(self):
+        """Directed boundary half-edges of every island (rows of U, device
+        int32 (nseg, 2)) and their offsets (device (nc + 1,), host copy),
+        found once on the device (uva_batch_boundary) and kept."""
+        if getattr(self, "_bnd", None) is None:
+            L = _lib.lib()
+            nb = C.c_int64()
+            check(L.uva_batch_boundary_scratch_bytes(C.byref(self.desc), C.byref(nb)), "uva_batch_boundary")
+            scratch = torch.empty(max(nb.value, 16), dtype=torch.uint8, device=self.dev)
+            sofs = torch.zeros(self.nc + 1, dtype=torch.int32, device=self.dev)
+            seg = torch.empty((max(3 * self.t, 1), 2), dtype=torch.int32, device=self.dev)
+            check(L.uva_batch_boundary(C.byref(self.desc), ptr(sofs), ptr(seg), ptr(scratch), nb.value,
+                                       self._stream()), "uva_batch_boundary")
+            sofs_h = sofs.cpu().numpy().astype(np.int64)
+            self._bnd = (seg[:int(sofs_h[-1])].clone(), sofs, sofs_h)
+        return self._bnd
+
+    def boundary_hits(self, mode=_lib.SEG_COUNT, max_report=1000, U=None):
+        """Per island (device int64): mode SEG_COUNT -> the capped boundary
+        crossing count of engine/charts.py:596-608 (-1: non-finite UVs);
+        SEG_ANY / SEG_ANY_ALL -> 1 if two boundary segments cross."""
+        seg, sofs, sofs_h = self.boundary_segments()
+        U = self.U if U is None else U.to(self.dev, torch.float64).contiguous()
+        L = _lib.lib()
+        nseg = int(sofs_h[-1])
+        if not hasattr(self, "_bnd_scratch"):
+            nb = C.c_int64()
+            check(L.uva_seg_scratch_bytes(self.nc, nseg, C.byref(nb)), "uva_seg_scratch_bytes")
+            self._bnd_scratch = torch.empty(max(nb.value, 16), dtype=torch.uint8, device=self.dev)
+        out = torch.empty(max(self.nc, 1), dtype=torch.int64, device=self.dev)
+        d = _lib.SegDesc()
+        d.nc, d.nseg, d.n, d.mode = self.nc, nseg, self.n, int(mode)
+        d.max_report = int(min(max(int(max_report), -(2 ** 31)), 2 ** 31 - 1))
+        d.U, d.vofs, d.seg_ofs = U.data_ptr(), self.vofs.data_ptr(), sofs.data_ptr()
+        d.seg = seg.data_ptr() if nseg else None
+        d.out, d.scratch, d.scratch_bytes = out.data_ptr(), self._bnd_scratch.data_ptr(), self._bnd_scratch.numel()
+        check(L.uva_boundary_hits(C.byref(d), self._stream()), "uva_boundary_hits")
+        return out[:self.nc]
+
     def island_status(self):
         """Per-island solver status (host numpy structured array)."""
         raw = self.status[:self.nc].cpu().numpy()

@@ -244,6 +244,13 @@ class Batch:
             return
         self.db.shrink(tri_idx, factor, floor, rings)
 
+    def boundary_intersections(self, max_report=1000):
+        """charts.boundary_intersections (engine/charts.py:596-608) of every
+        chart of the batch at its current UVs, in one launch: numpy int64 per
+        chart (-1 where the reference would raise for non-finite UVs). An
+        addition: the reference calls it chart by chart on the host."""
+        return self.db.boundary_hits(_lib.SEG_COUNT, max_report).cpu().numpy()
+
     def chart_uvs(self):
         U = self.db.uvs()
         return [U[a:b] for a, b in zip(self.offsets[:-1], self.offsets[1:])]
