@@ -187,6 +187,9 @@ typedef struct uva_solve_params {
     int32_t threads;          /* threads per island team (0: autotuned)         */
     int32_t rev_ctas;         /* CTAs that start with the small-island classes
                                  (0: automatic, < 0: none)                      */
+    int32_t fold_step;        /* 1: an island with a folded triangle (negative
+                                 UV area, frame ok) at the start of an iteration
+                                 takes the full step (engine/hier.py:549-552)   */
 } uva_solve_params;
 
 /* Frames, weights, matrix values, Jacobi diagonal, pins and pin weights.

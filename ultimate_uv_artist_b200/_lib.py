@@ -61,7 +61,7 @@ class BatchDesc(C.Structure):
 class SolveParams(C.Structure):
     _fields_ = [("iters", i32), ("line_search", i32), ("tol", C.c_double), ("energy_tol", C.c_double),
                 ("inner_eta", C.c_double), ("max_inner", i32), ("max_refine", i32), ("threads", i32),
-                ("rev_ctas", i32)]
+                ("rev_ctas", i32), ("fold_step", i32)]
 
 
 class SegDesc(C.Structure):

@@ -1090,6 +1090,15 @@ __device__ __forceinline__ double step_bound(const uva_batch& b, const Isl& I, i
     return t;
 }
 
+// 1 if triangle f is folded at U: negative signed UV area with a valid frame
+// (engine/hier.py:549)
+__device__ __forceinline__ int folded_tri(const uva_batch& b, const Isl& I, int f, const double2* U) {
+    if (reinterpret_cast<const double4*>(b.wtri)[f].w == 0.0) return 0;
+    const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
+    const double2 a = U[I.v0 + tv.x], c1 = U[I.v0 + tv.y], c2 = U[I.v0 + tv.z];
+    return ((c1.x - a.x) * (c2.y - a.y) - (c2.x - a.x) * (c1.y - a.y)) < 0.0 ? 1 : 0;
+}
+
 // ---- ARAP outer iterations of one island (gpu.py:230-249 / param.py:379-414)
 template <int NTT, int R>
 __device__ __forceinline__ void solve_arap(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, const Isl& I) {
@@ -1182,9 +1191,14 @@ __device__ __forceinline__ void solve_arap(const uva_batch& b, const uva_solve_p
         double step = 1.0;
         if (use_ls) {
             double tmin = 1e30;
-            for (int f = I.f0 + tid; f < I.f0 + I.nt; f += NTT) tmin = fmin(tmin, step_bound(b, I, f, U, x64, batch));
+            int folded = 0;
+            for (int f = I.f0 + tid; f < I.f0 + I.nt; f += NTT) {
+                tmin = fmin(tmin, step_bound(b, I, f, U, x64, batch));
+                if (prm.fold_step) folded |= folded_tri(b, I, f, U);
+            }
             tmin = team_min(tm, tmin);
-            step = fmin(0.9 * tmin, 1.0);
+            if (prm.fold_step) folded = team_or(tm, folded);   // folded islands: plain ARAP step
+            step = folded ? 1.0 : fmin(0.9 * tmin, 1.0);
         }
         if (tid == 0) gst->step = step;
         tm.sync();   // all line-search reads of U done

@@ -285,6 +285,7 @@ class DeviceBatch:
         P.inner_eta = float(base["inner_eta"]); P.max_inner = int(base["max_inner"])
         P.max_refine = int(base["max_refine"]); P.threads = int(threads)
         P.rev_ctas = int(over.get("rev_ctas") or 0)
+        P.fold_step = 1 if over.get("fold_step") else 0
         return P
 
     # ------------------------------------------------------------ solvers

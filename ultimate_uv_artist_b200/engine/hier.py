@@ -167,3 +167,238 @@ def chart_topology(F, FF, faces, loc, chart, CV, nchart, nv):
                 if find(v) == v:
                     loops[vchart[v]] += 1
     return chi, loops, ba, bb, bc
+
+
+# ------------------------------------------------------------------ GPU relaxation of a face subset
+class Solver:
+    """Drop-in for engine/hier.py:357-593: ``relax`` runs ARAP on any subset
+    of a mesh's charts, ``lscm`` maps every chart at once, ``bad_fraction``
+    reports the last relax's distortion.
+
+    ``relax`` lays the charts out as one device batch (islands = charts, in
+    chart order, each chart's UV vertices in id order) and runs the batch
+    kernels: orientation (uva_orient_positive), flip repair
+    (uva_repair_flips) before, halfway and after, and ARAP iterations
+    (uva_arap) with the reference's step rule, the flip-safe step
+    min(1, 0.9 t_max) except for charts that are folded at the start of the
+    iteration, which take the full step (``fold_step``). As in the drop-in
+    ``gpu.Batch``, each global step is solved per chart to a 2e-7 relative
+    residual checked in FP64, where the reference runs ``cg_iters`` (20)
+    Jacobi-CG iterations on the whole subset in FP32; ``cg_iters`` is kept
+    for signature compatibility. ``lscm`` assembles the reference's
+    soft-pinned LSCM system on the host and solves it with the FP64
+    Jacobi-PCG kernel (uva_csr_pcg) to a 1e-10 relative residual, where the
+    reference stops its FP32 CG at 1e-6 or 600 iterations.
+    """
+
+    def __init__(self, topo, dev=None):
+        from ..device import require_cuda
+        self.dev = require_cuda(dev)
+        self.V = np.asarray(topo.V, np.float64)
+        self.F = np.asarray(topo.F, np.int64)
+        self._q = None
+
+    # ---------------------------------------------------------------- layout
+    def _layout(self, faces, CV, nv, chart, nchart):
+        """Charts as batch islands: (order, P, T_local, vofs, tofs, forder)
+        with order = the UV vertices in batch order and forder = the faces in
+        batch order."""
+        faces = np.asarray(faces, np.int64)
+        CV = np.asarray(CV, np.int64).reshape(-1, 3)
+        chart = np.asarray(chart, np.int64)
+        n = len(faces)
+        if n and (CV.min() < 0 or CV.max() >= nv or chart.min() < 0 or chart.max() >= nchart):
+            raise ValueError("hier.Solver: CV or chart out of range")
+        vchart = -np.ones(nv, np.int64)
+        if n:
+            rev = CV.reshape(-1)[::-1]
+            uniq, first = np.unique(rev, return_index=True)
+            vchart[uniq] = np.repeat(chart, 3)[::-1][first]
+        if n and (vchart[CV] != chart[:, None]).any():
+            raise ValueError("hier.Solver: a UV vertex is shared by faces of different charts")
+        used = np.nonzero(vchart >= 0)[0]
+        order = used[np.argsort(vchart[used], kind="stable")]           # by chart, then id
+        newid = -np.ones(nv, np.int64)
+        newid[order] = np.arange(len(order))
+        vofs = np.zeros(nchart + 1, np.int64)
+        np.cumsum(np.bincount(vchart[used], minlength=nchart), out=vofs[1:])
+        forder = np.argsort(chart, kind="stable")
+        tofs = np.zeros(nchart + 1, np.int64)
+        np.cumsum(np.bincount(chart, minlength=nchart), out=tofs[1:])
+        Tb = newid[CV[forder]]
+        T_local = Tb - vofs[chart[forder]][:, None]
+        P = np.empty((len(order), 3))
+        P[newid[CV.reshape(-1)]] = self.V[self.F[faces][:, [0, 1, 2]].reshape(-1)]
+        return order, P, T_local, vofs, tofs, forder
+
+    # ---------------------------------------------------------------- relax
+    def relax(self, faces, CV, nv, chart, nchart, U0, iters=6, cg_iters=20, repair_rounds=24):
+        """faces (n,) global ids, CV (n,3) local vertex ids, chart (n,) local
+        chart ids, U0 (nv,2) initial UVs -> (U (nv,2) float64, flips per
+        chart, UV / 3D area scale per chart) (engine/hier.py:389-509)."""
+        import torch
+        from .. import _lib
+        from ..device import DeviceBatch
+        nv, nchart = int(nv), int(nchart)
+        U0 = np.asarray(U0, np.float64).reshape(-1, 2)
+        order, P, T_local, vofs, tofs, forder = self._layout(faces, CV, nv, chart, nchart)
+        out = U0.copy()
+        flips = np.zeros(nchart)
+        scale = np.zeros(nchart)
+        if len(order) == 0 or len(T_local) == 0:
+            self._q = None
+            return out, flips, scale
+        db = DeviceBatch(P, T_local, vofs, tofs, U=U0[order], semantics=_lib.SEM_BATCH, device=self.dev)
+        db.orient_positive()
+        db.repair_flips(repair_rounds)
+        first = min(int(iters), int(iters) // 2 + 1)
+        if first > 0:
+            db.arap(iters=first, line_search=True, fold_step=True)
+            db.repair_flips(repair_rounds)           # after iteration iters // 2
+        if int(iters) - first > 0:
+            db.arap(iters=int(iters) - first, line_search=True, fold_step=True)
+        db.repair_flips(repair_rounds)
+        # per-chart quality (engine/hier.py:493-508)
+        sa = db.signed_area().cpu().numpy()
+        J = db.jacobians().cpu().numpy()
+        area = db.frame[:db.t, 3].cpu().numpy()
+        ok = (db.wtri[:db.t, 3] != 0).cpu().numpy()
+        ct = np.repeat(np.arange(nchart), np.diff(tofs))
+        j00, j01, j10, j11 = J[:, 0], J[:, 1], J[:, 2], J[:, 3]
+        E = (j00 + j11) / 2; Fq = (j00 - j11) / 2; G = (j10 + j01) / 2; H = (j10 - j01) / 2
+        Q = np.sqrt(E * E + H * H); R = np.sqrt(Fq * Fq + G * G)
+        s1 = Q + R; s2 = np.abs(Q - R)
+        ar3 = area * ok
+        uva = np.bincount(ct, np.abs(sa) * ok, nchart)
+        a3 = np.bincount(ct, ar3, nchart)
+        scale = uva / np.maximum(a3, 1e-30)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            aniso = s1 / np.maximum(s2, 1e-12)
+            arat = (s1 * s2) / np.maximum(scale[ct], 1e-30)
+        flips = np.bincount(ct, ((sa < 0) & ok).astype(np.float64), nchart)
+        self._q = (aniso, arat, ar3, ct, nchart, a3)
+        out[order] = db.uvs()
+        torch.cuda.current_stream(self.dev).synchronize()
+        return out, flips, scale
+
+    def bad_fraction(self, max_aniso, max_area):
+        """Area fractions of each chart above the anisotropy / area-ratio
+        limits in the last relax (engine/hier.py:585-591)."""
+        if self._q is None:
+            return np.zeros(0), np.zeros(0)
+        aniso, arat, ar3, ct, nchart, a3 = self._q
+        badA = np.bincount(ct, ar3 * (aniso > max_aniso), nchart)
+        badR = np.bincount(ct, ar3 * ((arat > max_area) | (arat < 1.0 / max_area)), nchart)
+        return badA / np.maximum(a3, 1e-30), badR / np.maximum(a3, 1e-30)
+
+    # ---------------------------------------------------------------- lscm
+    def lscm(self, faces, CV, nv, chart, nchart, U0, ba, bb, iters=600):
+        """Free-boundary conformal map of every chart at once: the LSCM energy
+        with two soft pins per chart, the boundary vertices of smallest and
+        largest initial u (engine/hier.py:511-583). ``iters`` is accepted for
+        signature compatibility (see the class docstring)."""
+        import ctypes as C
+        import scipy.sparse as sp
+        import torch
+        from .. import _lib
+        nv, nchart = int(nv), int(nchart)
+        faces = np.asarray(faces, np.int64)
+        CV = np.asarray(CV, np.int64).reshape(-1, 3)
+        chart = np.asarray(chart, np.int64)
+        U0 = np.asarray(U0, np.float64).reshape(-1, 2)
+        ba = np.asarray(ba, np.int64); bb = np.asarray(bb, np.int64)
+        if nv == 0:
+            return U0.copy()
+        # cot weights of the faces, like the batch setup (engine/gpu.py:88-116)
+        w = _face_cots(self.V, self.F[faces])
+        I = np.concatenate([CV[:, 1], CV[:, 2], CV[:, 0]])
+        J = np.concatenate([CV[:, 2], CV[:, 0], CV[:, 1]])
+        Wl = np.concatenate([w[:, 0], w[:, 1], w[:, 2]])
+        hb = np.full(len(ba), 0.5)
+        rows = [I, J, I, J, I + nv, J + nv, I + nv, J + nv, ba, bb, ba + nv, bb + nv]
+        cols = [J, I, I, J, J + nv, I + nv, I + nv, J + nv, bb + nv, ba + nv, bb, ba]
+        vals = [-Wl, -Wl, Wl, Wl, -Wl, -Wl, Wl, Wl, -hb, hb, hb, -hb]
+        # two pins per chart: boundary vertices extreme along the initial u axis
+        cv = -np.ones(nv, np.int64)
+        if len(CV):
+            rev = CV.reshape(-1)[::-1]
+            uniq, first = np.unique(rev, return_index=True)
+            cv[uniq] = np.repeat(chart, 3)[::-1][first]
+        bv = np.unique(ba)
+        pins = []
+        if len(bv):
+            key = U0[bv, 0].astype(np.float32)      # the reference compares float32 keys
+            cb = cv[bv]
+            o_mn = np.lexsort((bv, key, cb))          # per chart: smallest u first
+            o_mx = np.lexsort((bv, -key, cb))         # per chart: largest u first
+            first_mn = o_mn[np.r_[True, cb[o_mn][1:] != cb[o_mn][:-1]]]
+            first_mx = o_mx[np.r_[True, cb[o_mx][1:] != cb[o_mx][:-1]]]
+            pins = np.concatenate([bv[first_mn], bv[first_mx]])
+        pins = np.asarray(pins, np.int64)
+        wpin = max(np.abs(Wl).max() if len(Wl) else 0.0, 1e-12) * 10
+        rows += [pins, pins + nv]; cols += [pins, pins + nv]; vals += [np.full(2 * len(pins), wpin)]
+        H = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                          shape=(2 * nv, 2 * nv)).tocsr()
+        H.sum_duplicates()
+        H.sort_indices()
+        b = np.zeros(2 * nv)
+        np.add.at(b, pins, wpin * U0[pins, 0])
+        np.add.at(b, pins + nv, wpin * U0[pins, 1])
+        x0 = np.concatenate([U0[:, 0], U0[:, 1]])
+        # unknowns of UV vertices that no face names have no equation: they keep U0
+        used = np.zeros(2 * nv, bool)
+        used[np.concatenate([CV.reshape(-1), CV.reshape(-1) + nv])] = True
+        idx = np.nonzero(used)[0]
+        if len(idx) == 0:
+            return U0.copy()
+        H = H[idx][:, idx].tocsr()
+        H.sort_indices()
+        b = b[idx]
+        x_all = x0.copy()
+        x0 = x0[idx]
+        d = self.dev
+        rp = torch.from_numpy(H.indptr.astype(np.int32)).to(d)
+        ci = torch.from_numpy(H.indices.astype(np.int32)).to(d)
+        va = torch.from_numpy(H.data.astype(np.float64)).to(d)
+        bd = torch.from_numpy(b).to(d)
+        xd = torch.from_numpy(x0).to(d)
+        N = len(idx)
+        scratch = torch.empty(3 * N, dtype=torch.float64, device=d)
+        its = torch.zeros(1, dtype=torch.int32, device=d)
+        L = _lib.lib()
+        L.uva_csr_pcg.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_int32, C.c_double, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.uva_csr_pcg.restype = C.c_int32
+        st = torch.cuda.current_stream(d)
+        _lib.check(L.uva_csr_pcg(N, rp.data_ptr(), ci.data_ptr(), va.data_ptr(), bd.data_ptr(), xd.data_ptr(), 1,
+                                 1e-10, max(20000, 40 * int(np.sqrt(N))), scratch.data_ptr(), its.data_ptr(),
+                                 C.c_void_p(st.cuda_stream)), "uva_csr_pcg")
+        x_all[idx] = xd.cpu().numpy()
+        U = np.stack([x_all[:nv], x_all[nv:]], 1)
+        return np.where(np.isfinite(U), U, U0)
+
+
+def _face_cots(V, Ff):
+    """Half cotangent weights (t, 3) of edge k (opposite corner k), 0 for
+    triangles too thin for a frame (engine/hier.py:362-382)."""
+    p0, p1, p2 = V[Ff[:, 0]], V[Ff[:, 1]], V[Ff[:, 2]]
+    e1 = p1 - p0; e2 = p2 - p0
+    l1 = np.linalg.norm(e1, axis=1)
+    nrm = np.cross(e1, e2)
+    dbl = np.linalg.norm(nrm, axis=1)
+    ok = (dbl > 1e-14 * np.maximum(l1 * l1, 1e-300)) & np.isfinite(dbl) & (l1 > 0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ex = e1 / np.maximum(l1, 1e-30)[:, None]
+        ey = np.cross(nrm / np.maximum(dbl, 1e-30)[:, None], ex)
+    X = np.zeros((len(Ff), 3, 2))
+    X[:, 1, 0] = l1; X[:, 2, 0] = (e2 * ex).sum(1); X[:, 2, 1] = (e2 * ey).sum(1)
+    X[~ok] = 0
+    cots = []
+    for k in range(3):
+        i, j, o = (k + 1) % 3, (k + 2) % 3, k
+        a = X[:, i] - X[:, o]; b = X[:, j] - X[:, o]
+        cr = np.maximum(np.abs(a[:, 0] * b[:, 1] - a[:, 1] * b[:, 0]), 1e-30)
+        cots.append(np.clip((a * b).sum(1) / cr, -1e4, 1e4))
+    w = 0.5 * np.stack(cots, 1)
+    w[~ok] = 0
+    return w
