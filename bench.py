@@ -553,11 +553,7 @@ def main():
         e2e_s = (time.perf_counter() - w0) / args.e2e_steps
         e2e_val = units / e2e_s
         dbb = bb.db
-        h2d = int(sum(getattr(dbb.plan, k).nbytes for k in ("tri4", "tri_edge", "sofs", "slice_ptr", "slot_col",
-                                                              "slot_edge", "slot_c", "vt_ptr", "vt", "vflags",
-                                                              "bofs", "bverts", "order", "vofs", "tofs",
-                                                              "row_vert", "vert_row", "agg_rows", "cofs"))
-                  + dbb.P.numel() * 8 + dbb.U.numel() * 8)
+        h2d = int(dbb.h2d_bytes)   # every host -> device copy of the batch constructor
         d2h = int(sum(u.nbytes for u in Us))
         del bb
         if ws > 1:

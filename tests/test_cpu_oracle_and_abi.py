@@ -210,3 +210,4 @@ def test_concat_charts_matches_numpy():
     assert np.array_equal(np.diff(vofs), [len(c[0]) for c in charts])
     with pytest.raises(ValueError):
         concat_charts([(np.zeros((4, 3)), np.zeros((1, 3), np.int64), np.zeros((3, 2)))])
+    assert concat_charts([c[:2] + (None,) for c in charts])[2] is None   # no UVs: nothing to upload

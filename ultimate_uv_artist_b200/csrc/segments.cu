@@ -37,6 +37,7 @@ constexpr int kTile = 128;          // segments per tile
 constexpr int kPrep = 256;          // threads of k_seg_prep
 constexpr int kPair = 256;          // threads of k_seg_pairs
 constexpr int kScan = 1024;         // threads of k_seg_scan
+constexpr int kRankMax = 1024;      // charts up to this many segments: one-pass rank select
 
 enum : int32_t { kFlagNone = 0, kFlagNonFinite = 1, kFlagRange = 2 };
 
@@ -137,6 +138,8 @@ __global__ void __launch_bounds__(kPrep) k_seg_prep(uva_seg_desc d, ChartGrid* g
     __shared__ int redi[kPrep / 32];
     __shared__ int hist[256];
     __shared__ unsigned long long sh[2];
+    __shared__ double slen[kRankMax];
+    __shared__ double ssel[2];
     __shared__ ChartGrid g;
     const double2* U = reinterpret_cast<const double2*>(d.U);
     for (int c = blockIdx.x; c < d.nc; c += gridDim.x) {
@@ -180,14 +183,30 @@ __global__ void __launch_bounds__(kPrep) k_seg_prep(uva_seg_desc d, ChartGrid* g
         }
         if (d.mode == UVA_SEG_COUNT && !bad && m >= 3 && !nonfin) {
             // L = |B - A| (np.linalg.norm(B - A, axis=1)), then its median
+            const bool small = m <= kRankMax;
             for (int s = threadIdx.x; s < m; s += blockDim.x) {
                 const double2 a = U[d.seg[2 * (s0 + s)]], b = U[d.seg[2 * (s0 + s) + 1]];
                 const double dx = b.x - a.x, dy = b.y - a.y;
-                len[s0 + s] = sqrt(dx * dx + dy * dy);
+                const double l = sqrt(dx * dx + dy * dy);
+                if (small) slen[s] = l; else len[s0 + s] = l;
             }
             __syncthreads();
             double med;
-            if (m & 1) {
+            if (small) {   // stable rank of every length; the middle one(s) publish their value
+                const int k1 = (m & 1) ? m / 2 : m / 2 - 1, k2 = m / 2;
+                for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                    const double v = slen[i];
+                    int r = 0;
+                    for (int j = 0; j < m; ++j) {
+                        const double w = slen[j];
+                        r += (w < v || (w == v && j < i)) ? 1 : 0;
+                    }
+                    if (r == k1) ssel[0] = v;
+                    if (r == k2) ssel[1] = v;
+                }
+                __syncthreads();
+                med = (m & 1) ? ssel[1] : (ssel[0] + ssel[1]) / 2.0;
+            } else if (m & 1) {
                 med = select_kth(len + s0, m, m / 2, hist, sh);
             } else {
                 const double x0 = select_kth(len + s0, m, m / 2 - 1, hist, sh);

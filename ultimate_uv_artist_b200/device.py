@@ -139,7 +139,8 @@ def _chart_array(a, width, codes, fallback):
 def concat_charts(charts, with_uv=True):
     """(P, T, U) per chart -> concatenated FP64 P, local int64 T, FP64 U, offsets
     (uva_concat_charts copies the charts in parallel; P and U in page-locked
-    memory for the uploads)."""
+    memory for the uploads). U is None when no chart brings UVs (nothing to
+    upload: the device UVs start at zero)."""
     nc = len(charts)
     Ps, Ts, Us = [], [], []
     pdt = np.empty(max(nc, 1), np.int8)
@@ -162,13 +163,15 @@ def concat_charts(charts, with_uv=True):
         Us.append(u)
     P = host_empty((int(vofs[-1]), 3), np.float64)
     T = np.empty((int(tofs[-1]), 3), np.int64)
-    U = host_empty((int(vofs[-1]), 2), np.float64)
+    any_uv = bool((udt[:nc] >= 0).any()) if nc else False
+    U = host_empty((int(vofs[-1]), 2), np.float64) if any_uv else None
     if nc:
         pp = np.array([x.ctypes.data for x in Ps], np.uintp)
         tp = np.array([x.ctypes.data for x in Ts], np.uintp)
         up_ = np.array([0 if x is None else x.ctypes.data for x in Us], np.uintp)
         check(_lib.lib().uva_concat_charts(nc, ptr(pp), ptr(pdt), ptr(tp), ptr(tdt), ptr(up_), ptr(udt), ptr(vofs),
-                                           ptr(tofs), ptr(P), ptr(T), ptr(U), 0), "uva_concat_charts")
+                                           ptr(tofs), ptr(P), ptr(T), ptr(U) if U is not None else None, 0),
+              "uva_concat_charts")
     return P, T, U, vofs, tofs
 
 
@@ -190,10 +193,13 @@ class DeviceBatch:
         self.nc, self.n, self.t = plan.nc, plan.n, plan.t
         d = self.dev
 
+        self.h2d_bytes = 0   # bytes copied host -> device by this constructor
+
         def up(a, dtype=None):
             t = torch.from_numpy(np.ascontiguousarray(a))
             if t.numel() == 0:
                 t = torch.zeros(1, dtype=t.dtype)
+            self.h2d_bytes += t.numel() * t.element_size()
             # page-locked sources (the plan's arrays) copy asynchronously on
             # the current stream; the plan keeps them alive
             nb = t.is_pinned()
