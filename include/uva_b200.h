@@ -330,6 +330,16 @@ int uva_gutter_scratch_bytes(int32_t res, int64_t m, int64_t* bytes);
  * FP64 as given (validate_uvs passes float32-rounded values).             */
 int uva_gutter(const double* UV, const int32_t* F, const int32_t* labels, int32_t m, int32_t res, int32_t radius,
                int32_t* img, void* scratch, int64_t scratch_bytes, double* out, void* stream);
+/* Texel-centre overlaps of one chart (engine/overlapfix.py:135-224 and
+ * 263-275): uv (n*2 FP64) already normalised like the reference,
+ * (U - lo) / ext * 0.999; F (m*3) rows of uv; the coverage rule of
+ * uva_raster_counts. flags (device, m bytes, may be null): 1 if the triangle
+ * shares a covered texel centre with another triangle (_raster_all). pair
+ * (device, 2 int32, may be null): the first pair the reference's serial
+ * raster meets (_raster_pair): (earlier triangle, later triangle), or -1 -1.
+ * Scratch: uva_gutter_scratch_bytes(res, m).                               */
+int uva_overlap_raster(const double* uv, const int32_t* F, int32_t m, int32_t res, uint8_t* flags, int32_t* pair,
+                       void* scratch, int64_t scratch_bytes, void* stream);
 /* Coverage counts per texel centre with the top-left rule, saturating at 255
  * (uv: FP64 as given); stats (device, 2 int64): covered, covered twice.    */
 int uva_raster_counts(const double* uv, const int32_t* F, int32_t m, int32_t res, uint8_t* counts, int64_t* stats,
@@ -415,7 +425,10 @@ int uva_sd_refine(uva_batch* b, int32_t steps, int32_t halvings, double cap, dou
  * (_hit) as called by chart_checks (:270-353): 1 if any two segments
  * cross, also when the endpoints' extent is not below 1e300.
  * UVA_SEG_ANY_ALL is the same test as called by charts_collide (:183-225),
- * which has no extent check.
+ * which has no extent check. UVA_SEG_FIRST replaces engine/overlapfix.py:
+ * 44-84 (_first_hit, as called by collision :283-296): the first crossing
+ * pair in the reference's scan (cells in row-major order, then segment
+ * order), with the count's grid at extent / 1024.
  * A crossing: the endpoints share no coordinates exactly and each segment's
  * endpoints lie strictly on both sides of the other, beyond 1e-9 times its
  * squared length (FP64, no fused multiply-add).
@@ -423,12 +436,13 @@ int uva_sd_refine(uva_batch* b, int32_t steps, int32_t halvings, double cap, dou
 #define UVA_SEG_COUNT 0
 #define UVA_SEG_ANY   1
 #define UVA_SEG_ANY_ALL 2
+#define UVA_SEG_FIRST   3
 
 typedef struct uva_seg_desc {
     int32_t nc;             /* charts                                         */
     int32_t nseg;           /* boundary segments of all charts                */
     int32_t n;              /* rows of U                                      */
-    int32_t mode;           /* UVA_SEG_COUNT, UVA_SEG_ANY or UVA_SEG_ANY_ALL  */
+    int32_t mode;           /* UVA_SEG_COUNT, _ANY, _ANY_ALL or _FIRST        */
     int32_t max_report;     /* UVA_SEG_COUNT: cap of the count                */
     int32_t reserved;
     const double* U;        /* n*2 FP64 UVs                                   */

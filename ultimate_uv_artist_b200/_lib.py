@@ -71,7 +71,7 @@ class SegDesc(C.Structure):
                 ("scratch_bytes", C.c_int64)]
 
 
-SEG_COUNT, SEG_ANY, SEG_ANY_ALL = 0, 1, 2
+SEG_COUNT, SEG_ANY, SEG_ANY_ALL, SEG_FIRST = 0, 1, 2, 3
 
 _SIGS = {
     "uva_plan_create": [vp, vp, vp, i32, i32, vp],
@@ -97,6 +97,8 @@ _SIGS = {
     "uva_jacobians": [vp, vp, vp, vp],
     "uva_shrink": [vp, vp, vp, i32, C.c_float, C.c_float, vp],
     "uva_seg_scratch_bytes": [i32, i32, vp],
+    "uva_overlap_raster": [vp, vp, i32, i32, vp, vp, vp, C.c_int64, vp],
+    "uva_gutter_scratch_bytes": [i32, C.c_int64, vp],
     "uva_boundary_hits": [vp, vp],
     "uva_batch_boundary_scratch_bytes": [vp, vp],
     "uva_batch_boundary": [vp, vp, vp, vp, C.c_int64, vp],

@@ -27,6 +27,7 @@ using namespace uva;
 namespace {
 
 constexpr int kSmallTexels = 256;   // triangles with larger boxes go to a block each
+constexpr int32_t kNoTri = 0x7f7f7f7f;   // "no triangle" (a byte-wise memset value above every index)
 
 struct RTri {
     double x0, y0, x1, y1, x2, y2;
@@ -272,6 +273,133 @@ __global__ void k_cover_final(const uint32_t* cnt, size_t ntex, uint8_t* out, un
     if ((threadIdx.x & 31) == 0 && mask) atomicAdd(stats + 1, static_cast<unsigned long long>(__popc(mask)));
 }
 
+// ---- texel-centre overlaps of one chart (engine/overlapfix.py:135-224):
+// the coverage rule above; every covered texel centre of triangle t in
+// row-major order of its box gets visit(q, texel), q the box-local index. A
+// box above kSmallTexels texels is queued on `big` instead (unless big_only,
+// where the block's threads split the box).
+template <typename Visit>
+__device__ void texel_walk(const double* uv, const int32_t* F, int t, int res, bool big_only, int32_t* big,
+                           int32_t* nbig, Visit visit) {
+    const int a = F[3 * t], b = F[3 * t + 1], c = F[3 * t + 2];
+    const double R = static_cast<double>(res);
+    double x0 = uv[2 * a] * R, y0 = uv[2 * a + 1] * R, x1 = uv[2 * b] * R, y1 = uv[2 * b + 1] * R;
+    double x2 = uv[2 * c] * R, y2 = uv[2 * c + 1] * R;
+    const double area = (x1 - x0) * (y2 - y0) - (x2 - x0) * (y1 - y0);
+    if (area == 0.0) return;
+    if (area < 0) { double tx = x1, ty = y1; x1 = x2; y1 = y2; x2 = tx; y2 = ty; }
+    const double fx0 = floor(fmin(x0, fmin(x1, x2)) - 0.5), fx1 = ceil(fmax(x0, fmax(x1, x2)) - 0.5);
+    const double fy0 = floor(fmin(y0, fmin(y1, y2)) - 0.5), fy1 = ceil(fmax(y0, fmax(y1, y2)) - 0.5);
+    if (!(isfinite(fx0) && isfinite(fx1) && isfinite(fy0) && isfinite(fy1))) return;
+    const int minx = fx0 < 0.0 ? 0 : (fx0 > R ? res : static_cast<int>(fx0));
+    const int miny = fy0 < 0.0 ? 0 : (fy0 > R ? res : static_cast<int>(fy0));
+    const int maxx = fx1 > R - 1.0 ? res - 1 : (fx1 < -1.0 ? -1 : static_cast<int>(fx1));
+    const int maxy = fy1 > R - 1.0 ? res - 1 : (fy1 < -1.0 ? -1 : static_cast<int>(fy1));
+    if (minx > maxx || miny > maxy) return;
+    const long long n = static_cast<long long>(maxx - minx + 1) * (maxy - miny + 1);
+    if (!big_only && n > kSmallTexels) { if (big) big[atomicAdd(nbig, 1)] = t; return; }
+    const double ex[3] = {x1 - x0, x2 - x1, x0 - x2}, ey[3] = {y1 - y0, y2 - y1, y0 - y2};
+    const double ox[3] = {x0, x1, x2}, oy[3] = {y0, y1, y2};
+    const int w = maxx - minx + 1;
+    const long long start = big_only ? threadIdx.x : 0, step = big_only ? blockDim.x : 1;
+    for (long long q = start; q < n; q += step) {
+        const int px = minx + static_cast<int>(q % w), py = miny + static_cast<int>(q / w);
+        const double cx = px + 0.5, cy = py + 0.5;
+        bool inside = true;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const double e = ex[k] * (cy - oy[k]) - ey[k] * (cx - ox[k]);
+            if (e < 0.0) { inside = false; break; }
+            if (e == 0.0) {
+                const bool top_left = (ey[k] == 0.0 && ex[k] < 0.0) || ey[k] > 0.0;
+                if (!top_left) { inside = false; break; }
+            }
+        }
+        if (inside) visit(q, static_cast<size_t>(py) * res + px);
+    }
+}
+
+// pass 1: coverage counts and the first (smallest) triangle on every texel
+__global__ void k_ov_cover(const double* uv, const int32_t* F, int m, int res, uint32_t* cnt, int32_t* owner,
+                           int32_t* big, int32_t* nbig) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    texel_walk(uv, F, t, res, false, big, nbig, [&](long long, size_t p) { atomicAdd(cnt + p, 1u); atomicMin(owner + p, t); });
+}
+__global__ void k_ov_cover_big(const double* uv, const int32_t* F, int res, uint32_t* cnt, int32_t* owner,
+                               const int32_t* big, const int32_t* nbig) {
+    for (int k = blockIdx.x; k < *nbig; k += gridDim.x) {
+        const int t = big[k];
+        texel_walk(uv, F, t, res, true, nullptr, nullptr,
+                   [&](long long, size_t p) { atomicAdd(cnt + p, 1u); atomicMin(owner + p, t); });
+    }
+}
+
+// pass 2: flags (a covered texel with two coverers) and the first triangle
+// that meets a texel an earlier triangle owns
+__global__ void k_ov_check(const double* uv, const int32_t* F, int m, int res, const uint32_t* cnt,
+                           const int32_t* owner, uint8_t* flags, int32_t* first_t) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    bool shared = false, earlier = false;
+    texel_walk(uv, F, t, res, false, nullptr, nullptr, [&](long long, size_t p) {
+        shared |= cnt[p] > 1u;
+        earlier |= owner[p] < t;
+    });
+    if (flags) flags[t] = shared ? 1 : 0;
+    if (earlier) atomicMin(first_t, t);
+}
+__global__ void k_ov_check_big(const double* uv, const int32_t* F, int res, const uint32_t* cnt, const int32_t* owner,
+                               const int32_t* big, const int32_t* nbig, uint8_t* flags, int32_t* first_t) {
+    __shared__ int s_shared, s_earlier;
+    for (int k = blockIdx.x; k < *nbig; k += gridDim.x) {
+        const int t = big[k];
+        if (threadIdx.x == 0) { s_shared = 0; s_earlier = 0; }
+        __syncthreads();
+        bool shared = false, earlier = false;
+        texel_walk(uv, F, t, res, true, nullptr, nullptr, [&](long long, size_t p) {
+            shared |= cnt[p] > 1u;
+            earlier |= owner[p] < t;
+        });
+        if (shared) s_shared = 1;
+        if (earlier) s_earlier = 1;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (flags) flags[t] = s_shared ? 1 : 0;
+            if (s_earlier) atomicMin(first_t, t);
+        }
+        __syncthreads();
+    }
+}
+
+// pass 3 (one block): the first texel, in the scan order of triangle
+// first_t, that an earlier triangle owns -> (its owner, first_t). The key
+// packs the box-local index (high word) over the owner (low word).
+__global__ void k_ov_pair(const double* uv, const int32_t* F, int res, const int32_t* owner, const int32_t* first_t,
+                          int32_t* pair) {
+    __shared__ unsigned long long s_key;
+    const int t = *first_t;
+    if (threadIdx.x == 0) s_key = ~0ull;
+    __syncthreads();
+    if (t != kNoTri) {
+        unsigned long long best = ~0ull;
+        texel_walk(uv, F, t, res, true, nullptr, nullptr, [&](long long q, size_t p) {
+            const int o = owner[p];
+            if (o < t) {
+                const unsigned long long key = (static_cast<unsigned long long>(q) << 32) | static_cast<uint32_t>(o);
+                if (key < best) best = key;
+            }
+        });
+        if (best != ~0ull) atomicMin(&s_key, best);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const bool none = t == kNoTri || s_key == ~0ull;
+        pair[0] = none ? -1 : static_cast<int32_t>(s_key & 0xffffffffull);
+        pair[1] = none ? -1 : t;
+    }
+}
+
 __global__ void k_gutter_init(double* out, double radius) {
     out[0] = 1e300; out[1] = 0.0; out[2] = 0.0; out[3] = radius;
 }
@@ -338,6 +466,38 @@ extern "C" int uva_gutter(const double* UV, const int32_t* F, const int32_t* lab
     UVA_CHECK_LAUNCH("uva_gutter");
     k_gutter_final<<<1, 1, 0, s>>>(filled, smalls + 2, out);
     UVA_CHECK_LAUNCH("uva_gutter/final");
+    return UVA_OK;
+}
+
+// Texel-centre overlaps of one chart (engine/overlapfix.py:135-224, 263-275).
+extern "C" int uva_overlap_raster(const double* uv, const int32_t* F, int32_t m, int32_t res, uint8_t* flags,
+                                  int32_t* pair, void* scratch, int64_t scratch_bytes, void* stream) {
+    if (m < 0 || m >= kNoTri || res <= 0 || res > 16384 || !scratch || (!flags && !pair) || (m > 0 && (!uv || !F))) {
+        uva_set_error("uva_overlap_raster: bad arguments");
+        return UVA_E_ARG;
+    }
+    if (scratch_bytes < static_cast<int64_t>(gutter_bytes(res, m))) { uva_set_error("uva_overlap_raster: scratch too small"); return UVA_E_ARG; }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t ntex = static_cast<size_t>(res) * res;
+    auto al = [](size_t x) { return (x + 255) & ~static_cast<size_t>(255); };
+    auto* base = static_cast<unsigned char*>(scratch);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(base); base += al(4 * ntex);
+    int32_t* owner = reinterpret_cast<int32_t*>(base); base += al(4 * ntex) * 3 + al(2 * ntex) * 2;
+    int32_t* big = reinterpret_cast<int32_t*>(base); base += al(4 * static_cast<size_t>(std::max(m, 1)));
+    int32_t* smalls = reinterpret_cast<int32_t*>(base);   // [0] big count, [1] first triangle
+    cudaMemsetAsync(cnt, 0, 4 * ntex, s);
+    cudaMemsetAsync(owner, 0x7f, 4 * ntex, s);            // kNoTri on every texel
+    cudaMemsetAsync(smalls, 0, 4, s);
+    cudaMemsetAsync(smalls + 1, 0x7f, 4, s);
+    const int tb = 256;
+    if (m > 0) {
+        k_ov_cover<<<(m + tb - 1) / tb, tb, 0, s>>>(uv, F, m, res, cnt, owner, big, smalls);
+        k_ov_cover_big<<<148, tb, 0, s>>>(uv, F, res, cnt, owner, big, smalls);
+        k_ov_check<<<(m + tb - 1) / tb, tb, 0, s>>>(uv, F, m, res, cnt, owner, flags, smalls + 1);
+        k_ov_check_big<<<148, tb, 0, s>>>(uv, F, res, cnt, owner, big, smalls, flags, smalls + 1);
+    }
+    if (pair) k_ov_pair<<<1, tb, 0, s>>>(uv, F, res, owner, smalls + 1, pair);
+    UVA_CHECK_LAUNCH("uva_overlap_raster");
     return UVA_OK;
 }
 

@@ -67,6 +67,7 @@ Layout layout(int64_t nc, int64_t nseg) {
 }
 
 __device__ __forceinline__ bool same_point(double2 p, double2 q) { return p.x == q.x && p.y == q.y; }
+__device__ __forceinline__ int g_nx(const ChartGrid* grid, int c) { return grid[c].nx; }
 
 // engine/charts.py:579-591 (the same test as engine/hier.py:251-264): segments
 // i (a -> b) and j (c -> d) cross properly; endpoints with identical
@@ -145,11 +146,13 @@ __global__ void __launch_bounds__(kPrep) k_seg_prep(uva_seg_desc d, ChartGrid* g
     for (int c = blockIdx.x; c < d.nc; c += gridDim.x) {
         const int s0 = d.seg_ofs[c], s1 = d.seg_ofs[c + 1];
         const int v0 = d.vofs ? d.vofs[c] : 0, v1 = d.vofs ? d.vofs[c + 1] : d.n;
+        const bool gridded_mode = d.mode == UVA_SEG_COUNT || d.mode == UVA_SEG_FIRST;
         int bad = (s0 < 0 || s1 < s0 || s1 > d.nseg) ? kFlagRange : kFlagNone;
-        if (d.mode == UVA_SEG_COUNT && (v0 < 0 || v1 < v0 || v1 > d.n)) bad = kFlagRange;
+        if (gridded_mode && (v0 < 0 || v1 < v0 || v1 > d.n)) bad = kFlagRange;
+        if (d.mode == UVA_SEG_FIRST && s1 - s0 >= (1 << 21)) bad = kFlagRange;   // 21-bit segment ids in the key
         const int m = bad ? 0 : s1 - s0;
         // every row a segment names lies in U (COUNT: in the chart's rows)
-        const int lo_row = d.mode == UVA_SEG_COUNT ? v0 : 0, hi_row = d.mode == UVA_SEG_COUNT ? v1 : d.n;
+        const int lo_row = gridded_mode ? v0 : 0, hi_row = gridded_mode ? v1 : d.n;
         int rb = 0;
         for (int s = threadIdx.x; s < m; s += blockDim.x) {
             const int a = d.seg[2 * (s0 + s)], b = d.seg[2 * (s0 + s) + 1];
@@ -160,7 +163,7 @@ __global__ void __launch_bounds__(kPrep) k_seg_prep(uva_seg_desc d, ChartGrid* g
         double lo0 = INFINITY, lo1 = INFINITY, hi0 = -INFINITY, hi1 = -INFINITY;
         int nonfin = 0;
         if (!bad && m >= 3) {
-            if (d.mode == UVA_SEG_COUNT) {   // lo = U.min(0), ext = U.max(0) - lo over the chart's rows
+            if (gridded_mode) {   // lo = U.min(0), ext = U.max(0) - lo over the chart's rows
                 for (int v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
                     const double2 u = U[v];
                     nonfin |= finite2(u) ? 0 : 1;
@@ -181,7 +184,7 @@ __global__ void __launch_bounds__(kPrep) k_seg_prep(uva_seg_desc d, ChartGrid* g
             hi0 = block_reduce<double>(hi0, redd, false);
             hi1 = block_reduce<double>(hi1, redd, false);
         }
-        if (d.mode == UVA_SEG_COUNT && !bad && m >= 3 && !nonfin) {
+        if (gridded_mode && !bad && m >= 3 && !nonfin) {
             // L = |B - A| (np.linalg.norm(B - A, axis=1)), then its median
             const bool small = m <= kRankMax;
             for (int s = threadIdx.x; s < m; s += blockDim.x) {
@@ -215,8 +218,9 @@ __global__ void __launch_bounds__(kPrep) k_seg_prep(uva_seg_desc d, ChartGrid* g
             }
             if (threadIdx.x == 0) {
                 const double ext0 = hi0 - lo0, ext1 = hi1 - lo1;
-                double cell = med * 4.0;                        // max(median * 4, ext.max() / 512, 1e-30)
-                const double e = (ext1 > ext0 ? ext1 : ext0) / 512.0;
+                // max(median * 4, ext.max() / 512, 1e-30); collision (FIRST): / 1024
+                double cell = med * 4.0;
+                const double e = (ext1 > ext0 ? ext1 : ext0) / (d.mode == UVA_SEG_FIRST ? 1024.0 : 512.0);
                 if (e > cell) cell = e;
                 if (1e-30 > cell) cell = 1e-30;
                 g.lo0 = lo0; g.lo1 = lo1; g.cell = cell;
@@ -237,12 +241,12 @@ __global__ void __launch_bounds__(kPrep) k_seg_prep(uva_seg_desc d, ChartGrid* g
         }
         if (threadIdx.x == 0) {
             ChartGrid& o = grid[c];
-            const bool gridded = d.mode == UVA_SEG_COUNT && !bad && m >= 3 && !nonfin;
+            const bool gridded = gridded_mode && !bad && m >= 3 && !nonfin;
             o.lo0 = gridded ? g.lo0 : 0.0; o.lo1 = gridded ? g.lo1 : 0.0; o.cell = gridded ? g.cell : 0.0;
             o.nx = gridded ? g.nx : 0; o.ny = gridded ? g.ny : 0;
             int flag = bad;
             if (!flag && m >= 3) {
-                if (d.mode == UVA_SEG_COUNT) {
+                if (gridded_mode) {
                     if (nonfin) flag = kFlagNonFinite;
                 } else {
                     const double ext0 = hi0 - lo0, ext1 = hi1 - lo1;
@@ -253,7 +257,7 @@ __global__ void __launch_bounds__(kPrep) k_seg_prep(uva_seg_desc d, ChartGrid* g
             }
             o.flag = flag;
             o.tiles = (!flag && m >= 3) ? (m + kTile - 1) / kTile : 0;
-            hits[c] = 0;
+            hits[c] = d.mode == UVA_SEG_FIRST ? ~0ull : 0ull;
         }
         __syncthreads();   // g is rewritten for the next chart
     }
@@ -295,7 +299,8 @@ __global__ void __launch_bounds__(kPair) k_seg_pairs(uva_seg_desc d, const Chart
     const double2* U = reinterpret_cast<const double2*>(d.U);
     const long long total = tile_ofs[d.nc];
     const unsigned long long cap = static_cast<unsigned long long>(d.max_report > 1 ? d.max_report : 1);
-    const bool count = d.mode == UVA_SEG_COUNT;
+    const bool count = d.mode == UVA_SEG_COUNT, first = d.mode == UVA_SEG_FIRST;
+    const bool boxes = count || first;
     for (long long w = blockIdx.x; w < total; w += gridDim.x) {
         __syncthreads();   // the previous item's shared data is consumed
         if (threadIdx.x == 0) {
@@ -310,7 +315,7 @@ __global__ void __launch_bounds__(kPair) k_seg_pairs(uva_seg_desc d, const Chart
             while (ti < k - 1 && l >= k - ti) { l -= k - ti; ++ti; }
             item[0] = lo; item[1] = ti; item[2] = ti + static_cast<int>(l);
             const unsigned long long sofar = *reinterpret_cast<volatile unsigned long long*>(hits + lo);
-            item[3] = count ? (sofar >= cap) : (sofar > 0);
+            item[3] = first ? 0 : count ? (sofar >= cap) : (sofar > 0);
             item[4] = d.seg_ofs[lo];
         }
         __syncthreads();
@@ -325,26 +330,37 @@ __global__ void __launch_bounds__(kPair) k_seg_pairs(uva_seg_desc d, const Chart
                 const int s = s0 + base + q;
                 sa[t][q] = U[d.seg[2 * s]];
                 sb[t][q] = U[d.seg[2 * s + 1]];
-                if (count) sbox[t][q] = box[s];
+                if (boxes) sbox[t][q] = box[s];
             }
         }
         __syncthreads();
-        unsigned long long acc = 0;
+        unsigned long long acc = first ? ~0ull : 0ull;
         const int i = threadIdx.x % kTile;
         if (i < ni) {
             const double2 a = sa[0][i], b = sb[0][i];
-            const int4 bi = count ? sbox[0][i] : make_int4(0, 0, 0, 0);
+            const int4 bi = boxes ? sbox[0][i] : make_int4(0, 0, 0, 0);
             const double ax0 = fmin(a.x, b.x), ax1 = fmax(a.x, b.x), ay0 = fmin(a.y, b.y), ay1 = fmax(a.y, b.y);
             const int jstart = ti == tj ? i + 1 : 0;
             // j = jstart + (tid / kTile) + 2 r: the two thread halves split the columns
             for (int j = jstart + threadIdx.x / kTile; j < nj; j += kPair / kTile) {
                 const double2 c2 = sa[1][j], d2 = sb[1][j];
-                if (count) {
+                if (boxes) {
                     const int4 bj = sbox[1][j];
                     const int ox = min(bi.y, bj.y) - max(bi.x, bj.x) + 1;
                     const int oy = min(bi.w, bj.w) - max(bi.z, bj.z) + 1;
-                    if (ox > 0 && oy > 0 && seg_cross(a, b, c2, d2))
-                        acc += static_cast<unsigned long long>(ox) * static_cast<unsigned long long>(oy);
+                    if (ox > 0 && oy > 0 && seg_cross(a, b, c2, d2)) {
+                        if (count) {
+                            acc += static_cast<unsigned long long>(ox) * static_cast<unsigned long long>(oy);
+                        } else {   // the reference meets the pair first in its first shared cell
+                            const unsigned long long cmin = static_cast<unsigned long long>(max(bi.z, bj.z)) *
+                                                                static_cast<unsigned long long>(g_nx(grid, c)) +
+                                                            static_cast<unsigned long long>(max(bi.x, bj.x));
+                            const unsigned long long gi = static_cast<unsigned long long>(ti * kTile + i);
+                            const unsigned long long gj = static_cast<unsigned long long>(tj * kTile + j);
+                            const unsigned long long key = (cmin << 42) | (gi << 21) | gj;
+                            if (key < acc) acc = key;
+                        }
+                    }
                 } else {
                     if (fmax(c2.x, d2.x) >= ax0 && fmin(c2.x, d2.x) <= ax1 && fmax(c2.y, d2.y) >= ay0 &&
                         fmin(c2.y, d2.y) <= ay1 && seg_cross(a, b, c2, d2))
@@ -353,13 +369,17 @@ __global__ void __launch_bounds__(kPair) k_seg_pairs(uva_seg_desc d, const Chart
             }
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long y = __shfl_xor_sync(0xffffffffu, acc, o);
+            acc = first ? (y < acc ? y : acc) : acc + y;
+        }
         if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = acc;
         __syncthreads();
         if (threadIdx.x == 0) {
-            unsigned long long s = 0;
-            for (int k = 0; k < kPair / 32; ++k) s += wsum[k];
-            if (s) atomicAdd(hits + c, s);
+            unsigned long long s = first ? ~0ull : 0ull;
+            for (int k = 0; k < kPair / 32; ++k) s = first ? (wsum[k] < s ? wsum[k] : s) : s + wsum[k];
+            if (first) { if (s != ~0ull) atomicMin(hits + c, s); }
+            else if (s) atomicAdd(hits + c, s);
         }
     }
 }
@@ -375,6 +395,9 @@ __global__ void k_seg_final(uva_seg_desc d, const ChartGrid* grid, const unsigne
     } else if (d.mode == UVA_SEG_COUNT) {
         const unsigned long long cap = static_cast<unsigned long long>(d.max_report > 1 ? d.max_report : 1);
         r = flag ? -1 : static_cast<int64_t>(h < cap ? h : cap);
+    } else if (d.mode == UVA_SEG_FIRST) {   // (i << 32) | j of the first crossing pair, -3: none
+        const unsigned long long mask = (1ull << 21) - 1;
+        r = flag ? -1 : (h == ~0ull ? -3 : static_cast<int64_t>((((h >> 21) & mask) << 32) | (h & mask)));
     } else {
         r = (flag || h > 0) ? 1 : 0;
     }
@@ -488,12 +511,13 @@ extern "C" int uva_seg_scratch_bytes(int32_t nc, int32_t nseg, int64_t* bytes) {
 
 extern "C" int uva_boundary_hits(const uva_seg_desc* d, void* stream) {
     if (!d || d->nc < 0 || d->nseg < 0 || d->n < 0 ||
-        (d->mode != UVA_SEG_COUNT && d->mode != UVA_SEG_ANY && d->mode != UVA_SEG_ANY_ALL)) {
+        (d->mode != UVA_SEG_COUNT && d->mode != UVA_SEG_ANY && d->mode != UVA_SEG_ANY_ALL &&
+         d->mode != UVA_SEG_FIRST)) {
         uva_set_error("uva_boundary_hits: bad arguments");
         return UVA_E_ARG;
     }
     if (d->nc == 0) return UVA_OK;
-    if (!d->seg_ofs || !d->out || !d->scratch || (d->mode == UVA_SEG_COUNT && !d->vofs) ||
+    if (!d->seg_ofs || !d->out || !d->scratch || ((d->mode == UVA_SEG_COUNT || d->mode == UVA_SEG_FIRST) && !d->vofs) ||
         (d->nseg > 0 && (!d->seg || !d->U || d->n == 0))) {
         uva_set_error("uva_boundary_hits: null pointer");
         return UVA_E_ARG;

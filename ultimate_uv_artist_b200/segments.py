@@ -16,7 +16,7 @@ import torch
 from . import _lib
 from .device import require_cuda
 
-COUNT, ANY, ANY_ALL = _lib.SEG_COUNT, _lib.SEG_ANY, _lib.SEG_ANY_ALL
+COUNT, ANY, ANY_ALL, FIRST = _lib.SEG_COUNT, _lib.SEG_ANY, _lib.SEG_ANY_ALL, _lib.SEG_FIRST
 
 
 def _dev_array(a, dtype, dev):
@@ -45,7 +45,7 @@ def boundary_hits(U, seg_ofs, seg, mode, max_report=1000, vofs=None, device=None
     n = int(Ud.shape[0])
     if max(n, nseg, int(seg_ofs[-1])) >= 2 ** 31:
         raise ValueError("boundary_hits: more than 2^31 - 1 rows or segments")
-    if mode == COUNT and vofs is None:
+    if mode in (COUNT, FIRST) and vofs is None:
         raise ValueError("boundary_hits: count mode needs the charts' UV rows (vofs)")
     seg_d = _dev_array(seg, torch.int32, dev) if nseg else torch.zeros((1, 2), dtype=torch.int32, device=dev)
     ofs_d = _dev_array(seg_ofs, torch.int32, dev)
