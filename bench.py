@@ -420,6 +420,62 @@ def bench_boundary(b, reps=5):
     return out
 
 
+def bench_hier(dev, reps=3):
+    """hier.Solver.relax (6 iterations), Solver.lscm and hier.chart_checks on a
+    256 x 256 bumpy grid mesh (131,072 faces) cut into 64 charts
+    (synth.mesh_charts): wall time of the API calls (host layout, device
+    work, download), best of ``reps`` after a warm-up call."""
+    import time
+    from types import SimpleNamespace
+    import torch
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.engine import hier
+    V, F, FF, faces, loc, chart, CV, nv, nchart, U0 = synth.mesh_charts()
+    S = hier.Solver(SimpleNamespace(V=V, F=F), dev=dev)
+    ba, bb = hier.boundary_directed(F, FF, faces, loc, chart, CV)
+
+    def best(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return min(ts), out
+
+    t_relax, (U, flips, _) = best(lambda: S.relax(faces, CV, nv, chart, nchart, U0, iters=6))
+    t_lscm, _ = best(lambda: S.lscm(faces, CV, nv, chart, nchart, U0, ba, bb))
+    t_chk, (col, _, _) = best(lambda: hier.chart_checks(F, FF, faces, loc, chart, CV, U, nchart, nv))
+    return {"workload": "mesh_charts_256x256_64_charts", "faces": int(len(F)), "charts": int(nchart),
+            "uv_vertices": int(nv), "relax_iters": 6, "relax_ms": 1e3 * t_relax,
+            "relax_face_iters_per_s": len(F) * 6 / t_relax, "lscm_ms": 1e3 * t_lscm,
+            "chart_checks_ms": 1e3 * t_chk, "flipped_after_relax": int(flips.sum()),
+            "charts_colliding": int(col.sum())}
+
+
+def bench_overlap(islands, uvs, count=16):
+    """overlapfix.overlapping_triangles and collision, chart by chart (the
+    reference's per-chart API), on the ``count`` largest charts of the batch
+    at their final UVs: wall time per chart."""
+    import time
+    import torch
+    from ultimate_uv_artist_b200.engine import overlapfix
+    pick = np.argsort([-len(t) for _, t in islands])[:count]
+    for i in pick[:2]:   # warm-up
+        overlapfix.overlapping_triangles(uvs[i], islands[i][1])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    bad = sum(int(overlapfix.overlapping_triangles(uvs[i], islands[i][1]).sum()) for i in pick)
+    t1 = time.perf_counter()
+    coll = sum(overlapfix.collision(uvs[i], islands[i][1]) is not None for i in pick)
+    t2 = time.perf_counter()
+    tris = int(sum(len(islands[i][1]) for i in pick))
+    return {"charts": int(len(pick)), "triangles": tris, "overlapping_triangles_ms_per_chart": 1e3 * (t1 - t0) / len(pick),
+            "collision_ms_per_chart": 1e3 * (t2 - t1) / len(pick), "overlapping": bad, "colliding_charts": int(coll)}
+
+
 def run_reference(args):
     """CPU reference arm: the oracle port of param.lscm + param.refine per
     island over all host cores, on a bounded sample of the same workload."""
@@ -583,9 +639,11 @@ def main():
         plain["speedup_vs_per_island"] = value / plain["per_island"]["value"]
         plain["speedup_vs_one_batch"] = value / plain["one_batch"]["value"]
 
-    bnd = None
+    bnd = hier_b = ovl = None
     if rank == 0 and not args.no_validate:
         bnd = bench_boundary(b)
+        hier_b = bench_hier(dev)
+        ovl = bench_overlap(islands, our_uvs)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -610,6 +668,10 @@ def main():
             bs, bsel, bwant = cpu_baseline.time_boundary(islands, our_uvs, args.cpu_budget_tris)
             cpu["boundary_checks"] = {"seconds": bs, "cores": 1, "kind": "port", "charts": len(bsel),
                                       "same_counts": bool(all(int(bnd["hits"][i]) == w for i, w in zip(bsel, bwant)))}
+        if hier_b is not None:   # hier.Solver.relax on the same mesh (oracle port, exact solves, one thread)
+            hs = cpu_baseline.time_hier_relax()
+            cpu["hier_relax"] = {"seconds": hs, "cores": 1, "kind": "port",
+                                 "face_iters_per_s": hier_b["faces"] * 6 / hs}
         err, ni, nt_ = cpu_baseline.uv_error_batch(islands, our_uvs, args.iters)
         cpu["uv_error_check"] = {"max_rel_uv_error": err, "islands": ni, "triangles": nt_,
                                  "against": "FP64 oracle of LSCM + gpu.Batch.arap with exact solves"}
@@ -642,6 +704,8 @@ def main():
             "clocks": ck,
             "validate": val,
             "boundary_checks": None if bnd is None else {k: v for k, v in bnd.items() if k != "hits"},
+            "hier_solver": hier_b,
+            "overlap_checks": ovl,
         }
         print(json.dumps(line), flush=True)
     if graphs:

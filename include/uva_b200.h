@@ -396,6 +396,13 @@ int uva_chart_op(int32_t op, int32_t arg, const double* P, const int64_t* T, con
  * stop at ||r|| <= tol ||b||. scratch: 3*n*ncol doubles; iters: ncol.      */
 int uva_csr_pcg(int32_t n, const int32_t* rowptr, const int32_t* col, const double* val, const double* b, double* x,
                 int32_t ncol, double tol, int32_t maxiter, double* scratch, int32_t* iters, void* stream);
+/* The same on a block-diagonal SPD CSR matrix (n rows): block s owns rows
+ * [sys_ofs[s], sys_ofs[s+1]) and only its own columns; each block is solved
+ * by its own CTA to ||r_s|| <= tol ||b_s||. scratch: 3n doubles; iters:
+ * nsys (device). Used by hier.Solver.lscm, one block per chart.           */
+int uva_csr_pcg_blocks(int32_t nsys, const int32_t* sys_ofs, int32_t n, const int32_t* rowptr, const int32_t* col,
+                       const double* val, const double* b, double* x, double tol, int32_t maxiter, double* scratch,
+                       int32_t* iters, void* stream);
 
 /* --------------------------------------------------------------------------
  * Distortion energies with backward passes (engine/param.py:294-319):

@@ -100,6 +100,17 @@ def time_boundary(islands, uvs, budget_tris):
     return time.perf_counter() - t0, [int(i) for i in pick], want
 
 
+def time_hier_relax():
+    """Seconds of the oracle's hier.Solver.relax (6 iterations, exact sparse
+    LU) on the bench's mesh_charts workload (one thread)."""
+    from oracle import hier as OH
+    from ultimate_uv_artist_b200 import synth
+    V, F, FF, faces, loc, chart, CV, nv, nchart, U0 = synth.mesh_charts()
+    t0 = time.perf_counter()
+    OH.relax(V, F, faces, CV, nv, chart, nchart, U0, iters=6)
+    return time.perf_counter() - t0
+
+
 def time_validation(V, F, UV, atlas=4096, padding=4):
     """Seconds of the oracle's validate_uvs (numpy + the C restatement of the
     reference's serial loops, one thread) on an atlas, and its report."""

@@ -97,6 +97,7 @@ _SIGS = {
     "uva_jacobians": [vp, vp, vp, vp],
     "uva_shrink": [vp, vp, vp, i32, C.c_float, C.c_float, vp],
     "uva_seg_scratch_bytes": [i32, i32, vp],
+    "uva_csr_pcg_blocks": [i32, vp, i32, vp, vp, vp, vp, vp, C.c_double, i32, vp, vp, vp],
     "uva_overlap_raster": [vp, vp, i32, i32, vp, vp, vp, C.c_int64, vp],
     "uva_gutter_scratch_bytes": [i32, C.c_int64, vp],
     "uva_boundary_hits": [vp, vp],

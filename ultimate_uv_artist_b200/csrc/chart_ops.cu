@@ -256,6 +256,68 @@ __global__ void __launch_bounds__(NT) k_csr_pcg(int n, const int32_t* rp, const 
     if (threadIdx.x == 0) iters_out[c] = it;
 }
 
+// ---- the same PCG on a block-diagonal CSR matrix, one CTA per diagonal
+// block: block s owns rows [so[s], so[s+1]) and its columns lie in the same
+// range; it stops at ||r_s|| <= tol ||b_s||.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_csr_pcg_blocks(int nsys, const int32_t* so, const int32_t* rp,
+                                                       const int32_t* ci, const double* val, const double* b,
+                                                       double* x, double* r, double* p, double* q, double tol,
+                                                       int maxiter, int32_t* iters_out) {
+    __shared__ double red[2 * 4 * (NT / 32)];
+    int phase = 0;
+    const int c = blockIdx.x;
+    if (c >= nsys) return;
+    const int r0 = so[c], r1 = so[c + 1];
+    auto diag = [&](int i) {
+        double d = 0.0;
+        for (int k = rp[i]; k < rp[i + 1]; ++k)
+            if (ci[k] == i) d += val[k];
+        return fabs(d) > 1e-300 ? d : 1.0;
+    };
+    double acc[2] = {0.0, 0.0};
+    for (int i = r0 + threadIdx.x; i < r1; i += NT) {
+        double ax = 0.0;
+        for (int k = rp[i]; k < rp[i + 1]; ++k) ax += val[k] * x[ci[k]];
+        const double ri = b[i] - ax;
+        r[i] = ri;
+        p[i] = ri / diag(i);
+        acc[0] += ri * p[i];
+        acc[1] += b[i] * b[i];
+    }
+    block_sum<NT, 2>(acc, red, phase);
+    double rz = acc[0];
+    const double bb = fmax(acc[1], 1e-300);
+    int it = 0;
+    for (; it < maxiter; ++it) {
+        double pq[1] = {0.0};
+        for (int i = r0 + threadIdx.x; i < r1; i += NT) {
+            double s = 0.0;
+            for (int k = rp[i]; k < rp[i + 1]; ++k) s += val[k] * p[ci[k]];
+            q[i] = s;
+            pq[0] += p[i] * s;
+        }
+        block_sum<NT, 1>(pq, red, phase);
+        if (!(pq[0] > 0.0)) break;
+        const double alpha = rz / pq[0];
+        double nz[2] = {0.0, 0.0};
+        for (int i = r0 + threadIdx.x; i < r1; i += NT) {
+            x[i] += alpha * p[i];
+            r[i] -= alpha * q[i];
+            const double z = r[i] / diag(i);
+            nz[0] += r[i] * z;
+            nz[1] += r[i] * r[i];
+        }
+        block_sum<NT, 2>(nz, red, phase);
+        if (nz[1] <= tol * tol * bb) { ++it; break; }
+        const double beta = nz[0] / rz;
+        rz = nz[0];
+        for (int i = r0 + threadIdx.x; i < r1; i += NT) p[i] = r[i] / diag(i) + beta * p[i];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) iters_out[c] = it;
+}
+
 }  // namespace
 
 extern "C" int uva_chart_op(int32_t op, int32_t arg, const double* P, const int64_t* T, const double* U,
@@ -269,6 +331,22 @@ extern "C" int uva_chart_op(int32_t op, int32_t arg, const double* P, const int6
     if (op == UVA_OP_ENERGY) cudaMemsetAsync(out, 0, sizeof(double), s);
     if (t > 0) k_chart_op<<<(t + 255) / 256, 256, 0, s>>>(a);
     UVA_CHECK_LAUNCH("uva_chart_op");
+    return UVA_OK;
+}
+
+extern "C" int uva_csr_pcg_blocks(int32_t nsys, const int32_t* sys_ofs, int32_t n, const int32_t* rowptr,
+                                  const int32_t* col, const double* val, const double* b, double* x, double tol,
+                                  int32_t maxiter, double* scratch, int32_t* iters, void* stream) {
+    if (nsys < 0 || n < 0 || (nsys > 0 && (!sys_ofs || !rowptr || !b || !x || !scratch || !iters))) {
+        uva_set_error("uva_csr_pcg_blocks: bad arguments");
+        return UVA_E_ARG;
+    }
+    if (nsys == 0 || n == 0) return UVA_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t N = static_cast<size_t>(n);
+    k_csr_pcg_blocks<256><<<nsys, 256, 0, s>>>(nsys, sys_ofs, rowptr, col, val, b, x, scratch, scratch + N,
+                                               scratch + 2 * N, tol, maxiter, iters);
+    UVA_CHECK_LAUNCH("uva_csr_pcg_blocks");
     return UVA_OK;
 }
 

@@ -187,8 +187,9 @@ class Solver:
     Jacobi-CG iterations on the whole subset in FP32; ``cg_iters`` is kept
     for signature compatibility. ``lscm`` assembles the reference's
     soft-pinned LSCM system on the host and solves it with the FP64
-    Jacobi-PCG kernel (uva_csr_pcg) to a 1e-10 relative residual, where the
-    reference stops its FP32 CG at 1e-6 or 600 iterations.
+    Jacobi-PCG kernel, one CTA per chart (uva_csr_pcg_blocks), to a 1e-10
+    relative residual per chart, where the reference stops its FP32 CG on
+    the whole system at 1e-6 or 600 iterations.
     """
 
     def __init__(self, topo, dev=None):
@@ -345,14 +346,23 @@ class Solver:
         np.add.at(b, pins, wpin * U0[pins, 0])
         np.add.at(b, pins + nv, wpin * U0[pins, 1])
         x0 = np.concatenate([U0[:, 0], U0[:, 1]])
-        # unknowns of UV vertices that no face names have no equation: they keep U0
+        # unknowns of UV vertices that no face names have no equation: they
+        # keep U0. The system is block-diagonal by chart: each chart's u and v
+        # unknowns form one block, solved by its own CTA.
         used = np.zeros(2 * nv, bool)
         used[np.concatenate([CV.reshape(-1), CV.reshape(-1) + nv])] = True
         idx = np.nonzero(used)[0]
         if len(idx) == 0:
             return U0.copy()
+        uc = np.concatenate([cv, cv])[idx]                 # chart of every unknown
+        idx = idx[np.argsort(uc, kind="stable")]
+        sys_ofs = np.zeros(nchart + 1, np.int64)
+        np.cumsum(np.bincount(np.concatenate([cv, cv])[idx], minlength=nchart), out=sys_ofs[1:])
         H = H[idx][:, idx].tocsr()
         H.sort_indices()
+        blk = np.repeat(np.arange(nchart), np.diff(sys_ofs))   # block of every (permuted) unknown
+        if len(H.indices) and (blk[H.indices] != np.repeat(blk, np.diff(H.indptr))).any():
+            raise ValueError("hier.Solver.lscm: a UV vertex is shared by faces of different charts")
         b = b[idx]
         x_all = x0.copy()
         x0 = x0[idx]
@@ -362,17 +372,16 @@ class Solver:
         va = torch.from_numpy(H.data.astype(np.float64)).to(d)
         bd = torch.from_numpy(b).to(d)
         xd = torch.from_numpy(x0).to(d)
+        so = torch.from_numpy(sys_ofs.astype(np.int32)).to(d)
         N = len(idx)
         scratch = torch.empty(3 * N, dtype=torch.float64, device=d)
-        its = torch.zeros(1, dtype=torch.int32, device=d)
+        its = torch.zeros(max(nchart, 1), dtype=torch.int32, device=d)
         L = _lib.lib()
-        L.uva_csr_pcg.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                  C.c_int32, C.c_double, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
-        L.uva_csr_pcg.restype = C.c_int32
         st = torch.cuda.current_stream(d)
-        _lib.check(L.uva_csr_pcg(N, rp.data_ptr(), ci.data_ptr(), va.data_ptr(), bd.data_ptr(), xd.data_ptr(), 1,
-                                 1e-10, max(20000, 40 * int(np.sqrt(N))), scratch.data_ptr(), its.data_ptr(),
-                                 C.c_void_p(st.cuda_stream)), "uva_csr_pcg")
+        _lib.check(L.uva_csr_pcg_blocks(nchart, so.data_ptr(), N, rp.data_ptr(), ci.data_ptr(), va.data_ptr(),
+                                        bd.data_ptr(), xd.data_ptr(), 1e-10, max(20000, 40 * int(np.sqrt(N))),
+                                        scratch.data_ptr(), its.data_ptr(), C.c_void_p(st.cuda_stream)),
+                   "uva_csr_pcg_blocks")
         x_all[idx] = xd.cpu().numpy()
         U = np.stack([x_all[:nv], x_all[nv:]], 1)
         return np.where(np.isfinite(U), U, U0)

@@ -369,3 +369,53 @@ def shelf_pack(uvs, atlas=4096, padding=4, fill=0.6):
             return [(u - l) * scale + place[i] for i, (u, l) in enumerate(zip(uvs, lo))]
         scale *= 0.9
     raise RuntimeError("shelf_pack: charts do not fit")
+
+
+def mesh_charts(seed=6000, nx=256, ny=256, block=32, fold_every=2):
+    """A bumpy grid mesh cut into block charts, in the input layout of
+    engine/hier.py (Solver.relax, chart_checks): returns (V, F, FF, faces,
+    loc, chart, CV, nv, nchart, U0). Every chart has its own UV vertices
+    (CV); U0 is the planar position with small noise, and every
+    ``fold_every``-th chart has two vertices reflected through its centre
+    (folds). Vectorised, for bench sizes."""
+    rng = np.random.default_rng(seed)
+    s = np.arange(nx + 1, dtype=np.float64)
+    X, Y = np.meshgrid(s, np.arange(ny + 1, dtype=np.float64))
+    V2 = np.stack([X.ravel(), Y.ravel()], 1) + rng.uniform(-0.2, 0.2, ((nx + 1) * (ny + 1), 2))
+    z = 0.6 * np.sin(V2[:, 0] / 4.0) * np.cos(V2[:, 1] / 5.0)
+    V = np.concatenate([V2, z[:, None]], 1)
+    cx, cy = np.meshgrid(np.arange(nx), np.arange(ny))
+    cx, cy = cx.ravel(), cy.ravel()
+    a = cy * (nx + 1) + cx
+    b, c, d = a + 1, a + nx + 1, a + nx + 2
+    F = np.stack([np.stack([a, b, d], 1), np.stack([a, d, c], 1)], 1).reshape(-1, 3).astype(np.int64)
+    fx, fy = np.repeat(cx, 2), np.repeat(cy, 2)
+    m = len(F)
+    # face adjacency: the face across corner edge k (F[f,k] -> F[f,k+1])
+    key = F * (len(V)) + F[:, [1, 2, 0]]
+    rkey = F[:, [1, 2, 0]] * (len(V)) + F
+    order = np.argsort(key.ravel())
+    sk = key.ravel()[order]
+    pos = np.searchsorted(sk, rkey.ravel())
+    pos = np.minimum(pos, len(sk) - 1)
+    hit = sk[pos] == rkey.ravel()
+    FF = np.where(hit, order[pos] // 3, -1).reshape(m, 3)
+    nbx = (nx + block - 1) // block
+    lab = (fx // block) + (fy // block) * nbx
+    faces = np.arange(m, dtype=np.int64)
+    loc = np.arange(m, dtype=np.int64)
+    _, chart = np.unique(lab, return_inverse=True)
+    nchart = int(chart.max()) + 1
+    ck = chart[:, None] * len(V) + F                      # (chart, mesh vertex) per corner
+    uk, CV = np.unique(ck.ravel(), return_inverse=True)
+    CV = CV.reshape(m, 3).astype(np.int64)
+    nv = len(uk)
+    vmesh = uk % len(V)
+    vch = uk // len(V)
+    U0 = V2[vmesh] * 0.9 + rng.normal(0, 0.03, (nv, 2))
+    for ch in range(0, nchart, max(int(fold_every), 1)):
+        ids = np.nonzero(vch == ch)[0]
+        mv = rng.choice(ids, 2, replace=False)
+        ctr = U0[ids].mean(0)
+        U0[mv] = ctr + (ctr - U0[mv]) * 0.3
+    return V, F, FF, faces, loc, chart.astype(np.int64), CV, int(nv), nchart, U0
