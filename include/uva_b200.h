@@ -86,6 +86,10 @@ enum {
  * Returns UVA_E_ARG if an index is out of its island's range.              */
 int uva_plan_create(const int64_t* tris, const int64_t* vofs, const int64_t* tofs,
                     int32_t nc, int32_t nthreads, uva_plan** out);
+/* The same from per-chart triangle arrays (island i: T[i], 3 t_i local ids,
+ * tdt[i] 0: int32, 1: int64), without concatenating them first.          */
+int uva_plan_create_charts(const void* const* T, const int8_t* tdt, const int64_t* vofs, const int64_t* tofs,
+                           int32_t nc, int32_t nthreads, uva_plan** out);
 int uva_plan_sizes(const uva_plan* plan, int64_t* sizes /* UVA_PLAN_NSIZES */);
 /* Copies the plan into caller-owned HOST arrays (sizes from uva_plan_sizes):
  *   tri4      t*4   local a,b,c and island id
@@ -116,7 +120,8 @@ void uva_plan_destroy(uva_plan* plan);
  * float32/float64: pdt 0/1), T (rows of 3 local ids, int32/int64: tdt 0/1)
  * and optional U (rows of 2, udt -1: none -> zeros, 0: float32, 1: float64;
  * U or udt may be null: all zeros) land in P_out (n*3 FP64), T_out (t*3
- * int64) and U_out (n*2 FP64, may be null) at vofs/tofs (nc+1 offsets).     */
+ * int64; may be null, then T and tdt are not read) and U_out (n*2 FP64, may
+ * be null) at vofs/tofs (nc+1 offsets).                                    */
 int uva_concat_charts(int32_t nc, const void* const* P, const int8_t* pdt, const void* const* T,
                       const int8_t* tdt, const void* const* U, const int8_t* udt, const int64_t* vofs,
                       const int64_t* tofs, double* P_out, int64_t* T_out, double* U_out, int32_t nthreads);

@@ -211,3 +211,25 @@ def test_concat_charts_matches_numpy():
     with pytest.raises(ValueError):
         concat_charts([(np.zeros((4, 3)), np.zeros((1, 3), np.int64), np.zeros((3, 2)))])
     assert concat_charts([c[:2] + (None,) for c in charts])[2] is None   # no UVs: nothing to upload
+
+
+def test_plan_from_chart_arrays_matches_concatenated():
+    """uva_plan_create_charts (per-chart int32 / int64 triangle arrays, no
+    concatenation) builds the same plan as uva_plan_create."""
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.device import Plan, concat_charts
+    isl = synth.uneven_islands(seed=61, count=30, tmin=20, tmax=3000)
+    charts = [(p, t.astype(np.int32) if k % 2 else t, None) for k, (p, t) in enumerate(isl)]
+    P, T, _, vofs, tofs = concat_charts(charts)
+    P2, Tc, _, vofs2, tofs2 = concat_charts(charts, with_t=False)
+    assert np.array_equal(P, P2) and np.array_equal(vofs, vofs2) and np.array_equal(tofs, tofs2)
+    a = Plan(T, vofs, tofs)
+    b = Plan(None, vofs2, tofs2, chart_tris=Tc[:2])
+    for k in ("tri4", "tri_edge", "sofs", "slice_ptr", "slot_col", "slot_edge", "slot_c", "vt_ptr", "vt", "vflags",
+              "bofs", "bverts", "order", "row_vert", "vert_row", "agg_rows", "cofs"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+    bad = [(p, t.copy(), None) for p, t, _ in charts]
+    bad[3][1][0, 0] = len(bad[3][0])                   # a vertex id outside its chart
+    _, Tb, _, vb, tb = concat_charts(bad, with_t=False)
+    with pytest.raises(ValueError):
+        Plan(None, vb, tb, chart_tris=Tb[:2])

@@ -75,6 +75,7 @@ SEG_COUNT, SEG_ANY, SEG_ANY_ALL, SEG_FIRST = 0, 1, 2, 3
 
 _SIGS = {
     "uva_plan_create": [vp, vp, vp, i32, i32, vp],
+    "uva_plan_create_charts": [vp, vp, vp, vp, i32, i32, vp],
     "uva_plan_sizes": [vp, vp],
     "uva_plan_export": [vp] * 13,
     "uva_plan_export_rows": [vp] * 5,

@@ -73,7 +73,8 @@ void blob_order(const IslandPlan& ip, int32_t n, int32_t agg, std::vector<int32_
     }
 }
 
-void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& bad) {
+template <typename I>   // int32_t or int64_t island-local vertex ids
+void build_island(const I* T, int32_t n, int32_t t, IslandPlan& ip, bool& bad) {
     ip.n = n; ip.t = t;
     // half-edges grouped by (lo, hi, half-edge id): a counting sort by lo
     // into contiguous (hi, 2 h + dir) pairs (dir 1: the half-edge runs lo ->
@@ -83,7 +84,7 @@ void build_island(const int64_t* T, int32_t n, int32_t t, IslandPlan& ip, bool& 
     std::vector<int32_t> bstart(n + 1, 0);
     for (int32_t f = 0; f < t; ++f) {
         for (int k = 0; k < 3; ++k) {
-            const int64_t a = T[3 * f + (k + 1) % 3], b = T[3 * f + (k + 2) % 3];
+            const int64_t a = static_cast<int64_t>(T[3 * f + (k + 1) % 3]), b = static_cast<int64_t>(T[3 * f + (k + 2) % 3]);
             if (a < 0 || a >= n || b < 0 || b >= n) { bad = true; return; }
             ++bstart[(a < b ? a : b) + 1];
         }
@@ -214,8 +215,10 @@ struct uva_plan {
     std::unique_ptr<int32_t[]> tri_local;   // 3t local ids (copied by the island workers)
 };
 
-extern "C" int uva_plan_create(const int64_t* tris, const int64_t* vofs, const int64_t* tofs, int32_t nc,
-                               int32_t nthreads, uva_plan** out) {
+// The plan of every island; island i's triangles come from tri_src(i):
+// (pointer to its 3 t_i local ids, true if int64 else int32).
+template <typename Src>
+int plan_create(Src tri_src, const int64_t* vofs, const int64_t* tofs, int32_t nc, int32_t nthreads, uva_plan** out) {
     if (!out || nc < 0 || (nc > 0 && (!vofs || !tofs))) { uva_set_error("uva_plan_create: bad arguments"); return UVA_E_ARG; }
     *out = nullptr;
     auto* p = new uva_plan();
@@ -226,13 +229,15 @@ extern "C" int uva_plan_create(const int64_t* tris, const int64_t* vofs, const i
         if (p->vofs[i + 1] < p->vofs[i] || p->tofs[i + 1] < p->tofs[i]) {
             delete p; uva_set_error("uva_plan_create: offsets must be non-decreasing"); return UVA_E_ARG;
         }
+        if (p->tofs[i + 1] > p->tofs[i] && !tri_src(i).first) {
+            delete p; uva_set_error("uva_plan_create: null triangles"); return UVA_E_ARG;
+        }
     }
     p->n = p->vofs[nc] - p->vofs[0];
     p->t = p->tofs[nc] - p->tofs[0];
     if (p->n > (int64_t(1) << 30) || 3 * p->t > (int64_t(1) << 30)) {
         delete p; uva_set_error("uva_plan_create: batch too large for 32-bit indices"); return UVA_E_TOOBIG;
     }
-    if (p->t > 0 && !tris) { delete p; uva_set_error("uva_plan_create: null triangles"); return UVA_E_ARG; }
     p->isl.resize(nc);
     p->tri_local.reset(new int32_t[static_cast<size_t>(3 * p->t) + 1]);   // uninitialised; filled per island
     // largest islands first for load balance
@@ -250,10 +255,19 @@ extern "C" int uva_plan_create(const int64_t* tris, const int64_t* vofs, const i
             const int32_t i = order[q];
             bool bad = false;
             const int64_t t0 = 3 * (p->tofs[i] - p->tofs[0]), tn = 3 * (p->tofs[i + 1] - p->tofs[i]);
-            build_island(tris + t0, static_cast<int32_t>(p->vofs[i + 1] - p->vofs[i]),
-                         static_cast<int32_t>(p->tofs[i + 1] - p->tofs[i]), p->isl[i], bad);
+            const int32_t ni = static_cast<int32_t>(p->vofs[i + 1] - p->vofs[i]);
+            const int32_t ti = static_cast<int32_t>(p->tofs[i + 1] - p->tofs[i]);
+            const auto src = tri_src(i);
+            if (src.second) {
+                const int64_t* tris = static_cast<const int64_t*>(src.first);
+                build_island(tris, ni, ti, p->isl[i], bad);
+                if (!bad) for (int64_t c = 0; c < tn; ++c) p->tri_local[t0 + c] = static_cast<int32_t>(tris[c]);
+            } else {
+                const int32_t* tris = static_cast<const int32_t*>(src.first);
+                build_island(tris, ni, ti, p->isl[i], bad);
+                if (!bad) std::memcpy(p->tri_local.get() + t0, tris, sizeof(int32_t) * static_cast<size_t>(tn));
+            }
             if (bad) anybad = true;
-            else for (int64_t c = 0; c < tn; ++c) p->tri_local[t0 + c] = static_cast<int32_t>(tris[t0 + c]);
         }
     };
     int32_t nt = nthreads > 0 ? nthreads : static_cast<int32_t>(std::thread::hardware_concurrency());
@@ -292,6 +306,23 @@ extern "C" int uva_plan_create(const int64_t* tris, const int64_t* vofs, const i
     }
     *out = p;
     return UVA_OK;
+}
+
+
+extern "C" int uva_plan_create(const int64_t* tris, const int64_t* vofs, const int64_t* tofs, int32_t nc,
+                               int32_t nthreads, uva_plan** out) {
+    if (nc > 0 && vofs && tofs && tofs[nc] > tofs[0] && !tris) { uva_set_error("uva_plan_create: null triangles"); return UVA_E_ARG; }
+    const int64_t base = (nc > 0 && tofs) ? tofs[0] : 0;
+    return plan_create([&](int32_t i) { return std::make_pair(static_cast<const void*>(tris + 3 * (tofs[i] - base)), true); },
+                       vofs, tofs, nc, nthreads, out);
+}
+
+extern "C" int uva_plan_create_charts(const void* const* T, const int8_t* tdt, const int64_t* vofs,
+                                      const int64_t* tofs, int32_t nc, int32_t nthreads, uva_plan** out) {
+    if (nc > 0 && (!T || !tdt)) { uva_set_error("uva_plan_create_charts: bad arguments"); return UVA_E_ARG; }
+    for (int32_t i = 0; i < nc; ++i)
+        if (tdt[i] < 0 || tdt[i] > 1) { uva_set_error("uva_plan_create_charts: dtype codes 0/1"); return UVA_E_ARG; }
+    return plan_create([&](int32_t i) { return std::make_pair(T[i], tdt[i] == 1); }, vofs, tofs, nc, nthreads, out);
 }
 
 extern "C" int uva_plan_sizes(const uva_plan* p, int64_t* s) {
@@ -442,17 +473,18 @@ extern "C" int uva_concat_charts(int32_t nc, const void* const* P, const int8_t*
                                  const int8_t* tdt, const void* const* U, const int8_t* udt, const int64_t* vofs,
                                  const int64_t* tofs, double* P_out, int64_t* T_out, double* U_out,
                                  int32_t nthreads) {
-    if (nc < 0 || (nc > 0 && (!P || !pdt || !T || !tdt || !vofs || !tofs || !P_out || !T_out))) {
+    if (nc < 0 || (nc > 0 && (!P || !pdt || !vofs || !tofs || !P_out || (T_out && (!T || !tdt))))) {
         uva_set_error("uva_concat_charts: bad arguments");
         return UVA_E_ARG;
     }
     for (int32_t i = 0; i < nc; ++i) {
-        if (vofs[i + 1] < vofs[i] || tofs[i + 1] < tofs[i] || pdt[i] < 0 || pdt[i] > 1 || tdt[i] < 0 || tdt[i] > 1 ||
+        if (vofs[i + 1] < vofs[i] || tofs[i + 1] < tofs[i] || pdt[i] < 0 || pdt[i] > 1 ||
+            (T_out && (tdt[i] < 0 || tdt[i] > 1)) ||
             (U && udt && (udt[i] < -1 || udt[i] > 1))) {
             uva_set_error("uva_concat_charts: offsets must be non-decreasing, dtype codes 0/1 (U: -1/0/1)");
             return UVA_E_ARG;
         }
-        if ((vofs[i + 1] > vofs[i] && !P[i]) || (tofs[i + 1] > tofs[i] && !T[i])) {
+        if ((vofs[i + 1] > vofs[i] && !P[i]) || (T_out && tofs[i + 1] > tofs[i] && !T[i])) {
             uva_set_error("uva_concat_charts: null chart array");
             return UVA_E_ARG;
         }
@@ -466,8 +498,10 @@ extern "C" int uva_concat_charts(int32_t nc, const void* const* P, const int8_t*
             const int64_t nv = std::max<int64_t>(vofs[i + 1] - vofs[i], 0), nt = std::max<int64_t>(tofs[i + 1] - tofs[i], 0);
             double* po = P_out + 3 * (vofs[i] - vofs[0]);
             if (pdt[i] == 0) widen<float>(P[i], po, 3 * nv); else std::memcpy(po, P[i], sizeof(double) * 3 * nv);
-            int64_t* to = T_out + 3 * (tofs[i] - tofs[0]);
-            if (tdt[i] == 0) widen<int32_t>(T[i], to, 3 * nt); else std::memcpy(to, T[i], sizeof(int64_t) * 3 * nt);
+            if (T_out) {
+                int64_t* to = T_out + 3 * (tofs[i] - tofs[0]);
+                if (tdt[i] == 0) widen<int32_t>(T[i], to, 3 * nt); else std::memcpy(to, T[i], sizeof(int64_t) * 3 * nt);
+            }
             if (U_out) {
                 double* uo = U_out + 2 * (vofs[i] - vofs[0]);
                 const int8_t d = (U && udt) ? udt[i] : -1;

@@ -13,6 +13,7 @@ triangles.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import threading
 
@@ -61,15 +62,23 @@ _TORCH_OF = {np.dtype(np.int32): torch.int32, np.dtype(np.int64): torch.int64, n
 class Plan:
     """Host topology plan (wraps uva_plan_create / uva_plan_export)."""
 
-    def __init__(self, T_local, vofs, tofs, nthreads=0):
+    def __init__(self, T_local, vofs, tofs, nthreads=0, chart_tris=None):
+        """T_local: concatenated island-local triangles; or None with
+        ``chart_tris`` = (pointer array, dtype code array) of per-chart
+        triangle arrays (uva_plan_create_charts: no concatenation)."""
         L = _lib.lib()
-        T_local = np.ascontiguousarray(T_local, np.int64).reshape(-1, 3)
         vofs = np.ascontiguousarray(vofs, np.int64)
         tofs = np.ascontiguousarray(tofs, np.int64)
         nc = len(vofs) - 1
         h = C.c_void_p()
-        check(L.uva_plan_create(ptr(T_local), ptr(vofs), ptr(tofs), nc, int(nthreads), C.byref(h)),
-              "uva_plan_create")
+        if chart_tris is not None:
+            tp, tdt = chart_tris
+            check(L.uva_plan_create_charts(ptr(tp), ptr(tdt), ptr(vofs), ptr(tofs), nc, int(nthreads), C.byref(h)),
+                  "uva_plan_create")
+        else:
+            T_local = np.ascontiguousarray(T_local, np.int64).reshape(-1, 3)
+            check(L.uva_plan_create(ptr(T_local), ptr(vofs), ptr(tofs), nc, int(nthreads), C.byref(h)),
+                  "uva_plan_create")
         try:
             sz = np.zeros(_lib.PLAN_NSIZES, np.int64)
             check(L.uva_plan_sizes(h, ptr(sz)), "uva_plan_sizes")
@@ -136,11 +145,13 @@ def _chart_array(a, width, codes, fallback):
     return a, codes[a.dtype]
 
 
-def concat_charts(charts, with_uv=True):
+def concat_charts(charts, with_uv=True, with_t=True):
     """(P, T, U) per chart -> concatenated FP64 P, local int64 T, FP64 U, offsets
     (uva_concat_charts copies the charts in parallel; P and U in page-locked
     memory for the uploads). U is None when no chart brings UVs (nothing to
-    upload: the device UVs start at zero)."""
+    upload: the device UVs start at zero). With ``with_t`` False the
+    triangles are not copied: T is then (pointer array, dtype codes, arrays)
+    of the per-chart arrays for Plan(chart_tris=...)."""
     nc = len(charts)
     Ps, Ts, Us = [], [], []
     pdt = np.empty(max(nc, 1), np.int8)
@@ -162,7 +173,7 @@ def concat_charts(charts, with_uv=True):
                 raise ValueError(f"chart {i}: U has {len(u)} rows for {len(a)} vertices")
         Us.append(u)
     P = host_empty((int(vofs[-1]), 3), np.float64)
-    T = np.empty((int(tofs[-1]), 3), np.int64)
+    T = np.empty((int(tofs[-1]), 3), np.int64) if with_t else None
     any_uv = bool((udt[:nc] >= 0).any()) if nc else False
     U = host_empty((int(vofs[-1]), 2), np.float64) if any_uv else None
     if nc:
@@ -170,8 +181,12 @@ def concat_charts(charts, with_uv=True):
         tp = np.array([x.ctypes.data for x in Ts], np.uintp)
         up_ = np.array([0 if x is None else x.ctypes.data for x in Us], np.uintp)
         check(_lib.lib().uva_concat_charts(nc, ptr(pp), ptr(pdt), ptr(tp), ptr(tdt), ptr(up_), ptr(udt), ptr(vofs),
-                                           ptr(tofs), ptr(P), ptr(T), ptr(U) if U is not None else None, 0),
+                                           ptr(tofs), ptr(P), ptr(T) if T is not None else None,
+                                           ptr(U) if U is not None else None, 0),
               "uva_concat_charts")
+    if not with_t:
+        tp = np.array([x.ctypes.data for x in Ts], np.uintp) if nc else np.zeros(1, np.uintp)
+        T = (tp, tdt, Ts)   # Ts keeps the arrays alive while the plan reads them
     return P, T, U, vofs, tofs
 
 
@@ -190,67 +205,72 @@ class DeviceBatch:
         tuned = autotune.lookup(plan, self.dev)
         if tuned is not None:
             plan.set_classes(tuned["mid"], tuned["small"])
-        self.nc, self.n, self.t = plan.nc, plan.n, plan.t
-        d = self.dev
+        # every copy and fill below runs on the batch stream, like its kernels
+        with (torch.cuda.stream(self.stream) if self.stream is not None else contextlib.nullcontext()):
+            self.nc, self.n, self.t = plan.nc, plan.n, plan.t
+            d = self.dev
 
-        self.h2d_bytes = 0   # bytes copied host -> device by this constructor
+            self.h2d_bytes = 0   # bytes copied host -> device by this constructor
 
-        def up(a, dtype=None):
-            t = torch.from_numpy(np.ascontiguousarray(a))
-            if t.numel() == 0:
-                t = torch.zeros(1, dtype=t.dtype)
-            self.h2d_bytes += t.numel() * t.element_size()
-            # page-locked sources (the plan's arrays) copy asynchronously on
-            # the current stream; the plan keeps them alive
-            nb = t.is_pinned()
-            return t.to(d, non_blocking=nb) if dtype is None else t.to(d, dtype, non_blocking=nb)
+            def up(a, dtype=None):
+                t = torch.from_numpy(np.ascontiguousarray(a))
+                if t.numel() == 0:
+                    t = torch.zeros(1, dtype=t.dtype)
+                self.h2d_bytes += t.numel() * t.element_size()
+                # page-locked sources (the plan's arrays) copy asynchronously on
+                # the current stream; the plan keeps them alive
+                nb = t.is_pinned()
+                return t.to(d, non_blocking=nb) if dtype is None else t.to(d, dtype, non_blocking=nb)
 
-        # topology
-        self.vofs = up(plan.vofs); self.tofs = up(plan.tofs); self.sofs = up(plan.sofs)
-        self.tri4 = up(plan.tri4); self.tri_edge = up(plan.tri_edge)
-        self.slice_ptr = up(plan.slice_ptr); self.slot_col = up(plan.slot_col)
-        self.slot_edge = up(plan.slot_edge); self.slot_c = up(plan.slot_c)
-        self.vt_ptr = up(plan.vt_ptr); self.vt = up(plan.vt); self.vflags = up(plan.vflags)
-        self.bofs = up(plan.bofs); self.bverts = up(plan.bverts); self.order = up(plan.order)
-        self.row_vert = up(plan.row_vert); self.vert_row = up(plan.vert_row)
-        self.agg_rows = up(plan.agg_rows); self.cofs = up(plan.cofs)
-        # geometry
-        n, t, nc = max(self.n, 1), max(self.t, 1), max(self.nc, 1)
-        f64, f32 = torch.float64, torch.float32
-        # asynchronous uploads read page-locked host memory until they finish:
-        # the batch keeps its host sources alive (the plan holds the rest)
-        self._host_src = (P, U)
-        self.P = up(np.asarray(P, np.float64).reshape(-1, 3)) if self.n else torch.zeros((1, 3), dtype=f64, device=d)
-        self.frame = torch.empty((t, 4), dtype=f64, device=d)
-        self.wtri = torch.empty((t, 4), dtype=f64, device=d)
-        self.tscale = torch.ones(t, dtype=f32, device=d)
-        self.wedge = torch.empty(max(plan.E, 1), dtype=f64, device=d)
-        self.slot_cw = torch.empty((max(plan.nslots, 1), 2), dtype=torch.int32, device=d)
-        self.wdiag = torch.empty(n, dtype=f64, device=d)
-        nco = max(plan.ncoarse, 1)
-        self.coarse_a = torch.empty(nco, dtype=f32, device=d)
-        self.coarse_l = torch.empty(4 * nco, dtype=f32, device=d)
-        self.coarse_work = torch.empty(4 * nco, dtype=f64, device=d)
-        self.cpart = torch.empty(2 * max(plan.nslices, 1), dtype=f32, device=d)
-        self.dinv = torch.empty(n, dtype=f32, device=d)
-        self.pins = torch.zeros((nc, 3), dtype=torch.int32, device=d)
-        self.wpin = torch.empty(nc, dtype=f64, device=d)
-        if U is None:
-            self.U = torch.zeros((n, 2), dtype=f64, device=d)
-        else:
-            self.U = up(np.asarray(U, np.float64).reshape(-1, 2)) if self.n else torch.zeros((1, 2), dtype=f64, device=d)
-        m = max(n, nc)
-        self.x64 = torch.empty((m, 2), dtype=f64, device=d)
-        self.b64 = torch.empty((m, 2), dtype=f64, device=d)
-        self.rc = torch.empty((t, 3, 2), dtype=f64, device=d)
-        self.r32 = torch.empty((n, 2), dtype=f32, device=d)
-        self.d32 = torch.empty((n, 2), dtype=f32, device=d)
-        self.p32 = torch.empty((n, 2), dtype=f32, device=d)
-        self.q32 = torch.empty((n, 2), dtype=f32, device=d)
-        self.hist = torch.empty((8, n, 2), dtype=f32, device=d)   # ARAP start history (4 updates, A d)
-        self.status = torch.zeros((nc, C.sizeof(_lib.IslandStatus)), dtype=torch.uint8, device=d)
-        self.work = torch.zeros(8, dtype=torch.int32, device=d)
-        self.rev_ctas = tuned["rev_ctas"] if tuned is not None else 0   # schedule knob (autotune.tune)
+            # topology
+            self.vofs = up(plan.vofs); self.tofs = up(plan.tofs); self.sofs = up(plan.sofs)
+            self.tri4 = up(plan.tri4); self.tri_edge = up(plan.tri_edge)
+            self.slice_ptr = up(plan.slice_ptr); self.slot_col = up(plan.slot_col)
+            self.slot_edge = up(plan.slot_edge); self.slot_c = up(plan.slot_c)
+            self.vt_ptr = up(plan.vt_ptr); self.vt = up(plan.vt); self.vflags = up(plan.vflags)
+            self.bofs = up(plan.bofs); self.bverts = up(plan.bverts); self.order = up(plan.order)
+            self.row_vert = up(plan.row_vert); self.vert_row = up(plan.vert_row)
+            self.agg_rows = up(plan.agg_rows); self.cofs = up(plan.cofs)
+            # geometry
+            n, t, nc = max(self.n, 1), max(self.t, 1), max(self.nc, 1)
+            f64, f32 = torch.float64, torch.float32
+            # asynchronous uploads read page-locked host memory until they finish:
+            # the batch keeps its host sources alive (the plan holds the rest)
+            self._host_src = (P, U)
+            if isinstance(P, torch.Tensor) and P.is_cuda:   # already on the device (uploaded by the caller)
+                self.P = P.to(d, f64).reshape(-1, 3)
+            else:
+                self.P = up(np.asarray(P, np.float64).reshape(-1, 3)) if self.n else torch.zeros((1, 3), dtype=f64, device=d)
+            self.frame = torch.empty((t, 4), dtype=f64, device=d)
+            self.wtri = torch.empty((t, 4), dtype=f64, device=d)
+            self.tscale = torch.ones(t, dtype=f32, device=d)
+            self.wedge = torch.empty(max(plan.E, 1), dtype=f64, device=d)
+            self.slot_cw = torch.empty((max(plan.nslots, 1), 2), dtype=torch.int32, device=d)
+            self.wdiag = torch.empty(n, dtype=f64, device=d)
+            nco = max(plan.ncoarse, 1)
+            self.coarse_a = torch.empty(nco, dtype=f32, device=d)
+            self.coarse_l = torch.empty(4 * nco, dtype=f32, device=d)
+            self.coarse_work = torch.empty(4 * nco, dtype=f64, device=d)
+            self.cpart = torch.empty(2 * max(plan.nslices, 1), dtype=f32, device=d)
+            self.dinv = torch.empty(n, dtype=f32, device=d)
+            self.pins = torch.zeros((nc, 3), dtype=torch.int32, device=d)
+            self.wpin = torch.empty(nc, dtype=f64, device=d)
+            if U is None:
+                self.U = torch.zeros((n, 2), dtype=f64, device=d)
+            else:
+                self.U = up(np.asarray(U, np.float64).reshape(-1, 2)) if self.n else torch.zeros((1, 2), dtype=f64, device=d)
+            m = max(n, nc)
+            self.x64 = torch.empty((m, 2), dtype=f64, device=d)
+            self.b64 = torch.empty((m, 2), dtype=f64, device=d)
+            self.rc = torch.empty((t, 3, 2), dtype=f64, device=d)
+            self.r32 = torch.empty((n, 2), dtype=f32, device=d)
+            self.d32 = torch.empty((n, 2), dtype=f32, device=d)
+            self.p32 = torch.empty((n, 2), dtype=f32, device=d)
+            self.q32 = torch.empty((n, 2), dtype=f32, device=d)
+            self.hist = torch.empty((8, n, 2), dtype=f32, device=d)   # ARAP start history (4 updates, A d)
+            self.status = torch.zeros((nc, C.sizeof(_lib.IslandStatus)), dtype=torch.uint8, device=d)
+            self.work = torch.zeros(8, dtype=torch.int32, device=d)
+            self.rev_ctas = tuned["rev_ctas"] if tuned is not None else 0   # schedule knob (autotune.tune)
         self.desc = self._make_desc()
         self.setup()
 

@@ -16,11 +16,13 @@ Batch without a CUDA device raises RuntimeError.
 """
 from __future__ import annotations
 
+import contextlib
+
 import numpy as np
 import torch
 
 from .. import _lib
-from ..device import DeviceBatch, concat_charts, require_cuda
+from ..device import DeviceBatch, Plan, concat_charts, require_cuda
 
 
 def csr32(A):
@@ -83,12 +85,22 @@ class Batch:
     def __init__(self, charts, dev=None, dtype=torch.float32, stream=None):
         self.dev = require_cuda(dev if dev is not None else device())
         self.dt = dtype
-        P, T, U, vofs, tofs = concat_charts(charts)
+        # positions (and UVs) are concatenated; the topology plan reads every
+        # chart's triangles where they are, and the positions' upload runs
+        # while the plan is built
+        P, Tc, U, vofs, tofs = concat_charts(charts, with_t=False)
         self.nc = len(charts)
         self.offsets = vofs.copy()
         self.n = int(vofs[-1])
         self._tofs = tofs
-        self.db = DeviceBatch(P, T, vofs, tofs, U=U, semantics=_lib.SEM_BATCH, device=self.dev, stream=stream)
+        with (torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()):
+            P_dev = torch.from_numpy(P).to(self.dev, non_blocking=True) if self.n else None
+        plan = Plan(None, vofs, tofs, chart_tris=Tc[:2])
+        self.db = DeviceBatch(P_dev if P_dev is not None else P, None, vofs, tofs, U=U, semantics=_lib.SEM_BATCH,
+                              device=self.dev, stream=stream, plan=plan)
+        self.db._host_src = (P, U)          # the asynchronous copies read these until they finish
+        if P_dev is not None:
+            self.db.h2d_bytes += P.nbytes
         self.last_status = None
 
     # ------------------------------------------------------------ attributes
