@@ -108,6 +108,16 @@ int uva_plan_sizes(const uva_plan* plan, int64_t* sizes /* UVA_PLAN_NSIZES */);
 int uva_plan_export(const uva_plan* plan, int32_t* tri4, int32_t* tri_edge, int32_t* sofs,
                     int32_t* slice_ptr, int32_t* slot_col, int32_t* slot_edge, float* slot_c,
                     int32_t* vt_ptr, int32_t* vt, uint8_t* vflags, int32_t* bofs, int32_t* bverts);
+/* The same for islands [i0, i1) only, into the same full-size arrays (each
+ * island's entries land in its own ranges; the closing offsets are written
+ * with the range that ends at nc), so a caller can copy finished ranges to
+ * the device while the next range is exported. The ranges of island i:
+ * uva_plan_island_offsets (3*(nc+1) int64: first slice, first slot, first
+ * boundary vertex of every island, then the totals).                       */
+int uva_plan_export_range(const uva_plan* plan, int32_t i0, int32_t i1, int32_t* tri4, int32_t* tri_edge,
+                          int32_t* sofs, int32_t* slice_ptr, int32_t* slot_col, int32_t* slot_edge, float* slot_c,
+                          int32_t* vt_ptr, int32_t* vt, uint8_t* vflags, int32_t* bofs, int32_t* bverts);
+int uva_plan_island_offsets(const uva_plan* plan, int64_t* out);
 /* Solver row order (island-local): row_vert / vert_row (n each), rows per
  * coarse aggregate per island (0: none) and offsets of each island's m*m
  * coarse block (nc+1). Rows are grouped in compact breadth-first blobs of

@@ -233,3 +233,29 @@ def test_plan_from_chart_arrays_matches_concatenated():
     _, Tb, _, vb, tb = concat_charts(bad, with_t=False)
     with pytest.raises(ValueError):
         Plan(None, vb, tb, chart_tris=Tb[:2])
+
+
+def test_plan_range_export_matches_full_export():
+    """uva_plan_export_range over consecutive island ranges writes the same
+    arrays as one uva_plan_export (the ranges a device copy pipeline uses)."""
+    import ctypes as C
+    from ultimate_uv_artist_b200 import _lib, synth
+    from ultimate_uv_artist_b200.device import Plan, concat_charts
+    isl = synth.uneven_islands(seed=62, count=25, tmin=20, tmax=3000)
+    P, T, _, vofs, tofs = concat_charts([(p, t) for p, t in isl], with_uv=False)
+    full = Plan(T, vofs, tofs)
+    L = _lib.lib()
+    Tl = np.ascontiguousarray(T, np.int64)
+    v64, t64 = np.ascontiguousarray(vofs, np.int64), np.ascontiguousarray(tofs, np.int64)
+    h = C.c_void_p()
+    _lib.check(L.uva_plan_create(_lib.ptr(Tl), _lib.ptr(v64), _lib.ptr(t64), len(vofs) - 1, 0, C.byref(h)), "create")
+    out = {k: np.full_like(getattr(full, k), 77) for k in Plan.EXPORTED}
+    args = [_lib.ptr(out[k]) for k in Plan.EXPORTED]
+    for i0, i1 in ((0, 7), (7, 8), (8, 20), (20, 25)):
+        _lib.check(L.uva_plan_export_range(h, i0, i1, *args), "export_range")
+    off = np.zeros(3 * 26, np.int64)
+    _lib.check(L.uva_plan_island_offsets(h, _lib.ptr(off)), "offsets")
+    L.uva_plan_destroy(h)
+    for k in Plan.EXPORTED:
+        assert np.array_equal(out[k], getattr(full, k)), k
+    assert np.array_equal(off[:26], full.sofs) and np.array_equal(off[52:], full.bofs)

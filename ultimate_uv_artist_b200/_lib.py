@@ -78,6 +78,8 @@ _SIGS = {
     "uva_plan_create_charts": [vp, vp, vp, vp, i32, i32, vp],
     "uva_plan_sizes": [vp, vp],
     "uva_plan_export": [vp] * 13,
+    "uva_plan_export_range": [vp, i32, i32] + [vp] * 12,
+    "uva_plan_island_offsets": [vp, vp],
     "uva_plan_export_rows": [vp] * 5,
     "uva_plan_destroy": [vp],
     "uva_concat_charts": [i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32],

@@ -338,14 +338,36 @@ extern "C" int uva_plan_export(const uva_plan* p, int32_t* tri4, int32_t* tri_ed
                                int32_t* slice_ptr, int32_t* slot_col, int32_t* slot_edge, float* slot_c,
                                int32_t* vt_ptr, int32_t* vt, uint8_t* vflags, int32_t* bofs, int32_t* bverts) {
     if (!p) { uva_set_error("uva_plan_export: null plan"); return UVA_E_ARG; }
+    return uva_plan_export_range(p, 0, p->nc, tri4, tri_edge, sofs, slice_ptr, slot_col, slot_edge, slot_c, vt_ptr,
+                                 vt, vflags, bofs, bverts);
+}
+
+extern "C" int uva_plan_island_offsets(const uva_plan* p, int64_t* out) {
+    if (!p || !out) { uva_set_error("uva_plan_island_offsets: null argument"); return UVA_E_ARG; }
     const int32_t nc = p->nc;
+    for (int32_t i = 0; i <= nc; ++i) {
+        out[i] = p->sofs[i];
+        out[(nc + 1) + i] = p->slotofs[i];
+        out[2 * (nc + 1) + i] = p->bofs[i];
+    }
+    return UVA_OK;
+}
+
+extern "C" int uva_plan_export_range(const uva_plan* p, int32_t i0, int32_t i1, int32_t* tri4, int32_t* tri_edge,
+                                     int32_t* sofs, int32_t* slice_ptr, int32_t* slot_col, int32_t* slot_edge,
+                                     float* slot_c, int32_t* vt_ptr, int32_t* vt, uint8_t* vflags, int32_t* bofs,
+                                     int32_t* bverts) {
+    if (!p) { uva_set_error("uva_plan_export: null plan"); return UVA_E_ARG; }
+    const int32_t nc = p->nc;
+    if (i0 < 0 || i1 < i0 || i1 > nc) { uva_set_error("uva_plan_export_range: bad island range"); return UVA_E_ARG; }
     const int64_t v0 = p->vofs.empty() ? 0 : p->vofs[0];
     const int64_t t0 = p->tofs.empty() ? 0 : p->tofs[0];
     // islands are independent: every array of island i lands in its own
     // range, so workers take islands from a shared counter, largest first
-    std::vector<int32_t> order(nc);
-    std::iota(order.begin(), order.end(), 0);
+    std::vector<int32_t> order(i1 - i0);
+    std::iota(order.begin(), order.end(), i0);
     std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return p->isl[a].t > p->isl[b].t; });
+    const int32_t cnt_isl = i1 - i0;
     std::atomic<int32_t> next{0};
     auto one = [&](int32_t i) {
         const IslandPlan& ip = p->isl[i];
@@ -410,20 +432,22 @@ extern "C" int uva_plan_export(const uva_plan* p, int32_t* tri4, int32_t* tri_ed
     auto worker = [&]() {
         for (;;) {
             const int32_t q = next.fetch_add(1);
-            if (q >= nc) break;
+            if (q >= cnt_isl) break;
             one(order[q]);
         }
     };
     int32_t nt = static_cast<int32_t>(std::thread::hardware_concurrency());
-    nt = std::max(1, std::min(nt, std::max(nc, 1)));
+    nt = std::max(1, std::min(nt, std::max(cnt_isl, 1)));
     std::vector<std::thread> pool;
     for (int32_t k = 1; k < nt; ++k) pool.emplace_back(worker);
     worker();
     for (auto& th : pool) th.join();
-    if (sofs) sofs[nc] = static_cast<int32_t>(p->nslices);
-    slice_ptr[p->nslices] = static_cast<int32_t>(p->nslots);
-    if (bofs) bofs[nc] = static_cast<int32_t>(p->nbverts);
-    vt_ptr[p->n] = static_cast<int32_t>(3 * p->t);
+    if (i1 == nc) {   // the closing offsets, with the last range
+        if (sofs) sofs[nc] = static_cast<int32_t>(p->nslices);
+        slice_ptr[p->nslices] = static_cast<int32_t>(p->nslots);
+        if (bofs) bofs[nc] = static_cast<int32_t>(p->nbverts);
+        vt_ptr[p->n] = static_cast<int32_t>(3 * p->t);
+    }
     return UVA_OK;
 }
 

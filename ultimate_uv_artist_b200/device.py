@@ -62,10 +62,19 @@ _TORCH_OF = {np.dtype(np.int32): torch.int32, np.dtype(np.int64): torch.int64, n
 class Plan:
     """Host topology plan (wraps uva_plan_create / uva_plan_export)."""
 
-    def __init__(self, T_local, vofs, tofs, nthreads=0, chart_tris=None):
+    # the arrays uva_plan_export writes, island by island
+    EXPORTED = ("tri4", "tri_edge", "sofs", "slice_ptr", "slot_col", "slot_edge", "slot_c", "vt_ptr", "vt", "vflags",
+                "bofs", "bverts")
+
+    def __init__(self, T_local, vofs, tofs, nthreads=0, chart_tris=None, device=None, stream=None, chunks=4):
         """T_local: concatenated island-local triangles; or None with
         ``chart_tris`` = (pointer array, dtype code array) of per-chart
-        triangle arrays (uva_plan_create_charts: no concatenation)."""
+        triangle arrays (uva_plan_create_charts: no concatenation).
+
+        With ``device``, the plan's arrays are also copied to that device
+        (``dev_arrays``): the export runs in ``chunks`` island ranges and the
+        copies of each finished range run on ``stream`` while the next range
+        is exported."""
         L = _lib.lib()
         vofs = np.ascontiguousarray(vofs, np.int64)
         tofs = np.ascontiguousarray(tofs, np.int64)
@@ -79,6 +88,7 @@ class Plan:
             T_local = np.ascontiguousarray(T_local, np.int64).reshape(-1, 3)
             check(L.uva_plan_create(ptr(T_local), ptr(vofs), ptr(tofs), nc, int(nthreads), C.byref(h)),
                   "uva_plan_create")
+        self.dev_arrays = None
         try:
             sz = np.zeros(_lib.PLAN_NSIZES, np.int64)
             check(L.uva_plan_sizes(h, ptr(sz)), "uva_plan_sizes")
@@ -97,10 +107,11 @@ class Plan:
             self.vflags = host_empty(self.n, np.uint8)
             self.bofs = host_empty(nc + 1, np.int32)
             self.bverts = host_empty(max(self.nbverts, 1), np.int32)
-            check(L.uva_plan_export(h, ptr(self.tri4), ptr(self.tri_edge), ptr(self.sofs), ptr(self.slice_ptr),
-                                    ptr(self.slot_col), ptr(self.slot_edge), ptr(self.slot_c), ptr(self.vt_ptr),
-                                    ptr(self.vt), ptr(self.vflags), ptr(self.bofs), ptr(self.bverts)),
-                  "uva_plan_export")
+            args = [ptr(getattr(self, k)) for k in self.EXPORTED]
+            if device is None or nc == 0:
+                check(L.uva_plan_export(h, *args), "uva_plan_export")
+            else:
+                self._export_to_device(L, h, args, vofs, tofs, device, stream, max(int(chunks), 1))
             self.row_vert = host_empty(max(self.n, 1), np.int32)
             self.vert_row = host_empty(max(self.n, 1), np.int32)
             self.agg_rows = host_empty(max(nc, 1), np.int32)
@@ -116,6 +127,33 @@ class Plan:
         # island work order: grouped by size class (whole CTA with global or
         # shared-memory vectors, 256-thread sub-team, warp), largest first
         self.set_classes(_lib.CLASS_MID, _lib.CLASS_SMALL)
+
+    def _export_to_device(self, L, h, args, vofs, tofs, device, stream, chunks):
+        """Export island ranges of about equal triangle counts and copy each
+        finished range (page-locked, asynchronous) to its device arrays."""
+        nc = self.nc
+        off = np.zeros(3 * (nc + 1), np.int64)
+        check(L.uva_plan_island_offsets(h, ptr(off)), "uva_plan_island_offsets")
+        so, sl, bo = off[:nc + 1], off[nc + 1:2 * (nc + 1)], off[2 * (nc + 1):]
+        vr, tr = vofs - int(vofs[0]), tofs - int(tofs[0])
+        # first element of island i in every exported array
+        starts = {"tri4": 4 * tr, "tri_edge": 3 * tr, "sofs": np.arange(nc + 1), "slice_ptr": so, "slot_col": sl,
+                  "slot_edge": sl, "slot_c": sl, "vt_ptr": vr, "vt": 3 * tr, "vflags": vr, "bofs": np.arange(nc + 1),
+                  "bverts": bo}
+        closing = {"sofs", "slice_ptr", "vt_ptr", "bofs"}   # one entry past the last island
+        dev = {k: torch.empty(max(getattr(self, k).size, 1), dtype=_TORCH_OF[getattr(self, k).dtype], device=device)
+               for k in self.EXPORTED}
+        cuts = np.searchsorted(tr, np.linspace(0, tr[-1], chunks + 1)[1:-1])
+        bounds = [0] + sorted(set(int(c) for c in cuts if 0 < c < nc)) + [nc]
+        ctx = torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()
+        for i0, i1 in zip(bounds[:-1], bounds[1:]):
+            check(L.uva_plan_export_range(h, i0, i1, *args), "uva_plan_export_range")
+            with ctx:
+                for k in self.EXPORTED:
+                    a, b = int(starts[k][i0]), int(starts[k][i1]) + (1 if (k in closing and i1 == nc) else 0)
+                    if b > a:
+                        dev[k][a:b].copy_(torch.from_numpy(getattr(self, k).reshape(-1)[a:b]), non_blocking=True)
+        self.dev_arrays = {k: v.view(getattr(self, k).shape) if getattr(self, k).size else v for k, v in dev.items()}
 
     def set_classes(self, mid, small):
         """Island work order for team thresholds ``mid`` (whole CTA above) and
@@ -223,12 +261,14 @@ class DeviceBatch:
                 return t.to(d, non_blocking=nb) if dtype is None else t.to(d, dtype, non_blocking=nb)
 
             # topology
-            self.vofs = up(plan.vofs); self.tofs = up(plan.tofs); self.sofs = up(plan.sofs)
-            self.tri4 = up(plan.tri4); self.tri_edge = up(plan.tri_edge)
-            self.slice_ptr = up(plan.slice_ptr); self.slot_col = up(plan.slot_col)
-            self.slot_edge = up(plan.slot_edge); self.slot_c = up(plan.slot_c)
-            self.vt_ptr = up(plan.vt_ptr); self.vt = up(plan.vt); self.vflags = up(plan.vflags)
-            self.bofs = up(plan.bofs); self.bverts = up(plan.bverts); self.order = up(plan.order)
+            self.vofs = up(plan.vofs); self.tofs = up(plan.tofs); self.order = up(plan.order)
+            pd = plan.dev_arrays if plan.dev_arrays is not None and plan.dev_arrays['tri4'].device == d else None
+            for k in Plan.EXPORTED:   # copied during the plan's export, or now
+                if pd is not None:
+                    setattr(self, k, pd[k] if pd[k].numel() else torch.zeros(1, dtype=pd[k].dtype, device=d))
+                    self.h2d_bytes += pd[k].numel() * pd[k].element_size()
+                else:
+                    setattr(self, k, up(getattr(plan, k)))
             self.row_vert = up(plan.row_vert); self.vert_row = up(plan.vert_row)
             self.agg_rows = up(plan.agg_rows); self.cofs = up(plan.cofs)
             # geometry
