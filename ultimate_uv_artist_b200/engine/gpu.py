@@ -86,8 +86,9 @@ class Batch:
         self.dev = require_cuda(dev if dev is not None else device())
         self.dt = dtype
         # positions (and UVs) are concatenated; the topology plan reads every
-        # chart's triangles where they are, and the positions' upload runs
-        # while the plan is built
+        # chart's triangles where they are; the positions' upload runs while
+        # the plan is built, and each finished range of the plan's arrays is
+        # copied while the next one is exported
         P, Tc, U, vofs, tofs = concat_charts(charts, with_t=False)
         self.nc = len(charts)
         self.offsets = vofs.copy()
@@ -95,7 +96,7 @@ class Batch:
         self._tofs = tofs
         with (torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()):
             P_dev = torch.from_numpy(P).to(self.dev, non_blocking=True) if self.n else None
-        plan = Plan(None, vofs, tofs, chart_tris=Tc[:2])
+        plan = Plan(None, vofs, tofs, chart_tris=Tc[:2], device=self.dev, stream=stream)   # export || copies
         self.db = DeviceBatch(P_dev if P_dev is not None else P, None, vofs, tofs, U=U, semantics=_lib.SEM_BATCH,
                               device=self.dev, stream=stream, plan=plan)
         self.db._host_src = (P, U)          # the asynchronous copies read these until they finish
