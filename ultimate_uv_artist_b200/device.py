@@ -195,35 +195,39 @@ def concat_charts(charts, with_uv=True, with_t=True):
     pdt = np.empty(max(nc, 1), np.int8)
     tdt = np.empty(max(nc, 1), np.int8)
     udt = np.full(max(nc, 1), -1, np.int8)
-    vofs = np.zeros(nc + 1, np.int64)
-    tofs = np.zeros(nc + 1, np.int64)
+    nvs, nts = [], []
+    any_uv = False
     for i, ch in enumerate(charts):
         a, pdt[i] = _chart_array(ch[0], 3, _FLOAT_CODE, np.float64)
         t, tdt[i] = _chart_array(ch[1], 3, _INT_CODE, np.int64)
         Ps.append(a)
         Ts.append(t)
-        vofs[i + 1] = vofs[i] + len(a)
-        tofs[i + 1] = tofs[i] + len(t)
+        nvs.append(a.shape[0])
+        nts.append(t.shape[0])
         u = None
         if with_uv and len(ch) > 2 and ch[2] is not None:
             u, udt[i] = _chart_array(ch[2], 2, _FLOAT_CODE, np.float64)
             if len(u) != len(a):
                 raise ValueError(f"chart {i}: U has {len(u)} rows for {len(a)} vertices")
+            any_uv = True
         Us.append(u)
+    vofs = np.zeros(nc + 1, np.int64)
+    tofs = np.zeros(nc + 1, np.int64)
+    if nc:
+        np.cumsum(nvs, out=vofs[1:])
+        np.cumsum(nts, out=tofs[1:])
     P = host_empty((int(vofs[-1]), 3), np.float64)
     T = np.empty((int(tofs[-1]), 3), np.int64) if with_t else None
-    any_uv = bool((udt[:nc] >= 0).any()) if nc else False
     U = host_empty((int(vofs[-1]), 2), np.float64) if any_uv else None
+    tp = np.fromiter((x.ctypes.data for x in Ts), np.uintp, nc) if nc else np.zeros(1, np.uintp)
     if nc:
-        pp = np.array([x.ctypes.data for x in Ps], np.uintp)
-        tp = np.array([x.ctypes.data for x in Ts], np.uintp)
-        up_ = np.array([0 if x is None else x.ctypes.data for x in Us], np.uintp)
-        check(_lib.lib().uva_concat_charts(nc, ptr(pp), ptr(pdt), ptr(tp), ptr(tdt), ptr(up_), ptr(udt), ptr(vofs),
-                                           ptr(tofs), ptr(P), ptr(T) if T is not None else None,
-                                           ptr(U) if U is not None else None, 0),
+        pp = np.fromiter((x.ctypes.data for x in Ps), np.uintp, nc)
+        up_ = np.fromiter((0 if x is None else x.ctypes.data for x in Us), np.uintp, nc) if any_uv else None
+        check(_lib.lib().uva_concat_charts(nc, ptr(pp), ptr(pdt), ptr(tp), ptr(tdt), ptr(up_) if any_uv else None,
+                                           ptr(udt) if any_uv else None, ptr(vofs), ptr(tofs), ptr(P),
+                                           ptr(T) if T is not None else None, ptr(U) if U is not None else None, 0),
               "uva_concat_charts")
     if not with_t:
-        tp = np.array([x.ctypes.data for x in Ts], np.uintp) if nc else np.zeros(1, np.uintp)
         T = (tp, tdt, Ts)   # Ts keeps the arrays alive while the plan reads them
     return P, T, U, vofs, tofs
 
