@@ -63,3 +63,27 @@ def test_solver_layout_groups_charts(gh):
     bad[0, 0] = G["CV"][np.nonzero(G["chart"] != G["chart"][0])[0][0], 0]   # a vertex of another chart
     with pytest.raises(ValueError):
         S._layout(G["faces"], bad, G["nv"], G["chart"], G["nchart"])
+
+
+def test_mesh_charts_workload_is_consistent():
+    """synth.mesh_charts (the bench's hier.Solver workload): face adjacency
+    across each corner edge, chart-private UV vertices, and the oracle's
+    chart topology (one boundary loop, disk charts) on a small instance."""
+    from oracle import segments as OS
+    from ultimate_uv_artist_b200 import synth
+    V, F, FF, faces, loc, chart, CV, nv, nchart, U0 = synth.mesh_charts(nx=24, ny=16, block=8)
+    owner = {}
+    for f, (a, b, c) in enumerate(F.tolist()):
+        for u, v in ((a, b), (b, c), (c, a)):
+            owner[(u, v)] = f
+    for f, (a, b, c) in enumerate(F.tolist()):
+        for k, (u, v) in enumerate(((a, b), (b, c), (c, a))):
+            assert FF[f, k] == owner.get((v, u), -1)
+    vch = -np.ones(nv, np.int64)
+    for i in range(len(CV)):
+        for v in CV[i]:
+            assert vch[v] in (-1, chart[i])
+            vch[v] = chart[i]
+    assert nchart == 6 and U0.shape == (nv, 2) and np.isfinite(U0).all()
+    col, chi, loops = OS.chart_checks(F, FF, faces, loc, chart, CV, U0, nchart, nv)
+    assert (chi == 1).all() and (loops == 1).all()
