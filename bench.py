@@ -25,6 +25,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -75,7 +76,7 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"uva_bench_clocks_{os.getpid()}_{index}.csv")
 
     def start(self):
         try:
@@ -121,6 +122,10 @@ class Clocks:
                 for nm, val in zip(names, parts[5:9]):
                     if val.lower().startswith("active"):
                         reasons.add(nm)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
 

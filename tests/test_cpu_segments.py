@@ -60,7 +60,7 @@ def test_hier_topology_matches_reference(gs, s):
     g = {k[3:]: gs[k] for k in gs.files if k.startswith(f"h{s}_")}
     ba, bb = hier.boundary_directed(g["F"], g["FF"], g["faces"], g["loc"], g["chart"], g["CV"])
     assert np.array_equal(ba, g["ba"]) and np.array_equal(bb, g["bb"])
-    chi, loops, ba2, bb2, bc = hier.chart_topology(g["F"], g["FF"], g["faces"], g["loc"], g["chart"], g["CV"],
+    chi, loops, ba2, bb2, bc = hier._boundary_topology(g["F"], g["FF"], g["faces"], g["loc"], g["chart"], g["CV"],
                                                    int(g["nchart"][0]), int(g["nv"][0]))
     assert np.array_equal(chi, g["chi"]) and np.array_equal(loops, g["loops"])
     assert len(ba2) == len(g["ba"]) and bc.min() >= 0
@@ -76,5 +76,5 @@ def test_hier_loops_mixed_components():
     faces = np.array([0, 1]); loc = np.array([0, 1]); chart = np.array([0, 1])
     CV = np.array([[0, 1, 2], [1, 3, 2]]); UV = np.zeros((4, 2))
     want = o.chart_checks(F, FF, faces, loc, chart, CV, UV, 2, 4)
-    chi, loops, *_ = hier.chart_topology(F, FF, faces, loc, chart, CV, 2, 4)
+    chi, loops, *_ = hier._boundary_topology(F, FF, faces, loc, chart, CV, 2, 4)
     assert np.array_equal(chi, want[1]) and np.array_equal(loops, want[2])

@@ -18,12 +18,22 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12   # same kernel, same per-island arithmetic: agreement to round-off
 
 
+# the caller's solver scratch, which the entry point must not read: a caller
+# without device scratch passes null for all of it
+SCRATCH_FIELDS = ("work", "cpart", "x64", "b64", "rc", "r32", "d32", "p32", "q32", "hist")
+
+
 def _batch():
     from ultimate_uv_artist_b200 import synth
     from ultimate_uv_artist_b200.device import DeviceBatch, concat_charts
+    rng = np.random.default_rng(516)
     isl = synth.uneven_islands(seed=515, count=10, tmin=20, tmax=4000)
+    # one island above UVA_CLASS_BIG (8,192 vertices): a whole CTA with its CG
+    # vectors in global memory, here in the static array
+    isl.append(synth.disk_patch(rng, 25000))
     P, T, _, vofs, tofs = concat_charts([(p, t) for p, t in isl], with_uv=False)
     assert vofs[-1] <= 32768 and tofs[-1] <= 65536
+    assert int(np.diff(vofs).max()) > 8192
     db = DeviceBatch(P, T, vofs, tofs)
     db.lscm()
     return db, vofs
@@ -45,6 +55,8 @@ def test_noalloc_matches_allocating_entry_point(cuda):
         status = torch.zeros_like(db.status)
         desc = _lib.BatchDesc.from_buffer_copy(db.desc)
         desc.status = status.data_ptr()
+        for f in SCRATCH_FIELDS:
+            setattr(desc, f, None)
         _lib.check(L.uva_arap_noalloc(C.byref(desc), C.byref(prm), stream), "uva_arap_noalloc")
         torch.cuda.synchronize()
         err = float((db.U - Uref).abs().max()) / ext
@@ -65,3 +77,8 @@ def test_noalloc_rejects_oversize_batch(cuda):
     rc = L.uva_arap_noalloc(C.byref(desc), C.byref(prm), db._stream())
     assert rc == _lib.UVA_E_TOOBIG
     assert b"32768" in L.uva_last_error()
+    # more islands than the fixed x64 / b64 rows can hold (max(n, nc) rows)
+    desc = _lib.BatchDesc.from_buffer_copy(db.desc)
+    desc.nc = 40000
+    rc = L.uva_arap_noalloc(C.byref(desc), C.byref(prm), db._stream())
+    assert rc == _lib.UVA_E_TOOBIG

@@ -1723,10 +1723,16 @@ cudaError_t ensure_islands_attr() {
     return e;
 }
 
-bool check_batch(const uva_batch* b) {
+// The batch's inputs (topology, geometry, coarse operators), without the
+// caller's solver scratch.
+bool check_batch_inputs(const uva_batch* b) {
     return b && b->nc >= 0 && b->n >= 0 && b->t >= 0 &&
-           (b->nc == 0 || (b->vofs && b->tofs && b->sofs && b->order && b->work && b->slot_cw && b->row_vert &&
-                           b->vert_row && b->agg_rows && b->cofs && b->coarse_a && b->coarse_l && b->cpart));
+           (b->nc == 0 || (b->vofs && b->tofs && b->sofs && b->order && b->slot_cw && b->row_vert &&
+                           b->vert_row && b->agg_rows && b->cofs && b->coarse_a && b->coarse_l));
+}
+
+bool check_batch(const uva_batch* b) {
+    return check_batch_inputs(b) && (b->nc == 0 || (b->work && b->cpart));
 }
 
 bool check_classes(const uva_batch* b) {
@@ -2214,11 +2220,13 @@ int noalloc_scratch(unsigned char** out) {
 }  // namespace
 
 extern "C" int uva_arap_noalloc(const uva_batch* b, const uva_solve_params* prm, void* stream) {
-    if (!check_batch(b) || !prm || !b->status || !b->U) {
+    // the caller's scratch fields (work, cpart, x64, ...) are not read
+    if (!check_batch_inputs(b) || !prm || !b->status || !b->U) {
         uva_set_error("uva_arap_noalloc: bad arguments (status and U are required outputs)");
         return UVA_E_ARG;
     }
-    if (b->n > kNoAllocMaxVerts || b->t > kNoAllocMaxTris || b->nslices > kNoAllocMaxVerts) {
+    if (b->n > kNoAllocMaxVerts || b->t > kNoAllocMaxTris || b->nslices > kNoAllocMaxVerts ||
+        b->nc > kNoAllocMaxVerts) {
         uva_set_error("uva_arap_noalloc: batch above the fixed scratch limit of 32768 vertices / 65536 triangles");
         return UVA_E_TOOBIG;
     }

@@ -114,12 +114,12 @@ def chart_checks(F, FF, faces, loc, chart, CV, UV, nchart, nv):
     (engine/hier.py:269-353): boundary edges from face adjacency, Euler
     characteristic chi = V - E + F, boundary loops (connected components of
     the boundary edges), and the exact boundary self-intersection test."""
-    chi, loops, ba, bb, bc = chart_topology(F, FF, faces, loc, chart, CV, nchart, nv)
+    chi, loops, ba, bb, bc = _boundary_topology(F, FF, faces, loc, chart, CV, nchart, nv)
     collide = _collide(UV, ba, bb, bc, int(nchart))
     return collide, chi, loops
 
 
-def chart_topology(F, FF, faces, loc, chart, CV, nchart, nv):
+def _boundary_topology(F, FF, faces, loc, chart, CV, nchart, nv):
     """The host half of chart_checks: (chi, loops, ba, bb, bc) with the
     boundary edges ba -> bb of chart bc in face order."""
     CV = np.asarray(CV, np.int64).reshape(-1, 3)
