@@ -490,6 +490,72 @@ int uva_batch_boundary_scratch_bytes(const uva_batch* b, int64_t* bytes);
 int uva_batch_boundary(const uva_batch* b, int32_t* seg_ofs, int32_t* seg, void* scratch, int64_t scratch_bytes,
                        void* stream);
 
+/* --------------------------------------------------------------------------
+ * Mesh edges and sparse helpers of engine/gpu.py:16-63 and
+ * engine/param.py:59-68, on the device (csrc/edges.cu).
+ * ------------------------------------------------------------------------ */
+/* gpu.unique_edges (gpu.py:39-49). T: t*3 int64 vertex ids in [0, n).
+ * Writes the E unique undirected edges in ascending (lo, hi) order: ea, eb
+ * (lo <= hi) and cnt (triangles using the edge), each of capacity 3t;
+ * inv (3t): unique edge of half-edge k*t + f, the edge of triangle f
+ * opposite corner k (corners k+1, k+2). *nedges (device int64) = E, or -1
+ * when a vertex id is outside [0, n). Scratch:
+ * uva_unique_edges_scratch_bytes.                                          */
+int uva_unique_edges_scratch_bytes(int64_t n, int64_t t, int64_t* bytes);
+int uva_unique_edges(const int64_t* T, int64_t t, int64_t n, int64_t* ea, int64_t* eb, int64_t* inv, int64_t* cnt,
+                     int64_t* nedges, void* scratch, int64_t scratch_bytes, void* stream);
+/* gpu.sym_csr (gpu.py:52-63): the n x n symmetric matrix with off[e] at
+ * (ea[e], eb[e]) and (eb[e], ea[e]) and diag on the diagonal, as CSR with
+ * int32 row offsets (crow, n+1) and columns (col, 2 ne + n), rows sorted by
+ * column. dtype 0: float32 values, 1: float64. *status (device int32) = 1
+ * when an endpoint is outside [0, n).                                      */
+int uva_sym_csr_scratch_bytes(int64_t n, int64_t* bytes);
+int uva_sym_csr(int64_t n, int64_t ne, const int64_t* ea, const int64_t* eb, const void* off, const void* diag,
+                int32_t dtype, int32_t* crow, int32_t* col, void* val, int32_t* status, void* scratch,
+                int64_t scratch_bytes, void* stream);
+/* gpu.spmm (gpu.py:23-28): Y = A X for an int32 CSR matrix (nrows rows,
+ * nnz entries) and k dense columns (X, Y row-major with k columns). dtype
+ * 0: float32, 1: float64 (values, X and Y).                               */
+int uva_csr_spmm(int32_t nrows, int32_t k, int64_t nnz, const int32_t* crow, const int32_t* col, const void* val,
+                 const void* X, void* Y, int32_t dtype, void* stream);
+/* param.boundary_edges_oriented (param.py:59-68): keep (3t bytes) = 1 for
+ * the directed half-edge k*t + f (corners k -> k+1 of triangle f) whose
+ * reverse half-edge is absent. *status = 1 for a vertex id outside
+ * [0, 2^31).                                                               */
+int uva_boundary_mask_scratch_bytes(int64_t t, int64_t* bytes);
+int uva_boundary_mask(const int64_t* T, int64_t t, uint8_t* keep, int32_t* status, void* scratch,
+                      int64_t scratch_bytes, void* stream);
+/* gpu.Batch._edges (gpu.py:128-129) of a device batch, from the plan's
+ * unique-edge numbering (which is the ascending global (lo, hi) order):
+ * ea, eb, cnt (b->E int64 each).                                           */
+int uva_batch_edges(const uva_batch* b, int64_t* ea, int64_t* eb, int64_t* cnt, void* stream);
+
+/* --------------------------------------------------------------------------
+ * Whole-mesh reports of engine/metrics.py:227-311 (csrc/report.cu).
+ * ------------------------------------------------------------------------ */
+/* metrics.seam_report (metrics.py:227-261). V (n*3 FP64), F (m*3 int64,
+ * numpy indexing: -n <= id < n), UV (n*2 FP64), weld (n int64 keys, or null:
+ * vertices with equal position values are one vertex). out (device, 6
+ * doubles): seam_edges, seam_length, open_boundary_edges,
+ * open_boundary_length, nonmanifold_edge_groups, surface_area. *status = 1
+ * for a face index out of range.                                           */
+int uva_seam_report_scratch_bytes(int64_t n, int64_t m, int64_t* bytes);
+int uva_seam_report(const double* V, int64_t n, const int64_t* F, int64_t m, const double* UV, const int64_t* weld,
+                    double* out, int32_t* status, void* scratch, int64_t scratch_bytes, void* stream);
+/* Exact per-corner equality of attribute rows (metrics.py:264-286,
+ * validate.py:191-199): rows A[fa[i]] and B[fb[i]], i < m, w columns each,
+ * compared by value as np.array_equal does (NaN unequal, -0.0 == 0.0;
+ * floats compared as FP64, integers exactly). Element codes: 0 f32, 1 f64,
+ * 2 f16, 3 u8, 4 i8, 5 i16, 6 u16, 7 i32, 8 u32, 9 i64, 10 u64, 11 bool.
+ * *result (device int32): bit 0 a row differs, bit 1 an index is outside
+ * its array (numpy indexing).                                              */
+int uva_corners_equal(const void* A, int32_t adt, int64_t na, const int64_t* fa, const void* B, int32_t bdt,
+                      int64_t nb, const int64_t* fb, int64_t m, int32_t w, int32_t* result, void* stream);
+/* out[seg[i]] = sum of x[i*stride] (np.bincount with weights,
+ * metrics.py:306-307); *status = 1 for a segment id outside [0, nseg).   */
+int uva_segment_sum(const double* x, int64_t stride, const int32_t* seg, int64_t m, int32_t nseg, double* out,
+                    int32_t* status, void* stream);
+
 /* Library info. */
 const char* uva_last_error(void);
 int uva_version(void);

@@ -259,3 +259,27 @@ def test_plan_range_export_matches_full_export():
     for k in Plan.EXPORTED:
         assert np.array_equal(out[k], getattr(full, k)), k
     assert np.array_equal(off[:26], full.sofs) and np.array_equal(off[52:], full.bofs)
+
+
+def test_boundary_loop_walk_against_reference():
+    """The host loop walk of param.boundary_loops on the reference's own
+    boundary half-edges (golden_reports.npz): same loops, same order."""
+    from ultimate_uv_artist_b200.engine.param import _trace_loops
+    g = np.load(os.path.join(ROOT, "tests", "golden", "golden_reports.npz"))
+    for name in ("disk", "grid", "annulus", "bowtie", "dups"):
+        loops = _trace_loops(g[f"t_{name}_bi"], g[f"t_{name}_bj"])
+        assert [len(x) for x in loops] == g[f"t_{name}_loop_len"].tolist(), name
+        flat = np.concatenate(loops) if loops else np.zeros(0, np.int64)
+        assert np.array_equal(flat, g[f"t_{name}_loops"]), name
+
+
+def test_cot_laplacian_assembly_against_reference():
+    """param.cot_laplacian (host scipy assembly) equals the reference's matrix."""
+    from ultimate_uv_artist_b200.engine import param as Pm
+    g = np.load(os.path.join(ROOT, "tests", "golden", "golden_reports.npz"))
+    D = Pm.cot_laplacian(len(g["l_P"]), g["l_T"], g["l_cots"]).toarray()
+    assert np.max(np.abs(D - g["l_dense"])) <= 1e-12 * np.max(np.abs(g["l_dense"]))
+    I, J, W = Pm._lap_triplets(g["l_T"], g["l_cots"])
+    import scipy.sparse as sp
+    D2 = sp.coo_matrix((W, (I, J)), shape=D.shape).toarray()
+    assert np.max(np.abs(D2 - g["l_dense"])) <= 1e-12 * np.max(np.abs(g["l_dense"]))

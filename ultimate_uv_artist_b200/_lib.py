@@ -106,6 +106,18 @@ _SIGS = {
     "uva_boundary_hits": [vp, vp],
     "uva_batch_boundary_scratch_bytes": [vp, vp],
     "uva_batch_boundary": [vp, vp, vp, vp, C.c_int64, vp],
+    "uva_unique_edges_scratch_bytes": [C.c_int64, C.c_int64, vp],
+    "uva_unique_edges": [vp, C.c_int64, C.c_int64, vp, vp, vp, vp, vp, vp, C.c_int64, vp],
+    "uva_sym_csr_scratch_bytes": [C.c_int64, vp],
+    "uva_sym_csr": [C.c_int64, C.c_int64, vp, vp, vp, vp, i32, vp, vp, vp, vp, vp, C.c_int64, vp],
+    "uva_csr_spmm": [i32, i32, C.c_int64, vp, vp, vp, vp, vp, i32, vp],
+    "uva_boundary_mask_scratch_bytes": [C.c_int64, vp],
+    "uva_boundary_mask": [vp, C.c_int64, vp, vp, vp, C.c_int64, vp],
+    "uva_batch_edges": [vp, vp, vp, vp, vp],
+    "uva_seam_report_scratch_bytes": [C.c_int64, C.c_int64, vp],
+    "uva_seam_report": [vp, C.c_int64, vp, C.c_int64, vp, vp, vp, vp, vp, C.c_int64, vp],
+    "uva_corners_equal": [vp, i32, C.c_int64, vp, vp, i32, C.c_int64, vp, C.c_int64, i32, vp, vp],
+    "uva_segment_sum": [vp, C.c_int64, vp, C.c_int64, i32, vp, vp, vp],
     "uva_last_error": [],
     "uva_version": [],
 }

@@ -17,26 +17,30 @@ Batch without a CUDA device raises RuntimeError.
 from __future__ import annotations
 
 import contextlib
+import ctypes as C
 
 import numpy as np
 import torch
 
-from .. import _lib
+from .. import _lib, meshops
 from ..device import DeviceBatch, Plan, concat_charts, require_cuda
 
 
 def csr32(A):
-    """CSR with int32 indices (engine/gpu.py:16-20)."""
-    A = A.to_sparse_csr() if A.layout != torch.sparse_csr else A
-    return torch.sparse_csr_tensor(A.crow_indices().to(torch.int32), A.col_indices().to(torch.int32),
-                                   A.values(), A.shape)
+    """The matrix as a torch CSR tensor with int32 row offsets and columns:
+    the layout the uva_csr_spmm kernel reads (engine/gpu.py:16-20)."""
+    if A.layout != torch.sparse_csr:
+        A = (A.coalesce() if A.layout == torch.sparse_coo else A).to_sparse_csr()
+    crow, col = A.crow_indices(), A.col_indices()
+    if crow.dtype == torch.int32 and col.dtype == torch.int32:
+        return A
+    return torch.sparse_csr_tensor(crow.to(torch.int32), col.to(torch.int32), A.values(), A.shape)
 
 
 def spmm(L, X):
-    """L @ X for a few dense columns (engine/gpu.py:23-28)."""
-    if X.dim() == 1:
-        return L @ X
-    return torch.stack([L @ X[:, k].contiguous() for k in range(X.shape[1])], 1)
+    """L @ X for a vector or a few dense columns (engine/gpu.py:23-28): one
+    uva_csr_spmm launch reads the matrix once for all columns."""
+    return meshops.csr_spmm(csr32(L), X)
 
 
 def device():
@@ -52,26 +56,20 @@ def device():
 
 
 def unique_edges(T, n):
-    """Undirected unique edges, inverse map and use counts (engine/gpu.py:39-49)."""
-    a = torch.cat([T[:, 1], T[:, 2], T[:, 0]])
-    b = torch.cat([T[:, 2], T[:, 0], T[:, 1]])
-    key = torch.minimum(a, b) * n + torch.maximum(a, b)
-    uk, inv = torch.unique(key, return_inverse=True)
-    cnt = torch.bincount(inv, minlength=len(uk))
-    return uk // n, uk % n, inv, cnt
+    """Unique undirected edges (ea < eb ascending), the edge of each of the
+    3t half-edges (k t + f: triangle f's edge opposite corner k) and the use
+    count of each edge (engine/gpu.py:39-49), by the uva_unique_edges
+    counting-sort kernels. Results live on T's device."""
+    T = torch.as_tensor(T)
+    out = meshops.unique_edges(T, n)
+    return tuple(o.to(T.device) for o in out) if not T.is_cuda else out
 
 
 def sym_csr(n, ea, eb, off, diag):
-    """Symmetric int32 CSR from unique edges (engine/gpu.py:52-63)."""
-    dev = ea.device
-    rows = torch.cat([ea, eb, torch.arange(n, device=dev)])
-    cols = torch.cat([eb, ea, torch.arange(n, device=dev)])
-    vals = torch.cat([off, off, diag])
-    order = torch.argsort(rows * n + cols)
-    rows, cols, vals = rows[order], cols[order], vals[order]
-    crow = torch.zeros(n + 1, dtype=torch.int64, device=dev)
-    crow[1:] = torch.cumsum(torch.bincount(rows, minlength=n), 0)
-    return torch.sparse_csr_tensor(crow.to(torch.int32), cols.to(torch.int32), vals, (n, n))
+    """Symmetric CSR (int32 indices) with ``off`` at (ea, eb) and (eb, ea)
+    and ``diag`` on the diagonal (engine/gpu.py:52-63), assembled by the
+    uva_sym_csr kernels."""
+    return meshops.sym_csr(n, ea, eb, off, diag)
 
 
 class Batch:
@@ -174,34 +172,49 @@ class Batch:
     def wpin(self):
         return self.db.wpin[0].to(self.dt) if self.nc else torch.tensor(1e-12, dtype=self.dt, device=self.dev)
 
-    def _wdiag_by_vertex(self):
-        """Row sums of the weights, reordered from solver rows to vertices."""
-        vr = self.db.vert_row[:self.n].to(torch.int64)
-        base = torch.repeat_interleave(self.db.vofs[:-1].to(torch.int64),
-                                       torch.as_tensor(np.diff(self.offsets), device=self.dev))
-        return self.db.wdiag[:self.n][base + vr]
+    def _diag(self, self_loops):
+        """FP64 diagonal of the soft-pinned Laplacian (gpu.py:131-140): the
+        summed edge weights at both endpoints of every edge, plus the pin
+        weights. With self_loops the edges of degenerate triangles that join
+        a vertex to itself count too, as in the reference's diagonal; their
+        off-diagonal entries cancel them in its matrix."""
+        ea, eb, _ = self._edges
+        w = self.db.wedge[:self.db.plan.E]
+        if not self_loops:
+            keep = ea != eb
+            ea, eb, w = ea[keep], eb[keep], w[keep]
+        w = w.contiguous()
+        d = meshops.segment_sum(w, ea, self.n) + meshops.segment_sum(w, eb, self.n)
+        d[self.pins] += self.db.wpin[:self.nc]
+        return d
 
     @property
     def dinv(self):
-        d = self._wdiag_by_vertex().clone()
-        d[self.pins] += self.db.wpin[:self.nc]
-        return (1.0 / d.clamp_min(1e-30)).to(self.dt)
+        return (1.0 / self._diag(True).clamp_min(1e-30)).to(self.dt)
 
     @property
     def L(self):
-        """The soft-pinned cotangent Laplacian as an int32 sparse CSR tensor."""
+        """The soft-pinned cotangent Laplacian as an int32 sparse CSR tensor:
+        the batch's summed edge weights off the diagonal, their row sums plus
+        the pin weights on it (self-loop edges of degenerate triangles cancel
+        and are left out)."""
         ea, eb, _ = self._edges
-        p = self.db.plan
-        wsum = self.db.wedge[:p.E].to(self.dt)
+        wsum = self.db.wedge[:self.db.plan.E].to(self.dt)
         keep = ea != eb
-        diag = self._wdiag_by_vertex().clone()
-        diag[self.pins] += self.db.wpin[:self.nc]
-        return sym_csr(self.n, ea[keep], eb[keep], -wsum[keep], diag.to(self.dt))
+        return sym_csr(self.n, ea[keep], eb[keep], -wsum[keep], self._diag(False).to(self.dt))
 
     @property
     def _edges(self):
-        """(ea, eb, cnt) of the unique edges, global vertex ids (gpu.py:129)."""
-        ea, eb, _, cnt = unique_edges(self.T, self.n)
+        """(ea, eb, cnt) of the unique edges in global vertex ids
+        (gpu.py:128-129), read off the plan's own edge numbering: the plan
+        numbers each island's edges in ascending (lo, hi) order and the
+        islands in order, which is the ascending global order."""
+        E = self.db.plan.E
+        ea = torch.empty(E, dtype=torch.int64, device=self.dev)
+        eb = torch.empty_like(ea)
+        cnt = torch.empty_like(ea)
+        _lib.check(_lib.lib().uva_batch_edges(C.byref(self.db.desc), meshops._p(ea), meshops._p(eb), meshops._p(cnt),
+                                              meshops._stream(self.dev)), "uva_batch_edges")
         return ea, eb, cnt
 
     # ------------------------------------------------------------ pieces

@@ -2,10 +2,10 @@
 
 Same functions and signatures (engine/metrics.py:13-373). Distortion
 (Jacobian singular values, anisotropy, density and chart-area ratios, angle
-error, weighted p95 quantiles), islands, coverage and label rasters and the
-gutter run in the uva_b200 CUDA kernels. ``seam_report`` and
-``preservation_report`` are whole-mesh bookkeeping over edge keys and
-attribute arrays; they keep the reference's numpy formulation on the host.
+error, weighted p95 quantiles), islands, coverage and label rasters, the
+gutter, the seam report (vertex weld and edge grouping by hash tables) and
+the exact corner comparison of the preservation report run in the uva_b200
+CUDA kernels.
 """
 from __future__ import annotations
 
@@ -14,7 +14,7 @@ import ctypes as C
 import numpy as np
 import torch
 
-from .. import _lib
+from .. import _lib, meshops
 from ..device import require_cuda
 
 vp = C.c_void_p
@@ -144,7 +144,11 @@ def triangle_jacobians(P, U):
     return per[:, 0], per[:, 1], per[:, 2], per[:, 3], per[:, 4] != 0
 
 
-def _distortion(V, F, UV, islands, n_islands):
+def _distortion(V, F, UV, islands, n_islands, per_tri="host", keep_per_tri=False):
+    """One uva_distortion_report pass: (report sums on the host, per-triangle
+    s1, s2, signed UV area, 3D area, good, angle error). per_tri "host":
+    numpy; with keep_per_tri the device tensor is returned instead; None:
+    not written (the kernel keeps it in its scratch)."""
     L = _sig()
     dev = require_cuda()
     Vt = torch.from_numpy(np.ascontiguousarray(V, np.float64).reshape(-1, 3)).to(dev)
@@ -153,25 +157,24 @@ def _distortion(V, F, UV, islands, n_islands):
     It = torch.from_numpy(np.ascontiguousarray(islands, np.int32)).to(dev) if islands is not None else None
     m = int(Ft.shape[0])
     out = torch.zeros(32, dtype=torch.float64, device=dev)
-    per = torch.empty((max(m, 1), 6), dtype=torch.float64, device=dev)
+    want = keep_per_tri or per_tri is not None
+    per = torch.empty((max(m, 1), 6), dtype=torch.float64, device=dev) if want else None
     nb = C.c_int64()
     _lib.check(L.uva_metrics_scratch_bytes(m, int(n_islands), C.byref(nb)), "uva_metrics_scratch_bytes")
     sc = _scratch(nb.value, dev)
     _lib.check(L.uva_distortion_report(_p(Vt), _p(Ut), _p(Ft), _p(It) if It is not None else None, int(Vt.shape[0]),
-                                       m, int(n_islands), _p(out), _p(per), _p(sc), nb.value, _stream(dev)),
+                                       m, int(n_islands), _p(out), _p(per) if want else None, _p(sc), nb.value,
+                                       _stream(dev)),
                "uva_distortion_report")
-    return out.cpu().numpy(), per[:m].cpu().numpy()
+    if keep_per_tri:
+        return out.cpu().numpy(), per[:m]
+    return out.cpu().numpy(), (per[:m].cpu().numpy() if want else None)
 
 
-def distortion_report(vertices, faces, uvs, islands=None, chunk=2_000_000):
-    """Area-weighted distortion statistics (engine/metrics.py:148-210).
-    ``chunk`` is accepted for signature compatibility (the device holds the
-    whole mesh)."""
-    faces = np.asarray(faces, np.int64)
-    n_is = int(np.asarray(islands).max()) + 1 if islands is not None and len(islands) else 0
-    s, _ = _distortion(vertices, faces, uvs, islands, n_is)
+def _distortion_fields(m, s, with_islands):
+    """The report dictionary of distortion_report from the pass's sums."""
     out = {}
-    out["triangles"] = int(len(faces))
+    out["triangles"] = int(m)
     out["collapsed_uv_triangles"] = int(round(s[2]))
     out["collapsed_uv_area_fraction"] = float(s[3])
     out["anisotropy_mean"] = float(s[4] / max(s[5], 1e-30))
@@ -180,7 +183,7 @@ def distortion_report(vertices, faces, uvs, islands=None, chunk=2_000_000):
     out["density_log2_dev_mean"] = float(s[8] / max(s[9], 1e-30))
     out["density_ratio_p95"] = float(2 ** s[25])
     out["stretch_L2"] = float(np.sqrt(s[10] / max(s[9], 1e-30)))
-    if islands is not None:
+    if with_islands:
         out["chart_area_log2_dev_mean"] = float(s[11] / max(s[9], 1e-30))
         out["chart_area_ratio_p95"] = float(2 ** s[26])
         out["flipped_triangles"] = int(round(s[12]))
@@ -188,6 +191,16 @@ def distortion_report(vertices, faces, uvs, islands=None, chunk=2_000_000):
         out["mirrored_islands"] = int(round(s[16]))
         out["island_density_ratio_p95"] = float(2 ** s[27])
     return out
+
+
+def distortion_report(vertices, faces, uvs, islands=None, chunk=2_000_000):
+    """Area-weighted distortion statistics (engine/metrics.py:148-210).
+    ``chunk`` is accepted for signature compatibility (the device holds the
+    whole mesh)."""
+    faces = np.asarray(faces, np.int64)
+    n_is = int(np.asarray(islands).max()) + 1 if islands is not None and len(islands) else 0
+    s, _ = _distortion(vertices, faces, uvs, islands, n_is, per_tri=None)
+    return _distortion_fields(len(faces), s, islands is not None)
 
 
 def _angle_error(P, U):
@@ -198,94 +211,73 @@ def _angle_error(P, U):
     return _distortion(P.reshape(-1, 3), F, U.reshape(-1, 2), None, 0)[1][:, 5]
 
 
-# ---------------------------------------------------------------- seams (host bookkeeping)
+# ---------------------------------------------------------------- seams and preservation
 def seam_report(vertices, faces, uvs, weld_keys=None):
-    """UV seam edges and lengths (engine/metrics.py:227-261)."""
-    if weld_keys is None:
-        _, weld_keys = np.unique(vertices, axis=0, return_inverse=True)
-    weld_keys = weld_keys.reshape(-1).astype(np.int64)
-    W = weld_keys[faces]
-    e0 = np.concatenate([W[:, 0], W[:, 1], W[:, 2]])
-    e1 = np.concatenate([W[:, 1], W[:, 2], W[:, 0]])
-    c0 = np.concatenate([faces[:, 0], faces[:, 1], faces[:, 2]])
-    c1 = np.concatenate([faces[:, 1], faces[:, 2], faces[:, 0]])
-    swap = e0 > e1
-    lo = np.where(swap, e1, e0)
-    hi = np.where(swap, e0, e1)
-    clo = np.where(swap, c1, c0)
-    chi = np.where(swap, c0, c1)
-    key = lo * (int(weld_keys.max()) + 1) + hi
-    o = np.argsort(key, kind="stable")
-    key = key[o]; clo = clo[o]; chi = chi[o]
-    start = np.r_[True, key[1:] != key[:-1]]
-    gid = np.cumsum(start) - 1
-    cnt = np.bincount(gid)
-    first = np.nonzero(start)[0]
-    interior = cnt == 2
-    i0 = first[interior]; i1 = i0 + 1
-    u = uvs.astype(np.float64)
-    mism = (np.any(u[clo[i0]] != u[clo[i1]], axis=1) | np.any(u[chi[i0]] != u[chi[i1]], axis=1))
-    P = vertices.astype(np.float64)
-    Ln = np.linalg.norm(P[clo[i0]] - P[chi[i0]], axis=1)
-    bnd = cnt == 1
-    Lb = np.linalg.norm(P[clo[first[bnd]]] - P[chi[first[bnd]]], axis=1)
-    area = 0.5 * np.linalg.norm(np.cross(P[faces[:, 1]] - P[faces[:, 0]], P[faces[:, 2]] - P[faces[:, 0]]), axis=1).sum()
-    return {"seam_edges": int(mism.sum()), "seam_length": float(Ln[mism].sum()),
-            "seam_length_per_sqrt_area": float(Ln[mism].sum() / np.sqrt(max(area, 1e-30))),
-            "open_boundary_edges": int(bnd.sum()), "open_boundary_length": float(Lb.sum()),
-            "nonmanifold_edge_groups": int((cnt > 2).sum()), "surface_area": float(area)}
+    """UV seam edges and lengths (engine/metrics.py:227-261), on the device
+    (``uva_seam_report``): vertices weld by equal position (or by equal
+    ``weld_keys``), the triangle edges of the welded mesh are grouped, and a
+    group of two whose corners disagree on UVs is a seam edge; groups of one
+    are open boundary, of more than two non-manifold."""
+    s = meshops.seam_report(vertices, faces, uvs, weld_keys)
+    seam_len, area = float(s[1]), float(s[5])
+    return {"seam_edges": int(s[0]), "seam_length": seam_len,
+            "seam_length_per_sqrt_area": float(seam_len / np.sqrt(max(area, 1e-30))),
+            "open_boundary_edges": int(s[2]), "open_boundary_length": float(s[3]),
+            "nonmanifold_edge_groups": int(s[4]), "surface_area": area}
 
 
 def preservation_report(in_v, in_f, out_v, out_f, in_attrs=None, out_attrs=None, chunk=2_000_000):
-    """Exact per-corner equality of positions and attributes (engine/metrics.py:264-286)."""
-    rep = {"triangle_count_equal": len(in_f) == len(out_f)}
-    if not rep["triangle_count_equal"]:
+    """Exact per-corner equality of positions and attributes between the
+    input and output meshes (engine/metrics.py:264-286), compared on the
+    device (``uva_corners_equal``). ``chunk`` is accepted for signature
+    compatibility: the device compares all corners in one launch."""
+    same_count = len(in_f) == len(out_f)
+    rep = {"triangle_count_equal": same_count}
+    if not same_count:
         rep["positions_exact"] = False
         return rep
-    ok = True
-    for b in range(0, len(in_f), chunk):
-        if not np.array_equal(in_v[in_f[b:b + chunk]], out_v[out_f[b:b + chunk]]):
-            ok = False
-            break
-    rep["positions_exact"] = ok
-    for name in (in_attrs or {}):
-        a, o = in_attrs[name], (out_attrs or {}).get(name)
+    rep["positions_exact"] = meshops.corners_equal(in_v, in_f, out_v, out_f)
+    out_attrs = out_attrs or {}
+    for name, a in (in_attrs or {}).items():
         if a is None:
             continue
-        if o is None:
-            rep[name + "_exact"] = False
-            continue
-        same = True
-        for b in range(0, len(in_f), chunk):
-            if not np.array_equal(a[in_f[b:b + chunk]], o[out_f[b:b + chunk]]):
-                same = False
-                break
-        rep[name + "_exact"] = same
+        o = out_attrs.get(name)
+        rep[name + "_exact"] = False if o is None else meshops.corners_equal(a, in_f, o, out_f)
     return rep
 
 
 def full_report(out_v, out_f, out_uv, raster_res=4096, in_v=None, in_f=None, in_attrs=None, out_attrs=None):
-    """engine/metrics.py:289-311."""
-    rep = {}
+    """Islands, coverage, distortion, seams, preservation and the island size
+    distribution of an unwrapped mesh (engine/metrics.py:289-311). Returns
+    (report, per-face island labels)."""
+    out_f = np.asarray(out_f)
     isl, n_is = uv_islands(out_f, len(out_v), out_uv, out_v)
-    rep["islands"] = n_is
-    uv_ok = bool(np.isfinite(out_uv).all())
-    rep["uv_finite"] = uv_ok
-    rep["uv_in_unit_square"] = bool(out_uv.min() >= -1e-6 and out_uv.max() <= 1 + 1e-6)
+    rep = {"islands": n_is}
+    uv = np.asarray(out_uv)
+    rep["uv_finite"] = bool(np.isfinite(uv).all())
+    rep["uv_in_unit_square"] = bool(uv.min() >= -1e-6 and uv.max() <= 1 + 1e-6)
     _, occ, ov = raster_coverage(out_uv, out_f, raster_res)
     rep["raster_res"] = raster_res
     rep["occupancy"] = occ
     rep["overlap_texels"] = ov
-    rep.update(distortion_report(out_v, out_f, out_uv, isl))
+    sums, per = _distortion(out_v, out_f, out_uv, isl, n_is, keep_per_tri=True)
+    rep.update(_distortion_fields(len(out_f), sums, True))
     rep.update(seam_report(out_v, out_f, out_uv))
     if in_v is not None:
         rep.update(preservation_report(in_v, in_f, out_v, out_f, in_attrs, out_attrs))
-    a3 = 0.5 * np.linalg.norm(np.cross(out_v[out_f[:, 1]] - out_v[out_f[:, 0]], out_v[out_f[:, 2]] - out_v[out_f[:, 0]]), axis=1)
-    ia = np.bincount(isl, weights=a3, minlength=n_is)
-    ia = np.sort(ia)[::-1] / max(ia.sum(), 1e-30)
-    rep["largest_island_area_frac"] = float(ia[0]) if n_is else 0.0
-    rep["islands_for_90pct_area"] = int(np.searchsorted(np.cumsum(ia), 0.9) + 1) if n_is else 0
-    rep["tiny_islands_lt_0.01pct"] = int((ia < 1e-4).sum())
+    # island 3D areas (the distortion pass's per-triangle areas summed per
+    # island), largest first, as fractions of the total
+    if n_is:
+        ia = meshops.segment_sum(per[:, 3].contiguous(), torch.from_numpy(np.asarray(isl, np.int32)), n_is)
+        ia = np.sort(ia.cpu().numpy())[::-1]
+        ia = ia / max(float(ia.sum()), 1e-30)
+        rep["largest_island_area_frac"] = float(ia[0])
+        rep["islands_for_90pct_area"] = int(np.searchsorted(np.cumsum(ia), 0.9) + 1)
+        rep["tiny_islands_lt_0.01pct"] = int((ia < 1e-4).sum())
+    else:
+        rep["largest_island_area_frac"] = 0.0
+        rep["islands_for_90pct_area"] = 0
+        rep["tiny_islands_lt_0.01pct"] = 0
     return rep, isl
 
 

@@ -17,7 +17,8 @@ runs in the uva_b200 CUDA kernels:
 
 ``cot_laplacian`` returns a scipy matrix and ``boundary_edges_oriented`` /
 ``boundary_loops`` / ``_far_pair`` return host index arrays, as the reference
-does; they are topology bookkeeping. ``refine(method="slim")`` (symmetric
+does; the twin test behind the boundary half-edges is a device hash kernel
+(``uva_boundary_mask``). ``refine(method="slim")`` (symmetric
 Dirichlet SLIM, used by the "artist" profile) runs ``uva_slim``: the SLIM
 normal equations applied without forming them, FP64 CG, the reference's
 flip-safe step and energy backtracking.
@@ -30,7 +31,7 @@ import numpy as np
 import scipy.sparse as sp
 import torch
 
-from .. import _lib
+from .. import _lib, meshops
 from ..device import DeviceBatch, Plan, require_cuda
 
 DIRECT_LIMIT = 220_000
@@ -99,54 +100,85 @@ def cot_weights(X):
 
 
 def _lap_triplets(T, cots):
-    """Triplets of the cotangent Laplacian (engine/param.py:47-51)."""
-    i = np.concatenate([T[:, 1], T[:, 2], T[:, 0]])
-    j = np.concatenate([T[:, 2], T[:, 0], T[:, 1]])
-    w = 0.5 * np.concatenate([cots[:, 0], cots[:, 1], cots[:, 2]])
-    return np.concatenate([i, j, i, j]), np.concatenate([j, i, i, j]), np.concatenate([-w, -w, w, w])
+    """(rows, cols, values) of the cotangent Laplacian (engine/param.py:47-51):
+    per triangle edge k (corners k+1, k+2, half cotangent w of the opposite
+    angle) the entries -w at (i, j) and (j, i) and +w at (i, i) and (j, j),
+    edge by edge. Summing duplicates gives the Laplacian."""
+    T = np.asarray(T, np.int64).reshape(-1, 3)
+    w = 0.5 * np.asarray(cots, np.float64).reshape(-1, 3)
+    i = T[:, [1, 2, 0]].reshape(-1)
+    j = T[:, [2, 0, 1]].reshape(-1)
+    wk = w.reshape(-1)
+    rows = np.stack([i, j, i, j], 1).reshape(-1)
+    cols = np.stack([j, i, i, j], 1).reshape(-1)
+    vals = np.stack([-wk, -wk, wk, wk], 1).reshape(-1)
+    return rows, cols, vals
 
 
 def cot_laplacian(n, T, cots):
-    """scipy CSC cotangent Laplacian (engine/param.py:54-56)."""
-    I, J, W = _lap_triplets(np.asarray(T, np.int64), np.asarray(cots, np.float64))
-    return sp.csc_matrix((W, (I, J)), shape=(n, n))
+    """The cotangent Laplacian as scipy CSC (engine/param.py:54-56): the
+    symmetric matrix of summed half cotangents W per undirected edge, L =
+    diag(row sums of W) - W."""
+    T = np.asarray(T, np.int64).reshape(-1, 3)
+    w = 0.5 * np.asarray(cots, np.float64).reshape(-1, 3)
+    i = T[:, [1, 2, 0]].reshape(-1)
+    j = T[:, [2, 0, 1]].reshape(-1)
+    W = sp.coo_matrix((w.reshape(-1), (i, j)), shape=(n, n)).tocsr()
+    W = W + W.T
+    return (sp.diags(np.asarray(W.sum(axis=1)).reshape(-1)) - W).tocsc()
 
 
 def boundary_edges_oriented(T):
-    """Directed half-edges (i -> j) whose reverse is absent (engine/param.py:59-68)."""
-    T = np.asarray(T, np.int64)
-    a = np.concatenate([T[:, 0], T[:, 1], T[:, 2]])
-    b = np.concatenate([T[:, 1], T[:, 2], T[:, 0]])
-    n = int(max(a.max(), b.max())) + 1
-    has_twin = np.isin(b * n + a, a * n + b)
-    return a[~has_twin], b[~has_twin]
+    """Directed half-edges (i -> j) whose reverse is absent, in triangle-edge
+    order: all corner 0 -> 1 edges, then 1 -> 2, then 2 -> 0 (engine/param.py:
+    59-68). The twin test is the uva_boundary_mask hash kernel."""
+    T = np.asarray(T, np.int64).reshape(-1, 3)
+    if T.size == 0:
+        raise ValueError("boundary_edges_oriented: empty triangle list")
+    keep = meshops.boundary_mask(T).cpu().numpy()
+    a = T.T.reshape(-1)
+    b = T[:, [1, 2, 0]].T.reshape(-1)
+    return a[keep], b[keep]
 
 
 def boundary_loops(T):
-    """Boundary loops as vertex lists (engine/param.py:71-94)."""
+    """Boundary loops as vertex arrays (engine/param.py:71-94). A loop starts
+    at the first unused boundary source in half-edge order and follows, from
+    each vertex, its first outgoing boundary half-edge (half-edge order) to a
+    vertex not yet used, or back to the start, which closes the loop."""
     bi, bj = boundary_edges_oriented(T)
+    return _trace_loops(bi, bj)
+
+
+def _trace_loops(bi, bj):
+    """The loop walk of boundary_loops over directed boundary half-edges."""
+    bi = np.asarray(bi, np.int64)
+    bj = np.asarray(bj, np.int64)
     if len(bi) == 0:
         return []
-    nxt = {}
-    for i, j in zip(bi.tolist(), bj.tolist()):
-        nxt.setdefault(i, []).append(j)
-    loops, used = [], set()
-    for s in bi.tolist():
-        if s in used:
+    order = np.argsort(bi, kind="stable")          # outgoing half-edges grouped by source
+    src = bi[order]
+    dst = bj[order].tolist()
+    starts = np.searchsorted(src, bi)              # first outgoing half-edge of each source
+    ends = np.searchsorted(src, bi, side="right")
+    first = dict(zip(bi.tolist(), zip(starts.tolist(), ends.tolist())))
+    used = set()
+    loops = []
+    for s0 in bi.tolist():
+        if s0 in used:
             continue
-        loop = [s]
-        used.add(s)
-        cur = s
+        used.add(s0)
+        loop = [s0]
+        v = s0
         while True:
-            cand = [x for x in nxt.get(cur, []) if x not in used or x == s]
-            if not cand:
+            a, b = first.get(v, (0, 0))
+            nxt = next((x for x in dst[a:b] if x == s0 or x not in used), None)
+            if nxt is None or nxt == s0:
                 break
-            cur = cand[0]
-            if cur == s:
-                break
-            loop.append(cur)
-            used.add(cur)
-        loops.append(np.array(loop, np.int64))
+            loop.append(nxt)
+            used.add(nxt)
+            v = nxt
+        loops.append(np.asarray(loop, np.int64))
     return loops
 
 

@@ -21,7 +21,7 @@ import ctypes as C
 import numpy as np
 import torch
 
-from .. import _lib
+from .. import _lib, meshops
 from ..device import require_cuda
 
 ULP = 2.0 ** -24
@@ -141,21 +141,9 @@ def validate_uvs(v, f, uv, atlas=4096, padding=None, in_v=None, in_f=None, in_no
 
 
 def _corners_equal(a, fa, b, fb):
-    """Exact per-corner equality a[fa] == b[fb] (engine/validate.py:195-199), on the device."""
-    if a.shape[1:] != b.shape[1:] or a.dtype != b.dtype:
-        return bool(np.array_equal(a[fa], b[fb]))
-    dev = require_cuda()
-    ta = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
-    tb = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
-    ia = torch.from_numpy(np.ascontiguousarray(fa.reshape(-1))).to(dev)
-    ib = torch.from_numpy(np.ascontiguousarray(fb.reshape(-1))).to(dev)
-    xa = ta.index_select(0, ia).view(torch.uint8) if ta.is_floating_point() else ta.index_select(0, ia)
-    xb = tb.index_select(0, ib).view(torch.uint8) if tb.is_floating_point() else tb.index_select(0, ib)
-    if ta.is_floating_point():
-        # np.array_equal compares values: +0.0 == -0.0 and NaN != NaN
-        return bool(torch.equal(ta.index_select(0, ia), tb.index_select(0, ib)) and
-                    not bool(torch.isnan(ta.index_select(0, ia)).any()))
-    return bool(torch.equal(xa, xb))
+    """np.array_equal(a[fa], b[fb]) (engine/validate.py:195-199), compared on
+    the device by uva_corners_equal."""
+    return meshops.corners_equal(a, fa, b, fb)
 
 
 def chart_overlaps(U, T):
