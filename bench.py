@@ -50,12 +50,15 @@ def _args():
     ap.add_argument("--iters", type=int, default=ITERS)
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--cpu-budget-tris", type=int, default=2_000_000)
+    ap.add_argument("--cpu-repeats", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-validate", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--plain-budget-tris", type=int, default=60_000)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--no-config5", action="store_true")
+    ap.add_argument("--no-config1", action="store_true")
     return ap.parse_args()
 
 
@@ -158,6 +161,20 @@ def arap_bytes(n, t, nnz, st):
     full = float((it * per_outer + K * cg + R * rf).sum())
     comp = float((it * (per_outer + cg + rf)).sum())
     return full, comp
+
+
+def lscm_bytes(n, nnz, nbnd, st):
+    """Algorithmic bytes of one LSCM launch: the PCG formula on the 2n
+    unknowns (u, v) of each island, whose matrix holds the Laplacian twice
+    plus the boundary coupling (nnz_H = 2 nnz + 4 boundary vertices): per CG
+    iteration 8 nnz_H + 56 n, per FP64 residual 8 nnz_H + 52 n, with K and R
+    as executed; the compulsory bytes count one of each."""
+    K = st["cg_iters"].astype(np.float64)
+    R = st["refinements"].astype(np.float64)
+    nnz_h = 2.0 * nnz + 4.0 * nbnd
+    cg = 8.0 * nnz_h + 56.0 * n
+    rf = 8.0 * nnz_h + 52.0 * n
+    return float((K * cg + R * rf).sum()), float((cg + rf).sum())
 
 
 class PlainBatch:
@@ -481,6 +498,137 @@ def bench_overlap(islands, uvs, count=16):
             "collision_ms_per_chart": 1e3 * (t2 - t1) / len(pick), "overlapping": bad, "colliding_charts": int(coll)}
 
 
+def _events(dev):
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def bench_config5(dev, iters=ITERS, steps=2):
+    """Config 5 end to end at its stated size: a 5M-triangle noisy sphere cut
+    into 3,000 k-means charts (disk components kept), batched LSCM + ARAP,
+    per-chart p95 metrics, packing and exact validation of the packed atlas.
+    Device times by CUDA events (solve, metrics, validation), the public-API
+    wall time of every stage, validation pairs per second."""
+    import torch
+    from ultimate_uv_artist_b200 import _lib, synth
+    from ultimate_uv_artist_b200.device import DeviceBatch
+    from ultimate_uv_artist_b200.engine import gpu, metrics
+    from ultimate_uv_artist_b200.engine import param as Pm
+    from ultimate_uv_artist_b200.engine import validate as GV
+    g0 = time.perf_counter()
+    V, F = synth.noisy_sphere(seed=5000, tris=5_000_000)
+    charts = synth.disk_charts(V, F, synth.kmeans_charts(V, F, k=3000, seed=5001, device=dev), min_tris=20)
+    gen_s = time.perf_counter() - g0
+    items = [(p, t, None) for p, t in charts]
+    tris = int(sum(len(t) for _, t in charts))
+    stream = torch.cuda.current_stream(dev)
+    # public API, wall: batch build (host plan + uploads), LSCM + ARAP, download
+    w0 = time.perf_counter()
+    b = gpu.Batch(items, dev=dev)
+    torch.cuda.synchronize(); w1 = time.perf_counter()
+    b.db.lscm(); b.db.arap(iters=iters, line_search=True)
+    U = b.chart_uvs()
+    torch.cuda.synchronize(); w2 = time.perf_counter()
+    # device: setup + LSCM + ARAP, inputs resident
+    db = b.db
+    ev = []
+    for _ in range(steps):
+        a, c, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True), \
+            torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        db.setup(); db.lscm()
+        c.record(stream)
+        db.arap(iters=iters, line_search=True)
+        e.record(stream)
+        ev.append((a, c, e))
+    torch.cuda.synchronize()
+    lscm_ms = float(np.mean([a.elapsed_time(c) for a, c, _ in ev]))
+    arap_ms = float(np.mean([c.elapsed_time(e) for _, c, e in ev]))
+    st = db.island_status()
+    # per-chart p95 metrics (param.chart_quality) on a PARAM batch over the same plan
+    w3 = time.perf_counter()
+    dq = DeviceBatch(db.P, None, b.offsets, b._tofs, U=np.concatenate(U), semantics=_lib.SEM_PARAM, device=dev,
+                     plan=db.plan)
+    q = Pm.chart_quality_batch(dq)
+    torch.cuda.synchronize(); w4 = time.perf_counter()
+    p95 = np.array([x["aniso_p95"] for x in q])
+    del dq, b, db
+    torch.cuda.empty_cache()
+    # packing (shelf placement; test scaffolding, not the product) and validation
+    w5 = time.perf_counter()
+    packed = synth.shelf_pack(U, atlas=4096, padding=4)
+    pack_s = time.perf_counter() - w5
+    offs = np.cumsum([0] + [len(p) for p, _ in charts])
+    Vall = np.concatenate([p for p, _ in charts]).astype(np.float32)
+    Fall = np.concatenate([t + o for (_, t), o in zip(charts, offs[:-1])])
+    UVall = np.concatenate(packed).astype(np.float32)
+    w6 = time.perf_counter()
+    rep, _ = GV.validate_uvs(Vall, Fall, UVall, atlas=4096, padding=4)
+    val_api_s = time.perf_counter() - w6
+    dv = GV.DeviceValidation(Vall.astype(np.float64), Fall.astype(np.int32), UVall, device=dev)
+    dv.run(); dv.run()
+    e0, e1 = _events(dev)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(3):
+        dv.run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    val_ms = e0.elapsed_time(e1) / 3
+    c = dv.host_counts()
+    t0 = time.perf_counter()
+    g = metrics.min_gutter_device(dv.UV.double(), dv.F, dv.labels, int(c[6]), 4096)
+    torch.cuda.synchronize()
+    gutter_ms = (time.perf_counter() - t0) * 1e3
+    pairs = int(c[10])
+    return {"workload": "noisy_sphere_5M_kmeans3000_disk_charts", "mesh_triangles": int(len(F)),
+            "charts": len(charts), "triangles": tris, "vertices": int(offs[-1]), "generate_s": gen_s,
+            "lscm_setup_ms": lscm_ms, "arap_ms": arap_ms, "arap_iters": iters,
+            "tri_iters_per_s": tris * iters / ((lscm_ms + arap_ms) / 1e3),
+            "max_resid": float(st["resid"].max()),
+            "api_batch_build_s": w1 - w0, "api_solve_download_s": w2 - w1, "api_chart_quality_s": w4 - w3,
+            "aniso_p95_median": float(np.median(p95)), "aniso_p95_max": float(p95.max()),
+            "pack_s_host_shelf": pack_s, "validate_api_s": val_api_s,
+            "validate_ms_per_pass": val_ms, "pairs_aabb": pairs, "pairs_per_s": pairs / (val_ms / 1e3),
+            "gutter_ms_wall": gutter_ms, "min_gutter_texels": float(g), "valid": bool(rep["valid"]),
+            "overlapping_triangles": int(rep["overlapping_triangles_exact"]),
+            "flipped": int(rep["flipped_triangles"]), "islands": int(rep["islands"])}
+
+
+def bench_config1(dev, reps=5):
+    """Config 1 per call through the drop-in API: param.lscm, then
+    param.refine(iters=10) on the 4,802-triangle hemisphere patch (wall time
+    of each call, host arrays in and out), beside the oracle's restatement of
+    the reference's per-chart CPU calls (one thread, exact LU)."""
+    import torch
+    from oracle import arap as O
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.engine import param as Pm
+    V, F = synth.hemisphere_patch(seed=1000, n=50, jitter=0.01)
+    P = V.astype(np.float64)
+
+    def best(fn):
+        out, ts = None, []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn()
+            ts.append(time.perf_counter() - t0)
+        return out, min(ts)
+
+    Pm.lscm(P, F); Pm.refine(P, F, Pm.lscm(P, F), iters=10, tol=0.0)      # warm
+    U0, lscm_s = best(lambda: Pm.lscm(P, F))
+    U1, ref_s = best(lambda: Pm.refine(P, F, U0, iters=10, tol=0.0)[0])
+    R0, o_lscm = best(lambda: O.lscm(P, F))
+    R1, o_ref = best(lambda: O.refine_arap(P, F, R0, iters=10, line_search=True, tol=0.0))
+    ext = float(np.ptp(R1, 0).max())
+    return {"workload": "hemisphere_50x50_4802_tris", "triangles": int(len(F)),
+            "lscm_ms": lscm_s * 1e3, "refine10_ms": ref_s * 1e3,
+            "oracle_cpu_lscm_ms": o_lscm * 1e3, "oracle_cpu_refine10_ms": o_ref * 1e3,
+            "speedup_per_call": (o_lscm + o_ref) / (lscm_s + ref_s),
+            "max_rel_uv_error": float(np.abs(U1 - R1).max() / ext)}
+
+
 def run_reference(args):
     """CPU reference arm: the oracle port of param.lscm + param.refine per
     island over all host cores, on a bounded sample of the same workload."""
@@ -543,25 +691,32 @@ def main():
         # time the ARAP launch alone)
         db.setup(); db.lscm(); db.arap(iters=1)
         torch.cuda.synchronize()
-        graphs = (db.step_graph(setup=True, lscm=True, arap_iters=0),
+        graphs = (db.step_graph(setup=True, lscm=False, arap_iters=0),
+                  db.step_graph(setup=False, lscm=True, arap_iters=0),
                   db.step_graph(setup=False, lscm=False, arap_iters=args.iters, line_search=True))
 
     def step(record):
+        if record:
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         if graphs:
             graphs[0].launch()
         else:
             db.setup()
-            db.lscm()
         if record:
-            e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
+            e[0].record(stream)
         if graphs:
             graphs[1].launch()
         else:
+            db.lscm()
+        if record:
+            e[1].record(stream)
+        if graphs:
+            graphs[2].launch()
+        else:
             db.arap(iters=args.iters, line_search=True)
         if record:
-            e1.record(stream)
-            ev.append((e0, e1))
+            e[2].record(stream)
+            ev.append(e)
 
     for _ in range(args.warmup):
         step(False)
@@ -581,9 +736,12 @@ def main():
     if ws > 1:
         dist.barrier()
     ms = t0.elapsed_time(t1) / args.steps
-    arap_ms = float(np.mean([a.elapsed_time(c) for a, c in ev]))
+    arap_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in ev]))
+    lscm_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in ev]))
     st = db.island_status()
     our_uvs = b.chart_uvs()
+    db.setup(); db.lscm()                 # the LSCM solve's own counters
+    st_lscm = db.island_status()
     n, t, nnz = _island_stats(b)
     full, comp = arap_bytes(n, t, nnz, st)
     units = float(tris * args.iters)
@@ -631,6 +789,8 @@ def main():
         hbm = 6650.0; peak_src = "fallback"
     achieved = full / (arap_ms / 1e3) / 1e9
     achieved_c = comp / (arap_ms / 1e3) / 1e9
+    nbnd = np.diff(db.plan.bofs.astype(np.int64))
+    lfull, lcomp = lscm_bytes(n, nnz, nbnd, st_lscm)
 
     val = None
     if rank == 0 and not args.no_validate:
@@ -649,21 +809,31 @@ def main():
         bnd = bench_boundary(b)
         hier_b = bench_hier(dev)
         ovl = bench_overlap(islands, our_uvs)
+    c5 = c1 = None
+    if rank == 0 and not args.no_config5:
+        c5 = bench_config5(dev)
+    if rank == 0 and not args.no_config1:
+        c1 = bench_config1(dev)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import cpu_baseline
         sample = cpu_baseline.sample_islands(islands, args.cpu_budget_tris)
-        v, dt, workers, stris = cpu_baseline.time_cpu(sample, args.iters)
-        cpu = {"value": v, "unit": UNIT, "cores": workers, "kind": "port",
+        v, dt, workers, stris = cpu_baseline.time_cpu(sample, args.iters, repeats=args.cpu_repeats)
+        small = cpu_baseline.sample_islands(islands, args.cpu_budget_tris // 16)
+        v1, dt1, _, stris1 = cpu_baseline.time_cpu(small, args.iters, workers=1)
+        cpu = {"value": v, "unit": UNIT, "cores": workers, "kind": "port", "cpu_model": cpu_baseline.cpu_model(),
                "sample": f"{len(sample)} size-stratified islands of {len(islands)} ({stris} triangles), "
                          f"LSCM + {args.iters} ARAP iterations per island (param.lscm + param.refine, "
-                         f"exact LU), {dt:.1f} s"}
-        if val is not None:   # the validation workload's CPU time (oracle port, one thread)
+                         f"exact LU), best of {args.cpu_repeats}: {dt:.1f} s",
+               "one_thread": {"value": v1, "unit": UNIT, "seconds": dt1, "triangles": stris1,
+                              "sample": f"{len(small)} size-stratified islands"}}
+        if val is not None:   # the validation workload's CPU time (oracle port; overlap scan on all cores)
             from ultimate_uv_artist_b200 import synth as _synth
             Vv, Fv, UVv, _ = _synth.validation_atlas(seed=3000)
             vs, vrep = cpu_baseline.time_validation(Vv, Fv, UVv)
-            cpu["validation"] = {"seconds": vs, "cores": 1, "kind": "port",
+            cpu["validation"] = {"seconds": vs, "cores": cpu_baseline.omp_threads(), "kind": "port",
+                                 "best_of": 3,
                                  "pairs_per_s": val["pairs_aabb"] / vs,
                                  "same_report": all(float(vrep[k]) == float(val[k2]) for k, k2 in
                                                     (("overlapping_triangles_exact", "overlapping_triangles"),
@@ -701,9 +871,19 @@ def main():
                          "cg_iters_total": int(st["cg_iters"].sum()),
                          "refinements_total": int(st["refinements"].sum()),
                          "max_resid": float(st["resid"].max())},
+            "roofline_lscm": {"kernel": "k_islands<OP_LSCM>", "bound": "hbm",
+                              "achieved": lfull / (lscm_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                              "frac": lfull / (lscm_ms / 1e3) / 1e9 / hbm, "peak_source": peak_src,
+                              "traffic": None, "kernel_ms": lscm_ms, "algorithmic_bytes": lfull,
+                              "compulsory_bytes": lcomp,
+                              "compulsory_frac": lcomp / (lscm_ms / 1e3) / 1e9 / hbm,
+                              "cg_iters_total": int(st_lscm["cg_iters"].sum()),
+                              "refinements_total": int(st_lscm["refinements"].sum()),
+                              "max_resid": float(st_lscm["resid"].max())},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": 8 * args.steps,   # setup 6 (frames, wpin, vert_isl, rows, far_pair, coarse) + LSCM + ARAP
+            "lscm_ms": lscm_ms, "arap_ms": arap_ms,
             "graph": graphs is not None,
             "plain_gpu": plain,
             "clocks": ck,
@@ -711,6 +891,8 @@ def main():
             "boundary_checks": None if bnd is None else {k: v for k, v in bnd.items() if k != "hits"},
             "hier_solver": hier_b,
             "overlap_checks": ovl,
+            "config5": c5,
+            "config1": c1,
         }
         print(json.dumps(line), flush=True)
     if graphs:

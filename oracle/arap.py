@@ -615,6 +615,48 @@ def repair_flips_param(U, T, rounds=60):
 
 
 # ====================================================================== helpers
+def chart_quality(P, T, U):
+    """engine/param.py:519-551: flips against the majority orientation, the
+    closed-form singular values s1 >= s2 of each triangle's Jacobian,
+    anisotropy s1 / s2 and area ratio s1 s2 / scale with its area-weighted
+    p95 (argsort, cumulative weights, first index reaching 0.95 of the total)
+    and means, stretch and scale."""
+    P = np.asarray(P, np.float64)
+    U = np.asarray(U, np.float64)
+    T = np.asarray(T, np.int64)
+    X, area = local_frames(P, T)
+    sa = signed_areas(U, T)
+    A = area.sum()
+    npos, nneg = int((sa > 0).sum()), int((sa < 0).sum())
+    flips = int((sa <= 0).sum()) if npos >= nneg else int((sa >= 0).sum())
+    x1, x2, y2 = X[:, 1, 0], X[:, 2, 0], X[:, 2, 1]
+    ok = np.abs(x1 * y2) > 1e-300
+    x1s, y2s = np.where(ok, x1, 1.0), np.where(ok, y2, 1.0)
+    d1 = U[T[:, 1]] - U[T[:, 0]]
+    d2 = U[T[:, 2]] - U[T[:, 0]]
+    j00, j10 = d1[:, 0] / x1s, d1[:, 1] / x1s
+    j01, j11 = (d2[:, 0] - j00 * x2) / y2s, (d2[:, 1] - j10 * x2) / y2s
+    q = np.sqrt(((j00 + j11) / 2) ** 2 + ((j10 - j01) / 2) ** 2)
+    r = np.sqrt(((j00 - j11) / 2) ** 2 + ((j10 + j01) / 2) ** 2)
+    s1, s2 = q + r, np.abs(q - r)
+    sc = np.abs(sa).sum() / max(A, 1e-300)
+    w = area / max(A, 1e-300)
+    an = s1 / np.maximum(s2, 1e-12)
+    ar = s1 * s2 / max(sc, 1e-300)
+    lar = np.abs(np.log2(np.maximum(ar, 1e-12)))
+
+    def p95(x):
+        o = np.argsort(x)
+        cw = np.cumsum(w[o])
+        return float(x[o][min(np.searchsorted(cw, 0.95 * cw[-1]), len(o) - 1)])
+
+    st2 = (s1 ** 2 + s2 ** 2) / 2 / max(sc, 1e-300)
+    return {"flips": flips, "aniso_p95": p95(an), "aniso_mean": float((an * w).sum()),
+            "area_p95": float(2 ** p95(lar)), "area_logdev": float((lar * w).sum()),
+            "stretch": float(np.sqrt((st2 * w).sum())), "scale": float(np.sqrt(sc)),
+            "per_tri_aniso": an, "per_tri_area": ar}
+
+
 def uv_rel_error(U, Uref, offsets):
     """Per chart max |U - Uref| divided by the chart's UV extent; returns the
     max over charts."""

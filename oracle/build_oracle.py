@@ -1,5 +1,7 @@
 """Build the C part of the oracle (test infrastructure only) into
-oracle/liboracle_c.so with gcc, without floating-point contraction.
+oracle/liboracle_c.so with gcc, without floating-point contraction; the
+overlap scan runs its cells on OpenMP threads (OMP_NUM_THREADS), as the
+reference's numba prange does.
 
     python oracle/build_oracle.py
 """
@@ -21,8 +23,8 @@ def build(force=False):
     if cc is None:
         raise RuntimeError("gcc not found: cannot build the C oracle")
     tmp = LIB + ".tmp"
-    subprocess.run([cc, "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared", SRC, "-o", tmp, "-lm"],
-                   check=True)
+    subprocess.run([cc, "-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared", SRC, "-o", tmp,
+                    "-lm"], check=True)
     os.replace(tmp, LIB)
     return LIB
 

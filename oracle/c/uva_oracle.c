@@ -139,6 +139,8 @@ int64_t uvo_overlaps(const double* U, const int64_t* F, const uint8_t* skip, int
     }
     memset(flag, 0, (size_t)m);
     int64_t tested = 0;
+    /* cells in parallel, like the reference's prange over cells */
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : tested)
     for (int64_t c = 0; c < G * G; ++c) {
         int64_t cy = c / G, cx = c % G;
         for (int64_t p = cnt[c]; p < cnt[c + 1]; ++p) {
@@ -149,7 +151,10 @@ int64_t uvo_overlaps(const double* U, const int64_t* F, const uint8_t* skip, int
                 if (x0[s] > x1[t] || x0[t] > x1[s] || y0[s] > y1[t] || y0[t] > y1[s]) continue;
                 ++tested;
                 int hit = strict ? tri_overlap_strict(U, F, s, t) : tri_overlap(U, F, s, t, rel);
-                if (hit) { flag[s] = 1; flag[t] = 1; }
+                if (hit) {
+                    __atomic_store_n(flag + s, (uint8_t)1, __ATOMIC_RELAXED);
+                    __atomic_store_n(flag + t, (uint8_t)1, __ATOMIC_RELAXED);
+                }
             }
         }
     }

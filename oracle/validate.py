@@ -333,9 +333,11 @@ def min_gutter(uv, faces, islands, res=4096):
 
 
 # ------------------------------------------------------------------ report
-def validate_uvs(v, f, uv, atlas=4096, padding=None, gutter=True, rel=1e-6):
+def validate_uvs(v, f, uv, atlas=4096, padding=None, gutter=True, rel=1e-6, count_pairs=True):
     """engine/validate.py:139-209 (without the preservation inputs).
-    Returns (report, problems mask, extras)."""
+    Returns (report, problems mask, extras). ``count_pairs`` adds the number
+    of candidate pairs with intersecting boxes (the pairs/s denominator; not
+    part of the reference's work)."""
     v = np.asarray(v, np.float64)
     f = np.asarray(f, np.int64)
     U = np.asarray(uv, np.float32).astype(np.float64)
@@ -366,7 +368,7 @@ def validate_uvs(v, f, uv, atlas=4096, padding=None, gutter=True, rel=1e-6):
     skip = ~has3d | sliver | ~np.isfinite(sa)
     G = int(np.clip(np.sqrt(len(f)) / 2, 64, 4096))
     ov, _ = overlaps_c(U, f, skip, G, rel)
-    npairs = count_bbox_pairs(U, f, skip)
+    npairs = count_bbox_pairs(U, f, skip) if count_pairs else None
     rep["overlapping_triangles_exact"] = int(ov.sum())
     ovs, _ = overlaps_c(U, f, skip, G, 0.0, strict=True)
     rep["float32_contacts"] = int((ovs & ~ov).sum())

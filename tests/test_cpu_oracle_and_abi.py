@@ -283,3 +283,15 @@ def test_cot_laplacian_assembly_against_reference():
     import scipy.sparse as sp
     D2 = sp.coo_matrix((W, (I, J)), shape=D.shape).toarray()
     assert np.max(np.abs(D2 - g["l_dense"])) <= 1e-12 * np.max(np.abs(g["l_dense"]))
+
+
+def test_oracle_chart_quality_against_reference(golden):
+    """oracle.arap.chart_quality equals the reference's param.chart_quality
+    (golden_small.npz, the refined hemisphere patch)."""
+    q = O.chart_quality(golden["p_P"], golden["p_T"], golden["p_U1"])
+    assert q["flips"] == int(golden["p_q_flips"])
+    assert abs(q["aniso_p95"] - float(golden["p_q_aniso_p95"])) <= 1e-12 * abs(float(golden["p_q_aniso_p95"]))
+    assert abs(q["area_p95"] - float(golden["p_q_area_p95"])) <= 1e-12 * abs(float(golden["p_q_area_p95"]))
+    assert abs(q["stretch"] - float(golden["p_q_stretch"])) <= 1e-12 * abs(float(golden["p_q_stretch"]))
+    assert np.allclose(q["per_tri_aniso"], golden["p_q_aniso"], rtol=1e-12)
+    assert np.allclose(q["per_tri_area"], golden["p_q_area"], rtol=1e-12)

@@ -76,3 +76,68 @@ def test_config5_dense_scan_reduced(cuda):
     UVall = np.concatenate(packed).astype(np.float32)
     rep = _validate_both(Vall, Fall, UVall, 2048, 4)
     assert rep["islands"] == len(charts)
+
+
+def test_config5_dense_scan_full_size(cuda):
+    """Config 5 at its stated size: a 5M-triangle sphere displaced by 4-octave
+    value noise (amplitude 0.05), cut into 3,000 k-means charts on normals,
+    split into connected components, the disk charts kept (at least 20
+    triangles). Batched LSCM + 20 ARAP iterations (gpu.Batch semantics) with
+    every global step at the FP64 residual bar; UVs against the FP64 oracle
+    on 12 size-stratified charts; per-chart p95 anisotropy and area ratio
+    (param.chart_quality) against the oracle on the same charts; then the
+    charts shelf-packed on a 4096 atlas (padding 4) and the validation report,
+    the overlap / strict-overlap / flip masks, the island partition and the
+    candidate-pair count compared with the oracle bit for bit."""
+    import torch
+    from oracle import cpu_baseline
+    from ultimate_uv_artist_b200 import _lib, synth
+    from ultimate_uv_artist_b200.device import DeviceBatch
+    from ultimate_uv_artist_b200.engine import gpu
+    from ultimate_uv_artist_b200.engine import param as Pm
+    from ultimate_uv_artist_b200.engine import validate as GV
+    V, F = synth.noisy_sphere(seed=5000, tris=5_000_000)
+    assert len(F) >= 4_900_000
+    charts = synth.disk_charts(V, F, synth.kmeans_charts(V, F, k=3000, seed=5001, device=cuda), min_tris=20)
+    tris = sum(len(t) for _, t in charts)
+    assert len(charts) >= 1500 and tris >= 3_000_000, (len(charts), tris)
+    b = gpu.Batch([(p, t, None) for p, t in charts])
+    b.lscm()
+    b.arap(20, line_search=True)
+    st = b.status()
+    assert (st["resid"] <= 2e-7 * 1.001).all() and (st["flags"] & 3 == 0).all()
+    U = b.chart_uvs()
+    err, ni, _ = cpu_baseline.uv_error_batch(charts, U, 20, count=12)
+    assert err < UV_TOL, err
+    # per-chart quality metrics (param.chart_quality) on a PARAM-semantics
+    # batch over the same plan, against the oracle on stratified charts
+    db = DeviceBatch(b.db.P, None, b.offsets, b._tofs, U=np.concatenate(U), semantics=_lib.SEM_PARAM,
+                     device=cuda, plan=b.db.plan)
+    q = Pm.chart_quality_batch(db)
+    order = np.argsort([len(t) for _, t in charts])
+    for i in order[np.linspace(0, len(order) - 1, 12).astype(int)]:
+        r = O.chart_quality(charts[i][0], charts[i][1], U[i])
+        assert q[i]["flips"] == r["flips"]
+        for k in ("aniso_p95", "area_p95"):
+            assert abs(q[i][k] - r[k]) <= 1e-4 * abs(r[k]), (i, k, q[i][k], r[k])
+    del db, b
+    torch.cuda.empty_cache()
+    packed = synth.shelf_pack(U, atlas=4096, padding=4)
+    offs = np.cumsum([0] + [len(p) for p, _ in charts])
+    Vall = np.concatenate([p for p, _ in charts]).astype(np.float32)
+    Fall = np.concatenate([t + o for (_, t), o in zip(charts, offs[:-1])])
+    UVall = np.concatenate(packed).astype(np.float32)
+    rep, problems = GV.validate_uvs(Vall, Fall, UVall, atlas=4096, padding=4)
+    ref, rprob, ex = OV.validate_uvs(Vall, Fall, UVall, atlas=4096, padding=4)
+    for k, v in ref.items():
+        if isinstance(v, (int, float, bool, np.integer, np.floating)):
+            assert float(rep[k]) == float(v), (k, rep[k], v)
+    assert np.array_equal(problems, rprob)
+    dv = GV.DeviceValidation(Vall.astype(np.float64), Fall.astype(np.int32), UVall).run()
+    fl = dv.flags()
+    assert np.array_equal((fl & 16) != 0, ex["ov"])
+    assert np.array_equal((fl & 32) != 0, ex["ov_strict"])
+    assert np.array_equal((fl & 8) != 0, ex["flipped"])
+    assert OV.same_partition(dv.labels.cpu().numpy()[:len(Fall)], ex["islands"])
+    assert int(dv.host_counts()[10]) == ex["pairs"]
+    assert rep["islands"] == len(charts)

@@ -193,10 +193,11 @@ def energy_islands(seed=4000, count=512, tmin=500, tmax=50000, degenerate=0.05, 
     for t in targets:
         P, T = disk_patch(rng, t / 0.785, bumps=8, amp=0.3)
         P = P.astype(np.float64)
-        inc = [[] for _ in range(len(P))]
-        for f, tri in enumerate(T):
-            for v in tri:
-                inc[v].append(f)
+        # faces incident to each vertex (CSR: vertex -> its corners' faces)
+        corner_v = T.reshape(-1)
+        by_v = np.argsort(corner_v, kind="stable")
+        vstart = np.searchsorted(corner_v[by_v], np.arange(len(P) + 1))
+        inc_f = by_v // 3
         k = int(degenerate * len(T))
         for f in rng.choice(len(T), k, replace=False):
             a, b, c = T[f]
@@ -208,7 +209,7 @@ def energy_islands(seed=4000, count=512, tmin=500, tmax=50000, degenerate=0.05, 
                 continue
             old = P[a].copy()
             P[a] = mid + (P[a] - mid) * (target_h / h)
-            tri = T[inc[a]]
+            tri = T[inc_f[vstart[a]:vstart[a + 1]]]
             u = P[tri][:, :, :2].astype(np.float32).astype(np.float64)   # as stored
             sa = (u[:, 1, 0] - u[:, 0, 0]) * (u[:, 2, 1] - u[:, 0, 1]) - (u[:, 2, 0] - u[:, 0, 0]) * (u[:, 1, 1] - u[:, 0, 1])
             if (sa <= 0).any():
@@ -269,10 +270,13 @@ def noisy_sphere(seed=5000, tris=5_000_000, amp=0.05):
     return V.astype(np.float32), F.astype(np.int64)
 
 
-def kmeans_charts(V, F, k=3000, seed=5001, iters=8):
+def kmeans_charts(V, F, k=3000, seed=5001, iters=8, device=None):
     """Cut a closed mesh into charts: k-means on face normals (plus a weak
     position term so charts stay compact), then split labels into connected
-    components. Returns a list of face-index arrays."""
+    components. Returns a list of face-index arrays. With a torch ``device``
+    the assignment steps run there (test-data generation at 5M faces)."""
+    import scipy.sparse as sp
+    from scipy.sparse.csgraph import connected_components
     rng = np.random.default_rng(seed)
     P = V.astype(np.float64)
     e1 = P[F[:, 1]] - P[F[:, 0]]; e2 = P[F[:, 2]] - P[F[:, 0]]
@@ -282,11 +286,24 @@ def kmeans_charts(V, F, k=3000, seed=5001, iters=8):
     C = feat[rng.choice(len(F), k, replace=False)]
     lab = np.zeros(len(F), np.int64)
     chunk = 1 << 18
+    if device is not None:
+        import torch
+        X = torch.from_numpy(feat).to(device)
+        x2 = (X * X).sum(1)
     for _ in range(iters):
-        for s in range(0, len(F), chunk):
-            x = feat[s:s + chunk]
-            d = (x * x).sum(1)[:, None] - 2 * x @ C.T + (C * C).sum(1)[None]
-            lab[s:s + chunk] = d.argmin(1)
+        if device is not None:
+            Ct = torch.from_numpy(C).to(device)
+            c2 = (Ct * Ct).sum(1)
+            lt = torch.empty(len(F), dtype=torch.int64, device=device)
+            for s in range(0, len(F), chunk):
+                d = x2[s:s + chunk, None] - 2 * X[s:s + chunk] @ Ct.T + c2[None]
+                lt[s:s + chunk] = d.argmin(1)
+            lab = lt.cpu().numpy()
+        else:
+            for s in range(0, len(F), chunk):
+                x = feat[s:s + chunk]
+                d = (x * x).sum(1)[:, None] - 2 * x @ C.T + (C * C).sum(1)[None]
+                lab[s:s + chunk] = d.argmin(1)
         cnt = np.bincount(lab, minlength=k)
         for j in range(feat.shape[1]):
             C[:, j] = np.bincount(lab, weights=feat[:, j], minlength=k) / np.maximum(cnt, 1)
@@ -299,18 +316,8 @@ def kmeans_charts(V, F, k=3000, seed=5001, iters=8):
     same = ks[1:] == ks[:-1]
     f0 = fs[:-1][same]; f1 = fs[1:][same]
     link = lab[f0] == lab[f1]
-    parent = np.arange(len(F))
-
-    def find(x):
-        while parent[x] != x:
-            parent[x] = parent[parent[x]]; x = parent[x]
-        return x
-    for u_, v_ in zip(f0[link].tolist(), f1[link].tolist()):
-        ru, rv = find(u_), find(v_)
-        if ru != rv:
-            parent[ru] = rv
-    roots = np.array([find(i) for i in range(len(F))])
-    _, comp = np.unique(roots, return_inverse=True)
+    G = sp.coo_matrix((np.ones(int(link.sum())), (f0[link], f1[link])), shape=(len(F), len(F)))
+    _, comp = connected_components(G, directed=False)
     order = np.argsort(comp, kind="stable")
     cuts = np.flatnonzero(np.diff(comp[order])) + 1
     return np.split(order, cuts)
