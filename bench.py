@@ -59,6 +59,7 @@ def _args():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--no-config5", action="store_true")
     ap.add_argument("--no-config1", action="store_true")
+    ap.add_argument("--no-config4", action="store_true")
     return ap.parse_args()
 
 
@@ -595,6 +596,58 @@ def bench_config5(dev, iters=ITERS, steps=2):
             "flipped": int(rep["flipped_triangles"]), "islands": int(rep["islands"])}
 
 
+def bench_energy(dev, hbm, reps=5):
+    """Config 4: the ARAP / symmetric-Dirichlet forward and backward kernels
+    on 512 islands of 500 to 50,000 triangles (5.8M, 5 % near-degenerate),
+    and 50 steps of p95-stretch refinement. Roofline per launch with FP64
+    UVs and positions: forward reads T (12 t) and P, U (24 n + 16 n);
+    backward reads the same and writes dU, dP (16 n + 24 n)."""
+    import torch
+    from ultimate_uv_artist_b200 import _lib, synth
+    from ultimate_uv_artist_b200.device import DeviceBatch, concat_charts
+    from ultimate_uv_artist_b200.energy import DistortionEnergy, sd_refine
+    from ultimate_uv_artist_b200.engine import param as Pm
+    isl = synth.energy_islands(seed=4000, count=512, tmin=500, tmax=50000)
+    P, T, _, vofs, tofs = concat_charts([(p, t) for p, t in isl], with_uv=False)
+    db = DeviceBatch(P, T, vofs, tofs, U=P[:, :2].copy(), semantics=_lib.SEM_PARAM, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    U = db.U[:db.n].clone().requires_grad_(True)
+    Pt = db.P[:db.n].clone().requires_grad_(True)
+    out = {"workload": "energy_islands_512_500_50000", "islands": db.nc, "triangles": db.t, "vertices": db.n}
+    for kind, name in ((0, "arap"), (1, "symmetric_dirichlet")):
+        for _ in range(2):
+            e = DistortionEnergy.apply(U, Pt, db, kind)
+            torch.autograd.grad(e.sum(), (U, Pt))
+        fw, bw = [], []
+        for _ in range(reps):
+            a, b_, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            a.record(stream)
+            e = DistortionEnergy.apply(U, Pt, db, kind)
+            b_.record(stream)
+            torch.autograd.grad(e.sum(), (U, Pt))
+            c.record(stream)
+            torch.cuda.synchronize()
+            fw.append(a.elapsed_time(b_)); bw.append(b_.elapsed_time(c))
+        fwd_b = 12.0 * db.t + 40.0 * db.n
+        bwd_b = 12.0 * db.t + 80.0 * db.n
+        f_ms, b_ms = min(fw), min(bw)
+        out[name] = {"fwd_ms": f_ms, "bwd_ms": b_ms, "fwd_bytes": fwd_b, "bwd_bytes": bwd_b,
+                     "fwd_gbs": fwd_b / (f_ms / 1e3) / 1e9, "bwd_gbs": bwd_b / (b_ms / 1e3) / 1e9,
+                     "fwd_frac": fwd_b / (f_ms / 1e3) / 1e9 / hbm, "bwd_frac": bwd_b / (b_ms / 1e3) / 1e9 / hbm}
+    q0 = np.array([q["aniso_p95"] for q in Pm.chart_quality_batch(db)])
+    a, c = _events(dev)
+    torch.cuda.synchronize()
+    a.record(stream)
+    sd_refine(db, steps=50)
+    c.record(stream)
+    torch.cuda.synchronize()
+    q1 = np.array([q["aniso_p95"] for q in Pm.chart_quality_batch(db)])
+    out["sd_refine_50_ms"] = a.elapsed_time(c)
+    out["aniso_p95_median_start"] = float(np.median(q0))
+    out["aniso_p95_median_after"] = float(np.median(q1))
+    return out
+
+
 def bench_config1(dev, reps=5):
     """Config 1 per call through the drop-in API: param.lscm, then
     param.refine(iters=10) on the 4,802-triangle hemisphere patch (wall time
@@ -809,9 +862,11 @@ def main():
         bnd = bench_boundary(b)
         hier_b = bench_hier(dev)
         ovl = bench_overlap(islands, our_uvs)
-    c5 = c1 = None
+    c5 = c1 = c4 = None
     if rank == 0 and not args.no_config5:
         c5 = bench_config5(dev)
+    if rank == 0 and not args.no_config4:
+        c4 = bench_energy(dev, hbm)
     if rank == 0 and not args.no_config1:
         c1 = bench_config1(dev)
 
@@ -892,6 +947,7 @@ def main():
             "hier_solver": hier_b,
             "overlap_checks": ovl,
             "config5": c5,
+            "config4_energy": c4,
             "config1": c1,
         }
         print(json.dumps(line), flush=True)

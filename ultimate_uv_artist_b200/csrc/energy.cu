@@ -94,19 +94,46 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// Triangles per thread of the forward pass: a thread sums a contiguous run
+// of triangles (islands are contiguous in triangle order), then the warp
+// folds runs of the same island, so an island's sum takes one FP64 atomic
+// per warp and island instead of one per triangle.
+constexpr int kFwdItems = 8;
+
 __global__ void k_energy_fwd(const uva_batch b, const double* P, const double* U, int kind, double* e_isl, double* e_tri) {
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= b.t) return;
-    const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
-    const EnTri t = en_tri(P, U, b.vofs[tv.w], tv);
-    double e = 0.0;
-    if (t.live) {
-        double f_, G[4];
-        en_f(t, kind, f_, G);
-        e = t.area * f_;
+    const int lane = threadIdx.x & 31;
+    const int64_t f0 = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * kFwdItems;
+    int isl = -1;
+    double acc = 0.0;
+    for (int k = 0; k < kFwdItems; ++k) {
+        const int64_t f = f0 + k;
+        if (f >= b.t) break;
+        const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
+        const EnTri t = en_tri(P, U, b.vofs[tv.w], tv);
+        double e = 0.0;
+        if (t.live) {
+            double f_, G[4];
+            en_f(t, kind, f_, G);
+            e = t.area * f_;
+        }
+        if (e_tri) e_tri[f] = e;
+        if (tv.w != isl) {   // a new island inside the run: flush the previous one
+            if (isl >= 0 && acc != 0.0) atomicAdd(e_isl + isl, acc);
+            isl = tv.w;
+            acc = 0.0;
+        }
+        acc += e;
     }
-    if (e_tri) e_tri[f] = e;
-    if (e != 0.0) atomicAdd(e_isl + tv.w, e);
+    // fold the lanes' last runs: island ids do not decrease along the lanes
+    // (idle lanes carry -1 and never match a live run)
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_down_sync(0xffffffffu, acc, o);
+        const int yi = __shfl_down_sync(0xffffffffu, isl, o);
+        if (lane + o < 32 && yi == isl) acc += y;
+    }
+    const int prev = __shfl_up_sync(0xffffffffu, isl, 1);
+    if (isl >= 0 && (lane == 0 || prev != isl) && acc != 0.0) atomicAdd(e_isl + isl, acc);
 }
 
 __global__ void k_energy_bwd(const uva_batch b, const double* P, const double* U, int kind, const double* gscale,
@@ -183,36 +210,53 @@ __device__ __forceinline__ void atomic_min_pos(double* addr, double v) {
     atomicMin(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(__double_as_longlong(v)));
 }
 
+// Minimum over the warp's lanes of the same island (island ids do not
+// decrease along the lanes), one atomic per island and warp.
+__device__ __forceinline__ void island_min_fold(double* tmax, int isl, double t, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_down_sync(0xffffffffu, t, o);
+        const int yi = __shfl_down_sync(0xffffffffu, isl, o);
+        if (lane + o < 32 && yi == isl && y < t) t = y;
+    }
+    const int prev = __shfl_up_sync(0xffffffffu, isl, 1);
+    if (isl >= 0 && (lane == 0 || prev != isl)) atomic_min_pos(tmax + isl, t);
+}
+
 // Per-island flip-safe bound (param.py:259-291 per island).
 __global__ void k_island_max_step(const uva_batch b, const double* U, const double* Dd, double* tmax) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= b.t) return;
-    const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
-    const int v0 = b.vofs[tv.w];
-    const double2* UU = reinterpret_cast<const double2*>(U);
-    const double2* DD = reinterpret_cast<const double2*>(Dd);
-    const double2 u0 = UU[v0 + tv.x], u1 = UU[v0 + tv.y], u2 = UU[v0 + tv.z];
-    const double2 d0 = DD[v0 + tv.x], d1 = DD[v0 + tv.y], d2 = DD[v0 + tv.z];
-    const double ux1 = u1.x - u0.x, uy1 = u1.y - u0.y, ux2 = u2.x - u0.x, uy2 = u2.y - u0.y;
-    const double dx1 = d1.x - d0.x, dy1 = d1.y - d0.y, dx2 = d2.x - d0.x, dy2 = d2.y - d0.y;
-    const double C = ux1 * uy2 - ux2 * uy1;
-    const double B = ux1 * dy2 + dx1 * uy2 - ux2 * dy1 - dx2 * uy1;
-    const double A = dx1 * dy2 - dx2 * dy1;
+    const int lane = threadIdx.x & 31;
+    int isl = -1;          // idle lanes join the warp's fold with no island
     double t = 1e30;
-    if (C > 0.0) {
-        if (A == 0.0 || fabs(A) < 1e-30 * fmax(fabs(B), 1e-300)) {
-            if (B < 0.0) t = -C / B;
-        } else {
-            const double disc = B * B - 4.0 * A * C;
-            if (disc >= 0.0) {
-                const double sq = sqrt(disc);
-                const double r1 = (-B - sq) / (2.0 * A), r2 = (-B + sq) / (2.0 * A);
-                if (r1 > 0.0 && r1 < t) t = r1;
-                if (r2 > 0.0 && r2 < t) t = r2;
+    if (f < b.t) {
+        const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
+        isl = tv.w;
+        const int v0 = b.vofs[tv.w];
+        const double2* UU = reinterpret_cast<const double2*>(U);
+        const double2* DD = reinterpret_cast<const double2*>(Dd);
+        const double2 u0 = UU[v0 + tv.x], u1 = UU[v0 + tv.y], u2 = UU[v0 + tv.z];
+        const double2 d0 = DD[v0 + tv.x], d1 = DD[v0 + tv.y], d2 = DD[v0 + tv.z];
+        const double ux1 = u1.x - u0.x, uy1 = u1.y - u0.y, ux2 = u2.x - u0.x, uy2 = u2.y - u0.y;
+        const double dx1 = d1.x - d0.x, dy1 = d1.y - d0.y, dx2 = d2.x - d0.x, dy2 = d2.y - d0.y;
+        const double C = ux1 * uy2 - ux2 * uy1;
+        const double B = ux1 * dy2 + dx1 * uy2 - ux2 * dy1 - dx2 * uy1;
+        const double A = dx1 * dy2 - dx2 * dy1;
+        if (C > 0.0) {
+            if (A == 0.0 || fabs(A) < 1e-30 * fmax(fabs(B), 1e-300)) {
+                if (B < 0.0) t = -C / B;
+            } else {
+                const double disc = B * B - 4.0 * A * C;
+                if (disc >= 0.0) {
+                    const double sq = sqrt(disc);
+                    const double r1 = (-B - sq) / (2.0 * A), r2 = (-B + sq) / (2.0 * A);
+                    if (r1 > 0.0 && r1 < t) t = r1;
+                    if (r2 > 0.0 && r2 < t) t = r2;
+                }
             }
         }
     }
-    atomic_min_pos(tmax + tv.w, t);
+    island_min_fold(tmax, isl, t, lane);
 }
 
 __global__ void k_trial(int n, const uva_batch b, const double* U, const double* Dd, const double* alpha,
@@ -266,7 +310,7 @@ extern "C" int uva_energy_fwd(const uva_batch* b, const double* P, const double*
     if (!b || !P || !U || !e_isl || (kind != 0 && kind != 1)) { uva_set_error("uva_energy_fwd: bad arguments"); return UVA_E_ARG; }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaMemsetAsync(e_isl, 0, sizeof(double) * static_cast<size_t>(std::max(b->nc, 1)), s);
-    if (b->t > 0) k_energy_fwd<<<nb(b->t), 256, 0, s>>>(*b, P, U, kind, e_isl, e_tri);
+    if (b->t > 0) k_energy_fwd<<<nb((b->t + kFwdItems - 1) / kFwdItems), 256, 0, s>>>(*b, P, U, kind, e_isl, e_tri);
     UVA_CHECK_LAUNCH("uva_energy_fwd");
     return UVA_OK;
 }
