@@ -137,6 +137,45 @@ int uva_concat_charts(int32_t nc, const void* const* P, const int8_t* pdt, const
                       const int64_t* tofs, double* P_out, int64_t* T_out, double* U_out, int32_t nthreads);
 
 /* --------------------------------------------------------------------------
+ * Topology plan built on the device (csrc/dplan.cu): the arrays of
+ * uva_plan_export / uva_plan_export_rows (same values, element for element)
+ * from the island-local triangle lists, replacing the host plan's passes and
+ * their upload (gpu.py:39-63 unique_edges / sym_csr, param.py:59-68 boundary
+ * search; rows, slices and incidence have no reference counterpart). All
+ * pointers are device memory. The host supplies what follows from the sizes
+ * alone: agg_rows (rows per coarse aggregate: 0 up to 256 vertices, else the
+ * smallest multiple of 64 giving at most 256 aggregates) and sofs (first
+ * 32-row slice of each island). uva_dplan_build writes everything but the
+ * slots and reports sizes = {E, nslots, nbverts, status}; status bit 0: a
+ * vertex id outside its island, bit 1: an edge used by more than 127
+ * triangles in one direction (both: the plan is invalid). uva_dplan_slots,
+ * given the slot arrays (nslots each) and the same scratch, writes the
+ * sliced-ELL slots. Capacities: tri4 4t, tri_edge 3t, slice_ptr nslices+1,
+ * vt_ptr n+1, vt 3t, vflags n, bofs nc+1, bverts n, row_vert / vert_row n. */
+typedef struct uva_dplan {
+    int32_t nc, n, t, nslices;
+    const int32_t* vofs;       /* nc+1, vofs[0] = 0 */
+    const int32_t* tofs;       /* nc+1, tofs[0] = 0 */
+    const int32_t* T;          /* t*3 island-local vertex ids               */
+    const int32_t* agg_rows;   /* nc                                         */
+    const int32_t* sofs;       /* nc+1                                       */
+    int32_t* tri4;   int32_t* tri_edge; int32_t* slice_ptr; int32_t* vt_ptr; int32_t* vt;
+    uint8_t* vflags; int32_t* bofs;     int32_t* bverts;    int32_t* row_vert; int32_t* vert_row;
+    int64_t* sizes;            /* 4                                          */
+    void* scratch;             /* uva_dplan_scratch_bytes, kept between calls */
+    int64_t scratch_bytes;
+} uva_dplan;
+
+/* Host side of the upload: per-chart triangle arrays (int32 / int64
+ * island-local ids, tdt 0 / 1) into one int32 array at tofs, in parallel;
+ * UVA_E_ARG for an id outside the int32 range.                             */
+int uva_concat_tris32(int32_t nc, const void* const* T, const int8_t* tdt, const int64_t* tofs, int32_t* out,
+                      int32_t nthreads);
+int uva_dplan_scratch_bytes(int64_t n, int64_t t, int64_t nslices, int64_t* bytes);
+int uva_dplan_build(const uva_dplan* d, void* stream);
+int uva_dplan_slots(const uva_dplan* d, int32_t* slot_col, int32_t* slot_edge, float* slot_c, void* stream);
+
+/* --------------------------------------------------------------------------
  * Device batch descriptor: plain device pointers, filled by the host layer.
  * ------------------------------------------------------------------------ */
 typedef struct uva_batch {

@@ -58,6 +58,15 @@ class BatchDesc(C.Structure):
                 ("status", vp), ("work", vp), ("hist", vp)]
 
 
+class DPlanDesc(C.Structure):
+    """Mirror of ``uva_dplan``."""
+    _fields_ = [("nc", i32), ("n", i32), ("t", i32), ("nslices", i32),
+                ("vofs", vp), ("tofs", vp), ("T", vp), ("agg_rows", vp), ("sofs", vp),
+                ("tri4", vp), ("tri_edge", vp), ("slice_ptr", vp), ("vt_ptr", vp), ("vt", vp),
+                ("vflags", vp), ("bofs", vp), ("bverts", vp), ("row_vert", vp), ("vert_row", vp),
+                ("sizes", vp), ("scratch", vp), ("scratch_bytes", C.c_int64)]
+
+
 class SolveParams(C.Structure):
     _fields_ = [("iters", i32), ("line_search", i32), ("tol", C.c_double), ("energy_tol", C.c_double),
                 ("inner_eta", C.c_double), ("max_inner", i32), ("max_refine", i32), ("threads", i32),
@@ -118,6 +127,10 @@ _SIGS = {
     "uva_seam_report": [vp, C.c_int64, vp, C.c_int64, vp, vp, vp, vp, vp, C.c_int64, vp],
     "uva_corners_equal": [vp, i32, C.c_int64, vp, vp, i32, C.c_int64, vp, C.c_int64, i32, vp, vp],
     "uva_segment_sum": [vp, C.c_int64, vp, C.c_int64, i32, vp, vp, vp],
+    "uva_concat_tris32": [i32, vp, vp, vp, vp, i32],
+    "uva_dplan_scratch_bytes": [C.c_int64, C.c_int64, C.c_int64, vp],
+    "uva_dplan_build": [vp, vp],
+    "uva_dplan_slots": [vp, vp, vp, vp, vp],
     "uva_last_error": [],
     "uva_version": [],
 }

@@ -9,6 +9,7 @@
 // reads one slot of 32 consecutive rows with one coalesced load. Slice widths
 // are padded to a multiple of 4 slots (padding: weight 0, column = the row).
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <cstring>
 #include <memory>
@@ -541,5 +542,53 @@ extern "C" int uva_concat_charts(int32_t nc, const void* const* P, const int8_t*
     for (int32_t k = 1; k < nt; ++k) pool.emplace_back(worker);
     worker();
     for (auto& th : pool) th.join();
+    return UVA_OK;
+}
+
+// Per-chart triangle arrays (int32 / int64 island-local ids) into one int32
+// array at tofs, charts in parallel: the upload of the device-built plan
+// (csrc/dplan.cu). An id outside the int32 range is an error (the device
+// plan checks the island ranges).
+extern "C" int uva_concat_tris32(int32_t nc, const void* const* T, const int8_t* tdt, const int64_t* tofs,
+                                 int32_t* out, int32_t nthreads) {
+    if (nc < 0 || (nc > 0 && (!T || !tdt || !tofs || !out))) {
+        uva_set_error("uva_concat_tris32: bad arguments");
+        return UVA_E_ARG;
+    }
+    for (int32_t i = 0; i < nc; ++i) {
+        if (tofs[i + 1] < tofs[i] || tdt[i] < 0 || tdt[i] > 1 || (tofs[i + 1] > tofs[i] && !T[i])) {
+            uva_set_error("uva_concat_tris32: offsets must be non-decreasing, dtype codes 0/1, arrays non-null");
+            return UVA_E_ARG;
+        }
+    }
+    std::atomic<int32_t> next{0};
+    std::atomic<bool> wide{false};
+    auto worker = [&]() {
+        for (;;) {
+            const int32_t i = next.fetch_add(1);
+            if (i >= nc) break;
+            const int64_t cnt = 3 * (tofs[i + 1] - tofs[i]);
+            int32_t* o = out + 3 * (tofs[i] - tofs[0]);
+            if (tdt[i] == 0) {
+                std::memcpy(o, T[i], sizeof(int32_t) * static_cast<size_t>(cnt));
+            } else {
+                const int64_t* s = static_cast<const int64_t*>(T[i]);
+                bool bad = false;
+                for (int64_t k = 0; k < cnt; ++k) {
+                    const int64_t v = s[k];
+                    bad |= v < INT32_MIN || v > INT32_MAX;
+                    o[k] = static_cast<int32_t>(v);
+                }
+                if (bad) wide = true;
+            }
+        }
+    };
+    int32_t nt = nthreads > 0 ? nthreads : static_cast<int32_t>(std::thread::hardware_concurrency());
+    nt = std::max(1, std::min(nt, std::max(nc, 1)));
+    std::vector<std::thread> pool;
+    for (int32_t k = 1; k < nt; ++k) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    if (wide) { uva_set_error("uva_concat_tris32: a triangle index outside the int32 range"); return UVA_E_ARG; }
     return UVA_OK;
 }

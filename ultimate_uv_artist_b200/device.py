@@ -173,6 +173,130 @@ class Plan:
         self.classes = (mid, small)
 
 
+def coarse_sizes(nv):
+    """Rows per coarse aggregate, aggregates and coarse-block offsets of
+    islands with ``nv`` vertices (plan.cpp's rule: no coarse level up to 256
+    vertices, else the smallest multiple of 64 rows giving at most 256
+    aggregates), and the 32-row slice offsets."""
+    nv = np.asarray(nv, np.int64)
+    agg = np.where(nv > 256, 64 * np.maximum(1, -(-nv // (256 * 64))), 0).astype(np.int64)
+    ncoarse = np.where(agg > 0, -(-nv // np.maximum(agg, 1)), 0)
+    cofs = np.zeros(len(nv) + 1, np.int64)
+    np.cumsum(ncoarse * ncoarse, out=cofs[1:])
+    sofs = np.zeros(len(nv) + 1, np.int64)
+    np.cumsum(-(-nv // 32), out=sofs[1:])
+    return agg, ncoarse, cofs, sofs
+
+
+class DevicePlan:
+    """The topology plan built on the device (uva_dplan_build /
+    uva_dplan_slots): the arrays of Plan, element for element, from the
+    charts' island-local triangles. The host concatenates the triangles as
+    int32 (page-locked, in parallel), uploads them with the offsets and the
+    size-only quantities (aggregate rows, slice and coarse offsets), and
+    reads back four sizes. Host copies of the arrays are made on first
+    access (``plan.slot_edge`` etc.), for the bench's statistics."""
+
+    EXPORTED = Plan.EXPORTED
+    on_device = True
+
+    def __init__(self, chart_tris, vofs, tofs, device, stream=None):
+        L = _lib.lib()
+        d = require_cuda(device)
+        vofs = np.ascontiguousarray(vofs, np.int64)
+        tofs = np.ascontiguousarray(tofs, np.int64)
+        nc = len(vofs) - 1
+        if nc and (vofs[0] != 0 or tofs[0] != 0 or (np.diff(vofs) < 0).any() or (np.diff(tofs) < 0).any()):
+            raise ValueError("DevicePlan: offsets must start at 0 and not decrease")
+        self.nc, self.n, self.t = nc, int(vofs[-1]), int(tofs[-1])
+        nv = np.diff(vofs)
+        if self.n > (1 << 30) or 3 * self.t > (1 << 30):
+            raise ValueError("uva_plan_create: batch too large for 32-bit indices")
+        if nc and int(nv.max()) >= (1 << 24):
+            raise ValueError("uva_plan_create: island above 16M vertices")
+        agg, ncoarse, cofs, sofs = coarse_sizes(nv)
+        self.nslices = int(sofs[-1])
+        self.ncoarse = int(cofs[-1])
+        self.maxrows = int(nv.max()) if nc else 0
+        self.vofs = vofs.astype(np.int32)
+        self.tofs = tofs.astype(np.int32)
+        self.h2d_bytes = 0
+        tp, tdt = chart_tris[0], chart_tris[1]
+        T32 = host_empty((max(self.t, 1), 3), np.int32)
+        if nc:
+            check(L.uva_concat_tris32(nc, ptr(tp), ptr(tdt), ptr(tofs), ptr(T32), 0), "uva_concat_tris32")
+        ctx = torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()
+        with ctx:
+            def up(a):
+                t = torch.from_numpy(np.ascontiguousarray(a))
+                self.h2d_bytes += t.numel() * t.element_size()
+                return t.to(d, non_blocking=t.is_pinned())
+            i32 = torch.int32
+            vd, td = up(self.vofs), up(self.tofs)
+            Td = up(T32)
+            self.agg_rows = up(agg.astype(np.int32) if nc else np.zeros(1, np.int32))
+            self.cofs = up(cofs.astype(np.int32))
+            sofs_d = up(sofs.astype(np.int32))
+            n1, t1 = max(self.n, 1), max(self.t, 1)
+            dev = {"tri4": torch.empty((t1, 4), dtype=i32, device=d), "tri_edge": torch.empty((t1, 3), dtype=i32, device=d),
+                   "sofs": sofs_d, "slice_ptr": torch.empty(self.nslices + 1, dtype=i32, device=d),
+                   "vt_ptr": torch.empty(self.n + 1, dtype=i32, device=d), "vt": torch.empty(3 * t1, dtype=i32, device=d),
+                   "vflags": torch.empty(n1, dtype=torch.uint8, device=d), "bofs": torch.empty(nc + 1, dtype=i32, device=d),
+                   "bverts": torch.empty(n1, dtype=i32, device=d)}
+            self.row_vert = torch.empty(n1, dtype=i32, device=d)
+            self.vert_row = torch.empty(n1, dtype=i32, device=d)
+            sizes = torch.zeros(4, dtype=torch.int64, device=d)
+            nb = C.c_int64()
+            check(L.uva_dplan_scratch_bytes(self.n, self.t, self.nslices, C.byref(nb)), "uva_dplan_scratch_bytes")
+            scratch = torch.empty(max(int(nb.value), 256), dtype=torch.uint8, device=d)
+            D = _lib.DPlanDesc()
+            D.nc, D.n, D.t, D.nslices = nc, self.n, self.t, self.nslices
+            D.vofs, D.tofs, D.T, D.agg_rows, D.sofs = (vd.data_ptr(), td.data_ptr(), Td.data_ptr(),
+                                                       self.agg_rows.data_ptr(), sofs_d.data_ptr())
+            for k in ("tri4", "tri_edge", "slice_ptr", "vt_ptr", "vt", "vflags", "bofs", "bverts"):
+                setattr(D, k, dev[k].data_ptr())
+            D.row_vert, D.vert_row = self.row_vert.data_ptr(), self.vert_row.data_ptr()
+            D.sizes, D.scratch, D.scratch_bytes = sizes.data_ptr(), scratch.data_ptr(), int(nb.value)
+            s = stream if stream is not None else torch.cuda.current_stream(d)
+            sh = C.c_void_p(s.cuda_stream)
+            check(L.uva_dplan_build(C.byref(D), sh), "uva_dplan_build")
+            sz = sizes.cpu().numpy()     # waits for the build
+            if sz[3] & 1:
+                raise ValueError("uva_plan_create: triangle index outside its island")
+            if sz[3] & 2:
+                raise ValueError("uva_plan_create: an edge is used by more than 127 triangles in one direction")
+            if sz[3] & 4:
+                raise RuntimeError("uva_dplan_build: the row walk ran out of vertices")
+            self.E, self.nslots, self.nbverts = int(sz[0]), int(sz[1]), int(sz[2])
+            if self.nslots < 0:
+                raise ValueError("uva_plan_create: plan too large for 32-bit offsets")
+            for k, dt in (("slot_col", i32), ("slot_edge", i32), ("slot_c", torch.float32)):
+                dev[k] = torch.empty(max(self.nslots, 1), dtype=dt, device=d)
+            check(L.uva_dplan_slots(C.byref(D), dev["slot_col"].data_ptr(), dev["slot_edge"].data_ptr(),
+                                    dev["slot_c"].data_ptr(), sh), "uva_dplan_slots")
+            dev["bverts"] = dev["bverts"][:max(self.nbverts, 1)]
+            self._keep = (Td, scratch, T32)   # in use until the stream passes the slot pass
+        self.dev_arrays = dev
+        self.set_classes(_lib.CLASS_MID, _lib.CLASS_SMALL)
+
+    set_classes = Plan.set_classes
+
+    def __getattr__(self, name):
+        # host copies of the device arrays, made on first access
+        if name in DevicePlan.EXPORTED:
+            a = self.__dict__["dev_arrays"][name]
+            sizes = {"bverts": self.nbverts, "slot_col": self.nslots, "slot_edge": self.nslots,
+                     "slot_c": self.nslots, "vflags": self.n}
+            out = a.cpu().numpy()
+            if name in sizes:
+                out = out[:sizes[name]]
+            elif name in ("tri4", "tri_edge", "vt"):
+                out = out[:self.t] if name != "vt" else out[:3 * self.t]
+            self.__dict__[name] = out
+            return out
+        raise AttributeError(name)
+
+
 _FLOAT_CODE = {np.dtype(np.float32): 0, np.dtype(np.float64): 1}
 _INT_CODE = {np.dtype(np.int32): 0, np.dtype(np.int64): 1}
 
@@ -259,6 +383,9 @@ class DeviceBatch:
             self.h2d_bytes = 0   # bytes copied host -> device by this constructor
 
             def up(a, dtype=None):
+                if isinstance(a, torch.Tensor):   # built on the device (DevicePlan)
+                    t = a if a.numel() else torch.zeros(1, dtype=a.dtype, device=d)
+                    return t.to(d) if dtype is None else t.to(d, dtype)
                 t = torch.from_numpy(np.ascontiguousarray(a))
                 if t.numel() == 0:
                     t = torch.zeros(1, dtype=t.dtype)
@@ -271,10 +398,14 @@ class DeviceBatch:
             # topology
             self.vofs = up(plan.vofs); self.tofs = up(plan.tofs); self.order = up(plan.order)
             pd = plan.dev_arrays if plan.dev_arrays is not None and plan.dev_arrays['tri4'].device == d else None
-            for k in Plan.EXPORTED:   # copied during the plan's export, or now
+            built_on_device = getattr(plan, "on_device", False)
+            if built_on_device:
+                self.h2d_bytes += plan.h2d_bytes   # triangles and offsets; the plan's arrays were made there
+            for k in Plan.EXPORTED:   # copied during the plan's export, or made on the device, or copied now
                 if pd is not None:
                     setattr(self, k, pd[k] if pd[k].numel() else torch.zeros(1, dtype=pd[k].dtype, device=d))
-                    self.h2d_bytes += pd[k].numel() * pd[k].element_size()
+                    if not built_on_device:
+                        self.h2d_bytes += pd[k].numel() * pd[k].element_size()
                 else:
                     setattr(self, k, up(getattr(plan, k)))
             self.row_vert = up(plan.row_vert); self.vert_row = up(plan.vert_row)

@@ -23,7 +23,7 @@ import numpy as np
 import torch
 
 from .. import _lib, meshops
-from ..device import DeviceBatch, Plan, concat_charts, require_cuda
+from ..device import DeviceBatch, DevicePlan, Plan, concat_charts, require_cuda
 
 
 def csr32(A):
@@ -80,7 +80,7 @@ class Batch:
     the CPU with param.lscm before building the Batch).
     """
 
-    def __init__(self, charts, dev=None, dtype=torch.float32, stream=None):
+    def __init__(self, charts, dev=None, dtype=torch.float32, stream=None, plan_on="device"):
         self.dev = require_cuda(dev if dev is not None else device())
         self.dt = dtype
         # positions (and UVs) are concatenated; the topology plan reads every
@@ -94,7 +94,13 @@ class Batch:
         self._tofs = tofs
         with (torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()):
             P_dev = torch.from_numpy(P).to(self.dev, non_blocking=True) if self.n else None
-        plan = Plan(None, vofs, tofs, chart_tris=Tc[:2], device=self.dev, stream=stream)   # export || copies
+        # the topology plan is built on the device from the triangles; the
+        # host plan (plan_on="host": built on the host cores, exported and
+        # copied range by range) gives the same arrays
+        if plan_on == "device":
+            plan = DevicePlan(Tc[:2], vofs, tofs, device=self.dev, stream=stream)
+        else:
+            plan = Plan(None, vofs, tofs, chart_tris=Tc[:2], device=self.dev, stream=stream)   # export || copies
         self.db = DeviceBatch(P_dev if P_dev is not None else P, None, vofs, tofs, U=U, semantics=_lib.SEM_BATCH,
                               device=self.dev, stream=stream, plan=plan)
         self.db._host_src = (P, U)          # the asynchronous copies read these until they finish
