@@ -171,6 +171,10 @@ typedef struct uva_dplan {
  * UVA_E_ARG for an id outside the int32 range.                             */
 int uva_concat_tris32(int32_t nc, const void* const* T, const int8_t* tdt, const int64_t* tofs, int32_t* out,
                       int32_t nthreads);
+/* Per-chart float32 rows (width floats) into one float32 array at ofs, in
+ * parallel (positions that are float32 upload as they are).               */
+int uva_concat_rows32(int32_t nc, const void* const* src, const int64_t* ofs, int32_t width, float* out,
+                      int32_t nthreads);
 int uva_dplan_scratch_bytes(int64_t n, int64_t t, int64_t nslices, int64_t* bytes);
 int uva_dplan_build(const uva_dplan* d, void* stream);
 int uva_dplan_slots(const uva_dplan* d, int32_t* slot_col, int32_t* slot_edge, float* slot_c, void* stream);

@@ -592,3 +592,36 @@ extern "C" int uva_concat_tris32(int32_t nc, const void* const* T, const int8_t*
     if (wide) { uva_set_error("uva_concat_tris32: a triangle index outside the int32 range"); return UVA_E_ARG; }
     return UVA_OK;
 }
+
+// Per-chart float32 rows (width floats each) into one float32 array at ofs,
+// charts in parallel: positions that are float32 already travel to the
+// device as they are (half the bytes of the FP64 batch copy).
+extern "C" int uva_concat_rows32(int32_t nc, const void* const* src, const int64_t* ofs, int32_t width, float* out,
+                                 int32_t nthreads) {
+    if (nc < 0 || width <= 0 || (nc > 0 && (!src || !ofs || !out))) {
+        uva_set_error("uva_concat_rows32: bad arguments");
+        return UVA_E_ARG;
+    }
+    for (int32_t i = 0; i < nc; ++i) {
+        if (ofs[i + 1] < ofs[i] || (ofs[i + 1] > ofs[i] && !src[i])) {
+            uva_set_error("uva_concat_rows32: offsets must be non-decreasing, arrays non-null");
+            return UVA_E_ARG;
+        }
+    }
+    std::atomic<int32_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const int32_t i = next.fetch_add(1);
+            if (i >= nc) break;
+            std::memcpy(out + width * (ofs[i] - ofs[0]), src[i],
+                        sizeof(float) * static_cast<size_t>(width * (ofs[i + 1] - ofs[i])));
+        }
+    };
+    int32_t nt = nthreads > 0 ? nthreads : static_cast<int32_t>(std::thread::hardware_concurrency());
+    nt = std::max(1, std::min(nt, std::max(nc, 1)));
+    std::vector<std::thread> pool;
+    for (int32_t k = 1; k < nt; ++k) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    return UVA_OK;
+}

@@ -200,7 +200,10 @@ class DevicePlan:
     EXPORTED = Plan.EXPORTED
     on_device = True
 
-    def __init__(self, chart_tris, vofs, tofs, device, stream=None):
+    def __init__(self, chart_tris, vofs, tofs, device, stream=None, finish=True):
+        """Launches the build on ``stream``; with ``finish`` False the caller
+        runs host work of its own and then calls finish() (which waits for
+        the build's sizes and launches the slot pass)."""
         L = _lib.lib()
         d = require_cuda(device)
         vofs = np.ascontiguousarray(vofs, np.int64)
@@ -258,8 +261,21 @@ class DevicePlan:
             D.row_vert, D.vert_row = self.row_vert.data_ptr(), self.vert_row.data_ptr()
             D.sizes, D.scratch, D.scratch_bytes = sizes.data_ptr(), scratch.data_ptr(), int(nb.value)
             s = stream if stream is not None else torch.cuda.current_stream(d)
-            sh = C.c_void_p(s.cuda_stream)
-            check(L.uva_dplan_build(C.byref(D), sh), "uva_dplan_build")
+            check(L.uva_dplan_build(C.byref(D), C.c_void_p(s.cuda_stream)), "uva_dplan_build")
+        self._pending = (D, sizes, dev, s, d, Td, scratch, T32)
+        self.dev_arrays = None
+        if finish:
+            self.finish()
+
+    def finish(self):
+        """Sizes of the build (waits for it), then the sliced-ELL slots."""
+        if self._pending is None:
+            return self
+        L = _lib.lib()
+        D, sizes, dev, s, d, Td, scratch, T32 = self._pending
+        i32 = torch.int32
+        sh = C.c_void_p(s.cuda_stream)
+        with torch.cuda.stream(s):
             sz = sizes.cpu().numpy()     # waits for the build
             if sz[3] & 1:
                 raise ValueError("uva_plan_create: triangle index outside its island")
@@ -275,9 +291,11 @@ class DevicePlan:
             check(L.uva_dplan_slots(C.byref(D), dev["slot_col"].data_ptr(), dev["slot_edge"].data_ptr(),
                                     dev["slot_c"].data_ptr(), sh), "uva_dplan_slots")
             dev["bverts"] = dev["bverts"][:max(self.nbverts, 1)]
-            self._keep = (Td, scratch, T32)   # in use until the stream passes the slot pass
+        self._keep = (Td, scratch, T32)   # in use until the stream passes the slot pass
+        self._pending = None
         self.dev_arrays = dev
         self.set_classes(_lib.CLASS_MID, _lib.CLASS_SMALL)
+        return self
 
     set_classes = Plan.set_classes
 
@@ -311,6 +329,80 @@ def _chart_array(a, width, codes, fallback):
     return a, codes[a.dtype]
 
 
+class ChartArrays:
+    """Per-chart arrays of a batch, checked and C-contiguous (no copies when
+    their dtypes are ones the host copies read), with dtype codes, pointer
+    arrays and vertex / triangle offsets."""
+
+    def __init__(self, charts, with_uv=True):
+        nc = len(charts)
+        self.nc = nc
+        self.Ps, self.Ts, self.Us = [], [], []
+        self.pdt = np.empty(max(nc, 1), np.int8)
+        self.tdt = np.empty(max(nc, 1), np.int8)
+        self.udt = np.full(max(nc, 1), -1, np.int8)
+        nvs, nts = [], []
+        self.any_uv = False
+        fc, ic = _FLOAT_CODE, _INT_CODE
+        for i, ch in enumerate(charts):
+            a, t = ch[0], ch[1]
+            # arrays already in a layout the copies read are taken as they are
+            if type(a) is np.ndarray and a.ndim == 2 and a.shape[1] == 3 and a.dtype in fc and a.flags.c_contiguous:
+                self.pdt[i] = fc[a.dtype]
+            else:
+                a, self.pdt[i] = _chart_array(a, 3, fc, np.float64)
+            if type(t) is np.ndarray and t.ndim == 2 and t.shape[1] == 3 and t.dtype in ic and t.flags.c_contiguous:
+                self.tdt[i] = ic[t.dtype]
+            else:
+                t, self.tdt[i] = _chart_array(t, 3, ic, np.int64)
+            self.Ps.append(a)
+            self.Ts.append(t)
+            nvs.append(a.shape[0])
+            nts.append(t.shape[0])
+            u = None
+            if with_uv and len(ch) > 2 and ch[2] is not None:
+                u, self.udt[i] = _chart_array(ch[2], 2, fc, np.float64)
+                if len(u) != len(a):
+                    raise ValueError(f"chart {i}: U has {len(u)} rows for {len(a)} vertices")
+                self.any_uv = True
+            self.Us.append(u)
+        self.vofs = np.zeros(nc + 1, np.int64)
+        self.tofs = np.zeros(nc + 1, np.int64)
+        if nc:
+            np.cumsum(nvs, out=self.vofs[1:])
+            np.cumsum(nts, out=self.tofs[1:])
+        self.tp = np.fromiter((x.__array_interface__["data"][0] for x in self.Ts), np.uintp, nc) if nc else \
+            np.zeros(1, np.uintp)
+        self.pp = np.fromiter((x.__array_interface__["data"][0] for x in self.Ps), np.uintp, nc) if nc else \
+            np.zeros(1, np.uintp)
+
+    @property
+    def chart_tris(self):
+        """(pointer array, dtype codes, arrays) of the triangles for the plans
+        (the arrays stay referenced while a plan reads them)."""
+        return self.tp, self.tdt, self.Ts
+
+    def points(self, fp32=False):
+        """(P, U): concatenated positions (page-locked; float32 when ``fp32``
+        and every chart is float32 and none brings UVs, else FP64) and FP64
+        UVs (None when no chart brings UVs), copied in parallel on the host."""
+        nc, n = self.nc, int(self.vofs[-1])
+        L = _lib.lib()
+        U = host_empty((n, 2), np.float64) if self.any_uv else None
+        if fp32 and nc and (self.pdt[:nc] == 0).all() and U is None:
+            P = host_empty((n, 3), np.float32)
+            check(L.uva_concat_rows32(nc, ptr(self.pp), ptr(self.vofs), 3, ptr(P), 0), "uva_concat_rows32")
+            return P, None
+        P = host_empty((n, 3), np.float64)
+        if nc:
+            up_ = np.fromiter((0 if x is None else x.ctypes.data for x in self.Us), np.uintp, nc) if self.any_uv else None
+            check(L.uva_concat_charts(nc, ptr(self.pp), ptr(self.pdt), ptr(self.tp), ptr(self.tdt),
+                                      ptr(up_) if self.any_uv else None, ptr(self.udt) if self.any_uv else None,
+                                      ptr(self.vofs), ptr(self.tofs), ptr(P), None, ptr(U) if U is not None else None,
+                                      0), "uva_concat_charts")
+        return P, U
+
+
 def concat_charts(charts, with_uv=True, with_t=True):
     """(P, T, U) per chart -> concatenated FP64 P, local int64 T, FP64 U, offsets
     (uva_concat_charts copies the charts in parallel; P and U in page-locked
@@ -318,46 +410,14 @@ def concat_charts(charts, with_uv=True, with_t=True):
     upload: the device UVs start at zero). With ``with_t`` False the
     triangles are not copied: T is then (pointer array, dtype codes, arrays)
     of the per-chart arrays for Plan(chart_tris=...)."""
-    nc = len(charts)
-    Ps, Ts, Us = [], [], []
-    pdt = np.empty(max(nc, 1), np.int8)
-    tdt = np.empty(max(nc, 1), np.int8)
-    udt = np.full(max(nc, 1), -1, np.int8)
-    nvs, nts = [], []
-    any_uv = False
-    for i, ch in enumerate(charts):
-        a, pdt[i] = _chart_array(ch[0], 3, _FLOAT_CODE, np.float64)
-        t, tdt[i] = _chart_array(ch[1], 3, _INT_CODE, np.int64)
-        Ps.append(a)
-        Ts.append(t)
-        nvs.append(a.shape[0])
-        nts.append(t.shape[0])
-        u = None
-        if with_uv and len(ch) > 2 and ch[2] is not None:
-            u, udt[i] = _chart_array(ch[2], 2, _FLOAT_CODE, np.float64)
-            if len(u) != len(a):
-                raise ValueError(f"chart {i}: U has {len(u)} rows for {len(a)} vertices")
-            any_uv = True
-        Us.append(u)
-    vofs = np.zeros(nc + 1, np.int64)
-    tofs = np.zeros(nc + 1, np.int64)
-    if nc:
-        np.cumsum(nvs, out=vofs[1:])
-        np.cumsum(nts, out=tofs[1:])
-    P = host_empty((int(vofs[-1]), 3), np.float64)
-    T = np.empty((int(tofs[-1]), 3), np.int64) if with_t else None
-    U = host_empty((int(vofs[-1]), 2), np.float64) if any_uv else None
-    tp = np.fromiter((x.ctypes.data for x in Ts), np.uintp, nc) if nc else np.zeros(1, np.uintp)
-    if nc:
-        pp = np.fromiter((x.ctypes.data for x in Ps), np.uintp, nc)
-        up_ = np.fromiter((0 if x is None else x.ctypes.data for x in Us), np.uintp, nc) if any_uv else None
-        check(_lib.lib().uva_concat_charts(nc, ptr(pp), ptr(pdt), ptr(tp), ptr(tdt), ptr(up_) if any_uv else None,
-                                           ptr(udt) if any_uv else None, ptr(vofs), ptr(tofs), ptr(P),
-                                           ptr(T) if T is not None else None, ptr(U) if U is not None else None, 0),
-              "uva_concat_charts")
+    ca = ChartArrays(charts, with_uv=with_uv)
+    P, U = ca.points()
     if not with_t:
-        T = (tp, tdt, Ts)   # Ts keeps the arrays alive while the plan reads them
-    return P, T, U, vofs, tofs
+        return P, ca.chart_tris, U, ca.vofs, ca.tofs
+    T = np.empty((int(ca.tofs[-1]), 3), np.int64)
+    for t, a, b in zip(ca.Ts, ca.tofs[:-1], ca.tofs[1:]):
+        T[a:b] = t
+    return P, T, U, ca.vofs, ca.tofs
 
 
 class DeviceBatch:

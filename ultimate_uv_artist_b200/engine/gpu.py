@@ -23,7 +23,7 @@ import numpy as np
 import torch
 
 from .. import _lib, meshops
-from ..device import DeviceBatch, DevicePlan, Plan, concat_charts, require_cuda
+from ..device import ChartArrays, DeviceBatch, DevicePlan, Plan, require_cuda
 
 
 def csr32(A):
@@ -83,24 +83,27 @@ class Batch:
     def __init__(self, charts, dev=None, dtype=torch.float32, stream=None, plan_on="device"):
         self.dev = require_cuda(dev if dev is not None else device())
         self.dt = dtype
-        # positions (and UVs) are concatenated; the topology plan reads every
-        # chart's triangles where they are; the positions' upload runs while
-        # the plan is built, and each finished range of the plan's arrays is
-        # copied while the next one is exported
-        P, Tc, U, vofs, tofs = concat_charts(charts, with_t=False)
+        ca = ChartArrays(charts)
+        vofs, tofs = ca.vofs, ca.tofs
         self.nc = len(charts)
         self.offsets = vofs.copy()
         self.n = int(vofs[-1])
         self._tofs = tofs
-        with (torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()):
-            P_dev = torch.from_numpy(P).to(self.dev, non_blocking=True) if self.n else None
-        # the topology plan is built on the device from the triangles; the
-        # host plan (plan_on="host": built on the host cores, exported and
-        # copied range by range) gives the same arrays
+        # The topology plan is built on the device from the triangles: its
+        # build runs while the host copies the positions (float32 charts
+        # travel as float32) and uploads them. plan_on="host" builds the same
+        # arrays on the host cores and copies them range by range.
+        ctx = torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()
+        plan = None
         if plan_on == "device":
-            plan = DevicePlan(Tc[:2], vofs, tofs, device=self.dev, stream=stream)
+            plan = DevicePlan(ca.chart_tris[:2], vofs, tofs, device=self.dev, stream=stream, finish=False)
+        P, U = ca.points(fp32=plan_on == "device")
+        with ctx:
+            P_dev = torch.from_numpy(P).to(self.dev, non_blocking=True) if self.n else None
+        if plan is not None:
+            plan.finish()
         else:
-            plan = Plan(None, vofs, tofs, chart_tris=Tc[:2], device=self.dev, stream=stream)   # export || copies
+            plan = Plan(None, vofs, tofs, chart_tris=ca.chart_tris[:2], device=self.dev, stream=stream)
         self.db = DeviceBatch(P_dev if P_dev is not None else P, None, vofs, tofs, U=U, semantics=_lib.SEM_BATCH,
                               device=self.dev, stream=stream, plan=plan)
         self.db._host_src = (P, U)          # the asynchronous copies read these until they finish
