@@ -10,6 +10,10 @@
  *                      cell, cell-box reject, exact predicates :21-91, :232-255
  *   uvo_raster_labels  engine/metrics.py:315-345 (last triangle wins)
  *   uvo_raster_counts  engine/metrics.py:13-54 (top-left rule, saturating)
+ *   uvo_pack_raster    engine/pack.py:52-79 (conservative chart raster)
+ *   uvo_pack_try       engine/pack.py:123-156, 232-256, 312-359 (greedy
+ *                      first fit of every chart, serial, with the free-run
+ *                      and occupied-run tables and the run-skipping scan)
  */
 #include <math.h>
 #include <stdint.h>
@@ -227,4 +231,135 @@ void uvo_raster_counts(const double* uv, const int64_t* F, int64_t m, int64_t re
             }
         }
     }
+}
+
+/* Conservative raster of one chart whose corners are already scaled and
+ * padded (engine/pack.py:52-79): a cell is set when the cell corner that
+ * maximises each edge function of a counter-clockwise triangle is on the
+ * inner side of all three edges. */
+void uvo_pack_raster(const double* V, const int64_t* T, int64_t t, int64_t h, int64_t w, uint8_t* mask) {
+    for (int64_t f = 0; f < t; ++f) {
+        double x0 = V[2 * T[3 * f]], y0 = V[2 * T[3 * f] + 1];
+        double x1 = V[2 * T[3 * f + 1]], y1 = V[2 * T[3 * f + 1] + 1];
+        double x2 = V[2 * T[3 * f + 2]], y2 = V[2 * T[3 * f + 2] + 1];
+        double area = (x1 - x0) * (y2 - y0) - (x2 - x0) * (y1 - y0);
+        if (area < 0) { double tx = x1, ty = y1; x1 = x2; y1 = y2; x2 = tx; y2 = ty; }
+        int64_t minx = (int64_t)floor(fmin(x0, fmin(x1, x2))), maxx = (int64_t)floor(fmax(x0, fmax(x1, x2)));
+        int64_t miny = (int64_t)floor(fmin(y0, fmin(y1, y2))), maxy = (int64_t)floor(fmax(y0, fmax(y1, y2)));
+        if (minx < 0) minx = 0;
+        if (miny < 0) miny = 0;
+        if (maxx > w - 1) maxx = w - 1;
+        if (maxy > h - 1) maxy = h - 1;
+        double ex[3] = {x1 - x0, x2 - x1, x0 - x2}, ey[3] = {y1 - y0, y2 - y1, y0 - y2};
+        double ox[3] = {x0, x1, x2}, oy[3] = {y0, y1, y2};
+        for (int64_t py = miny; py <= maxy; ++py)
+            for (int64_t px = minx; px <= maxx; ++px) {
+                int inside = 1;
+                for (int k = 0; k < 3 && inside; ++k) {
+                    double cx = (double)px + (ey[k] > 0 ? 0.0 : 1.0);
+                    double cy = (double)py + (ex[k] > 0 ? 1.0 : 0.0);
+                    if (ex[k] * (cy - oy[k]) - ey[k] * (cx - ox[k]) < 0) inside = 0;
+                }
+                if (inside) mask[py * w + px] = 1;
+            }
+    }
+}
+
+/* First fit of one variant: the smallest y, then the smallest x, where
+ * every run of every row lands on free cells (engine/pack.py:123-156). The
+ * rows are tested in `rows` order (longest run first); a failing run moves
+ * x past the occupied run that stopped it. */
+static int pk_find(const int32_t* R, const int32_t* O, const int64_t* rowmax, int64_t G, int64_t h, int64_t w,
+                   const int64_t* rp, const int64_t* ra, const int64_t* rb, const int64_t* need,
+                   const int64_t* rows, int64_t* ox, int64_t* oy) {
+    for (int64_t y = 0; y + h <= G; ++y) {
+        int ok = 1;
+        for (int64_t jj = 0; jj < h && ok; ++jj)
+            if (need[rows[jj]] > rowmax[y + rows[jj]]) ok = 0;
+        if (!ok) continue;
+        int64_t x = 0;
+        while (x <= G - w) {
+            int fits = 1;
+            int64_t skip = 1;
+            for (int64_t jj = 0; jj < h && fits; ++jj) {
+                const int64_t j = rows[jj];
+                for (int64_t q = rp[j]; q < rp[j + 1]; ++q) {
+                    const int64_t L = rb[q] - ra[q] + 1;
+                    const int64_t r = R[(y + j) * G + x + ra[q]];
+                    if (r < L) {
+                        const int64_t c = x + ra[q] + r;
+                        skip = r + (c < G ? O[(y + j) * G + c] : 1);
+                        fits = 0;
+                        break;
+                    }
+                }
+            }
+            if (fits) { *ox = x; *oy = y; return 1; }
+            x += skip;
+        }
+    }
+    return 0;
+}
+
+/* Mark one placed variant and rebuild the free-run (R), occupied-run (O)
+ * and longest-free-run tables of its rows (engine/pack.py:232-256). */
+static void pk_place(uint8_t* occ, int32_t* R, int32_t* O, int64_t* rowmax, int64_t G, int64_t x, int64_t y,
+                     int64_t h, const int64_t* rp, const int64_t* ra, const int64_t* rb) {
+    for (int64_t j = 0; j < h; ++j) {
+        uint8_t* row = occ + (y + j) * G;
+        for (int64_t q = rp[j]; q < rp[j + 1]; ++q)
+            for (int64_t i = ra[q]; i <= rb[q]; ++i) row[x + i] = 1;
+        int32_t run = 0, orun = 0;
+        int64_t mx = 0;
+        for (int64_t i = G - 1; i >= 0; --i) {
+            if (row[i]) { run = 0; ++orun; } else { ++run; orun = 0; }
+            R[(y + j) * G + i] = run;
+            O[(y + j) * G + i] = orun;
+            if (run > mx) mx = run;
+        }
+        rowmax[y + j] = mx;
+    }
+}
+
+/* Greedy placement of nc charts in `order` on a G x G page (engine/pack.py
+ * :312-359). Variant v = c * nk + k has vh[v] x vw[v] cells (vh 0: none) and
+ * rows var_row[v] .. var_row[v + 1] - 1 of the row arrays: run offsets rp
+ * (absolute, one more entry than rows, per variant), longest run need and
+ * test order rows (variant-local). Per chart the variant of smallest
+ * (y + h) G + (x + w) wins, the first on ties. Writes placement (k, x, y per
+ * chart) and occ; returns 0, or -1 - p when the chart at position p fits
+ * nowhere. */
+int64_t uvo_pack_try(int64_t nc, int64_t nk, int64_t G, const int64_t* order, const int64_t* vh, const int64_t* vw,
+                     const int64_t* var_row, const int64_t* var_rp, const int64_t* ra, const int64_t* rb,
+                     const int64_t* need, const int64_t* rows, int64_t* placement, uint8_t* occ) {
+    int32_t* R = (int32_t*)malloc(sizeof(int32_t) * G * G);
+    int32_t* O = (int32_t*)calloc((size_t)(G * G), sizeof(int32_t));
+    int64_t* rowmax = (int64_t*)malloc(sizeof(int64_t) * G);
+    int64_t rc = 0;
+    memset(occ, 0, (size_t)(G * G));
+    for (int64_t y = 0; y < G; ++y) {
+        rowmax[y] = G;
+        for (int64_t x = 0; x < G; ++x) R[y * G + x] = (int32_t)(G - x);
+    }
+    for (int64_t p = 0; p < nc; ++p) {
+        const int64_t c = order[p];
+        int64_t best = -1, bk = -1, bx = 0, by = 0;
+        for (int64_t k = 0; k < nk; ++k) {
+            const int64_t v = c * nk + k, h = vh[v], w = vw[v];
+            if (h <= 0 || h > G || w > G) continue;
+            int64_t x, y;
+            const int64_t r0 = var_row[v];
+            if (!pk_find(R, O, rowmax, G, h, w, var_rp + r0 + v, ra, rb, need + r0, rows + r0, &x, &y)) continue;
+            const int64_t score = (y + h) * G + (x + w);
+            if (bk < 0 || score < best) { best = score; bk = k; bx = x; by = y; }
+        }
+        if (bk < 0) { rc = -1 - p; break; }
+        const int64_t v = c * nk + bk;
+        pk_place(occ, R, O, rowmax, G, bx, by, vh[v], var_rp + var_row[v] + v, ra, rb);
+        placement[3 * c] = bk;
+        placement[3 * c + 1] = bx;
+        placement[3 * c + 2] = by;
+    }
+    free(R); free(O); free(rowmax);
+    return rc;
 }

@@ -34,6 +34,10 @@ def clib():
         lib.uvo_raster_labels.restype = None
         lib.uvo_raster_counts.argtypes = [vp, vp, C.c_int64, C.c_int64, vp]
         lib.uvo_raster_counts.restype = None
+        lib.uvo_pack_raster.argtypes = [vp, vp, C.c_int64, C.c_int64, C.c_int64, vp]
+        lib.uvo_pack_raster.restype = None
+        lib.uvo_pack_try.argtypes = [C.c_int64, C.c_int64, C.c_int64] + [vp] * 11
+        lib.uvo_pack_try.restype = C.c_int64
         _CLIB = lib
     return _CLIB
 
