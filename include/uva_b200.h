@@ -599,6 +599,65 @@ int uva_corners_equal(const void* A, int32_t adt, int64_t na, const int64_t* fa,
 int uva_segment_sum(const double* x, int64_t stride, const int32_t* seg, int64_t m, int32_t nseg, double* out,
                     int32_t* status, void* stream);
 
+/* --------------------------------------------------------------------------
+ * Raster atlas packing, one attempt at one texel scale (pack.py:53-363,
+ * csrc/pack.cu). A mask source is a chart at one pre-rotation angle
+ * (source c * nangles + a); a variant is a source turned by 0..3 quarter
+ * turns (variant c * nk + k, k = a * nturns + turn). The host gives what
+ * follows from the sizes alone: each source's texel scale and mask size
+ * (h = ceil(max y * scale + pad + pad) + 1, w likewise, pack.py:84-86), the
+ * mask offsets, the variants (var_src -1: none) and their row offsets.
+ * uva_pack_masks writes the masks (conservative raster, square dilation by
+ * pad), the runs of every variant row (run_ofs, run_a / run_b first and last
+ * cell), the longest run of each row, the set cells of every variant
+ * (var_area) and a key naming its row with the longest run; status[2] = 1
+ * when run_cap was too small (a row of w cells has at most (w + 1) / 2
+ * runs). uva_pack_place places the charts in `order` on a G x G page by
+ * first fit (pack.py:124-156, 312-359) in one cooperative launch and
+ * writes placement (variant, x, y per chart), R (per cell the free run to
+ * its right), rowmax, occupied (cells with R = 0) and status[0]: 0 all
+ * placed, bit 0 a chart did not fit (status[1]: its position in order),
+ * bit 1 a grid barrier timed out. uva_pack_uv writes the UVs of all charts
+ * (pack.py:541-549): (U s) dens + pad inside the mask, turned, moved by
+ * (x, y), over G; out is nv x 2 at the chart offsets cofs. All pointers
+ * are device memory. G at most 8192, nk at most 64.                       */
+typedef struct uva_pack_attempt {
+    int32_t nsrc, nc, nk, G, pad, reserved;
+    int64_t ntri, ncells, nrows, run_cap;
+    const double* V;           /* oriented source coordinates, 2 per vertex  */
+    const int64_t* vofs;       /* nsrc+1 vertex offsets of the sources       */
+    const int32_t* T;          /* ntri*3 source-local vertex ids             */
+    const int64_t* tofs;       /* nsrc+1 triangle offsets                    */
+    const double* scale;       /* nsrc texel scales                          */
+    const int32_t* hw;         /* nsrc*2 mask height, width                  */
+    const int64_t* mofs;       /* nsrc+1 mask byte offsets, mofs[nsrc] = ncells */
+    const int32_t* var_src;    /* nc*nk source of every variant, -1: none    */
+    const int32_t* var_turn;   /* nc*nk quarter turns                        */
+    const int64_t* var_row;    /* nc*nk+1 first row of every variant         */
+    const int64_t* order;      /* nc charts in placing order                 */
+    uint8_t* mask;             /* ncells                                     */
+    int32_t* row_need;         /* nrows longest run                          */
+    int32_t* run_ofs;          /* nrows+1                                    */
+    int32_t* run_a;            /* run_cap                                    */
+    int32_t* run_b;            /* run_cap                                    */
+    int64_t* var_area;         /* nc*nk                                      */
+    int64_t* var_key;          /* nc*nk                                      */
+    int32_t* R;                /* G*G                                        */
+    int32_t* rowmax;           /* G                                          */
+    int32_t* placement;        /* nc*3                                       */
+    int32_t* status;           /* 4                                          */
+    int64_t* occupied;         /* 1                                          */
+    void* scratch;             /* uva_pack_scratch_bytes                     */
+    int64_t scratch_bytes;
+} uva_pack_attempt;
+
+int uva_pack_scratch_bytes(int64_t ntri, int64_t ncells, int64_t nrows, int32_t nk, int32_t G, int64_t* bytes);
+int uva_pack_masks(const uva_pack_attempt* a, void* stream);
+/* blocks_per_sm: resident blocks of the placement launch per SM (0: 2). */
+int uva_pack_place(const uva_pack_attempt* a, int32_t blocks_per_sm, void* stream);
+int uva_pack_uv(const uva_pack_attempt* a, int32_t nangles, int32_t nturns, const int64_t* cofs, int64_t nv,
+                double s, const double* dens, double* out, void* stream);
+
 /* Library info. */
 const char* uva_last_error(void);
 int uva_version(void);

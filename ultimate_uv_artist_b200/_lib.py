@@ -132,6 +132,10 @@ _SIGS = {
     "uva_dplan_scratch_bytes": [C.c_int64, C.c_int64, C.c_int64, vp],
     "uva_dplan_build": [vp, vp],
     "uva_dplan_slots": [vp, vp, vp, vp, vp],
+    "uva_pack_scratch_bytes": [C.c_int64, C.c_int64, C.c_int64, i32, i32, vp],
+    "uva_pack_masks": [vp, vp],
+    "uva_pack_place": [vp, i32, vp],
+    "uva_pack_uv": [vp, i32, i32, vp, C.c_int64, C.c_double, vp, vp, vp],
     "uva_last_error": [],
     "uva_version": [],
 }

@@ -22,13 +22,13 @@ LIB = os.path.join(HERE, "libuva_b200.so")
 BUILD_DIR = os.path.join(ROOT, "_build")
 
 CU_SOURCES = ["capi.cu", "solve.cu", "ops.cu", "chart_ops.cu", "validate.cu", "metrics.cu", "energy.cu", "gutter.cu",
-              "segments.cu", "edges.cu", "report.cu", "dplan.cu"]
+              "segments.cu", "edges.cu", "report.cu", "dplan.cu", "pack.cu"]
 CXX_SOURCES = ["plan.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-Xptxas", "-O3"]
 # validation predicates are exact FP64: no FMA contraction in those files
-NO_FMA = {"validate.cu", "gutter.cu", "segments.cu", "report.cu"}
+NO_FMA = {"validate.cu", "gutter.cu", "segments.cu", "report.cu", "pack.cu"}
 
 
 def _nvcc():
