@@ -504,12 +504,14 @@ def _events(dev):
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def bench_config5(dev, iters=ITERS, steps=2):
+def bench_config5(dev, iters=ITERS, steps=2, cpu=True):
     """Config 5 end to end at its stated size: a 5M-triangle noisy sphere cut
     into 3,000 k-means charts (disk components kept), batched LSCM + ARAP,
     per-chart p95 metrics, packing and exact validation of the packed atlas.
     Device times by CUDA events (solve, metrics, validation), the public-API
-    wall time of every stage, validation pairs per second."""
+    wall time of every stage, validation pairs per second; packing by
+    engine.pack with the reference's default schedule (wall time, attempts)
+    and one full-grid attempt beside the oracle's on one host core."""
     import torch
     from ultimate_uv_artist_b200 import _lib, synth
     from ultimate_uv_artist_b200.device import DeviceBatch
@@ -555,10 +557,32 @@ def bench_config5(dev, iters=ITERS, steps=2):
     p95 = np.array([x["aniso_p95"] for x in q])
     del dq, b, db
     torch.cuda.empty_cache()
-    # packing (shelf placement; test scaffolding, not the product) and validation
-    w5 = time.perf_counter()
-    packed = synth.shelf_pack(U, atlas=4096, padding=4)
-    pack_s = time.perf_counter() - w5
+    # packing (engine.pack: the reference's schedule, attempts on the device)
+    from ultimate_uv_artist_b200.engine import pack as EPK
+    uv_charts = [(U[i].astype(np.float64), charts[i][1]) for i in range(len(charts))]
+    torch.cuda.synchronize(); w5 = time.perf_counter()
+    packed, pinfo = EPK.pack(uv_charts, atlas=4096, padding=4)
+    torch.cuda.synchronize(); pack_s = time.perf_counter() - w5
+    # one full-grid attempt at 0.97 of the found scale: device (CUDA events) and the oracle (one core)
+    Us = [EPK.orient(u) for u, _ in uv_charts]
+    Ts = [t for _, t in uv_charts]
+    P = EPK.Packer(Us, Ts, np.ones(len(Us)))
+    s_att = 0.97 * pinfo["texel_scale_grid"]
+    P.attempt(2048, 2, [0, 1, 2, 3], s_att, "area")
+    a0, a1 = _events(dev)
+    a0.record(stream)
+    att = P.attempt(2048, 2, [0, 1, 2, 3], s_att, "area")
+    a1.record(stream)
+    torch.cuda.synchronize()
+    attempt_ms = a0.elapsed_time(a1)
+    pack_cpu = None
+    if cpu:
+        from oracle import pack as OPK
+        t0 = time.perf_counter()
+        ref_att = OPK.attempt(Us, Ts, np.ones(len(Us)), 2048, 2, [0, 1, 2, 3], s_att, "area")
+        pack_cpu = {"attempt_s": time.perf_counter() - t0, "cores": 1, "kind": "port",
+                    "same_placement": bool(att is not None and ref_att is not None
+                                           and att.placement == ref_att[1][0])}
     offs = np.cumsum([0] + [len(p) for p, _ in charts])
     Vall = np.concatenate([p for p, _ in charts]).astype(np.float32)
     Fall = np.concatenate([t + o for (_, t), o in zip(charts, offs[:-1])])
@@ -589,7 +613,10 @@ def bench_config5(dev, iters=ITERS, steps=2):
             "max_resid": float(st["resid"].max()),
             "api_batch_build_s": w1 - w0, "api_solve_download_s": w2 - w1, "api_chart_quality_s": w4 - w3,
             "aniso_p95_median": float(np.median(p95)), "aniso_p95_max": float(p95.max()),
-            "pack_s_host_shelf": pack_s, "validate_api_s": val_api_s,
+            "pack": {"api_s": pack_s, "attempts": pinfo["attempts"], "attempt_s_total": pinfo["attempt_seconds"],
+                     "texel_scale_grid": pinfo["texel_scale_grid"], "plan_occupancy": pinfo["plan_occupancy"],
+                     "grid": pinfo["grid"], "attempt_ms_2048": attempt_ms, "cpu_oracle": pack_cpu},
+            "validate_api_s": val_api_s,
             "validate_ms_per_pass": val_ms, "pairs_aabb": pairs, "pairs_per_s": pairs / (val_ms / 1e3),
             "gutter_ms_wall": gutter_ms, "min_gutter_texels": float(g), "valid": bool(rep["valid"]),
             "overlapping_triangles": int(rep["overlapping_triangles_exact"]),
@@ -864,7 +891,7 @@ def main():
         ovl = bench_overlap(islands, our_uvs)
     c5 = c1 = c4 = None
     if rank == 0 and not args.no_config5:
-        c5 = bench_config5(dev)
+        c5 = bench_config5(dev, cpu=not args.no_cpu_baseline)
     if rank == 0 and not args.no_config4:
         c4 = bench_energy(dev, hbm)
     if rank == 0 and not args.no_config1:

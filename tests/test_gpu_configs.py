@@ -86,7 +86,8 @@ def test_config5_dense_scan_full_size(cuda):
     every global step at the FP64 residual bar; UVs against the FP64 oracle
     on 12 size-stratified charts; per-chart p95 anisotropy and area ratio
     (param.chart_quality) against the oracle on the same charts; then the
-    charts shelf-packed on a 4096 atlas (padding 4) and the validation report,
+    charts packed by engine.pack on a 4096 atlas (padding 4; one full-grid
+    attempt against the oracle's placement) and the validation report,
     the overlap / strict-overlap / flip masks, the island partition and the
     candidate-pair count compared with the oracle bit for bit."""
     import torch
@@ -122,7 +123,21 @@ def test_config5_dense_scan_full_size(cuda):
             assert abs(q[i][k] - r[k]) <= 1e-4 * abs(r[k]), (i, k, q[i][k], r[k])
     del db, b
     torch.cuda.empty_cache()
-    packed = synth.shelf_pack(U, atlas=4096, padding=4)
+    # the reference's packer (engine/pack.py) with its default schedule; one
+    # full-grid attempt of it against the oracle's placement
+    from oracle import pack as OPK
+    from ultimate_uv_artist_b200.engine import pack as EPK
+    uv_charts = [(U[i].astype(np.float64), charts[i][1]) for i in range(len(charts))]
+    packed, pinfo = EPK.pack(uv_charts, atlas=4096, padding=4)
+    assert pinfo["grid"] == 2048 and pinfo["grid_padding"] == 2 and pinfo["plan_occupancy"] > 0.5
+    Us = [EPK.orient(u) for u, _ in uv_charts]
+    Ts = [t for _, t in uv_charts]
+    s_att = 0.97 * pinfo["texel_scale_grid"]
+    att = EPK.Packer(Us, Ts, np.ones(len(Us))).attempt(2048, 2, [0, 1, 2, 3], s_att, "area")
+    ref_att = OPK.attempt(Us, Ts, np.ones(len(Us)), 2048, 2, [0, 1, 2, 3], s_att, "area")
+    assert (att is None) == (ref_att is None)
+    if att is not None:
+        assert att.placement == ref_att[1][0]
     offs = np.cumsum([0] + [len(p) for p, _ in charts])
     Vall = np.concatenate([p for p, _ in charts]).astype(np.float32)
     Fall = np.concatenate([t + o for (_, t), o in zip(charts, offs[:-1])])
@@ -133,6 +148,8 @@ def test_config5_dense_scan_full_size(cuda):
         if isinstance(v, (int, float, bool, np.integer, np.floating)):
             assert float(rep[k]) == float(v), (k, rep[k], v)
     assert np.array_equal(problems, rprob)
+    # the packer keeps islands apart by at least the gutter
+    assert rep["gutter_ok"], rep
     dv = GV.DeviceValidation(Vall.astype(np.float64), Fall.astype(np.int32), UVall).run()
     fl = dv.flags()
     assert np.array_equal((fl & 16) != 0, ex["ov"])

@@ -23,22 +23,28 @@
 // Placement (uva_pack_place), one cooperative launch for all charts. The
 // page keeps, per cell, the free run to its right (R = 0: occupied) and, per
 // row, the longest free run. For every chart in turn (pack.py:312-359):
-//   A. every (variant k, row y) pair is an item; blocks take items in
-//      increasing y. An item whose rows need a longer free run than the page
-//      row has is rejected, else the block searches the smallest x where
-//      every run of the variant fits (R at the run's start at least its
-//      length), threads taking x in increasing order, a warp giving up when
-//      all its lanes failed. A success lowers ybest[k] (atomic minimum), and
-//      items below ybest[k] are skipped: ybest[k], bestx[k][ybest[k]] is the
-//      reference's first fit (smallest y, then smallest x, pack.py:124-156).
-//   B. after a grid barrier every block picks, from the same values, the
-//      variant of smallest (y + h) G + (x + w), the first on ties
-//      (pack.py:345-351); none: the attempt fails and every block returns.
-//   C. blocks rebuild the free runs of the rows the chart covers, then a
-//      second barrier ends the chart.
+//   A1. one thread per (row y, variant k) item tests every row of the
+//       variant against the longest free run of the page row it would land
+//       on; the items that pass are bits in (y, k) order. Grid barrier.
+//   A2. blocks take the passing items by rank (block b: ranks b, b + nb, ...,
+//       so in increasing y). Per item every x is a bit of one thread: the
+//       widest run of the variant's longest-run row and of seven rows spread
+//       over its height must land on free runs at least as long (loads in
+//       flight together); the x left are candidates, tested whole in
+//       increasing x, one per warp, the lanes taking the rows. A fit lowers
+//       ybest[k] (atomic minimum); items below ybest[k] are skipped, and a
+//       block stops once every variant fits higher than its next item.
+//       ybest[k], bestx[k][ybest[k]] is the reference's first fit (smallest
+//       y, then smallest x, pack.py:124-156). Grid barrier.
+//   B.  every block picks, from the same values, the variant of smallest
+//       (y + h) G + (x + w), the first on ties (pack.py:345-351); none: the
+//       attempt fails and every block returns.
+//   C.  blocks rebuild the free runs of the rows the chart covers; a grid
+//       barrier ends the chart.
 // Values written inside the launch are read with ld.global.cg (L2), so no
-// block sees a stale line of its own L1. The barrier spins a bounded number
-// of times and reports a timeout in the status instead of waiting for good.
+// block sees a stale line of its own L1. The barrier spins a bounded time
+// (two seconds) and reports a timeout in the status instead of waiting for
+// good.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -300,7 +306,6 @@ __device__ bool grid_sync(GridBar* bar, unsigned nblocks) {
                     ok = 0;
                     break;
                 }
-                __nanosleep(32);
             }
         }
         __threadfence();
@@ -329,80 +334,273 @@ struct PlaceArgs {
     int32_t* status;
     int32_t* bestx;   // nk * G
     int32_t* ybest;   // 2 * nk, alternating per chart
+    unsigned* cand;   // 2 * cand_words item bits, alternating per chart
+    int64_t cand_words;
     GridBar* bar;
 };
 
-// Dynamic shared memory: G occupancy bytes, then G free-run ints.
-__global__ void __launch_bounds__(kTB) k_pk_place(PlaceArgs a) {
+constexpr int kMaxVariants = 64;
+constexpr int kFilters = 8;   // widest run of the longest-run row and of 7 rows spread over the height
+constexpr int kWarps = kTB / 32;
+
+// The variants of one chart, staged in shared memory once per chart: size,
+// first row, and the filter runs (row, first cell, length; length 0: none)
+// tested for every x before the whole variant is.
+struct ChartVariants {
+    int32_t h[kMaxVariants], w[kMaxVariants], first[kMaxVariants];
+    int64_t r0[kMaxVariants];
+    int32_t fy[kMaxVariants][kFilters], fa[kMaxVariants][kFilters], fl[kMaxVariants][kFilters];
+};
+
+// Does the variant (h rows from r0) fit with its corner at (x, y)? The
+// lanes of one warp take the rows, loads independent of each other.
+__device__ __forceinline__ bool warp_fits(const int32_t* R, const int32_t* run_ofs, const int32_t* run_a,
+                                          const int32_t* run_b, int32_t G, int32_t y, int32_t x, int32_t h,
+                                          int64_t r0, int lane) {
+    bool ok = true;
+    for (int32_t j = lane; j < h; j += 32) {
+        const int32_t* Rrow = R + static_cast<int64_t>(y + j) * G + x;
+        const int32_t q1 = __ldg(run_ofs + r0 + j + 1);
+        for (int32_t q = __ldg(run_ofs + r0 + j); q < q1; ++q) {
+            const int32_t qa = __ldg(run_a + q);
+            ok &= __ldcg(Rrow + qa) >= __ldg(run_b + q) - qa + 1;
+        }
+    }
+    return __all_sync(0xffffffffu, ok);
+}
+
+// Dynamic shared memory: G free-run ints, then G occupancy bytes.
+__global__ void __launch_bounds__(kTB, 4) k_pk_place(PlaceArgs a) {
     extern __shared__ __align__(16) uint8_t s_dyn[];
     int32_t* s_R = reinterpret_cast<int32_t*>(s_dyn);
     uint8_t* s_occ = s_dyn + 4 * static_cast<size_t>(a.G);
+    __shared__ ChartVariants cv;
     __shared__ int32_t s_wmin[kTB / 32], s_wmax[kTB / 32];
     __shared__ int32_t s_sel[3];
+    __shared__ int32_t s_best;
+    __shared__ int64_t s_chart;
+    __shared__ unsigned s_cand[kWarps];
+    __shared__ unsigned s_slots;
+    __shared__ unsigned s_word[kTB];
+    __shared__ int32_t s_yb[2][kMaxVariants];
+    __shared__ int32_t s_pref[kTB];
     const int32_t G = a.G, nk = a.nk;
     const unsigned nb = gridDim.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __shared__ int32_t s_best;
     for (int32_t p = 0; p < a.nc; ++p) {
-        const int64_t c = a.order[p];
+        // ---- the chart's variants: usable ones get h > 0
+        __syncthreads();
+        if (threadIdx.x == 0) s_chart = a.order[p];
+        __syncthreads();
+        const int64_t c = s_chart;
         int32_t* yb = a.ybest + (p & 1) * nk;
-        // ---- A: first fit of every variant
-        const int64_t items = static_cast<int64_t>(nk) * G;
-        for (int64_t it = blockIdx.x; it < items; it += nb) {
-            const int32_t y = static_cast<int32_t>(it / nk), k = static_cast<int32_t>(it - static_cast<int64_t>(y) * nk);
+        for (int32_t k = threadIdx.x; k < nk; k += blockDim.x) {
             const int64_t v = c * nk + k;
             const Variant vr = variant_of(v, a.var_src, a.var_turn, a.hw);
-            if (vr.src < 0 || vr.h <= 0 || vr.h > G || vr.w > G || y > G - vr.h) continue;
-            if (threadIdx.x == 0) s_best = kNone;
-            // a higher row already fits this variant
-            if (__syncthreads_or(threadIdx.x == 0 && __ldcg(yb + k) < y)) continue;
-            const int64_t r0 = a.var_row[v];
-            int bad = 0;
-            for (int32_t j = threadIdx.x; j < vr.h; j += blockDim.x)
-                bad |= a.row_need[r0 + j] > __ldcg(a.rowmax + y + j);
-            if (__syncthreads_or(bad)) continue;
-            const int32_t first = static_cast<int32_t>(~static_cast<uint32_t>(a.var_key[v] & 0xffffffffull));
-            for (int32_t x0 = 0; x0 <= G - vr.w; x0 += blockDim.x) {
-                const int32_t x = x0 + threadIdx.x;
-                bool fits = x <= G - vr.w;
-                const int32_t xs = fits ? x : 0;
-                for (int32_t jj = 0; jj < vr.h; ++jj) {
-                    if (!__any_sync(0xffffffffu, fits)) break;
-                    const int32_t j = jj == 0 ? first : (jj <= first ? jj - 1 : jj);
-                    const int32_t* Rrow = a.R + static_cast<int64_t>(y + j) * G + xs;
-                    const int32_t q1 = a.run_ofs[r0 + j + 1];
-                    for (int32_t q = a.run_ofs[r0 + j]; q < q1; ++q) {
-                        const int32_t qa = a.run_a[q];
-                        if (fits && __ldcg(Rrow + qa) < a.run_b[q] - qa + 1) fits = false;
-                        if (!__any_sync(0xffffffffu, fits)) break;
+            const bool ok = vr.src >= 0 && vr.h > 0 && vr.h <= G && vr.w <= G;
+            cv.h[k] = ok ? vr.h : 0;
+            cv.w[k] = vr.w;
+            cv.r0[k] = a.var_row[v];
+            cv.first[k] = static_cast<int32_t>(~static_cast<uint32_t>(__ldg(a.var_key + v) & 0xffffffffull));
+        }
+        __syncthreads();
+        for (int32_t t = threadIdx.x; t < kFilters * nk; t += blockDim.x) {
+            const int32_t k = t / kFilters, i = t - kFilters * k, h = cv.h[k];
+            int32_t row = 0, fa = 0, fl = 0;
+            if (h > 0) {
+                row = i == 0 ? cv.first[k] : static_cast<int32_t>((static_cast<int64_t>(i - 1) * (h - 1)) / 6);
+                const int32_t q1 = __ldg(a.run_ofs + cv.r0[k] + row + 1);
+                for (int32_t q = __ldg(a.run_ofs + cv.r0[k] + row); q < q1; ++q) {
+                    const int32_t qa = __ldg(a.run_a + q), len = __ldg(a.run_b + q) - qa + 1;
+                    if (len > fl) { fl = len; fa = qa; }
+                }
+            }
+            cv.fy[k][i] = row;
+            cv.fa[k][i] = fa;
+            cv.fl[k][i] = fl;
+        }
+        __syncthreads();
+        // ---- A1: the items (y, k) whose rows all fit the longest free runs of
+        // the page rows below them, one thread per item, as bits in y-major order
+        const int64_t items = static_cast<int64_t>(nk) * G;
+        unsigned* cb = a.cand + (p & 1) * a.cand_words;
+        for (int32_t i = threadIdx.x; i < G; i += blockDim.x) s_R[i] = __ldcg(a.rowmax + i);   // s_R: rowmax here
+        __syncthreads();
+        // a warp owns the word of its 32 items (it = warp-aligned base + lane)
+        for (int64_t base = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) & ~int64_t(31);
+             base < items; base += static_cast<int64_t>(nb) * blockDim.x) {
+            const int64_t it = base + lane;
+            bool ok = false;
+            if (it < items) {
+                const int32_t y = static_cast<int32_t>(it / nk), k = static_cast<int32_t>(it - static_cast<int64_t>(y) * nk);
+                const int32_t h = cv.h[k];
+                if (h > 0 && y <= G - h) {
+                    const int32_t* need = a.row_need + cv.r0[k];
+                    const int32_t* rm = s_R + y;
+                    ok = true;
+                    for (int32_t j = 0; j < h && ok; j += 4) {   // four rows a step, the last row again past the end
+                        const int32_t j1 = min(j + 1, h - 1), j2 = min(j + 2, h - 1), j3 = min(j + 3, h - 1);
+                        ok = (__ldg(need + j) <= rm[j]) & (__ldg(need + j1) <= rm[j1]) & (__ldg(need + j2) <= rm[j2]) &
+                             (__ldg(need + j3) <= rm[j3]);
                     }
                 }
-                if (fits) atomicMin(&s_best, x);
-                if (__syncthreads_or(fits)) break;
             }
-            if (threadIdx.x == 0 && s_best != kNone) {
-                a.bestx[static_cast<int64_t>(k) * G + y] = s_best;
-                __threadfence();
-                atomicMin(yb + k, y);
-            }
+            const unsigned bits = __ballot_sync(0xffffffffu, ok);
+            if (lane == 0 && bits) cb[base >> 5] = bits;
         }
         if (!grid_sync(a.bar, nb)) {
             if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, 2);
             return;
         }
-        // ---- B: the variant of smallest (y + h) G + (x + w), the first on ties
-        if (threadIdx.x == 0) {
-            int32_t bk = -1, bx = 0, by = 0;
-            long long bs = 0;
-            for (int32_t k = 0; k < nk; ++k) {
+        // ---- A2: first fit of every variant over the items of A1, in
+        // increasing (y, k); block b takes the items of rank b, b + nb, ...
+        int64_t carry = 0;
+        bool all_done = false;
+        int r_par = 0;
+        for (int64_t w0 = 0; w0 < a.cand_words && !all_done; w0 += blockDim.x) {
+            __syncthreads();   // s_word / s_pref of the previous tile are read
+            const int64_t wi = w0 + threadIdx.x;
+            const unsigned word = wi < a.cand_words ? __ldcg(cb + wi) : 0u;
+            int32_t incl = __popc(word);
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            if (lane == 31) s_wmin[warp] = incl;
+            __syncthreads();
+            int32_t wbase = 0, total = 0;
+            for (int w2 = 0; w2 < kWarps; ++w2) {
+                if (w2 < warp) wbase += s_wmin[w2];
+                total += s_wmin[w2];
+            }
+            s_word[threadIdx.x] = word;
+            s_pref[threadIdx.x] = wbase + incl - __popc(word);   // exclusive
+            __syncthreads();
+            const int64_t r_first = carry + ((static_cast<int64_t>(blockIdx.x) - carry) % nb + nb) % nb;
+            for (int64_t r = r_first; r < carry + total; r += nb) {
+                const int32_t rr = static_cast<int32_t>(r - carry);
+                int32_t lo = 0, hi = kTB - 1;   // the last thread whose exclusive prefix is <= rr
+                while (lo < hi) {
+                    const int32_t mid = (lo + hi + 1) >> 1;
+                    if (s_pref[mid] <= rr) lo = mid; else hi = mid - 1;
+                }
+                const int bit = __fns(s_word[lo], 0, rr - s_pref[lo] + 1);
+                const int64_t it = (w0 + lo) * 32 + bit;
+                const int32_t y = static_cast<int32_t>(it / nk), k = static_cast<int32_t>(it - static_cast<int64_t>(y) * nk);
+                const int32_t h = cv.h[k], w = cv.w[k];
+                const int64_t r0 = cv.r0[k];
+                if (threadIdx.x == 0) { s_best = kNone; s_slots = 0; }
+                // every x is a slot bit of one thread (x = m * blockDim.x + tid).
+                // One round of loads: the first filter for all slots, and the
+                // rows' longest runs against the page rows' longest free runs
+                const int32_t nx = G - w + 1, M = (nx + blockDim.x - 1) / blockDim.x;   // M <= 32: G <= 8192
+                unsigned cand = 0;
+                {
+                    const int32_t* Rrow = a.R + static_cast<int64_t>(y + cv.fy[k][0]) * G + cv.fa[k][0];
+                    const int32_t fl = cv.fl[k][0];
+#pragma unroll 8
+                    for (int32_t m = 0; m < M; ++m) {
+                        const int32_t x = m * blockDim.x + threadIdx.x;
+                        const bool ok = x < nx && __ldcg(Rrow + min(x, nx - 1)) >= fl;
+                        cand |= static_cast<unsigned>(ok) << m;
+                    }
+                }
+                // skip: a higher row already fits this variant; done: a higher
+                // row fits every variant (this block's later items are lower)
+                int32_t* syb = s_yb[r_par];
+                r_par ^= 1;
+                if (threadIdx.x < nk) syb[threadIdx.x] = __ldcg(yb + threadIdx.x);
+                __syncthreads();
+                bool done = true;
+                for (int32_t kk = 0; kk < nk; ++kk) done &= cv.h[kk] == 0 || syb[kk] < y;
+                if (done) { all_done = true; break; }
+                if (syb[k] < y) continue;
+                // the other filters, all loads of one slot in flight together
+                for (unsigned live = cand; live; live &= live - 1) {
+                    const int32_t m = __ffs(live) - 1;
+                    const int32_t x = m * static_cast<int32_t>(blockDim.x) + static_cast<int32_t>(threadIdx.x);
+                    bool ok = true;
+#pragma unroll
+                    for (int f = 1; f < kFilters; ++f)
+                        ok &= __ldcg(a.R + static_cast<int64_t>(y + cv.fy[k][f]) * G + cv.fa[k][f] + x) >= cv.fl[k][f];
+                    if (!ok) cand &= ~(1u << m);
+                }
+                // slot by slot in increasing x, the candidates, one per warp,
+                // checked whole by the warp's lanes; the first slot with a fit ends it
+                if (cand) atomicOr(&s_slots, cand);
+                __syncthreads();
+                unsigned slots = s_slots;
+                bool found = false;
+                while (slots) {
+                    const int32_t m = __ffs(slots) - 1;
+                    slots &= slots - 1;
+                    // word `warp` holds the candidates m * blockDim.x + warp * 32 + lane
+                    const unsigned bits = __ballot_sync(0xffffffffu, (cand >> m) & 1u);
+                    if (lane == 0) s_cand[warp] = bits;
+                    __syncthreads();
+                    const unsigned word = lane < kWarps ? s_cand[lane] : 0u;
+                    int32_t incl = __popc(word);
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    const int32_t ncand = __shfl_sync(0xffffffffu, incl, 31);
+                    for (int32_t base = 0; base < ncand; base += kWarps) {
+                        const int32_t r = base + warp;
+                        bool ok = false;
+                        if (r < ncand) {
+                            const unsigned above = __ballot_sync(0xffffffffu, incl > r);
+                            const int wi = __ffs(above) - 1;
+                            const unsigned wbits = __shfl_sync(0xffffffffu, word, wi);
+                            const int32_t before = __shfl_sync(0xffffffffu, incl - __popc(word), wi);
+                            const int bit = __fns(wbits, 0, r - before + 1);
+                            const int32_t x = m * static_cast<int32_t>(blockDim.x) + wi * 32 + bit;
+                            ok = warp_fits(a.R, a.run_ofs, a.run_a, a.run_b, G, y, x, h, r0, lane);
+                            if (ok && lane == 0) atomicMin(&s_best, x);
+                        }
+                        found = __syncthreads_or(ok && lane == 0);
+                        if (found) break;
+                    }
+                    if (found) break;
+                    __syncthreads();   // s_cand is rewritten for the next slot
+                }
+                if (threadIdx.x == 0 && s_best != kNone) {
+                    a.bestx[static_cast<int64_t>(k) * G + y] = s_best;
+                    __threadfence();
+                    atomicMin(yb + k, y);
+                }
+            }
+            carry += total;
+        }
+        if (!grid_sync(a.bar, nb)) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, 2);
+            return;
+        }
+        // ---- B: the variant of smallest (y + h) G + (x + w), the first on ties (warp 0)
+        if (warp == 0) {
+            unsigned long long key = ~0ull;
+            for (int32_t k = lane; k < nk; k += 32) {
                 const int32_t yv = __ldcg(yb + k);
                 if (yv == kNone) continue;
                 const int32_t xv = __ldcg(a.bestx + static_cast<int64_t>(k) * G + yv);
-                const Variant vr = variant_of(c * nk + k, a.var_src, a.var_turn, a.hw);
-                const long long score = static_cast<long long>(yv + vr.h) * G + (xv + vr.w);
-                if (bk < 0 || score < bs) { bs = score; bk = k; bx = xv; by = yv; }
+                const unsigned long long score =
+                    static_cast<unsigned long long>(yv + cv.h[k]) * static_cast<unsigned long long>(G) + (xv + cv.w[k]);
+                key = min(key, (score << 6) | static_cast<unsigned long long>(k));
             }
-            s_sel[0] = bk; s_sel[1] = bx; s_sel[2] = by;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) key = min(key, __shfl_xor_sync(0xffffffffu, key, o));
+            if (lane == 0) {
+                if (key == ~0ull) {
+                    s_sel[0] = -1;
+                } else {
+                    const int32_t k = static_cast<int32_t>(key & 63);
+                    s_sel[0] = k;
+                    s_sel[2] = __ldcg(yb + k);
+                    s_sel[1] = __ldcg(a.bestx + static_cast<int64_t>(k) * G + s_sel[2]);
+                }
+            }
         }
         __syncthreads();
         const int32_t bk = s_sel[0], bx = s_sel[1], by = s_sel[2];
@@ -411,17 +609,17 @@ __global__ void __launch_bounds__(kTB) k_pk_place(PlaceArgs a) {
             return;
         }
         // ---- C: mark the chart's cells, rebuild the free runs of its rows
-        const int64_t v = c * nk + bk;
-        const Variant vr = variant_of(v, a.var_src, a.var_turn, a.hw);
-        const int64_t r0 = a.var_row[v];
-        for (int32_t j = blockIdx.x; j < vr.h; j += nb) {
+        const int64_t r0 = cv.r0[bk];
+        for (int32_t j = blockIdx.x; j < cv.h[bk]; j += nb) {
             int32_t* Rrow = a.R + static_cast<int64_t>(by + j) * G;
             __syncthreads();
             for (int32_t i = threadIdx.x; i < G; i += blockDim.x) s_occ[i] = __ldcg(Rrow + i) == 0;
             __syncthreads();
-            const int32_t q1 = a.run_ofs[r0 + j + 1];
-            for (int32_t q = a.run_ofs[r0 + j]; q < q1; ++q)
-                for (int32_t i = a.run_a[q] + threadIdx.x; i <= a.run_b[q]; i += blockDim.x) s_occ[bx + i] = 1;
+            const int32_t q1 = __ldg(a.run_ofs + r0 + j + 1);
+            for (int32_t q = __ldg(a.run_ofs + r0 + j); q < q1; ++q) {
+                const int32_t qb = __ldg(a.run_b + q);
+                for (int32_t i = __ldg(a.run_a + q) + threadIdx.x; i <= qb; i += blockDim.x) s_occ[bx + i] = 1;
+            }
             __syncthreads();
             // chunk per thread: its first occupied cell, the first occupied
             // cell right of it (suffix minimum), then the chunk backwards
@@ -456,6 +654,12 @@ __global__ void __launch_bounds__(kTB) k_pk_place(PlaceArgs a) {
                 for (int w2 = 0; w2 < static_cast<int>(blockDim.x >> 5); ++w2) m = max(m, s_wmax[w2]);
                 a.rowmax[by + j] = m;
             }
+        }
+        {   // the next chart's item bits, last read before the previous chart's end
+            unsigned* nxt = a.cand + ((p + 1) & 1) * a.cand_words;
+            for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < a.cand_words;
+                 i += static_cast<int64_t>(nb) * blockDim.x)
+                nxt[i] = 0u;
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             a.placement[3 * c] = bk;
@@ -523,6 +727,8 @@ struct PackScratch {
     int32_t* sums;
     int32_t* bestx;
     int32_t* ybest;
+    unsigned* cand;
+    int64_t cand_words;
     GridBar* bar;
     int64_t total;
 };
@@ -542,6 +748,8 @@ PackScratch carve(void* base, int64_t ntri, int64_t ncells, int64_t nrows, int32
     s.sums = reinterpret_cast<int32_t*>(take(4 * xscan_sums(nrows + 1)));
     s.bestx = reinterpret_cast<int32_t*>(take(4 * static_cast<int64_t>(nk) * G));
     s.ybest = reinterpret_cast<int32_t*>(take(8 * static_cast<int64_t>(nk)));
+    s.cand_words = (static_cast<int64_t>(nk) * G + 31) / 32;
+    s.cand = reinterpret_cast<unsigned*>(take(8 * s.cand_words));
     s.bar = reinterpret_cast<GridBar*>(take(sizeof(GridBar)));
     s.total = o;
     return s;
@@ -630,6 +838,7 @@ extern "C" int uva_pack_place(const uva_pack_attempt* a, int32_t blocks_per_sm, 
     cudaMemsetAsync(a->occupied, 0, sizeof(int64_t), st);
     cudaMemsetAsync(s.ybest, 0x7f, 8 * static_cast<size_t>(a->nk), st);
     cudaMemsetAsync(s.bar, 0, sizeof(GridBar), st);
+    cudaMemsetAsync(s.cand, 0, 8 * static_cast<size_t>(s.cand_words), st);
     if (a->nc > 0) cudaMemsetAsync(a->placement, 0xff, 12 * static_cast<size_t>(a->nc), st);
     k_pk_page_init<<<blocks_for(cells), kTB, 0, st>>>(a->G, a->R, a->rowmax);
     UVA_CHECK_LAUNCH("uva_pack_place/init");
@@ -652,6 +861,7 @@ extern "C" int uva_pack_place(const uva_pack_attempt* a, int32_t blocks_per_sm, 
         pa.var_key = reinterpret_cast<const unsigned long long*>(a->var_key);
         pa.R = a->R; pa.rowmax = a->rowmax; pa.placement = a->placement; pa.status = a->status;
         pa.bestx = s.bestx; pa.ybest = s.ybest; pa.bar = s.bar;
+        pa.cand = s.cand; pa.cand_words = s.cand_words;
         void* args[] = {&pa};
         e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_pk_place), dim3(grid), dim3(kTB), args, smem,
                                         st);
