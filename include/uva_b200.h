@@ -653,8 +653,12 @@ typedef struct uva_pack_attempt {
 
 int uva_pack_scratch_bytes(int64_t ntri, int64_t ncells, int64_t nrows, int32_t nk, int32_t G, int64_t* bytes);
 int uva_pack_masks(const uva_pack_attempt* a, void* stream);
-/* blocks_per_sm: resident blocks of the placement launch per SM (0: 2). */
+/* blocks_per_sm: resident blocks of the placement launch per SM (0: 4). */
 int uva_pack_place(const uva_pack_attempt* a, int32_t blocks_per_sm, void* stream);
+/* 1 to 4 independent attempts on the same page size in one cooperative
+ * launch, the blocks shared out between them (the probes of one round of
+ * the k-ary scale search, pack.py:418-445).                               */
+int uva_pack_place_pages(const uva_pack_attempt* const* attempts, int32_t n, int32_t blocks_per_sm, void* stream);
 int uva_pack_uv(const uva_pack_attempt* a, int32_t nangles, int32_t nturns, const int64_t* cofs, int64_t nv,
                 double s, const double* dens, double* out, void* stream);
 

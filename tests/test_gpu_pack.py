@@ -142,3 +142,25 @@ def test_device_pack_edge_cases(EP):
     assert uvs == []
     with pytest.raises(IndexError):
         EP.Packer([tri[0][0]], [np.array([[0, 1, 3]])], [1.0])
+
+
+def test_device_probes_in_one_launch_match_single_attempts(EP):
+    """Four attempts at different scales in one placement launch (the
+    probes of a k-ary round) give what four separate attempts give."""
+    from oracle import pack as OP
+    charts = _random_charts(23, 400, lo=20, hi=1500)
+    Us = [OP.orient(U) for U, _ in charts]
+    Ts = [T for _, T in charts]
+    tot = sum(OP.uv_area(U, T) for U, T in zip(Us, Ts))
+    G = 512
+    s0 = float(np.sqrt(0.62 * G * G / tot))
+    scales = [0.6 * s0, 0.8 * s0, 0.95 * s0, 1.3 * s0]   # the last one does not fit
+    P = EP.Packer(Us, Ts, np.ones(len(Us)))
+    many = P.attempts_at(G, 2, [0, 1, 2, 3], scales, "bbox")
+    one = [P.attempt(G, 2, [0, 1, 2, 3], s, "bbox") for s in scales]
+    assert many[-1] is None and one[-1] is None
+    for a, b in zip(many, one):
+        assert (a is None) == (b is None)
+        if a is not None:
+            assert a.placement == b.placement and a.occupied == b.occupied
+    assert many[0] is not None

@@ -135,6 +135,7 @@ _SIGS = {
     "uva_pack_scratch_bytes": [C.c_int64, C.c_int64, C.c_int64, i32, i32, vp],
     "uva_pack_masks": [vp, vp],
     "uva_pack_place": [vp, i32, vp],
+    "uva_pack_place_pages": [vp, i32, i32, vp],
     "uva_pack_uv": [vp, i32, i32, vp, C.c_int64, C.c_double, vp, vp, vp],
     "uva_last_error": [],
     "uva_version": [],

@@ -370,7 +370,19 @@ __device__ __forceinline__ bool warp_fits(const int32_t* R, const int32_t* run_o
 }
 
 // Dynamic shared memory: G free-run ints, then G occupancy bytes.
-__global__ void __launch_bounds__(kTB, 4) k_pk_place(PlaceArgs a) {
+// Several pages (independent attempts) in one launch: block b works on page
+// b % np, as block b / np of that page's b-blocks.
+constexpr int kMaxPages = 4;
+struct PlaceMulti {
+    PlaceArgs page[kMaxPages];
+    int32_t np;
+};
+
+__global__ void __launch_bounds__(kTB, 4) k_pk_place(PlaceMulti pm) {
+    const int32_t g = static_cast<int32_t>(blockIdx.x % static_cast<unsigned>(pm.np));
+    const PlaceArgs& a = pm.page[g];
+    const unsigned nb = (gridDim.x - static_cast<unsigned>(g) + pm.np - 1) / static_cast<unsigned>(pm.np);
+    const unsigned bid = blockIdx.x / static_cast<unsigned>(pm.np);
     extern __shared__ __align__(16) uint8_t s_dyn[];
     int32_t* s_R = reinterpret_cast<int32_t*>(s_dyn);
     uint8_t* s_occ = s_dyn + 4 * static_cast<size_t>(a.G);
@@ -385,7 +397,6 @@ __global__ void __launch_bounds__(kTB, 4) k_pk_place(PlaceArgs a) {
     __shared__ int32_t s_yb[2][kMaxVariants];
     __shared__ int32_t s_pref[kTB];
     const int32_t G = a.G, nk = a.nk;
-    const unsigned nb = gridDim.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int32_t p = 0; p < a.nc; ++p) {
         // ---- the chart's variants: usable ones get h > 0
@@ -427,7 +438,7 @@ __global__ void __launch_bounds__(kTB, 4) k_pk_place(PlaceArgs a) {
         for (int32_t i = threadIdx.x; i < G; i += blockDim.x) s_R[i] = __ldcg(a.rowmax + i);   // s_R: rowmax here
         __syncthreads();
         // a warp owns the word of its 32 items (it = warp-aligned base + lane)
-        for (int64_t base = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) & ~int64_t(31);
+        for (int64_t base = (bid * static_cast<int64_t>(blockDim.x) + threadIdx.x) & ~int64_t(31);
              base < items; base += static_cast<int64_t>(nb) * blockDim.x) {
             const int64_t it = base + lane;
             bool ok = false;
@@ -449,7 +460,7 @@ __global__ void __launch_bounds__(kTB, 4) k_pk_place(PlaceArgs a) {
             if (lane == 0 && bits) cb[base >> 5] = bits;
         }
         if (!grid_sync(a.bar, nb)) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, 2);
+            if (bid == 0 && threadIdx.x == 0) atomicOr(a.status, 2);
             return;
         }
         // ---- A2: first fit of every variant over the items of A1, in
@@ -477,7 +488,7 @@ __global__ void __launch_bounds__(kTB, 4) k_pk_place(PlaceArgs a) {
             s_word[threadIdx.x] = word;
             s_pref[threadIdx.x] = wbase + incl - __popc(word);   // exclusive
             __syncthreads();
-            const int64_t r_first = carry + ((static_cast<int64_t>(blockIdx.x) - carry) % nb + nb) % nb;
+            const int64_t r_first = carry + ((static_cast<int64_t>(bid) - carry) % nb + nb) % nb;
             for (int64_t r = r_first; r < carry + total; r += nb) {
                 const int32_t rr = static_cast<int32_t>(r - carry);
                 int32_t lo = 0, hi = kTB - 1;   // the last thread whose exclusive prefix is <= rr
@@ -575,7 +586,7 @@ __global__ void __launch_bounds__(kTB, 4) k_pk_place(PlaceArgs a) {
             carry += total;
         }
         if (!grid_sync(a.bar, nb)) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, 2);
+            if (bid == 0 && threadIdx.x == 0) atomicOr(a.status, 2);
             return;
         }
         // ---- B: the variant of smallest (y + h) G + (x + w), the first on ties (warp 0)
@@ -605,12 +616,12 @@ __global__ void __launch_bounds__(kTB, 4) k_pk_place(PlaceArgs a) {
         __syncthreads();
         const int32_t bk = s_sel[0], bx = s_sel[1], by = s_sel[2];
         if (bk < 0) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) { atomicOr(a.status, 1); a.status[1] = p; }
+            if (bid == 0 && threadIdx.x == 0) { atomicOr(a.status, 1); a.status[1] = p; }
             return;
         }
         // ---- C: mark the chart's cells, rebuild the free runs of its rows
         const int64_t r0 = cv.r0[bk];
-        for (int32_t j = blockIdx.x; j < cv.h[bk]; j += nb) {
+        for (int32_t j = bid; j < cv.h[bk]; j += nb) {
             int32_t* Rrow = a.R + static_cast<int64_t>(by + j) * G;
             __syncthreads();
             for (int32_t i = threadIdx.x; i < G; i += blockDim.x) s_occ[i] = __ldcg(Rrow + i) == 0;
@@ -657,11 +668,11 @@ __global__ void __launch_bounds__(kTB, 4) k_pk_place(PlaceArgs a) {
         }
         {   // the next chart's item bits, last read before the previous chart's end
             unsigned* nxt = a.cand + ((p + 1) & 1) * a.cand_words;
-            for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < a.cand_words;
+            for (int64_t i = bid * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < a.cand_words;
                  i += static_cast<int64_t>(nb) * blockDim.x)
                 nxt[i] = 0u;
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (bid == 0 && threadIdx.x == 0) {
             a.placement[3 * c] = bk;
             a.placement[3 * c + 1] = bx;
             a.placement[3 * c + 2] = by;
@@ -669,7 +680,7 @@ __global__ void __launch_bounds__(kTB, 4) k_pk_place(PlaceArgs a) {
             for (int32_t k = 0; k < nk; ++k) other[k] = kNone;
         }
         if (!grid_sync(a.bar, nb)) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, 2);
+            if (bid == 0 && threadIdx.x == 0) atomicOr(a.status, 2);
             return;
         }
     }
@@ -829,32 +840,26 @@ extern "C" int uva_pack_masks(const uva_pack_attempt* a, void* stream) {
     return UVA_OK;
 }
 
-extern "C" int uva_pack_place(const uva_pack_attempt* a, int32_t blocks_per_sm, void* stream) {
-    if (!attempt_ok(a, "uva_pack_place: bad arguments or scratch too small", true)) return UVA_E_ARG;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    PackScratch s = carve(a->scratch, a->ntri, a->ncells, a->nrows, a->nk, a->G);
-    const int64_t cells = static_cast<int64_t>(a->G) * a->G;
-    cudaMemsetAsync(a->status, 0, 2 * sizeof(int32_t), st);
-    cudaMemsetAsync(a->occupied, 0, sizeof(int64_t), st);
-    cudaMemsetAsync(s.ybest, 0x7f, 8 * static_cast<size_t>(a->nk), st);
-    cudaMemsetAsync(s.bar, 0, sizeof(GridBar), st);
-    cudaMemsetAsync(s.cand, 0, 8 * static_cast<size_t>(s.cand_words), st);
-    if (a->nc > 0) cudaMemsetAsync(a->placement, 0xff, 12 * static_cast<size_t>(a->nc), st);
-    k_pk_page_init<<<blocks_for(cells), kTB, 0, st>>>(a->G, a->R, a->rowmax);
-    UVA_CHECK_LAUNCH("uva_pack_place/init");
-    if (a->nc > 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const size_t smem = 5 * static_cast<size_t>(a->G);
-        if (smem > 48 * 1024)
-            cudaFuncSetAttribute(k_pk_place, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pk_place, kTB, smem);
-        if (e != cudaSuccess) return uva_cuda_status(e, "uva_pack_place/occupancy");
-        if (per_sm < 1) { uva_set_error("uva_pack_place: kernel does not fit one SM"); return UVA_E_CUDA; }
-        const int want = blocks_per_sm > 0 ? blocks_per_sm : 2;
-        const unsigned grid = static_cast<unsigned>(sms * std::min(per_sm, want));
-        PlaceArgs pa;
+namespace {
+
+// Page set-up, one cooperative launch over all pages, occupancy per page.
+int place_pages(const uva_pack_attempt* const* as, int32_t np, int32_t blocks_per_sm, cudaStream_t st) {
+    PlaceMulti pm{};
+    pm.np = np;
+    int32_t placing = 0;
+    for (int32_t g = 0; g < np; ++g) {
+        const uva_pack_attempt* a = as[g];
+        if (a->G != as[0]->G) { uva_set_error("uva_pack_place_pages: pages of different sizes"); return UVA_E_ARG; }
+        PackScratch s = carve(a->scratch, a->ntri, a->ncells, a->nrows, a->nk, a->G);
+        const int64_t cells = static_cast<int64_t>(a->G) * a->G;
+        cudaMemsetAsync(a->status, 0, 2 * sizeof(int32_t), st);
+        cudaMemsetAsync(a->occupied, 0, sizeof(int64_t), st);
+        cudaMemsetAsync(s.ybest, 0x7f, 8 * static_cast<size_t>(a->nk), st);
+        cudaMemsetAsync(s.bar, 0, sizeof(GridBar), st);
+        cudaMemsetAsync(s.cand, 0, 8 * static_cast<size_t>(s.cand_words), st);
+        if (a->nc > 0) cudaMemsetAsync(a->placement, 0xff, 12 * static_cast<size_t>(a->nc), st);
+        k_pk_page_init<<<blocks_for(cells), kTB, 0, st>>>(a->G, a->R, a->rowmax);
+        PlaceArgs& pa = pm.page[g];
         pa.G = a->G; pa.nc = a->nc; pa.nk = a->nk; pa.order = a->order;
         pa.var_src = a->var_src; pa.var_turn = a->var_turn; pa.var_row = a->var_row; pa.hw = a->hw;
         pa.row_need = a->row_need; pa.run_ofs = a->run_ofs; pa.run_a = a->run_a; pa.run_b = a->run_b;
@@ -862,15 +867,53 @@ extern "C" int uva_pack_place(const uva_pack_attempt* a, int32_t blocks_per_sm, 
         pa.R = a->R; pa.rowmax = a->rowmax; pa.placement = a->placement; pa.status = a->status;
         pa.bestx = s.bestx; pa.ybest = s.ybest; pa.bar = s.bar;
         pa.cand = s.cand; pa.cand_words = s.cand_words;
-        void* args[] = {&pa};
+        placing += a->nc > 0;
+    }
+    UVA_CHECK_LAUNCH("uva_pack_place/init");
+    if (placing > 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const size_t smem = 5 * static_cast<size_t>(as[0]->G);
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(k_pk_place, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pk_place, kTB, smem);
+        if (e != cudaSuccess) return uva_cuda_status(e, "uva_pack_place/occupancy");
+        if (per_sm < 1) { uva_set_error("uva_pack_place: kernel does not fit one SM"); return UVA_E_CUDA; }
+        const int want = blocks_per_sm > 0 ? blocks_per_sm : 4;
+        // a multiple of the page count, every page at least one block
+        unsigned grid = static_cast<unsigned>(sms * std::min(per_sm, want));
+        grid = std::max<unsigned>(static_cast<unsigned>(np), grid - grid % static_cast<unsigned>(np));
+        void* args[] = {&pm};
         e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_pk_place), dim3(grid), dim3(kTB), args, smem,
                                         st);
         if (e != cudaSuccess) return uva_cuda_status(e, "uva_pack_place/launch");
     }
-    k_pk_occupied<<<std::min<unsigned>(blocks_for(cells), 1024), kTB, 0, st>>>(
-        cells, a->R, reinterpret_cast<unsigned long long*>(a->occupied));
+    for (int32_t g = 0; g < np; ++g) {
+        const int64_t cells = static_cast<int64_t>(as[g]->G) * as[g]->G;
+        k_pk_occupied<<<std::min<unsigned>(blocks_for(cells), 1024), kTB, 0, st>>>(
+            cells, as[g]->R, reinterpret_cast<unsigned long long*>(as[g]->occupied));
+    }
     UVA_CHECK_LAUNCH("uva_pack_place");
     return UVA_OK;
+}
+
+}  // namespace
+
+extern "C" int uva_pack_place(const uva_pack_attempt* a, int32_t blocks_per_sm, void* stream) {
+    if (!attempt_ok(a, "uva_pack_place: bad arguments or scratch too small", true)) return UVA_E_ARG;
+    return place_pages(&a, 1, blocks_per_sm, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int uva_pack_place_pages(const uva_pack_attempt* const* attempts, int32_t n, int32_t blocks_per_sm,
+                                    void* stream) {
+    if (!attempts || n < 1 || n > kMaxPages) {
+        uva_set_error("uva_pack_place_pages: 1 to 4 attempts");
+        return UVA_E_ARG;
+    }
+    for (int32_t g = 0; g < n; ++g)
+        if (!attempt_ok(attempts[g], "uva_pack_place_pages: bad arguments or scratch too small", true)) return UVA_E_ARG;
+    return place_pages(attempts, n, blocks_per_sm, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int uva_pack_uv(const uva_pack_attempt* a, int32_t nangles, int32_t nturns, const int64_t* cofs,

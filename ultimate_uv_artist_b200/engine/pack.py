@@ -263,11 +263,9 @@ class Packer:
             out.append(ms)
         return out
 
-    def attempt(self, G, pad, rot_set, s, ordering="area", blocks_per_sm=0):
-        """Masks at texel scale s, then the first fit of every chart on a
-        G x G page: an Attempt, or None when a chart fits nowhere
-        (pack.py:398-402)."""
-        t0 = time.perf_counter()
+    def _prepare(self, G, pad, rot_set, s, ordering):
+        """Masks and runs at texel scale s and the placing order; the
+        descriptor (order set) and what it points to."""
         if ordering not in ORDERINGS:
             raise ValueError(f"unknown ordering {ordering!r}")
         extra = ()
@@ -282,12 +280,11 @@ class Packer:
             order = torch.argsort(-A["var_area"][:nc * nk].view(nc, nk)[:, 0], stable=True) if nc else A["var_area"][:0]
         else:
             order = rest[0]
-        order = order.contiguous()
-        d.order = _ptr(order)
-        _lib.check(_lib.lib().uva_pack_place(C.byref(d), int(blocks_per_sm), _stream(self.dev)), "uva_pack_place")
-        st = A["status"].cpu().numpy()
-        self.attempts += 1
-        self.seconds += time.perf_counter() - t0
+        A["order"] = order.contiguous()
+        d.order = _ptr(A["order"])
+        return d, lay, A
+
+    def _result(self, s, G, pad, rot_set, lay, A, st):
         if st[2]:
             raise RuntimeError("uva_pack_masks: run table capacity exceeded")
         if st[0] & 2:
@@ -296,6 +293,31 @@ class Packer:
             return None
         return Attempt(s, G, pad, lay["hw"].reshape(-1, 2), A["placement"], int(A["occupied"].item()),
                        len(rot_set), self.nA)
+
+    def attempt(self, G, pad, rot_set, s, ordering="area", blocks_per_sm=0):
+        """Masks at texel scale s, then the first fit of every chart on a
+        G x G page: an Attempt, or None when a chart fits nowhere
+        (pack.py:398-402)."""
+        t0 = time.perf_counter()
+        d, lay, A = self._prepare(G, pad, rot_set, s, ordering)
+        _lib.check(_lib.lib().uva_pack_place(C.byref(d), int(blocks_per_sm), _stream(self.dev)), "uva_pack_place")
+        st = A["status"].cpu().numpy()
+        self.attempts += 1
+        self.seconds += time.perf_counter() - t0
+        return self._result(s, G, pad, rot_set, lay, A, st)
+
+    def attempts_at(self, G, pad, rot_set, scales, ordering="area", blocks_per_sm=0):
+        """Up to four attempts at different scales placed in one launch (the
+        probes of one k-ary search round): a list of Attempt or None."""
+        t0 = time.perf_counter()
+        prep = [self._prepare(G, pad, rot_set, s, ordering) for s in scales]
+        descs = (C.c_void_p * len(prep))(*[C.cast(C.pointer(d), C.c_void_p) for d, _, _ in prep])
+        _lib.check(_lib.lib().uva_pack_place_pages(descs, len(prep), int(blocks_per_sm), _stream(self.dev)),
+                   "uva_pack_place_pages")
+        sts = torch.stack([A["status"] for _, _, A in prep]).cpu().numpy()
+        self.attempts += len(prep)
+        self.seconds += time.perf_counter() - t0
+        return [self._result(s, G, pad, rot_set, lay, A, st) for s, (_, lay, A), st in zip(scales, prep, sts)]
 
     def uvs(self, att):
         """Per chart the UVs in [0, 1] of a successful attempt
@@ -331,8 +353,8 @@ def _search(attempt_fn, n, s, iters, tol=0.004, lo=0.0, hi=None, best=None, dead
 
 def _search_kary(attempt_fn, s, iters, tol, lo, hi, best, deadline):
     """pack.py:418-445: the bracket shrinks about five times per round of
-    four probes; the probes run one after another on the device (only which
-    of them fit decides the next round)."""
+    four probes; the probes of a round share one placement launch (only
+    which of them fit decides the next round)."""
     k = max(PROBES, 4)
     for _ in range(max(2, int(np.ceil(iters / np.log2(k + 1))))):
         if hi is not None and lo > 0 and (hi - lo) / lo < tol:
@@ -347,7 +369,8 @@ def _search_kary(attempt_fn, s, iters, tol, lo, hi, best, deadline):
             cand = hi * np.array([0.55, 0.7, 0.8, 0.9])[:k]
         else:
             cand = np.linspace(lo, hi, k + 2)[1:-1]
-        res = [attempt_fn(float(sc)) for sc in cand]
+        many = getattr(attempt_fn, "many", None)
+        res = many([float(sc) for sc in cand]) if many else [attempt_fn(float(sc)) for sc in cand]
         for sc, r in zip(cand, res):
             if r is not None and sc > lo:
                 best, lo = r, float(sc)
@@ -402,7 +425,9 @@ def pack(charts, atlas=4096, padding=4, grid=None, rotations=4, density=None, it
     P = Packer(Us, Ts, dens, ANGLES)
 
     def at(G, p, o):
-        return lambda sc: P.attempt(G, p, rot_set, sc, o)
+        fn = lambda sc: P.attempt(G, p, rot_set, sc, o)  # noqa: E731
+        fn.many = lambda scs: P.attempts_at(G, p, rot_set, scs, o)
+        return fn
 
     best = None
     if grid >= 1024:
