@@ -60,6 +60,10 @@ def _args():
     ap.add_argument("--no-config5", action="store_true")
     ap.add_argument("--no-config1", action="store_true")
     ap.add_argument("--no-config4", action="store_true")
+    ap.add_argument("--no-pack", action="store_true")
+    ap.add_argument("--pack-charts", type=int, default=3000)
+    ap.add_argument("--pack-only", action="store_true",
+                    help="only the packing leg, as one JSON line (for launch lists of the packer)")
     return ap.parse_args()
 
 
@@ -623,6 +627,61 @@ def bench_config5(dev, iters=ITERS, steps=2, cpu=True):
             "flipped": int(rep["flipped_triangles"]), "islands": int(rep["islands"])}
 
 
+def bench_pack(dev, nch=3000, cpu=True):
+    """engine.pack on synthetic disk charts (log-uniform 100 to 6,000
+    triangles, stretched up to 6.7x, random in-plane turns) with the
+    reference's default schedule (atlas 4096, padding 4, grid 2048, four
+    turns, three orderings, no time budget): wall time, attempts, and the
+    device time of one full-grid attempt and of one four-probe round (CUDA
+    events) beside the oracle's serial first fit of the same attempt on one
+    host core."""
+    import torch
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.engine import pack as EPK
+    rng = np.random.default_rng(3)
+    charts = []
+    for _ in range(nch):
+        P, T = synth.disk_patch(rng, int(np.exp(rng.uniform(np.log(100), np.log(6000)))))
+        charts.append((P[:, :2].astype(np.float64) * rng.uniform(0.3, 2.0, 2), np.asarray(T, np.int64)))
+    stream = torch.cuda.current_stream(dev)
+    torch.cuda.synchronize(); w0 = time.perf_counter()
+    uvs, info = EPK.pack(charts, atlas=4096, padding=4)
+    torch.cuda.synchronize(); pack_s = time.perf_counter() - w0
+    Us = [EPK.orient(u) for u, _ in charts]
+    Ts = [t for _, t in charts]
+    P = EPK.Packer(Us, Ts, np.ones(nch))
+    s_att = 0.97 * info["texel_scale_grid"]
+    P.attempt(2048, 2, [0, 1, 2, 3], s_att, "area")
+    a0, a1 = _events(dev)
+    a0.record(stream)
+    att = P.attempt(2048, 2, [0, 1, 2, 3], s_att, "area")
+    a1.record(stream)
+    torch.cuda.synchronize()
+    attempt_ms = a0.elapsed_time(a1)
+    s_half = s_att * 1024 / 2048
+    probes = [s_half * f for f in (0.88, 0.92, 0.96, 1.0)]
+    P.attempts_at(1024, 1, [0, 1, 2, 3], probes, "area")
+    a0.record(stream)
+    P.attempts_at(1024, 1, [0, 1, 2, 3], probes, "area")
+    a1.record(stream)
+    torch.cuda.synchronize()
+    round_ms = a0.elapsed_time(a1)
+    out = {"workload": f"disk_charts_{nch}", "charts": nch, "triangles": int(sum(len(t) for t in Ts)),
+           "api_s": pack_s, "attempts": info["attempts"], "attempt_s_total": info["attempt_seconds"],
+           "texel_scale_grid": info["texel_scale_grid"], "plan_occupancy": info["plan_occupancy"],
+           "attempt_ms_2048": attempt_ms, "us_per_chart_2048": attempt_ms * 1e3 / nch,
+           "probe_round_ms_1024": round_ms}
+    if cpu:
+        from oracle import pack as OPK
+        t0 = time.perf_counter()
+        ref_att = OPK.attempt(Us, Ts, np.ones(nch), 2048, 2, [0, 1, 2, 3], s_att, "area")
+        cs = time.perf_counter() - t0
+        out["cpu_oracle"] = {"attempt_s": cs, "cores": 1, "kind": "port", "speedup_attempt": cs / (attempt_ms / 1e3),
+                             "same_placement": bool(att is not None and ref_att is not None
+                                                    and att.placement == ref_att[1][0])}
+    return out
+
+
 def bench_energy(dev, hbm, reps=5):
     """Config 4: the ARAP / symmetric-Dirichlet forward and backward kernels
     on 512 islands of 500 to 50,000 triangles (5.8M, 5 % near-degenerate),
@@ -748,6 +807,12 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.pack_only:
+        if rank == 0:
+            print(json.dumps({"pack": bench_pack(dev, args.pack_charts, cpu=not args.no_cpu_baseline)}))
+        if ws > 1:
+            dist.destroy_process_group()
+        return
     from ultimate_uv_artist_b200 import synth
     from ultimate_uv_artist_b200.engine import gpu
 
@@ -889,7 +954,9 @@ def main():
         bnd = bench_boundary(b)
         hier_b = bench_hier(dev)
         ovl = bench_overlap(islands, our_uvs)
-    c5 = c1 = c4 = None
+    c5 = c1 = c4 = pk = None
+    if rank == 0 and not args.no_pack:
+        pk = bench_pack(dev, args.pack_charts, cpu=not args.no_cpu_baseline)
     if rank == 0 and not args.no_config5:
         c5 = bench_config5(dev, cpu=not args.no_cpu_baseline)
     if rank == 0 and not args.no_config4:
@@ -974,6 +1041,7 @@ def main():
             "hier_solver": hier_b,
             "overlap_checks": ovl,
             "config5": c5,
+            "pack": pk,
             "config4_energy": c4,
             "config1": c1,
         }

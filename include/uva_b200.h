@@ -357,10 +357,22 @@ typedef struct uva_val_desc {
     int64_t* counts;        /* out, UVA_VC_N counters                         */
     void* scratch;          /* device scratch of uva_validate_scratch_bytes   */
     int64_t scratch_bytes;
+    int32_t shard, nshards; /* nshards > 1: test only the candidate pairs whose
+                               first shared cell lies in cell rows
+                               [G shard / nshards, G (shard + 1) / nshards);
+                               0 / 0: all pairs                               */
 } uva_val_desc;
 
 int uva_validate_scratch_bytes(int64_t n, int64_t m, int32_t grid, int64_t* bytes);
 int uva_validate(const uva_val_desc* d, void* stream);
+/* Several shards (one per GPU): every shard runs
+ * uva_validate with its band, the overlap bits 16 and 32 of tflags are
+ * merged across shards (OR: an all-reduce MAX of each bit) and the
+ * UVA_VC_PAIRS counts summed; then uva_validate_finish, with the same
+ * descriptor and scratch, recounts UVA_VC_OVERLAP, UVA_VC_CONTACTS and
+ * UVA_VC_ISLANDS_OV from the merged bits. The other counts, labels and
+ * flags do not depend on the band.                                         */
+int uva_validate_finish(const uva_val_desc* d, void* stream);
 /* engine/metrics.py:91-103: face islands; weld != 0 merges vertices with
  * identical float32 (position, uv) bytes. count: device int64.
  * Scratch: uva_validate_scratch_bytes(n, m, 0).                            */

@@ -115,9 +115,20 @@ static int64_t cell_of(double u, int64_t G) {
     return c < 0 ? 0 : (c > G - 1 ? G - 1 : c);
 }
 
-/* Returns the number of tested candidate pairs (cell boxes intersecting). */
+/* Returns the number of tested candidate pairs (cell boxes intersecting).
+ * Only cells of rows [band_lo, band_hi) are scanned: every pair is tested
+ * in its first shared cell, so bands that cover the rows once test every
+ * pair once (the sharded validation). */
+int64_t uvo_overlaps_band(const double* U, const int64_t* F, const uint8_t* skip, int64_t m, int64_t G, double rel,
+                          int strict, int64_t band_lo, int64_t band_hi, uint8_t* flag);
+
 int64_t uvo_overlaps(const double* U, const int64_t* F, const uint8_t* skip, int64_t m, int64_t G, double rel,
                      int strict, uint8_t* flag) {
+    return uvo_overlaps_band(U, F, skip, m, G, rel, strict, 0, G, flag);
+}
+
+int64_t uvo_overlaps_band(const double* U, const int64_t* F, const uint8_t* skip, int64_t m, int64_t G, double rel,
+                          int strict, int64_t band_lo, int64_t band_hi, uint8_t* flag) {
     int64_t* x0 = malloc(sizeof(int64_t) * (size_t)m * 4);
     int64_t *x1 = x0 + m, *y0 = x0 + 2 * m, *y1 = x0 + 3 * m;
     for (int64_t t = 0; t < m; ++t) {
@@ -145,7 +156,7 @@ int64_t uvo_overlaps(const double* U, const int64_t* F, const uint8_t* skip, int
     int64_t tested = 0;
     /* cells in parallel, like the reference's prange over cells */
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : tested)
-    for (int64_t c = 0; c < G * G; ++c) {
+    for (int64_t c = band_lo * G; c < band_hi * G; ++c) {
         int64_t cy = c / G, cx = c % G;
         for (int64_t p = cnt[c]; p < cnt[c + 1]; ++p) {
             int64_t s = items[p];

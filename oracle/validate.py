@@ -30,6 +30,9 @@ def clib():
         vp = C.c_void_p
         lib.uvo_overlaps.argtypes = [vp, vp, vp, C.c_int64, C.c_int64, C.c_double, C.c_int, vp]
         lib.uvo_overlaps.restype = C.c_int64
+        lib.uvo_overlaps_band.argtypes = [vp, vp, vp, C.c_int64, C.c_int64, C.c_double, C.c_int, C.c_int64,
+                                          C.c_int64, vp]
+        lib.uvo_overlaps_band.restype = C.c_int64
         lib.uvo_raster_labels.argtypes = [vp, vp, vp, C.c_int64, C.c_int64, vp]
         lib.uvo_raster_labels.restype = None
         lib.uvo_raster_counts.argtypes = [vp, vp, C.c_int64, C.c_int64, vp]
@@ -46,14 +49,18 @@ def _p(a):
     return C.c_void_p(a.ctypes.data)
 
 
-def overlaps_c(U, F, skip, G, rel=1e-6, strict=False):
+def overlaps_c(U, F, skip, G, rel=1e-6, strict=False, band=None):
     """engine/validate.py:95-136 / :258-300 exactly as the reference loops
-    (grid G, serial binning), in C. Returns (flags, tested cell-box pairs)."""
+    (grid G, serial binning), in C. Returns (flags, tested cell-box pairs).
+    band: (lo, hi) cell rows: only the pairs whose first shared cell lies in
+    those rows (one shard of a sharded validation)."""
     U = np.ascontiguousarray(U, np.float64)
     F = np.ascontiguousarray(F, np.int64)
     sk = np.ascontiguousarray(skip, np.uint8)
     flag = np.zeros(len(F), np.uint8)
-    n = clib().uvo_overlaps(_p(U), _p(F), _p(sk), len(F), int(G), float(rel), 1 if strict else 0, _p(flag))
+    lo, hi = (0, int(G)) if band is None else (int(band[0]), int(band[1]))
+    n = clib().uvo_overlaps_band(_p(U), _p(F), _p(sk), len(F), int(G), float(rel), 1 if strict else 0, lo, hi,
+                                 _p(flag))
     return flag.astype(bool), int(n)
 
 

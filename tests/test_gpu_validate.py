@@ -115,3 +115,58 @@ def test_edge_cases(cuda):
     # no triangles
     rep, prob = GV.validate_uvs(V2, np.zeros((0, 3), np.int64), UV2, atlas=64, gutter=False)
     assert rep["islands"] == 0 and rep["valid"] and len(prob) == 0
+
+
+def test_validation_shards_merge_to_the_whole(cuda):
+    """Sharded validation on one GPU, the shards one after another: each
+    shard's overlap bits equal the oracle's scan of the same band of cell
+    rows, the bits OR'd together and the pair counts summed give the
+    unsharded flags, and uva_validate_finish the unsharded counts; with a
+    process group (gloo, one rank) validate_uvs gives the whole report."""
+    import datetime
+    import socket
+    import torch
+    import torch.distributed as dist
+    from ultimate_uv_artist_b200 import shard, synth
+    from ultimate_uv_artist_b200.engine import validate as GV
+    V, F, UV, _ = synth.validation_atlas(seed=3100, islands=800, tris_per_island=200, atlas=2048, padding=4,
+                                         overlap_rate=3e-4, fold_rate=5e-5, mirrored=3, outside=20)
+    F32 = F.astype(np.int32)
+    whole = GV.DeviceValidation(V, F32, UV).run()
+    w_flags, w_counts = whole.flags(), whole.host_counts()
+    _, _, ex = OV.validate_uvs(V, F, UV, atlas=2048, padding=4, gutter=False, count_pairs=False)
+    U = np.asarray(UV, np.float32).astype(np.float64)
+    G = int(np.clip(np.sqrt(len(F)) / 2, 64, 4096))
+    world = 3
+    parts = [GV.DeviceValidation(V, F32, UV, shard=r, nshards=world).run() for r in range(world)]
+    bits = np.zeros(len(F), np.uint8)
+    pairs = 0
+    for r, dv in enumerate(parts):
+        fl = dv.flags()
+        band = shard.band_rows(G, r, world)
+        ov, _ = OV.overlaps_c(U, F, ex["skip"], G, 1e-6, band=band)
+        ovs, _ = OV.overlaps_c(U, F, ex["skip"], G, 0.0, strict=True, band=band)
+        assert np.array_equal((fl & 16) != 0, ov) and np.array_equal((fl & 32) != 0, ovs), r
+        assert np.array_equal(fl & 15, w_flags & 15), r     # the band leaves the other bits alone
+        bits |= fl & 48
+        pairs += int(dv.host_counts()[GV.VC_PAIRS])
+    head = parts[0]
+    head.tflags[:len(F)] = torch.from_numpy((head.flags() & 207) | bits).to(head.tflags.device)
+    head.counts[GV.VC_PAIRS] = pairs
+    head.finish()
+    assert np.array_equal(head.flags(), w_flags)
+    assert np.array_equal(head.host_counts(), w_counts)
+    # the process-group path (one gloo rank: the merge is the identity, finish recounts)
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        rep_g, prob_g = GV.validate_uvs(V, F, UV, atlas=2048, padding=4, group=dist.group.WORLD)
+        dv = GV.DeviceValidation(V, F32, UV).run().merge(dist.group.WORLD)
+        assert np.array_equal(dv.host_counts(), w_counts)
+    finally:
+        dist.destroy_process_group()
+    rep, prob = GV.validate_uvs(V, F, UV, atlas=2048, padding=4)
+    assert rep_g == rep and np.array_equal(prob_g, prob)

@@ -127,6 +127,7 @@ _SIGS = {
     "uva_seam_report": [vp, C.c_int64, vp, C.c_int64, vp, vp, vp, vp, vp, C.c_int64, vp],
     "uva_corners_equal": [vp, i32, C.c_int64, vp, vp, i32, C.c_int64, vp, C.c_int64, i32, vp, vp],
     "uva_segment_sum": [vp, C.c_int64, vp, C.c_int64, i32, vp, vp, vp],
+    "uva_validate_finish": [vp, vp],
     "uva_concat_tris32": [i32, vp, vp, vp, vp, i32],
     "uva_concat_rows32": [i32, vp, vp, i32, vp, i32],
     "uva_dplan_scratch_bytes": [C.c_int64, C.c_int64, C.c_int64, vp],

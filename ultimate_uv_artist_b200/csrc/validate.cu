@@ -451,13 +451,14 @@ __device__ __forceinline__ void test_pair(int s, int t, const UVT* UV, const int
 
 // One thread per (cell, item): pairs with the later items of the cell, each
 // pair once (in the first cell both cell boxes share, engine/validate.py:130).
+// Only cells of rows [band_lo, band_hi): a shard's band of the atlas.
 template <typename UVT>
 __global__ void k_pairs_items(const int32_t* nitems, const int32_t* items, const int32_t* item_cell, const int32_t* cofs,
                               const int4* cbox, int G, const UVT* UV, const int32_t* F, double rel, uint8_t* tflags,
-                              unsigned long long* counts) {
+                              unsigned long long* counts, int band_lo, int band_hi) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long npairs = 0;
-    if (p < *nitems) {
+    if (p < *nitems && item_cell[p] / G >= band_lo && item_cell[p] / G < band_hi) {
         const int cell = item_cell[p];
         const int cx = cell % G, cy = cell / G;
         const int end = cofs[cell + 1];
@@ -485,10 +486,12 @@ __global__ void k_item_cells(int ncells, const int32_t* cofs, int32_t* item_cell
 }
 
 // Big triangles (more than kMaxCells cells) against every non-skipped
-// triangle; big-big pairs once (lower index first).
+// triangle; big-big pairs once (lower index first). A pair belongs to the
+// band holding the row of its first shared cell, as on the binned path.
 template <typename UVT>
 __global__ void k_pairs_big(int m, const int32_t* big, const int32_t* nbig, const int4* cbox, const uint8_t* skipf,
-                            const UVT* UV, const int32_t* F, double rel, uint8_t* tflags, unsigned long long* counts) {
+                            const UVT* UV, const int32_t* F, double rel, uint8_t* tflags, unsigned long long* counts,
+                            int band_lo, int band_hi) {
     const int nb = *nbig;
     unsigned long long npairs = 0;
     for (int k = blockIdx.x; k < nb; k += gridDim.x) {
@@ -500,6 +503,8 @@ __global__ void k_pairs_big(int m, const int32_t* big, const int32_t* nbig, cons
             const int ntc = (bt.y - bt.x + 1) * (bt.w - bt.z + 1);
             if (ntc > kMaxCells && t < s) continue;   // big-big: tested from the lower index
             if (bs.x > bt.y || bt.x > bs.y || bs.z > bt.w || bt.z > bs.w) continue;
+            const int cy = max(bs.z, bt.z);
+            if (cy < band_lo || cy >= band_hi) continue;
             bool counted = false;
             test_pair(s, t, UV, F, rel, tflags, counted);
             npairs += counted ? 1 : 0;
@@ -510,6 +515,27 @@ __global__ void k_pairs_big(int m, const int32_t* big, const int32_t* nbig, cons
 }
 
 // ------------------------------------------------------------------ final flags and counts
+// After the overlap bits of every shard are merged into tflags: the counts
+// that depend on them, again (uva_validate_finish).
+__global__ void k_recount(int m, const uint8_t* tflags, const int32_t* labels, int32_t* island_ov,
+                          unsigned long long* counts) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    bool ov = false, contact = false;
+    if (t < m) {
+        const uint8_t f = tflags[t];
+        ov = f & 16;
+        contact = (f & 32) && !ov;
+        if (ov) island_ov[labels[t]] = 1;
+    }
+    count_add(counts + UVA_VC_OVERLAP, ov);
+    count_add(counts + UVA_VC_CONTACTS, contact);
+}
+
+__global__ void k_zero_counts(unsigned long long* counts) {
+    counts[UVA_VC_OVERLAP] = 0;
+    counts[UVA_VC_CONTACTS] = 0;
+    counts[UVA_VC_ISLANDS_OV] = 0;
+}
 __global__ void k_final(int m, const double* sa, const int32_t* labels, const int8_t* dom, uint8_t* tflags,
                         int32_t* island_ov, unsigned long long* counts) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -713,9 +739,13 @@ extern "C" int uva_validate(const uva_val_desc* d, void* stream) {
     UVA_CHECK_LAUNCH("uva_validate/binning");
     // the number of items is bounded by kMaxCells * m; threads beyond the
     // actual count read cofs[ncell] as the end and do nothing
+    const int nsh = std::max(1, d->nshards), sh = nsh > 1 ? d->shard : 0;
+    const int band_lo = static_cast<int>(static_cast<int64_t>(G) * sh / nsh);
+    const int band_hi = static_cast<int>(static_cast<int64_t>(G) * (sh + 1) / nsh);
     k_pairs_items<float><<<blocks(kMaxCells * m), 256, 0, s>>>(nitems, items, item_cell, cofs, cbox, G, d->UV, d->F,
-                                                                d->rel, d->tflags, counts);
-    k_pairs_big<float><<<148, 256, 0, s>>>(m, big, nbig, cbox, d->tflags, d->UV, d->F, d->rel, d->tflags, counts);
+                                                                d->rel, d->tflags, counts, band_lo, band_hi);
+    k_pairs_big<float><<<148, 256, 0, s>>>(m, big, nbig, cbox, d->tflags, d->UV, d->F, d->rel, d->tflags, counts,
+                                           band_lo, band_hi);
     UVA_CHECK_LAUNCH("uva_validate/pairs");
     cudaMemsetAsync(isl_ov, 0, 4 * static_cast<size_t>(m + 1), s);
     k_final<<<blocks(m), 256, 0, s>>>(m, d->sa, d->labels, dom, d->tflags, isl_ov, counts);
@@ -723,6 +753,30 @@ extern "C" int uva_validate(const uva_val_desc* d, void* stream) {
     k_count_flags<<<blocks(m), 256, 0, s>>>(m, isl_ov, counts, UVA_VC_ISLANDS_OV);
     k_store_pairs_meta<<<1, 1, 0, s>>>(nbig, namb, counts);
     UVA_CHECK_LAUNCH("uva_validate/final");
+    return UVA_OK;
+}
+
+extern "C" int uva_validate_finish(const uva_val_desc* d, void* stream) {
+    if (!d || d->n < 0 || d->m < 0 || !d->counts || (d->m > 0 && (!d->tflags || !d->labels || !d->scratch))) {
+        uva_set_error("uva_validate_finish: bad arguments");
+        return UVA_E_ARG;
+    }
+    if (d->m == 0) return UVA_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int m = d->m;
+    const Layout L = layout(d->n, m, auto_grid(m, d->grid));
+    if (d->scratch_bytes < static_cast<int64_t>(L.total)) {
+        uva_set_error("uva_validate_finish: scratch too small");
+        return UVA_E_ARG;
+    }
+    int32_t* isl_ov = reinterpret_cast<int32_t*>(static_cast<unsigned char*>(d->scratch) + L.off[19]);
+    unsigned long long* counts = reinterpret_cast<unsigned long long*>(d->counts);
+    auto blocks = [](int x) { return std::max(1, (x + 255) / 256); };
+    cudaMemsetAsync(isl_ov, 0, 4 * static_cast<size_t>(m + 1), s);
+    k_zero_counts<<<1, 1, 0, s>>>(counts);
+    k_recount<<<blocks(m), 256, 0, s>>>(m, d->tflags, d->labels, isl_ov, counts);
+    k_count_flags<<<blocks(m), 256, 0, s>>>(m, isl_ov, counts, UVA_VC_ISLANDS_OV);
+    UVA_CHECK_LAUNCH("uva_validate_finish");
     return UVA_OK;
 }
 
@@ -762,8 +816,8 @@ extern "C" int uva_chart_overlaps(const double* U, const int32_t* F, int32_t n, 
     k_bin_fill<<<blocks(m), 256, 0, s>>>(m, cbox, G, cofs, cursor, items);
     k_item_cells<<<blocks(ncell), 256, 0, s>>>(ncell, cofs, item_cell);
     k_pairs_items<double><<<blocks(kMaxCells * m), 256, 0, s>>>(smalls + 3, items, item_cell, cofs, cbox, G, U, F, 1e-6,
-                                                                 tflags, counts);
-    k_pairs_big<double><<<148, 256, 0, s>>>(m, big, smalls + 1, cbox, tflags, U, F, 1e-6, tflags, counts);
+                                                                 tflags, counts, 0, G);
+    k_pairs_big<double><<<148, 256, 0, s>>>(m, big, smalls + 1, cbox, tflags, U, F, 1e-6, tflags, counts, 0, G);
     UVA_CHECK_LAUNCH("uva_chart_overlaps");
     return UVA_OK;
 }

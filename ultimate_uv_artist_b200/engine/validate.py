@@ -36,7 +36,7 @@ class ValDesc(C.Structure):
     _fields_ = [("n", C.c_int32), ("m", C.c_int32), ("grid", C.c_int32), ("reserved", C.c_int32),
                 ("V", C.c_void_p), ("UV", C.c_void_p), ("F", C.c_void_p), ("rel", C.c_double),
                 ("tflags", C.c_void_p), ("labels", C.c_void_p), ("sa", C.c_void_p), ("counts", C.c_void_p),
-                ("scratch", C.c_void_p), ("scratch_bytes", C.c_int64)]
+                ("scratch", C.c_void_p), ("scratch_bytes", C.c_int64), ("shard", C.c_int32), ("nshards", C.c_int32)]
 
 
 def _sig():
@@ -53,7 +53,7 @@ def _sig():
 class DeviceValidation:
     """One validation pass on the device; results stay on the device until read."""
 
-    def __init__(self, V, F, UV32, rel=1e-6, grid=0, device=None, stream=None):
+    def __init__(self, V, F, UV32, rel=1e-6, grid=0, device=None, stream=None, shard=0, nshards=1):
         L = _sig()
         self.dev = require_cuda(device)
         d = self.dev
@@ -76,12 +76,35 @@ class DeviceValidation:
         D.tflags, D.labels, D.sa, D.counts = (self.tflags.data_ptr(), self.labels.data_ptr(), self.sa.data_ptr(),
                                               self.counts.data_ptr())
         D.scratch, D.scratch_bytes = self.scratch.data_ptr(), int(nb.value)
+        D.shard, D.nshards = int(shard), int(nshards)
         self.desc = D
         self.stream = stream
 
     def run(self):
         s = self.stream if self.stream is not None else torch.cuda.current_stream(self.dev)
         _lib.check(_sig().uva_validate(C.byref(self.desc), C.c_void_p(s.cuda_stream)), "uva_validate")
+        return self
+
+    def merge(self, group=None):
+        """Several shards (one per rank of `group`, each validating its band
+        of cell rows): OR the overlap bits of every rank into tflags, sum the
+        candidate-pair counts, and recount what depends on the bits
+        (uva_validate_finish). Every rank ends with the whole report."""
+        from .. import shard as S
+        m = self.m
+        if m:
+            bits = self.tflags[:m]
+            ov = S.allreduce_max(((bits & 16) != 0).to(torch.uint8), group)
+            st = S.allreduce_max(((bits & 32) != 0).to(torch.uint8), group)
+            self.tflags[:m] = (bits & 207) | (ov * 16) | (st * 32)
+        self.counts[VC_PAIRS:VC_PAIRS + 1] = S.allreduce_sum(self.counts[VC_PAIRS:VC_PAIRS + 1].clone(), group)
+        return self.finish()
+
+    def finish(self):
+        """Recount the overlap-dependent counts from tflags after the bits of
+        other shards were merged into it (uva_validate_finish)."""
+        s = self.stream if self.stream is not None else torch.cuda.current_stream(self.dev)
+        _lib.check(_lib.lib().uva_validate_finish(C.byref(self.desc), C.c_void_p(s.cuda_stream)), "uva_validate_finish")
         return self
 
     def host_counts(self):
@@ -92,12 +115,21 @@ class DeviceValidation:
 
 
 def validate_uvs(v, f, uv, atlas=4096, padding=None, in_v=None, in_f=None, in_normals=None, out_normals=None,
-                 in_colors=None, out_colors=None, xref=None, gutter=True):
-    """Checks on final UVs (engine/validate.py:139-209). Returns (report, per-triangle problem mask)."""
+                 in_colors=None, out_colors=None, xref=None, gutter=True, group=None):
+    """Checks on final UVs (engine/validate.py:139-209). Returns (report, per-triangle problem mask).
+
+    group: a torch.distributed process group over several GPUs (one rank
+    each, every rank holding the whole mesh): each rank tests the overlap
+    pairs of its band of the atlas, the overlap bits and pair counts are
+    all-reduced, and every rank returns the same report."""
     v = np.asarray(v, np.float64)
     f = np.asarray(f, np.int64)
     uv32 = np.asarray(uv, np.float32)
-    dv = DeviceValidation(v, f.astype(np.int32), uv32).run()
+    from .. import shard as S
+    rank, world = S.rank_world(group)
+    dv = DeviceValidation(v, f.astype(np.int32), uv32, shard=rank, nshards=world).run()
+    if world > 1:
+        dv.merge(group)
     c = dv.host_counts()
     fl = dv.flags()
     rep = {}

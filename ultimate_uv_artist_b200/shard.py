@@ -11,6 +11,13 @@ the final gather of per-island results and the reduction of step timings.
 * ``gather_chart_uvs``: per-island UV arrays of all ranks back in the
   original island order (on every rank, or on rank 0 only).
 * ``reduce_step``: max over ranks of a step time and sum of the units done.
+
+Validation shards with one exchange step: every rank holds the whole mesh
+and tests the candidate overlap pairs whose first shared grid cell lies in
+its band of cell rows (``band_rows``); the per-triangle overlap bits are
+combined by an all-reduce MAX (``allreduce_max``) and the pair counts by a
+SUM (``allreduce_sum``), after which every rank holds the whole report
+(``engine.validate.validate_uvs(..., group=...)``).
 """
 from __future__ import annotations
 
@@ -80,3 +87,41 @@ def reduce_step(ms, units, device=None, group=None):
     sm = t.clone()
     dist.all_reduce(sm, op=dist.ReduceOp.SUM, group=group)
     return float(mx[0]), float(sm[1])
+
+
+def rank_world(group=None):
+    """(rank, world) of an explicit process group; (0, 1) without one (a
+    validation without a group is a whole, local one)."""
+    if group is None:
+        return 0, 1
+    import torch.distributed as dist
+    return dist.get_rank(group), dist.get_world_size(group)
+
+
+def band_rows(G, rank, world):
+    """Cell rows [lo, hi) of a rank's band of a G x G validation grid (the
+    rows uva_validate's pair kernels keep for shard rank of world)."""
+    return (G * rank) // world, (G * (rank + 1)) // world
+
+
+def _allreduce(t, op, group):
+    import torch.distributed as dist
+    if t.is_cuda and dist.get_backend(group) == "gloo":   # gloo reduces host tensors
+        h = t.cpu()
+        dist.all_reduce(h, op=op, group=group)
+        return h.to(t.device)
+    dist.all_reduce(t, op=op, group=group)
+    return t
+
+
+def allreduce_max(t, group=None):
+    """Element-wise maximum over the ranks of `group` (in place when the
+    backend reduces the tensor where it lives); returns the result."""
+    import torch.distributed as dist
+    return _allreduce(t, dist.ReduceOp.MAX, group)
+
+
+def allreduce_sum(t, group=None):
+    """Element-wise sum over the ranks of `group`; returns the result."""
+    import torch.distributed as dist
+    return _allreduce(t, dist.ReduceOp.SUM, group)
