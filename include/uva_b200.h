@@ -67,7 +67,9 @@ typedef struct uva_island_status {
     int64_t t_begin;       /* %globaltimer (ns) when the island's team took it */
     int64_t t_end;         /* %globaltimer (ns) when the team finished it    */
     int32_t sm;            /* SM that ran the island                        */
-    int32_t team;          /* team width that ran it (1024, 256 or 32)      */
+    int32_t team;          /* team width that ran it (1024, 256 or 32; the
+                              whole GPU, 148 * 1024, for islands above 16,384
+                              vertices)                                     */
 } uva_island_status;
 
 /* --------------------------------------------------------------------------
@@ -200,7 +202,9 @@ typedef struct uva_batch {
                                  the inverse scale (FP32)                      */
     float*  coarse_l;         /* 4*cofs[nc] floats: the same for LSCM          */
     double* coarse_work;      /* 4*cofs[nc]: FP64 workspace of the setup        */
-    float*  cpart;            /* 2*nslices floats of solve scratch (reserved)   */
+    float*  cpart;            /* 2*nslices floats of solve scratch: the whole-GPU
+                                 team of islands above 16,384 vertices keeps its
+                                 barrier, sums and coarse vectors here         */
     int32_t class_ofs[5];     /* host values: class c owns order[ofs[c]..ofs[c+1]) */
     /* geometry, written by uva_batch_setup */
     const double*  P;         /* n*3 positions (FP64)                          */

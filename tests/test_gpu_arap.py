@@ -170,6 +170,51 @@ def test_large_island_global_memory_class_vs_oracle(cuda):
     assert O.uv_rel_error(np.concatenate(b.chart_uvs()), ref.U, off) < UV_TOL
 
 
+def test_wide_class_islands_vs_oracle(cuda):
+    """Islands above 16,384 vertices are solved by the whole GPU as one team
+    (k_wide, before the persistent launch): two of them, an island of the
+    single-CTA global-memory class and small ones. LSCM and 4 ARAP
+    iterations against the FP64 oracle; the status names the team; the
+    same steps captured in a CUDA graph (the cooperative launch as a graph
+    node) give the same UVs to the tolerance (the team's cross-CTA sums are
+    atomic, so not bit for bit)."""
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.engine import gpu
+    rng = np.random.default_rng(12)
+    isl = [synth.disk_patch(rng, 90000, amp=0.3), synth.disk_patch(rng, 300), synth.disk_patch(rng, 50000, amp=0.4),
+           synth.disk_patch(rng, 24000), synth.disk_patch(rng, 3000), synth.disk_patch(rng, 40)]
+    nv = np.array([len(p) for p, _ in isl])
+    wide = nv > 16384
+    assert wide.sum() == 2 and ((nv > 8192) & ~wide).sum() == 1
+    b = gpu.Batch([(p, t, None) for p, t in isl])
+    b.lscm()
+    st = b.status()
+    assert (st["team"][wide] == 148 * 1024).all() and (st["team"][~wide] <= 1024).all()
+    items = [(p.astype(np.float64), t, O.lscm(p.astype(np.float64), t)) for p, t in isl]
+    off = _offsets(items)
+    assert O.uv_rel_error(np.concatenate(b.chart_uvs()), np.concatenate([u for _, _, u in items]), off) < UV_TOL
+    ref = O.BatchRef(items)
+    b.U = torch.from_numpy(ref.U)
+    b.arap(4, line_search=True)
+    ref.arap(4, line_search=True)
+    st = b.status()
+    assert (st["resid"] <= 2e-7 * 1.001).all() and (st["flags"] & 3 == 0).all()
+    assert (st["team"][wide] == 148 * 1024).all()
+    assert O.uv_rel_error(np.concatenate(b.chart_uvs()), ref.U, off) < UV_TOL
+    db = b.db
+    db.setup(); db.lscm(); db.arap(iters=4)
+    torch.cuda.synchronize()
+    direct = db.uvs()
+    g = db.step_graph(setup=True, lscm=True, arap_iters=4)
+    db.U.zero_()
+    g.launch()
+    torch.cuda.synchronize()
+    g.close()
+    st = db.island_status()
+    assert (st["resid"] <= 2e-7 * 1.001).all() and (st["team"][wide] == 148 * 1024).all()
+    assert O.uv_rel_error(db.uvs(), direct, off) < UV_TOL
+
+
 def test_batch_edge_cases(cuda):
     """Empty batch; one-triangle and degenerate charts; a chart with
     non-finite UVs keeps them while its neighbours solve normally

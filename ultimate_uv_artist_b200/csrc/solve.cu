@@ -205,6 +205,69 @@ constexpr size_t kDynSmem = sizeof(float2) * 3 * KB * RB;   // 196,608 bytes
 
 enum Op { OP_ARAP = 0, OP_LSCM = 1 };
 
+// Class W: islands above kWideMin vertices are solved by the whole GPU as
+// one team (k_wide: a cooperative launch of kWideCtas 1024-thread CTAs, one
+// per SM), one island after another, before the persistent launch takes the
+// other islands. A single CTA would keep them for hundreds of milliseconds
+// while the rest of the batch is done in tens. The team syncs with a grid
+// barrier and reduces across CTAs with atomics into rotating accumulators;
+// the coarse level's g and y live in global memory. Everything it needs
+// sits in the batch's cpart scratch.
+constexpr int kWideMin = 16384;
+constexpr int kWideCtas = 148;
+constexpr int kWideNTT = KB * kWideCtas;
+constexpr int kRedMaxW = 10;   // values per reduction (the solver's kRedMax)
+
+struct WideScratch {
+    unsigned count, gen;                // grid barrier
+    int abort, reserved;                // a barrier gave up: later barriers pass at once
+    double acc[3][kRedMaxW];            // sums, three in rotation
+    unsigned long long mn[3];           // minima of non-negative doubles (as ordered keys)
+    int orv[3];                         // ors
+    int pad[5];
+};
+constexpr int kWideHdr = 320;           // bytes before the coarse g (16-byte aligned)
+static_assert(sizeof(WideScratch) <= kWideHdr, "WideScratch grew past its header");
+
+__device__ __forceinline__ unsigned wide_ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long wide_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid barrier of the class-W team (all kWideCtas CTAs resident: a
+// cooperative launch). A CTA that waits more than two seconds sets `abort`;
+// from then on every barrier passes at once and the island's status says so.
+__device__ __noinline__ void wide_sync(WideScratch* ws) {
+    __syncthreads();
+    if (threadIdx.x == 0 && !*reinterpret_cast<volatile int*>(&ws->abort)) {
+        const unsigned g = wide_ld_acquire(&ws->gen);
+        __threadfence();
+        if (atomicAdd(&ws->count, 1u) == static_cast<unsigned>(kWideCtas) - 1u) {
+            atomicExch(&ws->count, 0u);
+            __threadfence();
+            atomicAdd(&ws->gen, 1u);
+        } else {
+            const unsigned long long t0 = wide_ns();
+            unsigned spins = 0;
+            while (wide_ld_acquire(&ws->gen) == g) {
+                if ((++spins & 255u) == 0 && wide_ns() - t0 > 2000000000ull) {
+                    atomicExch(&ws->abort, 1);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
 template <int NTT>
 __device__ __forceinline__ void team_sync(int bar) {
     if constexpr (NTT == 32) {
@@ -229,8 +292,29 @@ struct Team {
     int sc_cap;             // its capacity (slices + 1)
     __nv_bfloat16* dc;      // Jacobi diagonal of the current island (shared memory, or null)
     int dc_cap;             // its capacity (rows)
-    __device__ __forceinline__ void sync() { team_sync<NTT>(bar); }
+    WideScratch* ws;        // class W only: barrier and cross-CTA accumulators
+    int wph;                // class W only: accumulator in use (0..2, the same on every thread)
+    __device__ __forceinline__ void sync() {
+        if constexpr (NTT == kWideNTT) wide_sync(ws);
+        else team_sync<NTT>(bar);
+    }
 };
+
+// Class W: the accumulators of reduction `ph` are read after its barrier;
+// CTA 0 clears the next ones before it (their last readers passed a barrier
+// since).
+template <int NTT>
+__device__ __forceinline__ int wide_phase(Team<NTT>& tm) {
+    const int ph = tm.wph;
+    tm.wph = ph == 2 ? 0 : ph + 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int nx = tm.wph;
+        for (int k = 0; k < kRedMaxW; ++k) tm.ws->acc[nx][k] = 0.0;
+        tm.ws->mn[nx] = 0ull;
+        tm.ws->orv[nx] = 0;
+    }
+    return ph;
+}
 
 // All-reduce of K values over the team; every thread gets bitwise-identical
 // totals (xor butterflies are symmetric; the cross-warp sum runs in one order).
@@ -244,7 +328,35 @@ __device__ __forceinline__ void team_sum(Team<NTT>& tm, T (&v)[K], T* red) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
     }
-    if constexpr (NTT > 32) {
+    if constexpr (NTT == kWideNTT) {
+        // CTA partials (fixed order) added to the team's accumulator by atomics
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        T* buf = red + tm.phase * K * 32;
+        tm.phase ^= 1;
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) buf[k * 32 + warp] = v[k];
+        }
+        __syncthreads();
+        const int ph = wide_phase(tm);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                double c = 0.0;
+                for (int w = 0; w < 32; ++w) c += static_cast<double>(buf[k * 32 + w]);
+                atomicAdd(&tm.ws->acc[ph][k], c);
+            }
+        }
+        wide_sync(tm.ws);
+        // one read per CTA: after an abandoned barrier the CTA still agrees
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) buf[k * 32] = static_cast<T>(__ldcg(&tm.ws->acc[ph][k]));
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = buf[k * 32];
+    } else if constexpr (NTT > 32) {
         constexpr int NW = NTT / 32;
         const int lane = tm.tid & 31, warp = tm.tid >> 5;
         T* buf = red + tm.phase * K * NW;
@@ -271,7 +383,27 @@ template <int NTT>
 __device__ __forceinline__ double team_min(Team<NTT>& tm, double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if constexpr (NTT > 32) {
+    if constexpr (NTT == kWideNTT) {
+        // non-negative doubles order like their bit patterns: the minimum is
+        // the largest key 0x7fff...f - bits
+        double* buf = tm.redd + tm.phase * 4 * 32;
+        tm.phase ^= 1;
+        if ((threadIdx.x & 31) == 0) buf[threadIdx.x >> 5] = v;
+        __syncthreads();
+        const int ph = wide_phase(tm);
+        if (threadIdx.x == 0) {
+            double c = buf[0];
+            for (int w = 1; w < 32; ++w) c = fmin(c, buf[w]);
+            const unsigned long long key =
+                0x7fffffffffffffffull - static_cast<unsigned long long>(__double_as_longlong(fmax(c, 0.0)));
+            atomicMax(&tm.ws->mn[ph], key);
+        }
+        wide_sync(tm.ws);
+        if (threadIdx.x == 0)
+            buf[0] = __longlong_as_double(static_cast<long long>(0x7fffffffffffffffull - __ldcg(&tm.ws->mn[ph])));
+        __syncthreads();
+        v = buf[0];
+    } else if constexpr (NTT > 32) {
         constexpr int NW = NTT / 32;
         double* buf = tm.redd + tm.phase * 4 * NW;
         tm.phase ^= 1;
@@ -289,7 +421,13 @@ __device__ __forceinline__ double team_min(Team<NTT>& tm, double v) {
 template <int NTT>
 __device__ __forceinline__ int team_or(Team<NTT>& tm, int v) {
     v = __any_sync(0xffffffffu, v) ? 1 : 0;
-    if constexpr (NTT > 32) {
+    if constexpr (NTT == kWideNTT) {
+        const int c = __syncthreads_or(v);
+        const int ph = wide_phase(tm);
+        if (threadIdx.x == 0 && c) atomicOr(&tm.ws->orv[ph], 1);
+        wide_sync(tm.ws);
+        v = __syncthreads_or(threadIdx.x == 0 && __ldcg(&tm.ws->orv[ph]) != 0);
+    } else if constexpr (NTT > 32) {
         constexpr int NW = NTT / 32;
         int* buf = tm.redi + tm.phase * NW;
         tm.phase ^= 1;
@@ -1333,8 +1471,15 @@ __device__ __forceinline__ unsigned sm_id() {
     return r;
 }
 
+// A class-G island that the class-W team solves: above kWideMin vertices,
+// and its coarse g and y fit the batch's cpart after the team's header.
+__device__ __forceinline__ bool wide_island(const uva_batch& b, const Isl& I) {
+    return I.n > kWideMin && kWideHdr + 4ll * (4ll * I.M + 8) <= 8ll * b.nslices;
+}
+
 template <int NTT, int R, Op OP>
-__device__ __forceinline__ void run_class(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, int cls) {
+__device__ __forceinline__ void run_class(const uva_batch& b, const uva_solve_params& prm, Team<NTT>& tm, int cls,
+                                          bool skip_wide = false) {
     const int lo = b.class_ofs[cls], hi = b.class_ofs[cls + 1];
     if (lo >= hi) return;
     for (;;) {
@@ -1351,6 +1496,7 @@ __device__ __forceinline__ void run_class(const uva_batch& b, const uva_solve_pa
         }
         if (lo + qi >= hi) break;
         Isl I = load_island<OP>(b, b.order[lo + qi]);
+        if (R == 0 && skip_wide && wide_island(b, I)) continue;   // solved by k_wide
         if (R > 0 && I.n > NTT * R) {   // the team's shared-memory vectors hold NTT * R rows
             if (tm.tid == 0) {
                 uva_island_status st{};
@@ -1394,8 +1540,39 @@ __device__ __forceinline__ void run_class(const uva_batch& b, const uva_solve_pa
 // the many small islands are latency bound and long-lived for their size,
 // so starting some of them at once keeps them out of the launch's tail,
 // while the other CTAs start with the largest islands.
+// Class W: every class-G island above kWideMin vertices, one after another,
+// each by the whole grid (gridDim.x == kWideCtas, cooperative launch).
 template <Op OP>
-__global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params prm, int nrev) {
+__global__ void __launch_bounds__(KB, 1) k_wide(uva_batch b, uva_solve_params prm) {
+    __shared__ double redd[2 * kRedMax * 32];
+    __shared__ float redf[2 * kRedMax * 32];
+    __shared__ int redi[2 * 32];
+    WideScratch* ws = reinterpret_cast<WideScratch*>(b.cpart);
+    float* cg = reinterpret_cast<float*>(reinterpret_cast<char*>(b.cpart) + kWideHdr);
+    Team<kWideNTT> tm{static_cast<int>(blockIdx.x * KB + threadIdx.x), 0, 0, redd, redf, redi, nullptr,
+                      nullptr, nullptr, nullptr, cg, nullptr, nullptr, 0, nullptr, 0, ws, 0};
+    const int lo = b.class_ofs[0], hi = b.class_ofs[1];
+    for (int q = lo; q < hi; ++q) {
+        const Isl I = load_island<OP>(b, b.order[q]);
+        if (!wide_island(b, I)) continue;
+        tm.cy = cg + 2 * I.M + 4;
+        const long long t0 = global_ns();
+        if (OP == OP_ARAP) solve_arap<kWideNTT, 0>(b, prm, tm, I);
+        else solve_lscm<kWideNTT, 0>(b, prm, tm, I);
+        tm.sync();   // the status below comes after every thread's part
+        if (tm.tid == 0) {
+            uva_island_status& st = b.status[I.id];
+            st.t_begin = t0;
+            st.t_end = global_ns();
+            st.sm = static_cast<int32_t>(sm_id());
+            st.team = kWideNTT;
+            if (*reinterpret_cast<volatile int*>(&ws->abort)) st.flags |= UVA_ST_NONFINITE | UVA_ST_MAXITER;
+        }
+    }
+}
+
+template <Op OP>
+__global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params prm, int nrev, int wide) {
     extern __shared__ __align__(16) float2 dyn[];   // 16-byte aligned: refine_solve stages FP64 pairs here
     __shared__ double redd[2 * kRedMax * 32];
     __shared__ float redf[2 * kRedMax * 32];
@@ -1408,7 +1585,7 @@ __global__ void __launch_bounds__(KB, 1) k_islands(uva_batch b, uva_solve_params
     auto whole_cta = [&]() {
         Team<KB> tm{static_cast<int>(threadIdx.x), 0, 0, redd, redf, redi, &slots[0], nullptr, nullptr, nullptr,
                     coarse_buf, coarse_buf + 512, sc_buf, 288, dinv_buf, KB * RB};
-        run_class<KB, 0, OP>(b, prm, tm, 0);
+        run_class<KB, 0, OP>(b, prm, tm, 0, wide != 0);
         tm.sp = dyn; tm.sd = dyn + KB * RB; tm.sr = dyn + 2 * KB * RB;   // sp, sd adjacent (see refine_solve)
         run_class<KB, RB, OP>(b, prm, tm, 1);
     };
@@ -1760,7 +1937,27 @@ int launch_islands(const uva_batch* b, const uva_solve_params* prm, cudaStream_t
     const int nwarp = b->class_ofs[4] - b->class_ofs[3];
     int nrev = big > 0 ? std::min(grid / 4, (nwarp + 127) / 128) : 0;
     if (prm->rev_ctas != 0) nrev = std::max(0, std::min(grid, prm->rev_ctas));
-    k_islands<OP><<<grid, KB, kDynSmem, s>>>(*b, *prm, nrev);
+    // class W first, on the whole GPU (cooperative: every CTA resident)
+    int wide = 0;
+    if (b->class_ofs[1] > b->class_ofs[0] && b->cpart && sm_count() >= kWideCtas &&
+        8ll * b->nslices > kWideHdr + 4ll * (4 * (kWideMin / 128) + 8)) {
+        e = cudaMemsetAsync(b->cpart, 0, kWideHdr, s);
+        if (e != cudaSuccess) return uva_cuda_status(e, "uva_islands/memset");
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(kWideCtas);
+        cfg.blockDim = dim3(KB);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, k_wide<OP>, *b, *prm);
+        if (e != cudaSuccess) return uva_cuda_status(e, "uva_islands/k_wide");
+        wide = 1;
+    }
+    k_islands<OP><<<grid, KB, kDynSmem, s>>>(*b, *prm, nrev, wide);
     UVA_CHECK_LAUNCH(OP == OP_ARAP ? "uva_arap" : "uva_lscm");
     return UVA_OK;
 }
