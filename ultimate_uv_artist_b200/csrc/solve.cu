@@ -294,6 +294,7 @@ struct Team {
     int dc_cap;             // its capacity (rows)
     WideScratch* ws;        // class W only: barrier and cross-CTA accumulators
     int wph;                // class W only: accumulator in use (0..2, the same on every thread)
+    int gsel;               // class W only: coarse g buffer in use (0, 1)
     __device__ __forceinline__ void sync() {
         if constexpr (NTT == kWideNTT) wide_sync(ws);
         else team_sync<NTT>(bar);
@@ -693,8 +694,19 @@ __host__ __device__ constexpr int coarse_stride(int N, int vec) { return (N + ve
 // call). The restriction g = P^T r is deterministic: T threads per aggregate
 // (a power of two, T * M <= NTT where possible) add rows a*agg + t, + T, ...
 // and fold with xor shuffles in a fixed order. Ends with a barrier: y complete.
+// Class W layout after the team's header in cpart: two coarse g buffers
+// (alternating: one fills while the other is cleared) and y.
+__device__ __forceinline__ int wide_gstride(int M) { return (2 * M + 4 + 3) & ~3; }
+
+template <Op OP>
+__device__ void coarse_solve_wide(const uva_batch& b, Team<kWideNTT>& tm, const Isl& I, const float2* r);
+
 template <int NTT, Op OP>
 __device__ __forceinline__ void coarse_solve(const uva_batch& b, Team<NTT>& tm, const Isl& I, const float2* r) {
+    if constexpr (NTT == kWideNTT) {
+        coarse_solve_wide<OP>(b, tm, I, r);
+        return;
+    }
     int lt = 5;   // log2 T
     while (lt > 0 && (I.M << lt) > NTT) --lt;
     const int T = 1 << lt, groups = NTT >> lt;
@@ -776,6 +788,79 @@ __device__ __forceinline__ float2 prolong(const Team<NTT>& tm, const Isl& I, int
     const int a = agg_of(I, i);
     if (OP == OP_ARAP) return make_float2(tm.cy[a], tm.cy[I.M + a]);
     return make_float2(tm.cy[2 * a], tm.cy[2 * a + 1]);
+}
+
+// Class W coarse correction with one grid barrier: every warp adds the
+// residual of its 32 rows (one aggregate: agg is a multiple of 32) to g by
+// atomics, which needs only the thread's own rows; after the barrier every
+// CTA computes y for the aggregates of its own rows (an aggregate shared
+// with a neighbouring CTA gets the same value from both) and prolong reads
+// only those. CTA 0 clears the other g buffer for the next call.
+template <Op OP>
+__device__ void coarse_solve_wide(const uva_batch& b, Team<kWideNTT>& tm, const Isl& I, const float2* r) {
+    const int M = I.M, gs = wide_gstride(M);
+    float* g = tm.cg + tm.gsel * gs;
+    slice_loop<kWideNTT, 0>(tm.tid, I.n, [&](int i, int, bool valid) {
+        float2 v = valid ? r[i] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+        }
+        if ((threadIdx.x & 31) == 0 && valid) {
+            const int a = agg_of(I, i);
+            atomicAdd(g + (OP == OP_ARAP ? a : 2 * a), v.x);
+            atomicAdd(g + (OP == OP_ARAP ? M + a : 2 * a + 1), v.y);
+        }
+    });
+    wide_sync(tm.ws);   // g complete
+    if (blockIdx.x == 0) {
+        float* other = tm.cg + (tm.gsel ^ 1) * gs;
+        for (int k = threadIdx.x; k < gs; k += KB) other[k] = 0.f;
+    }
+    tm.gsel ^= 1;
+    constexpr int G = 8;
+    const int S = coarse_stride(M, 2);
+    const float* blockf = OP == OP_ARAP ? b.coarse_a + I.co : b.coarse_l + 4 * static_cast<size_t>(I.co);
+    const __half* A = reinterpret_cast<const __half*>(blockf);
+    const float isc = __ldg(coarse_scale(blockf, (OP == OP_ARAP ? 1 : 2) * M * S));
+    const int gl = threadIdx.x & (G - 1);
+    const int cpl = ((M + G - 1) / G + 1) & ~1;   // entries per lane, even
+    const int c_beg = gl * cpl, c_end = min(c_beg + cpl, M);
+    for (int base = static_cast<int>(blockIdx.x) * KB; base < I.n; base += kWideNTT) {
+        const int a0 = base / I.agg, a1 = min(M - 1, (min(base + KB, I.n) - 1) / I.agg);
+        const int o = a0 + static_cast<int>(threadIdx.x) / G;   // at most KB / 64 + 1 aggregates: one pass
+        float au = 0.f, av = 0.f;
+        if (o <= a1) {
+            for (int c = c_beg; c < c_end; c += 2) {
+                if constexpr (OP == OP_ARAP) {
+                    const unsigned raw = __ldg(reinterpret_cast<const unsigned*>(A + static_cast<size_t>(o) * S + c));
+                    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw));
+                    au = fmaf(a.x, __ldcg(g + c), au); au = fmaf(a.y, __ldcg(g + c + 1), au);
+                    av = fmaf(a.x, __ldcg(g + M + c), av); av = fmaf(a.y, __ldcg(g + M + c + 1), av);
+                } else {
+                    const uint2 raw = __ldg(reinterpret_cast<const uint2*>(A + 2 * (static_cast<size_t>(o) * S + c)));
+                    const float2 z0 = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
+                    const float2 z1 = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
+                    const float4 gg = __ldcg(reinterpret_cast<const float4*>(g + 2 * c));
+                    au = fmaf(z0.x, gg.x, au); au = fmaf(-z0.y, gg.y, au);
+                    av = fmaf(z0.y, gg.x, av); av = fmaf(z0.x, gg.y, av);
+                    au = fmaf(z1.x, gg.z, au); au = fmaf(-z1.y, gg.w, au);
+                    av = fmaf(z1.y, gg.z, av); av = fmaf(z1.x, gg.w, av);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = G / 2; k > 0; k >>= 1) {
+            au += __shfl_xor_sync(0xffffffffu, au, k);
+            av += __shfl_xor_sync(0xffffffffu, av, k);
+        }
+        if (gl == 0 && o <= a1) {
+            if (OP == OP_ARAP) { tm.cy[o] = au * isc; tm.cy[M + o] = av * isc; }
+            else { tm.cy[2 * o] = au * isc; tm.cy[2 * o + 1] = av * isc; }
+        }
+    }
+    __syncthreads();   // y of this CTA's aggregates complete
 }
 
 // The last m updates of the ARAP iterate and their images under A (FP32,
@@ -1059,7 +1144,7 @@ __device__ __forceinline__ int refine_solve(const uva_batch& b, const Isl& I, co
             });
             apend[0] = alpha[0]; apend[1] = alpha[1];
             if (two_level) {
-                tm.sync();   // residual complete
+                if constexpr (NTT != kWideNTT) tm.sync();   // residual complete (class W reads only its own rows)
                 coarse_solve<NTT, OP>(b, tm, I, sr);
             }
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
@@ -1474,7 +1559,8 @@ __device__ __forceinline__ unsigned sm_id() {
 // A class-G island that the class-W team solves: above kWideMin vertices,
 // and its coarse g and y fit the batch's cpart after the team's header.
 __device__ __forceinline__ bool wide_island(const uva_batch& b, const Isl& I) {
-    return I.n > kWideMin && kWideHdr + 4ll * (4ll * I.M + 8) <= 8ll * b.nslices;
+    return I.n > kWideMin && I.agg > 0 && (I.agg & 31) == 0 &&
+           kWideHdr + 4ll * (6ll * I.M + 24) <= 8ll * b.nslices;
 }
 
 template <int NTT, int R, Op OP>
@@ -1550,12 +1636,17 @@ __global__ void __launch_bounds__(KB, 1) k_wide(uva_batch b, uva_solve_params pr
     WideScratch* ws = reinterpret_cast<WideScratch*>(b.cpart);
     float* cg = reinterpret_cast<float*>(reinterpret_cast<char*>(b.cpart) + kWideHdr);
     Team<kWideNTT> tm{static_cast<int>(blockIdx.x * KB + threadIdx.x), 0, 0, redd, redf, redi, nullptr,
-                      nullptr, nullptr, nullptr, cg, nullptr, nullptr, 0, nullptr, 0, ws, 0};
+                      nullptr, nullptr, nullptr, cg, nullptr, nullptr, 0, nullptr, 0, ws, 0, 0};
     const int lo = b.class_ofs[0], hi = b.class_ofs[1];
     for (int q = lo; q < hi; ++q) {
         const Isl I = load_island<OP>(b, b.order[q]);
         if (!wide_island(b, I)) continue;
-        tm.cy = cg + 2 * I.M + 4;
+        const int gs = wide_gstride(I.M);
+        tm.cy = cg + 2 * gs;
+        tm.gsel = 0;
+        if (blockIdx.x == 0)
+            for (int k = threadIdx.x; k < 2 * gs; k += KB) cg[k] = 0.f;   // both g buffers
+        tm.sync();
         const long long t0 = global_ns();
         if (OP == OP_ARAP) solve_arap<kWideNTT, 0>(b, prm, tm, I);
         else solve_lscm<kWideNTT, 0>(b, prm, tm, I);
@@ -1940,7 +2031,7 @@ int launch_islands(const uva_batch* b, const uva_solve_params* prm, cudaStream_t
     // class W first, on the whole GPU (cooperative: every CTA resident)
     int wide = 0;
     if (b->class_ofs[1] > b->class_ofs[0] && b->cpart && sm_count() >= kWideCtas &&
-        8ll * b->nslices > kWideHdr + 4ll * (4 * (kWideMin / 128) + 8)) {
+        8ll * b->nslices > kWideHdr + 4ll * (6 * (kWideMin / 128) + 24)) {
         e = cudaMemsetAsync(b->cpart, 0, kWideHdr, s);
         if (e != cudaSuccess) return uva_cuda_status(e, "uva_islands/memset");
         cudaLaunchConfig_t cfg{};
