@@ -61,6 +61,7 @@ def _args():
     ap.add_argument("--no-config1", action="store_true")
     ap.add_argument("--no-config4", action="store_true")
     ap.add_argument("--no-pack", action="store_true")
+    ap.add_argument("--no-giant", action="store_true")
     ap.add_argument("--pack-charts", type=int, default=3000)
     ap.add_argument("--pack-only", action="store_true",
                     help="only the packing leg, as one JSON line (for launch lists of the packer)")
@@ -627,6 +628,37 @@ def bench_config5(dev, iters=ITERS, steps=2, cpu=True):
             "flipped": int(rep["flipped_triangles"]), "islands": int(rep["islands"])}
 
 
+def bench_giant(dev, iters=ITERS, big_tris=200_000):
+    """The north star's upper island size: the 2,000-island batch plus one
+    disk island of about 200k triangles (solved by the whole-GPU class-W
+    team before the persistent launch). Setup + LSCM and 20 ARAP iterations
+    (CUDA events), the batch's tri-iters/s, and the large island's own
+    launch time, CG iterations and team."""
+    import torch
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.engine import gpu
+    isl = list(synth.uneven_islands(seed=2000, count=2000))
+    isl.append(synth.disk_patch(np.random.default_rng(5), big_tris))
+    b = gpu.Batch([(p, t, None) for p, t in isl], dev=dev)
+    db = b.db
+    stream = torch.cuda.current_stream(dev)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    for _ in range(2):
+        e0.record(stream); db.setup(); db.lscm(); e1.record(stream)
+        db.arap(iters=iters, line_search=True); e2.record(stream)
+        torch.cuda.synchronize()
+    st = db.island_status()
+    tris = int(sum(len(t) for _, t in isl))
+    last = len(isl) - 1
+    lscm_ms, arap_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    return {"workload": f"uneven_islands_2000_plus_one_{len(isl[-1][1])}_tri_island", "triangles": tris,
+            "large_island_vertices": int(len(isl[-1][0])), "lscm_setup_ms": lscm_ms, "arap_ms": arap_ms,
+            "tri_iters_per_s": tris * iters / ((lscm_ms + arap_ms) / 1e3),
+            "large_island_arap_ms": float((st["t_end"][last] - st["t_begin"][last]) / 1e6),
+            "large_island_cg_iters": int(st["cg_iters"][last]), "large_island_team": int(st["team"][last]),
+            "max_resid": float(st["resid"].max())}
+
+
 def bench_pack(dev, nch=3000, cpu=True):
     """engine.pack on synthetic disk charts (log-uniform 100 to 6,000
     triangles, stretched up to 6.7x, random in-plane turns) with the
@@ -954,7 +986,9 @@ def main():
         bnd = bench_boundary(b)
         hier_b = bench_hier(dev)
         ovl = bench_overlap(islands, our_uvs)
-    c5 = c1 = c4 = pk = None
+    c5 = c1 = c4 = pk = gi = None
+    if rank == 0 and not args.no_giant:
+        gi = bench_giant(dev, args.iters)
     if rank == 0 and not args.no_pack:
         pk = bench_pack(dev, args.pack_charts, cpu=not args.no_cpu_baseline)
     if rank == 0 and not args.no_config5:
@@ -1042,6 +1076,7 @@ def main():
             "overlap_checks": ovl,
             "config5": c5,
             "pack": pk,
+            "giant_island": gi,
             "config4_energy": c4,
             "config1": c1,
         }
