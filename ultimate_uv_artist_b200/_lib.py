@@ -172,6 +172,29 @@ def lib():
     return _load()
 
 
+_pyhost = None
+
+
+def pyhost():
+    """The batch constructor's host helper (libuva_pyhost.so, called with the
+    GIL held), or None when it is missing: the constructor then reads the
+    charts in Python."""
+    global _pyhost
+    if _pyhost is None:
+        path = os.path.join(HERE, "libuva_pyhost.so")
+        handle = False
+        if os.path.exists(path):
+            try:
+                h = C.PyDLL(path)
+                h.uva_py_charts.argtypes = [C.py_object, i32] + [vp] * 9
+                h.uva_py_charts.restype = C.c_int64
+                handle = h
+            except OSError:
+                handle = False
+        _pyhost = handle
+    return _pyhost or None
+
+
 def exported_symbols():
     """Names this binding expects the library to export."""
     return sorted(_SIGS)

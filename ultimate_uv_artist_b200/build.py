@@ -19,6 +19,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libuva_b200.so")
+PYHOST_LIB = os.path.join(HERE, "libuva_pyhost.so")   # the batch constructor's charts pass (CPython API)
 BUILD_DIR = os.path.join(ROOT, "_build")
 
 CU_SOURCES = ["capi.cu", "solve.cu", "ops.cu", "chart_ops.cu", "validate.cu", "metrics.cu", "energy.cu", "gutter.cu",
@@ -52,8 +53,37 @@ def _digest(files, flags):
     return h.hexdigest()
 
 
+def build_pyhost(force=False, verbose=False):
+    """csrc/pyhost.cpp into PYHOST_LIB with g++ against this interpreter's
+    headers (skipped when up to date). Returns the path, or None without a
+    C++ compiler or Python headers."""
+    import sysconfig
+    src = os.path.join(CSRC, "pyhost.cpp")
+    inc = sysconfig.get_paths().get("include")
+    gxx = shutil.which("g++")
+    if not (os.path.exists(src) and inc and os.path.exists(os.path.join(inc, "Python.h")) and gxx):
+        return None
+    digest = _digest([src], [inc, sys.version])
+    stamp = PYHOST_LIB + ".sha256"
+    if not force and os.path.exists(PYHOST_LIB) and os.path.exists(stamp):
+        with open(stamp) as fh:
+            if fh.read().strip() == digest:
+                return PYHOST_LIB
+    tmp = PYHOST_LIB + ".tmp"
+    cmd = [gxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-I", inc, src, "-o", tmp]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, PYHOST_LIB)
+    with open(stamp, "w") as fh:
+        fh.write(digest)
+    return PYHOST_LIB
+
+
 def build(force=False, verbose=False):
-    """Compile every CUDA / C++ source into LIB (skipped when up to date)."""
+    """Compile every CUDA / C++ source into LIB (skipped when up to date),
+    and the batch constructor's host helper into PYHOST_LIB."""
+    build_pyhost(force, verbose)
     cu, cxx = _sources()
     deps = [os.path.join(CSRC, s) for s in cu + cxx]
     deps += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]

@@ -337,44 +337,49 @@ class ChartArrays:
     def __init__(self, charts, with_uv=True):
         nc = len(charts)
         self.nc = nc
-        self.Ps, self.Ts, self.Us = [], [], []
-        self.pdt = np.empty(max(nc, 1), np.int8)
-        self.tdt = np.empty(max(nc, 1), np.int8)
-        self.udt = np.full(max(nc, 1), -1, np.int8)
-        nvs, nts = [], []
-        self.any_uv = False
+        n1 = max(nc, 1)
+        self.pdt = np.zeros(n1, np.int8)
+        self.tdt = np.zeros(n1, np.int8)
+        self.udt = np.full(n1, -1, np.int8)
+        self.pp = np.zeros(n1, np.uintp)
+        self.tp = np.zeros(n1, np.uintp)
+        up = np.zeros(n1, np.uintp)
+        nvs = np.zeros(n1, np.int64)
+        nts = np.zeros(n1, np.int64)
+        ok = np.zeros(n1, np.int8)
+        ph = _lib.pyhost() if isinstance(charts, (list, tuple)) else None
+        if ph is not None and nc:
+            # one native pass: pointers, rows and codes of the arrays the host
+            # copies read as they are; the other charts go through Python below
+            ph.uva_py_charts(charts, 1 if with_uv else 0, ptr(self.pp), ptr(self.pdt), ptr(self.tp), ptr(self.tdt),
+                             ptr(up), ptr(self.udt), ptr(nvs), ptr(nts), ptr(ok))
+        self.Ps = [ch[0] for ch in charts]
+        self.Ts = [ch[1] for ch in charts]
+        self.Us = [(ch[2] if with_uv and len(ch) > 2 else None) for ch in charts]
         fc, ic = _FLOAT_CODE, _INT_CODE
-        for i, ch in enumerate(charts):
-            a, t = ch[0], ch[1]
-            # arrays already in a layout the copies read are taken as they are
-            if type(a) is np.ndarray and a.ndim == 2 and a.shape[1] == 3 and a.dtype in fc and a.flags.c_contiguous:
-                self.pdt[i] = fc[a.dtype]
-            else:
-                a, self.pdt[i] = _chart_array(a, 3, fc, np.float64)
-            if type(t) is np.ndarray and t.ndim == 2 and t.shape[1] == 3 and t.dtype in ic and t.flags.c_contiguous:
-                self.tdt[i] = ic[t.dtype]
-            else:
-                t, self.tdt[i] = _chart_array(t, 3, ic, np.int64)
-            self.Ps.append(a)
-            self.Ts.append(t)
-            nvs.append(a.shape[0])
-            nts.append(t.shape[0])
+        for i in np.flatnonzero(ok[:nc] == 0).tolist():
+            ch = charts[i]
+            a, self.pdt[i] = _chart_array(ch[0], 3, fc, np.float64)
+            t, self.tdt[i] = _chart_array(ch[1], 3, ic, np.int64)
+            self.Ps[i], self.Ts[i] = a, t
+            nvs[i], nts[i] = a.shape[0], t.shape[0]
+            self.pp[i], self.tp[i] = a.ctypes.data, t.ctypes.data
             u = None
+            self.udt[i] = -1
+            up[i] = 0
             if with_uv and len(ch) > 2 and ch[2] is not None:
                 u, self.udt[i] = _chart_array(ch[2], 2, fc, np.float64)
                 if len(u) != len(a):
                     raise ValueError(f"chart {i}: U has {len(u)} rows for {len(a)} vertices")
-                self.any_uv = True
-            self.Us.append(u)
+                up[i] = u.ctypes.data
+            self.Us[i] = u
+        self.up = up
+        self.any_uv = bool(nc and (self.udt[:nc] >= 0).any())
         self.vofs = np.zeros(nc + 1, np.int64)
         self.tofs = np.zeros(nc + 1, np.int64)
         if nc:
-            np.cumsum(nvs, out=self.vofs[1:])
-            np.cumsum(nts, out=self.tofs[1:])
-        self.tp = np.fromiter((x.__array_interface__["data"][0] for x in self.Ts), np.uintp, nc) if nc else \
-            np.zeros(1, np.uintp)
-        self.pp = np.fromiter((x.__array_interface__["data"][0] for x in self.Ps), np.uintp, nc) if nc else \
-            np.zeros(1, np.uintp)
+            np.cumsum(nvs[:nc], out=self.vofs[1:])
+            np.cumsum(nts[:nc], out=self.tofs[1:])
 
     @property
     def chart_tris(self):
@@ -395,7 +400,7 @@ class ChartArrays:
             return P, None
         P = host_empty((n, 3), np.float64)
         if nc:
-            up_ = np.fromiter((0 if x is None else x.ctypes.data for x in self.Us), np.uintp, nc) if self.any_uv else None
+            up_ = self.up if self.any_uv else None
             check(L.uva_concat_charts(nc, ptr(self.pp), ptr(self.pdt), ptr(self.tp), ptr(self.tdt),
                                       ptr(up_) if self.any_uv else None, ptr(self.udt) if self.any_uv else None,
                                       ptr(self.vofs), ptr(self.tofs), ptr(P), None, ptr(U) if U is not None else None,
