@@ -295,3 +295,29 @@ def test_oracle_chart_quality_against_reference(golden):
     assert abs(q["stretch"] - float(golden["p_q_stretch"])) <= 1e-12 * abs(float(golden["p_q_stretch"]))
     assert np.allclose(q["per_tri_aniso"], golden["p_q_aniso"], rtol=1e-12)
     assert np.allclose(q["per_tri_area"], golden["p_q_area"], rtol=1e-12)
+
+
+def test_chart_arrays_native_pass_matches_python_path(monkeypatch):
+    """The native charts pass (libuva_pyhost.so) and the Python path give
+    the same codes, offsets and concatenated arrays, for charts the host
+    copies read as they are and for charts that need a conversion."""
+    from ultimate_uv_artist_b200 import _lib
+    from ultimate_uv_artist_b200.device import ChartArrays
+    assert _lib.pyhost() is not None
+    rng = np.random.default_rng(3)
+    charts = [(rng.random((5, 3)).astype(np.float32), np.array([[0, 1, 2], [2, 3, 4]], np.int32), None),
+              (rng.random((4, 3)), np.array([[0, 1, 2]], np.uint32), rng.random((4, 2)).astype(np.float32)),
+              (rng.random(9).tolist(), [[0, 1, 2]], None),
+              (np.asfortranarray(rng.random((3, 3))), np.array([[0, 1, 2]]), rng.random((3, 2)).astype(np.float16)),
+              (rng.random((6, 3)), np.array([[0, 1, 2], [3, 4, 5]], np.int64), rng.random((6, 2)))]
+    fast = ChartArrays(charts)
+    Pf, Uf = fast.points()
+    monkeypatch.setattr(_lib, "_pyhost", False)
+    slow = ChartArrays(charts)
+    Ps, Us = slow.points()
+    for k in ("pdt", "tdt", "udt", "vofs", "tofs"):
+        assert np.array_equal(getattr(fast, k), getattr(slow, k)), k
+    assert fast.any_uv == slow.any_uv
+    assert np.array_equal(Pf, Ps) and np.array_equal(Uf, Us)
+    with pytest.raises(ValueError):
+        ChartArrays([(np.zeros((4, 3)), np.zeros((1, 3), np.int64), np.zeros((3, 2)))])
