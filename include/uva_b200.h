@@ -204,7 +204,8 @@ typedef struct uva_batch {
     double* coarse_work;      /* 4*cofs[nc]: FP64 workspace of the setup        */
     float*  cpart;            /* 2*nslices floats of solve scratch: the whole-GPU
                                  team of islands above 16,384 vertices keeps its
-                                 barrier, sums and coarse vectors here         */
+                                 grid barrier here (and its reduction slots in
+                                 coarse_work, free after the setup)           */
     int32_t class_ofs[5];     /* host values: class c owns order[ofs[c]..ofs[c+1]) */
     /* geometry, written by uva_batch_setup */
     const double*  P;         /* n*3 positions (FP64)                          */

@@ -210,24 +210,24 @@ enum Op { OP_ARAP = 0, OP_LSCM = 1 };
 // per SM), one island after another, before the persistent launch takes the
 // other islands. A single CTA would keep them for hundreds of milliseconds
 // while the rest of the batch is done in tens. The team syncs with a grid
-// barrier and reduces across CTAs with atomics into rotating accumulators;
-// the coarse level's g and y live in global memory. Everything it needs
-// sits in the batch's cpart scratch.
+// barrier (in the batch's cpart) and reduces across CTAs through per-CTA
+// slots that every CTA adds up in the same order (in the batch's
+// coarse_work), so its results are as reproducible as a single CTA's.
 constexpr int kWideMin = 16384;
 constexpr int kWideCtas = 148;
 constexpr int kWideNTT = KB * kWideCtas;
 constexpr int kRedMaxW = 10;   // values per reduction (the solver's kRedMax)
 
-struct WideScratch {
+struct WideScratch {                    // at the start of the batch's cpart
     unsigned count, gen;                // grid barrier
     int abort, reserved;                // a barrier gave up: later barriers pass at once
-    double acc[3][kRedMaxW];            // sums, three in rotation
-    unsigned long long mn[3];           // minima of non-negative doubles (as ordered keys)
-    int orv[3];                         // ors
-    int pad[5];
 };
-constexpr int kWideHdr = 320;           // bytes before the coarse g (16-byte aligned)
-static_assert(sizeof(WideScratch) <= kWideHdr, "WideScratch grew past its header");
+constexpr int kWideHdr = 16;
+// In the batch's coarse_work (the setup's FP64 workspace, free during the
+// solves): per-CTA partials of the team's reductions, two sets in turn
+// (kWideCtas x kRedMaxW doubles each), then the per-warp residual sums of
+// the coarse restriction (one float2 per 32 rows).
+constexpr int kWidePart = 2 * kWideCtas * kRedMaxW;
 
 __device__ __forceinline__ unsigned wide_ld_acquire(const unsigned* p) {
     unsigned v;
@@ -292,29 +292,24 @@ struct Team {
     int sc_cap;             // its capacity (slices + 1)
     __nv_bfloat16* dc;      // Jacobi diagonal of the current island (shared memory, or null)
     int dc_cap;             // its capacity (rows)
-    WideScratch* ws;        // class W only: barrier and cross-CTA accumulators
-    int wph;                // class W only: accumulator in use (0..2, the same on every thread)
-    int gsel;               // class W only: coarse g buffer in use (0, 1)
+    WideScratch* ws;        // class W only: grid barrier
+    int wph;                // class W only: partial set in use (0, 1; the same on every thread)
+    double* wpart;          // class W only: 2 x kWideCtas x kRedMaxW partials
+    float2* wgw;            // class W only: per-warp residual sums of the coarse restriction
     __device__ __forceinline__ void sync() {
         if constexpr (NTT == kWideNTT) wide_sync(ws);
         else team_sync<NTT>(bar);
     }
 };
 
-// Class W: the accumulators of reduction `ph` are read after its barrier;
-// CTA 0 clears the next ones before it (their last readers passed a barrier
-// since).
+// Class W: reduction partials alternate between two sets; a set is written
+// again two reductions later, after every CTA has read it and passed a
+// barrier since.
 template <int NTT>
-__device__ __forceinline__ int wide_phase(Team<NTT>& tm) {
-    const int ph = tm.wph;
-    tm.wph = ph == 2 ? 0 : ph + 1;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const int nx = tm.wph;
-        for (int k = 0; k < kRedMaxW; ++k) tm.ws->acc[nx][k] = 0.0;
-        tm.ws->mn[nx] = 0ull;
-        tm.ws->orv[nx] = 0;
-    }
-    return ph;
+__device__ __forceinline__ double* wide_slots(Team<NTT>& tm) {
+    double* p = tm.wpart + tm.wph * (kWideCtas * kRedMaxW);
+    tm.wph ^= 1;
+    return p;
 }
 
 // All-reduce of K values over the team; every thread gets bitwise-identical
@@ -330,7 +325,9 @@ __device__ __forceinline__ void team_sum(Team<NTT>& tm, T (&v)[K], T* red) {
         for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
     }
     if constexpr (NTT == kWideNTT) {
-        // CTA partials (fixed order) added to the team's accumulator by atomics
+        // CTA partial (warps in a fixed order) into this CTA's slot; after
+        // the barrier every CTA's warp 0 adds the slots in the same order,
+        // so every thread of the team gets the same bits
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         T* buf = red + tm.phase * K * 32;
         tm.phase ^= 1;
@@ -339,20 +336,30 @@ __device__ __forceinline__ void team_sum(Team<NTT>& tm, T (&v)[K], T* red) {
             for (int k = 0; k < K; ++k) buf[k * 32 + warp] = v[k];
         }
         __syncthreads();
-        const int ph = wide_phase(tm);
+        double* slots = wide_slots(tm);
         if (threadIdx.x == 0) {
 #pragma unroll
             for (int k = 0; k < K; ++k) {
                 double c = 0.0;
                 for (int w = 0; w < 32; ++w) c += static_cast<double>(buf[k * 32 + w]);
-                atomicAdd(&tm.ws->acc[ph][k], c);
+                slots[blockIdx.x * kRedMaxW + k] = c;
             }
         }
         wide_sync(tm.ws);
-        // one read per CTA: after an abandoned barrier the CTA still agrees
-        if (threadIdx.x == 0) {
+        if (warp < K) {   // warp k adds value k: every load of a lane in flight at once
+            constexpr int J = (kWideCtas + 31) / 32;
+            double part[J];
 #pragma unroll
-            for (int k = 0; k < K; ++k) buf[k * 32] = static_cast<T>(__ldcg(&tm.ws->acc[ph][k]));
+            for (int j = 0; j < J; ++j) {
+                const int q = lane + 32 * j;
+                part[j] = q < kWideCtas ? __ldcg(slots + q * kRedMaxW + warp) : 0.0;
+            }
+            double c = 0.0;
+#pragma unroll
+            for (int j = 0; j < J; ++j) c += part[j];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+            if (lane == 0) buf[warp * 32] = static_cast<T>(c);
         }
         __syncthreads();
 #pragma unroll
@@ -385,23 +392,25 @@ __device__ __forceinline__ double team_min(Team<NTT>& tm, double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
     if constexpr (NTT == kWideNTT) {
-        // non-negative doubles order like their bit patterns: the minimum is
-        // the largest key 0x7fff...f - bits
         double* buf = tm.redd + tm.phase * 4 * 32;
         tm.phase ^= 1;
         if ((threadIdx.x & 31) == 0) buf[threadIdx.x >> 5] = v;
         __syncthreads();
-        const int ph = wide_phase(tm);
+        double* slots = wide_slots(tm);
         if (threadIdx.x == 0) {
             double c = buf[0];
             for (int w = 1; w < 32; ++w) c = fmin(c, buf[w]);
-            const unsigned long long key =
-                0x7fffffffffffffffull - static_cast<unsigned long long>(__double_as_longlong(fmax(c, 0.0)));
-            atomicMax(&tm.ws->mn[ph], key);
+            slots[blockIdx.x * kRedMaxW] = c;
         }
         wide_sync(tm.ws);
-        if (threadIdx.x == 0)
-            buf[0] = __longlong_as_double(static_cast<long long>(0x7fffffffffffffffull - __ldcg(&tm.ws->mn[ph])));
+        if (threadIdx.x < 32) {
+            double c = 1e300;
+#pragma unroll
+            for (int q = threadIdx.x; q < kWideCtas; q += 32) c = fmin(c, __ldcg(slots + q * kRedMaxW));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) c = fmin(c, __shfl_xor_sync(0xffffffffu, c, o));
+            if (threadIdx.x == 0) buf[0] = c;
+        }
         __syncthreads();
         v = buf[0];
     } else if constexpr (NTT > 32) {
@@ -424,10 +433,14 @@ __device__ __forceinline__ int team_or(Team<NTT>& tm, int v) {
     v = __any_sync(0xffffffffu, v) ? 1 : 0;
     if constexpr (NTT == kWideNTT) {
         const int c = __syncthreads_or(v);
-        const int ph = wide_phase(tm);
-        if (threadIdx.x == 0 && c) atomicOr(&tm.ws->orv[ph], 1);
+        double* slots = wide_slots(tm);
+        if (threadIdx.x == 0) slots[blockIdx.x * kRedMaxW] = c ? 1.0 : 0.0;
         wide_sync(tm.ws);
-        v = __syncthreads_or(threadIdx.x == 0 && __ldcg(&tm.ws->orv[ph]) != 0);
+        int any = 0;
+        if (threadIdx.x < 32) {
+            for (int q = threadIdx.x; q < kWideCtas; q += 32) any |= __ldcg(slots + q * kRedMaxW) != 0.0;
+        }
+        v = __syncthreads_or(any);
     } else if constexpr (NTT > 32) {
         constexpr int NW = NTT / 32;
         int* buf = tm.redi + tm.phase * NW;
@@ -694,10 +707,6 @@ __host__ __device__ constexpr int coarse_stride(int N, int vec) { return (N + ve
 // call). The restriction g = P^T r is deterministic: T threads per aggregate
 // (a power of two, T * M <= NTT where possible) add rows a*agg + t, + T, ...
 // and fold with xor shuffles in a fixed order. Ends with a barrier: y complete.
-// Class W layout after the team's header in cpart: two coarse g buffers
-// (alternating: one fills while the other is cleared) and y.
-__device__ __forceinline__ int wide_gstride(int M) { return (2 * M + 4 + 3) & ~3; }
-
 template <Op OP>
 __device__ void coarse_solve_wide(const uva_batch& b, Team<kWideNTT>& tm, const Isl& I, const float2* r);
 
@@ -790,16 +799,14 @@ __device__ __forceinline__ float2 prolong(const Team<NTT>& tm, const Isl& I, int
     return make_float2(tm.cy[2 * a], tm.cy[2 * a + 1]);
 }
 
-// Class W coarse correction with one grid barrier: every warp adds the
-// residual of its 32 rows (one aggregate: agg is a multiple of 32) to g by
-// atomics, which needs only the thread's own rows; after the barrier every
-// CTA computes y for the aggregates of its own rows (an aggregate shared
-// with a neighbouring CTA gets the same value from both) and prolong reads
-// only those. CTA 0 clears the other g buffer for the next call.
+// Class W coarse correction with one grid barrier: every warp stores the
+// residual sum of its 32 rows (one aggregate: agg is a multiple of 32);
+// after the barrier every CTA rebuilds g from those sums in a fixed order
+// (the same bits in every CTA) in its shared memory and computes y for the
+// aggregates of its own rows, the only ones prolong reads.
 template <Op OP>
 __device__ void coarse_solve_wide(const uva_batch& b, Team<kWideNTT>& tm, const Isl& I, const float2* r) {
-    const int M = I.M, gs = wide_gstride(M);
-    float* g = tm.cg + tm.gsel * gs;
+    const int M = I.M;
     slice_loop<kWideNTT, 0>(tm.tid, I.n, [&](int i, int, bool valid) {
         float2 v = valid ? r[i] : make_float2(0.f, 0.f);
 #pragma unroll
@@ -807,18 +814,33 @@ __device__ void coarse_solve_wide(const uva_batch& b, Team<kWideNTT>& tm, const 
             v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
             v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
         }
-        if ((threadIdx.x & 31) == 0 && valid) {
-            const int a = agg_of(I, i);
-            atomicAdd(g + (OP == OP_ARAP ? a : 2 * a), v.x);
-            atomicAdd(g + (OP == OP_ARAP ? M + a : 2 * a + 1), v.y);
-        }
+        if ((threadIdx.x & 31) == 0 && valid) tm.wgw[i >> 5] = v;
     });
-    wide_sync(tm.ws);   // g complete
-    if (blockIdx.x == 0) {
-        float* other = tm.cg + (tm.gsel ^ 1) * gs;
-        for (int k = threadIdx.x; k < gs; k += KB) other[k] = 0.f;
+    wide_sync(tm.ws);   // warp sums complete
+    float* g = tm.cg;   // shared memory of this CTA
+    const int wpa = I.agg >> 5, nw = (I.n + 31) >> 5;
+    {   // four threads per aggregate (M <= 256), each a quarter of its warp
+        // sums (loads in flight together), folded in a fixed order
+        const int a = threadIdx.x >> 2, part = threadIdx.x & 3;
+        float gx = 0.f, gy = 0.f;
+        if (a < M) {
+            const int w0 = a * wpa, w1 = min(w0 + wpa, nw);
+            for (int w = w0 + part; w < w1; w += 4) {
+                const float2 v = __ldcg(tm.wgw + w);
+                gx += v.x; gy += v.y;
+            }
+        }
+        gx += __shfl_xor_sync(0xffffffffu, gx, 1); gy += __shfl_xor_sync(0xffffffffu, gy, 1);
+        gx += __shfl_xor_sync(0xffffffffu, gx, 2); gy += __shfl_xor_sync(0xffffffffu, gy, 2);
+        if (part == 0 && a < M) {
+            if (OP == OP_ARAP) { g[a] = gx; g[M + a] = gy; }
+            else { g[2 * a] = gx; g[2 * a + 1] = gy; }
+        }
     }
-    tm.gsel ^= 1;
+    // the products' last pair may read one entry past the end (against a
+    // zero matrix entry): it must hold a finite value
+    if (threadIdx.x < 4) g[2 * M + threadIdx.x] = 0.f;
+    __syncthreads();
     constexpr int G = 8;
     const int S = coarse_stride(M, 2);
     const float* blockf = OP == OP_ARAP ? b.coarse_a + I.co : b.coarse_l + 4 * static_cast<size_t>(I.co);
@@ -836,13 +858,13 @@ __device__ void coarse_solve_wide(const uva_batch& b, Team<kWideNTT>& tm, const 
                 if constexpr (OP == OP_ARAP) {
                     const unsigned raw = __ldg(reinterpret_cast<const unsigned*>(A + static_cast<size_t>(o) * S + c));
                     const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw));
-                    au = fmaf(a.x, __ldcg(g + c), au); au = fmaf(a.y, __ldcg(g + c + 1), au);
-                    av = fmaf(a.x, __ldcg(g + M + c), av); av = fmaf(a.y, __ldcg(g + M + c + 1), av);
+                    au = fmaf(a.x, g[c], au); au = fmaf(a.y, g[c + 1], au);
+                    av = fmaf(a.x, g[M + c], av); av = fmaf(a.y, g[M + c + 1], av);
                 } else {
                     const uint2 raw = __ldg(reinterpret_cast<const uint2*>(A + 2 * (static_cast<size_t>(o) * S + c)));
                     const float2 z0 = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
                     const float2 z1 = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
-                    const float4 gg = __ldcg(reinterpret_cast<const float4*>(g + 2 * c));
+                    const float4 gg = *reinterpret_cast<const float4*>(g + 2 * c);
                     au = fmaf(z0.x, gg.x, au); au = fmaf(-z0.y, gg.y, au);
                     av = fmaf(z0.y, gg.x, av); av = fmaf(z0.x, gg.y, av);
                     au = fmaf(z1.x, gg.z, au); au = fmaf(-z1.y, gg.w, au);
@@ -1558,9 +1580,11 @@ __device__ __forceinline__ unsigned sm_id() {
 
 // A class-G island that the class-W team solves: above kWideMin vertices,
 // and its coarse g and y fit the batch's cpart after the team's header.
-__device__ __forceinline__ bool wide_island(const uva_batch& b, const Isl& I) {
-    return I.n > kWideMin && I.agg > 0 && (I.agg & 31) == 0 &&
-           kWideHdr + 4ll * (6ll * I.M + 24) <= 8ll * b.nslices;
+// (Its reduction partials and warp sums fit its own block of the batch's
+// coarse_work, 4 M^2 doubles; its coarse vectors fit shared memory, M <= 256.)
+__device__ __forceinline__ bool wide_island(const uva_batch&, const Isl& I) {
+    return I.n > kWideMin && I.agg > 0 && (I.agg & 31) == 0 && I.M >= 64 && I.M <= 256 &&
+           kWidePart + (I.n + 31) / 32 <= 4ll * I.M * I.M;
 }
 
 template <int NTT, int R, Op OP>
@@ -1633,20 +1657,17 @@ __global__ void __launch_bounds__(KB, 1) k_wide(uva_batch b, uva_solve_params pr
     __shared__ double redd[2 * kRedMax * 32];
     __shared__ float redf[2 * kRedMax * 32];
     __shared__ int redi[2 * 32];
+    __shared__ __align__(16) float wg[2 * 256 + 8];   // coarse g (all aggregates)
+    __shared__ float wy[2 * 256];                      // coarse y (this CTA's aggregates)
     WideScratch* ws = reinterpret_cast<WideScratch*>(b.cpart);
-    float* cg = reinterpret_cast<float*>(reinterpret_cast<char*>(b.cpart) + kWideHdr);
+    double* part = b.coarse_work;
     Team<kWideNTT> tm{static_cast<int>(blockIdx.x * KB + threadIdx.x), 0, 0, redd, redf, redi, nullptr,
-                      nullptr, nullptr, nullptr, cg, nullptr, nullptr, 0, nullptr, 0, ws, 0, 0};
+                      nullptr, nullptr, nullptr, wg, wy, nullptr, 0, nullptr, 0, ws, 0, part,
+                      reinterpret_cast<float2*>(part + kWidePart)};
     const int lo = b.class_ofs[0], hi = b.class_ofs[1];
     for (int q = lo; q < hi; ++q) {
         const Isl I = load_island<OP>(b, b.order[q]);
         if (!wide_island(b, I)) continue;
-        const int gs = wide_gstride(I.M);
-        tm.cy = cg + 2 * gs;
-        tm.gsel = 0;
-        if (blockIdx.x == 0)
-            for (int k = threadIdx.x; k < 2 * gs; k += KB) cg[k] = 0.f;   // both g buffers
-        tm.sync();
         const long long t0 = global_ns();
         if (OP == OP_ARAP) solve_arap<kWideNTT, 0>(b, prm, tm, I);
         else solve_lscm<kWideNTT, 0>(b, prm, tm, I);
@@ -2030,8 +2051,7 @@ int launch_islands(const uva_batch* b, const uva_solve_params* prm, cudaStream_t
     if (prm->rev_ctas != 0) nrev = std::max(0, std::min(grid, prm->rev_ctas));
     // class W first, on the whole GPU (cooperative: every CTA resident)
     int wide = 0;
-    if (b->class_ofs[1] > b->class_ofs[0] && b->cpart && sm_count() >= kWideCtas &&
-        8ll * b->nslices > kWideHdr + 4ll * (6 * (kWideMin / 128) + 24)) {
+    if (b->class_ofs[1] > b->class_ofs[0] && b->cpart && b->coarse_work && sm_count() >= kWideCtas) {
         e = cudaMemsetAsync(b->cpart, 0, kWideHdr, s);
         if (e != cudaSuccess) return uva_cuda_status(e, "uva_islands/memset");
         cudaLaunchConfig_t cfg{};
