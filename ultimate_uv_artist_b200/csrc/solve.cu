@@ -1869,13 +1869,21 @@ constexpr size_t kCoarseSmem = sizeof(double2) * kCoarseSmemC * kCoarseSmemC;   
 constexpr int kCoarseSmemN = 166;   // sizeof(double) * 166 * 166 <= kCoarseSmem
 static_assert(sizeof(double) * kCoarseSmemN * kCoarseSmemN <= kCoarseSmem, "real work matrix must fit");
 
-__global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
+// One CTA per island of b.order[first, first + count): NT = 1024 with
+// kCoarseSmem of dynamic shared memory for the whole-CTA classes (one CTA
+// per SM), NT = 256 with kCoarseSmallSmem for the sub-team classes, whose
+// operators are at most 32 x 32 (several CTAs per SM).
+constexpr int kCoarseSmallM = 32;
+constexpr size_t kCoarseSmallSmem = sizeof(double2) * kCoarseSmallM * kCoarseSmallM;   // 16 KB
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_coarse(uva_batch b, int first, int count) {
     extern __shared__ __align__(16) double wsm[];
     __shared__ double2 colk2[256], rowk2[256];   // pivot column / row (complex; the real pass uses 256 doubles of each)
     double* colk = reinterpret_cast<double*>(colk2);
     double* rowk = reinterpret_cast<double*>(rowk2);
-    if (static_cast<int>(blockIdx.x) >= b.nc) return;
-    const int isl = b.order[blockIdx.x];   // largest islands first (b.order is by size)
+    if (static_cast<int>(blockIdx.x) >= count) return;
+    const int isl = b.order[first + blockIdx.x];   // largest islands first (b.order is by size)
     const int agg = b.agg_rows[isl];
     if (agg <= 0) return;
     const int v0 = b.vofs[isl], n = b.vofs[isl + 1] - v0, s0 = b.sofs[isl];
@@ -1888,7 +1896,9 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
         q0 = p0s + (r & 31);
         width = (p1s - p0s) >> 5;
     };
-    auto work = [&](int N) { return N <= kCoarseSmemN ? wsm : b.coarse_work + 4 * static_cast<size_t>(co); };
+    constexpr int kRealN = NT == 1024 ? kCoarseSmemN : 45;            // 8 N^2 bytes of shared memory
+    constexpr int kCplxN = NT == 1024 ? kCoarseSmemC : kCoarseSmallM;  // 16 N^2 bytes
+    auto work = [&](int N) { return N <= kRealN ? wsm : b.coarse_work + 4 * static_cast<size_t>(co); };
     // ---- ARAP
     double* W = work(M);
     for (int e = threadIdx.x; e < M * M; e += blockDim.x) W[e] = 0.0;
@@ -1925,8 +1935,8 @@ __global__ void __launch_bounds__(1024) k_coarse(uva_batch b) {
     const int p0 = b.vert_row[v0 + pv0], p1 = b.vert_row[v0 + pv1];
     // the (u, v) operator per aggregate is the real form [[P, -Q], [Q, P]] of
     // the complex Hermitian Hc = P + i Q: assembled and inverted as complex
-    double2* Wc = M <= kCoarseSmemC ? reinterpret_cast<double2*>(wsm)
-                                    : reinterpret_cast<double2*>(b.coarse_work + 4 * static_cast<size_t>(co));
+    double2* Wc = M <= kCplxN ? reinterpret_cast<double2*>(wsm)
+                              : reinterpret_cast<double2*>(b.coarse_work + 4 * static_cast<size_t>(co));
     for (int e = threadIdx.x; e < M * M; e += blockDim.x) Wc[e] = make_double2(0.0, 0.0);
     __syncthreads();
     for (int a = threadIdx.x; a < M; a += blockDim.x) {
@@ -1975,7 +1985,8 @@ cudaError_t ensure_coarse_attr() {
     std::lock_guard<std::mutex> lk(mu);
     if (static_cast<int>(done.size()) <= dev) done.resize(dev + 1, 0);
     if (done[dev]) return cudaSuccess;
-    e = cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kCoarseSmem));
+    e = cudaFuncSetAttribute(k_coarse<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kCoarseSmem));
     if (e == cudaSuccess) done[dev] = 1;
     return e;
 }
@@ -2376,7 +2387,11 @@ extern "C" int uva_batch_setup(uva_batch* b, void* stream) {
     if (b->coarse_a && b->coarse_l && b->coarse_work) {
         const cudaError_t e = ensure_coarse_attr();   // 128 KB of dynamic shared memory
         if (e != cudaSuccess) return uva_cuda_status(e, "uva_batch_setup/coarse attribute");
-        k_coarse<<<b->nc, 1024, kCoarseSmem, s>>>(*b);
+        // whole-CTA classes (W, G, A: islands above 2048 vertices), then the
+        // smaller ones (aggregates of 64 rows: at most 32 x 32 operators)
+        const int big = std::min(std::max(b->class_ofs[2], 0), b->nc), rest = b->nc - big;
+        if (big > 0) k_coarse<1024><<<big, 1024, kCoarseSmem, s>>>(*b, 0, big);
+        if (rest > 0) k_coarse<256><<<rest, 256, kCoarseSmallSmem, s>>>(*b, big, rest);
         UVA_CHECK_LAUNCH("uva_batch_setup/coarse");
     }
     return UVA_OK;
