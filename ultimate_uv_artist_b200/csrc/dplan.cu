@@ -310,10 +310,17 @@ namespace {
 // the blob continues from the next lowest one; when the blob is full, the
 // queued but unplaced vertices are released for later blobs. A vertex's
 // neighbours join the queue in ascending order (a ballot and a prefix count
-// keep the order across lanes). st: bit 0 placed, bit 1 queued.
+// keep the order across lanes). st: bit 0 placed, bit 1 queued. Islands of
+// up to kBlobCap vertices keep st and the queue in shared memory (the walk
+// is one dependent chain per vertex, so each global round trip taken out of
+// it counts); larger ones use the global scratch.
+constexpr int kBlobCap = 8192;
+constexpr size_t kBlobSmem = 5 * static_cast<size_t>(kBlobCap);   // st bytes, then the queue (ints)
+
 __global__ void __launch_bounds__(32) k_dp_blob(int32_t nc, const int32_t* vofs, const int32_t* agg_rows,
                                                 const int32_t* row_ptr, const int32_t* adj, uint8_t* st,
                                                 int32_t* queue, int32_t* row_vert, int32_t* status) {
+    extern __shared__ __align__(16) unsigned char blob_smem[];
     if (*status & kBadIndex) return;
     const int lane = threadIdx.x;
     constexpr unsigned kAll = 0xffffffffu;
@@ -324,8 +331,13 @@ __global__ void __launch_bounds__(32) k_dp_blob(int32_t nc, const int32_t* vofs,
             for (int32_t v = lane; v < n; v += 32) rv[v] = v;
             continue;
         }
-        uint8_t* s = st + v0;
-        int32_t* q = queue + v0;
+        const bool local = n <= kBlobCap;
+        uint8_t* s = local ? blob_smem : st + v0;
+        int32_t* q = local ? reinterpret_cast<int32_t*>(blob_smem + kBlobCap) : queue + v0;
+        if (local) {
+            for (int32_t v = lane; v < n; v += 32) s[v] = 0;
+            __syncwarp();
+        }
         const int32_t* rp = row_ptr + v0;
         int32_t norder = 0, seed = 0;
         while (norder < n) {
@@ -352,12 +364,12 @@ __global__ void __launch_bounds__(32) k_dp_blob(int32_t nc, const int32_t* vofs,
                     if (lane == 0) { s[v] |= 1; rv[norder] = v; }
                     ++norder;
                     __syncwarp();
-                    const int32_t a = rp[v], b = rp[v + 1];
+                    const int32_t a = __ldg(rp + v), b = __ldg(rp + v + 1);
                     for (int32_t k0 = a; k0 < b; k0 += 32) {
                         const int32_t k = k0 + lane;
                         int32_t w = 0;
                         bool take = false;
-                        if (k < b) { w = adj[k]; take = (s[w] & 3) == 0; }
+                        if (k < b) { w = __ldg(adj + k); take = (s[w] & 3) == 0; }
                         const unsigned m = __ballot_sync(kAll, take);
                         if (take) {
                             q[qlen + __popc(m & ((1u << lane) - 1u))] = w;
@@ -583,7 +595,8 @@ extern "C" int uva_dplan_build(const uva_dplan* d, void* stream) {
     k_dp_vflags<<<blocks_for(n), kTB, 0, st>>>(n, s.vflag32, d->vflags);
     UVA_CHECK_LAUNCH("uva_dplan_build/edges");
     // 5. solver rows
-    k_dp_blob<<<gi, 32, 0, st>>>(nc, d->vofs, d->agg_rows, row_ptr, s.adj, s.bfs, s.queue, d->row_vert, s.status);
+    k_dp_blob<<<gi, 32, kBlobSmem, st>>>(nc, d->vofs, d->agg_rows, row_ptr, s.adj, s.bfs, s.queue, d->row_vert,
+                                         s.status);
     k_dp_vert_row<<<blocks_for(n), kTB, 0, st>>>(n, s.vbase, d->row_vert, d->vert_row, s.status);
     // 6. slices
     if (d->nslices > 0)
