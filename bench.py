@@ -37,7 +37,7 @@ METRIC = "ARAP tris/sec @1e-6 resid, batched-FP32+FP64-refine"
 UNIT = "tri-iters/s"
 ITERS = 20
 ISLANDS = 2000
-TRAFFIC_ARAP = 33.58e9   # bytes per ARAP launch of the default workload (ncu dram__bytes_read + write)
+TRAFFIC_ARAP = 32.78e9   # bytes per ARAP launch of the default workload (ncu dram__bytes_read + write)
 
 
 def _args():
