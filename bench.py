@@ -969,8 +969,11 @@ def main():
     nbnd = np.diff(db.plan.bofs.astype(np.int64))
     lfull, lcomp = lscm_bytes(n, nnz, nbnd, st_lscm)
 
+    # the single-GPU legs (diagnostics beside the headline step) run only
+    # without torchrun: a scaling run holds every GPU while rank 0 works
+    solo = rank == 0 and ws == 1
     val = None
-    if rank == 0 and not args.no_validate:
+    if solo and not args.no_validate:
         val = bench_validation(dev)
 
     plain = None
@@ -982,20 +985,20 @@ def main():
         plain["speedup_vs_one_batch"] = value / plain["one_batch"]["value"]
 
     bnd = hier_b = ovl = None
-    if rank == 0 and not args.no_validate:
+    if solo and not args.no_validate:
         bnd = bench_boundary(b)
         hier_b = bench_hier(dev)
         ovl = bench_overlap(islands, our_uvs)
     c5 = c1 = c4 = pk = gi = None
-    if rank == 0 and not args.no_giant:
+    if solo and not args.no_giant:
         gi = bench_giant(dev, args.iters)
-    if rank == 0 and not args.no_pack:
+    if solo and not args.no_pack:
         pk = bench_pack(dev, args.pack_charts, cpu=not args.no_cpu_baseline)
-    if rank == 0 and not args.no_config5:
+    if solo and not args.no_config5:
         c5 = bench_config5(dev, cpu=not args.no_cpu_baseline)
-    if rank == 0 and not args.no_config4:
+    if solo and not args.no_config4:
         c4 = bench_energy(dev, hbm)
-    if rank == 0 and not args.no_config1:
+    if solo and not args.no_config1:
         c1 = bench_config1(dev)
 
     cpu = None
