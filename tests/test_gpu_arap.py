@@ -1,7 +1,7 @@
 """GPU parity of the batched LSCM / ARAP path against the reference's own
 outputs (golden fixtures) and the FP64 oracle.
 
-Tolerances (BASELINE north star): UVs within 1e-5 relative to each chart's UV
+Tolerances: UVs within 1e-5 relative to each chart's UV
 extent; p95 anisotropy within 1e-4; global steps at 1e-6 relative residual
 per column, checked in FP64.
 """

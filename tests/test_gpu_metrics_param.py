@@ -2,7 +2,7 @@
 (engine/param.py) against the reference's own outputs (golden fixtures).
 
 Tolerances: FP64 geometry 1e-9 relative; p95 quantiles 1e-4 relative (the
-north-star bound on p95 anisotropy); rasters, counts and the serial flip
+the stated bound on p95 anisotropy); rasters, counts and the serial flip
 repair bit-exact."""
 import numpy as np
 import pytest

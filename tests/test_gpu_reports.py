@@ -12,7 +12,7 @@ Tolerances: counts, masks, index arrays and booleans exact; summed lengths,
 areas and distortion means 1e-9 relative (summation order differs), island
 area fractions 1e-6 (the reference sums float32 cross products); FP32
 products 1e-5;
-p95 quantiles 1e-4; Tutte UVs 1e-9 of the extent
+p95 quantiles 1e-4 (the stated bound); Tutte UVs 1e-9 of the extent
 (iterative FP64 solve to 1e-12 against the reference's LU).
 """
 import os
