@@ -629,9 +629,9 @@ def bench_config5(dev, iters=ITERS, steps=2, cpu=True):
 
 
 def bench_giant(dev, iters=ITERS, big_tris=200_000):
-    """The upper island size of the workloads (200k triangles): the 2,000-island batch plus one
-    disk island of about 200k triangles (solved by the whole-GPU class-W
-    team before the persistent launch). Setup + LSCM and 20 ARAP iterations
+    """Islands up to 200k triangles: the 2,000-island batch plus one disk
+    island of about 200k triangles (solved by the whole-GPU class-W team
+    before the persistent launch). Setup + LSCM and 20 ARAP iterations
     (CUDA events), the batch's tri-iters/s, and the large island's own
     launch time, CG iterations and team."""
     import torch
