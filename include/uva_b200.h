@@ -479,6 +479,23 @@ int uva_csr_pcg_blocks(int32_t nsys, const int32_t* sys_ofs, int32_t n, const in
                        const double* val, const double* b, double* x, double tol, int32_t maxiter, double* scratch,
                        int32_t* iters, void* stream);
 
+/* hier.Solver.lscm (engine/hier.py:534-585) with the system assembled on
+ * the device: half-cot weights of the mesh faces `faces` (rows of F, (nf,3),
+ * positions V (nvp,3)), the soft-pinned LSCM system of every chart (UV
+ * corners CV (t,3), chart per face, directed boundary edges ba -> bb (nb)),
+ * unknowns grouped by chart, then uva_csr_pcg_blocks to ||r_c|| <= tol
+ * ||b_c|| per chart (at most maxiter iterations). U (nv,2): the solution,
+ * U0 for UV vertices no face names and for non-finite values. flags (one
+ * device int32, zeroed here): bit 0 a UV vertex or boundary edge joins two
+ * charts, bit 1 an index out of range (faces, F, CV, ba, bb), bit 2 a chart
+ * id out of range; offending entries are left out, so the solve stays in
+ * bounds. Index arrays are int32. scratch: uva_hier_lscm_scratch_bytes.   */
+int uva_hier_lscm_scratch_bytes(int64_t nv, int64_t t, int64_t nb, int32_t nchart, int64_t* bytes);
+int uva_hier_lscm(const double* V, int64_t nvp, const int32_t* F, int64_t nf, const int32_t* faces, const int32_t* CV,
+                  const int32_t* chart, int64_t t, int64_t nv, int32_t nchart, const double* U0, const int32_t* ba,
+                  const int32_t* bb, int64_t nb, double tol, int32_t maxiter, void* scratch, int64_t scratch_bytes,
+                  double* U, int32_t* flags, void* stream);
+
 /* --------------------------------------------------------------------------
  * Distortion energies with backward passes (engine/param.py:294-319):
  * kind 0 ARAP, kind 1 symmetric Dirichlet (inf for inverted triangles),

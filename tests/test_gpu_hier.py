@@ -67,3 +67,77 @@ def test_relax_iteration_counts(cuda, gh):
                                 iters=iters)
         assert np.abs(U - Uo).max() <= 1e-5 * np.abs(Uo).max(), iters
         assert np.array_equal(flips, fo)
+
+
+def _mesh_case(nx=48, ny=40, block=16, seed=6100):
+    from ultimate_uv_artist_b200 import synth
+    from ultimate_uv_artist_b200.engine import hier
+    V, F, FF, faces, loc, chart, CV, nv, nchart, U0 = synth.mesh_charts(seed=seed, nx=nx, ny=ny, block=block)
+    ba, bb = hier.boundary_directed(F, FF, faces, loc, chart, CV)
+    return V, F, faces, CV, nv, chart, nchart, U0, ba, bb
+
+
+def test_lscm_device_assembly_vs_oracle_and_repeatable(cuda):
+    """The device-assembled system (uva_hier_lscm) on a bumpy 48 x 40 grid
+    cut into 12 charts, against the oracle's exact solve; two calls give the
+    same bits (fixed entry order, no atomics in the sums)."""
+    from oracle import hier as oh
+    from ultimate_uv_artist_b200.engine import hier
+    V, F, faces, CV, nv, chart, nchart, U0, ba, bb = _mesh_case()
+    S = hier.Solver(SimpleNamespace(V=V, F=F), dev=cuda)
+    U = S.lscm(faces, CV, nv, chart, nchart, U0, ba, bb)
+    Uo = oh.lscm(V, F, faces, CV, nv, chart, nchart, U0, ba, bb)
+    ext = np.abs(Uo).max()
+    assert np.abs(U - Uo).max() <= 1e-6 * ext
+    assert np.array_equal(U, S.lscm(faces, CV, nv, chart, nchart, U0, ba, bb))
+
+
+def test_lscm_permuted_ids_unused_vertices_and_empty_charts(cuda):
+    """UV vertex ids shuffled across charts (the chart grouping is a sort, not
+    an id range), 25 UV vertices that no face names (they keep U0, NaN
+    included), faces in shuffled order, two more chart ids than charts used,
+    and negative indices (counted from the end, as numpy indexing does)."""
+    from oracle import hier as oh
+    from ultimate_uv_artist_b200.engine import hier
+    V, F, faces, CV, nv, chart, nchart, U0, ba, bb = _mesh_case(nx=32, ny=32, block=16, seed=6200)
+    rng = np.random.default_rng(7)
+    extra = 25
+    perm = rng.permutation(nv + extra)            # old id -> new id
+    CVp = perm[CV]
+    bap, bbp = perm[ba], perm[bb]
+    U0p = rng.normal(0, 1, (nv + extra, 2))
+    U0p[perm[:nv]] = U0
+    U0p[perm[nv:][:3]] = np.nan
+    fo = rng.permutation(len(faces))
+    S = hier.Solver(SimpleNamespace(V=V, F=F), dev=cuda)
+    args = (faces[fo], CVp[fo], nv + extra, chart[fo], nchart + 2, U0p, bap, bbp)
+    U = S.lscm(*args)
+    Uo = oh.lscm(V, F, *args)
+    unused = perm[nv:]
+    assert np.array_equal(U[unused], U0p[unused], equal_nan=True)
+    used = perm[:nv]
+    assert np.abs(U[used] - Uo[used]).max() <= 1e-6 * np.abs(Uo[used]).max()
+    neg = (faces[fo] - len(F), CVp[fo] - (nv + extra), nv + extra, chart[fo], nchart + 2, U0p,
+           bap - (nv + extra), bbp)
+    assert np.array_equal(S.lscm(*neg), U, equal_nan=True)
+
+
+def test_lscm_rejects_shared_vertices_and_bad_indices(cuda):
+    from ultimate_uv_artist_b200.engine import hier
+    V, F, faces, CV, nv, chart, nchart, U0, ba, bb = _mesh_case(nx=32, ny=16, block=16, seed=6300)
+    S = hier.Solver(SimpleNamespace(V=V, F=F), dev=cuda)
+    CVs = CV.copy()
+    other = np.nonzero(chart != chart[0])[0][0]
+    CVs[other, 0] = CV[0, 0]                       # a UV vertex of chart 0 in a face of another chart
+    with pytest.raises(ValueError):
+        S.lscm(faces, CVs, nv, chart, nchart, U0, ba, bb)
+    CVb = CV.copy(); CVb[3, 1] = nv
+    with pytest.raises(IndexError):
+        S.lscm(faces, CVb, nv, chart, nchart, U0, ba, bb)
+    chb = chart.copy(); chb[5] = nchart
+    with pytest.raises(ValueError):
+        S.lscm(faces, CV, nv, chb, nchart, U0, ba, bb)
+    # the call after a rejected one is unaffected
+    U = S.lscm(faces, CV, nv, chart, nchart, U0, ba, bb)
+    assert np.isfinite(U).all()
+    assert S.lscm(faces[:0], CV[:0], 0, chart[:0], 0, U0[:0], ba[:0], bb[:0]).shape == (0, 2)

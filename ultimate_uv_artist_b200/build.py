@@ -23,7 +23,7 @@ PYHOST_LIB = os.path.join(HERE, "libuva_pyhost.so")   # the batch constructor's 
 BUILD_DIR = os.path.join(ROOT, "_build")
 
 CU_SOURCES = ["capi.cu", "solve.cu", "ops.cu", "chart_ops.cu", "validate.cu", "metrics.cu", "energy.cu", "gutter.cu",
-              "segments.cu", "edges.cu", "report.cu", "dplan.cu", "pack.cu"]
+              "segments.cu", "edges.cu", "report.cu", "dplan.cu", "pack.cu", "hier.cu"]
 CXX_SOURCES = ["plan.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

@@ -191,19 +191,98 @@ __global__ void k_chart_op(ChartArgs a) {
 
 __global__ void k_fill(double* p, double v) { *p = v; }
 
+constexpr int kPcgNT = 1024;
+constexpr size_t kPcgRowBytes = 5 * sizeof(double) + sizeof(int32_t);
+constexpr size_t kPcgSmem = 220 * 1024;
+constexpr int kPcgCap = static_cast<int>((kPcgSmem - 2 * sizeof(int32_t)) / kPcgRowBytes);
+
+template <int NT>
+__device__ void pcg_block_smem(int r0, int n, const int32_t* rp, const int32_t* ci, const double* val,
+                               const double* b, double* x, double tol, int maxiter, int32_t* it_out, double* red,
+                               double* dsm, int cap) {
+    int phase = 0;
+    double* X = dsm;
+    double* R = X + cap;
+    double* P = R + cap;
+    double* Q = P + cap;
+    double* D = Q + cap;
+    int32_t* RP = reinterpret_cast<int32_t*>(D + cap);   // n + 1 row starts, relative to the block's first entry
+    const int32_t e0 = rp[r0];
+    for (int i = threadIdx.x; i <= n; i += NT) RP[i] = rp[r0 + i] - e0;
+    ci += e0;
+    val += e0;
+    for (int i = threadIdx.x; i < n; i += NT) {
+        X[i] = x[r0 + i];
+        double d = 0.0;
+        for (int k = rp[r0 + i] - e0; k < rp[r0 + i + 1] - e0; ++k)
+            if (ci[k] == r0 + i) d += val[k];
+        D[i] = 1.0 / (fabs(d) > 1e-300 ? d : 1.0);
+    }
+    __syncthreads();
+    double acc[2] = {0.0, 0.0};
+    for (int i = threadIdx.x; i < n; i += NT) {
+        double ax = 0.0;
+        for (int k = RP[i]; k < RP[i + 1]; ++k) ax += val[k] * X[ci[k] - r0];
+        const double bi = b[r0 + i];
+        const double ri = bi - ax;
+        R[i] = ri;
+        P[i] = ri * D[i];
+        acc[0] += ri * P[i];
+        acc[1] += bi * bi;
+    }
+    block_sum<NT, 2>(acc, red, phase);   // also publishes P
+    double rz = acc[0];
+    const double bb = fmax(acc[1], 1e-300);
+    int it = 0;
+    for (; it < maxiter; ++it) {
+        double pq[1] = {0.0};
+        for (int i = threadIdx.x; i < n; i += NT) {
+            double sacc = 0.0;
+            for (int k = RP[i]; k < RP[i + 1]; ++k) sacc += val[k] * P[ci[k] - r0];
+            Q[i] = sacc;
+            pq[0] += P[i] * sacc;
+        }
+        block_sum<NT, 1>(pq, red, phase);
+        if (!(pq[0] > 0.0)) break;
+        const double alpha = rz / pq[0];
+        double nz[2] = {0.0, 0.0};
+        for (int i = threadIdx.x; i < n; i += NT) {
+            X[i] += alpha * P[i];
+            const double ri = R[i] - alpha * Q[i];
+            R[i] = ri;
+            nz[0] += ri * ri * D[i];
+            nz[1] += ri * ri;
+        }
+        block_sum<NT, 2>(nz, red, phase);
+        if (nz[1] <= tol * tol * bb) { ++it; break; }
+        const double beta = nz[0] / rz;
+        rz = nz[0];
+        for (int i = threadIdx.x; i < n; i += NT) P[i] = R[i] * D[i] + beta * P[i];
+        __syncthreads();
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += NT) x[r0 + i] = X[i];
+    if (threadIdx.x == 0) *it_out = it;
+}
+
 // ---- FP64 Jacobi-PCG for one CSR SPD matrix, ncol right-hand sides, one CTA
 // per column (param.py:119-132 with the SuperLU branch replaced by PCG to a
-// tight tolerance).
+// tight tolerance); matrices of at most `cap` rows iterate in shared memory.
 template <int NT>
 __global__ void __launch_bounds__(NT) k_csr_pcg(int n, const int32_t* rp, const int32_t* ci, const double* val,
                                                 const double* b, double* x, double* r, double* p, double* q,
-                                                int ncol, double tol, int maxiter, int32_t* iters_out) {
+                                                int ncol, double tol, int maxiter, int32_t* iters_out, int cap) {
     __shared__ double red[2 * 4 * (NT / 32)];
+    extern __shared__ double dsm[];
     int phase = 0;
     const int c = blockIdx.x;
     if (c >= ncol) return;
     const double* bc = b + static_cast<size_t>(c) * n;
     double* xc = x + static_cast<size_t>(c) * n;
+    if (n <= cap) {
+        pcg_block_smem<NT>(0, n, rp, ci, val, bc, xc, tol, maxiter, iters_out + c, red, dsm, cap);
+        return;
+    }
     double* rc = r + static_cast<size_t>(c) * n;
     double* pc = p + static_cast<size_t>(c) * n;
     double* qc = q + static_cast<size_t>(c) * n;
@@ -258,17 +337,27 @@ __global__ void __launch_bounds__(NT) k_csr_pcg(int n, const int32_t* rp, const 
 
 // ---- the same PCG on a block-diagonal CSR matrix, one CTA per diagonal
 // block: block s owns rows [so[s], so[s+1]) and its columns lie in the same
-// range; it stops at ||r_s|| <= tol ||b_s||.
+// range; it stops at ||r_s|| <= tol ||b_s||. A block of at most `cap` rows
+// keeps its iterate, residual, direction, product, inverse diagonal and
+// row pointers in shared memory (kPcgRowBytes per row), so each iteration
+// reads only its matrix entries from L2 and gathers from shared memory;
+// larger blocks run the same iteration on the global scratch, the diagonal
+// re-read from the row.
 template <int NT>
 __global__ void __launch_bounds__(NT) k_csr_pcg_blocks(int nsys, const int32_t* so, const int32_t* rp,
                                                        const int32_t* ci, const double* val, const double* b,
                                                        double* x, double* r, double* p, double* q, double tol,
-                                                       int maxiter, int32_t* iters_out) {
+                                                       int maxiter, int32_t* iters_out, int cap) {
     __shared__ double red[2 * 4 * (NT / 32)];
+    extern __shared__ double dsm[];
     int phase = 0;
     const int c = blockIdx.x;
     if (c >= nsys) return;
     const int r0 = so[c], r1 = so[c + 1];
+    if (r1 - r0 <= cap) {
+        pcg_block_smem<NT>(r0, r1 - r0, rp, ci, val, b, x, tol, maxiter, iters_out + c, red, dsm, cap);
+        return;
+    }
     auto diag = [&](int i) {
         double d = 0.0;
         for (int k = rp[i]; k < rp[i + 1]; ++k)
@@ -344,8 +433,11 @@ extern "C" int uva_csr_pcg_blocks(int32_t nsys, const int32_t* sys_ofs, int32_t 
     if (nsys == 0 || n == 0) return UVA_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t N = static_cast<size_t>(n);
-    k_csr_pcg_blocks<256><<<nsys, 256, 0, s>>>(nsys, sys_ofs, rowptr, col, val, b, x, scratch, scratch + N,
-                                               scratch + 2 * N, tol, maxiter, iters);
+    const cudaError_t e = cudaFuncSetAttribute(k_csr_pcg_blocks<kPcgNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(kPcgSmem));
+    if (e != cudaSuccess) return uva_cuda_status(e, "uva_csr_pcg_blocks/cudaFuncSetAttribute");
+    k_csr_pcg_blocks<kPcgNT><<<nsys, kPcgNT, kPcgSmem, s>>>(nsys, sys_ofs, rowptr, col, val, b, x, scratch,
+                                                           scratch + N, scratch + 2 * N, tol, maxiter, iters, kPcgCap);
     UVA_CHECK_LAUNCH("uva_csr_pcg_blocks");
     return UVA_OK;
 }
@@ -357,8 +449,11 @@ extern "C" int uva_csr_pcg(int32_t n, const int32_t* rowptr, const int32_t* col,
     if (n == 0) return UVA_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t N = static_cast<size_t>(n) * ncol;
-    k_csr_pcg<512><<<ncol, 512, 0, s>>>(n, rowptr, col, val, b, x, scratch, scratch + N, scratch + 2 * N, ncol, tol,
-                                        maxiter, iters);
+    const cudaError_t e = cudaFuncSetAttribute(k_csr_pcg<kPcgNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(kPcgSmem));
+    if (e != cudaSuccess) return uva_cuda_status(e, "uva_csr_pcg/cudaFuncSetAttribute");
+    k_csr_pcg<kPcgNT><<<ncol, kPcgNT, kPcgSmem, s>>>(n, rowptr, col, val, b, x, scratch, scratch + N, scratch + 2 * N,
+                                                    ncol, tol, maxiter, iters, kPcgCap);
     UVA_CHECK_LAUNCH("uva_csr_pcg");
     return UVA_OK;
 }

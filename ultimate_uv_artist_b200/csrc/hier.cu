@@ -1,0 +1,491 @@
+// hier.Solver.lscm on the device (engine/hier.py:534-585): the soft-pinned
+// LSCM system of every chart assembled from the faces, then solved per chart
+// by the FP64 Jacobi-PCG of chart_ops.cu (uva_csr_pcg_blocks).
+//
+// The system (2 nv unknowns: u then v of each UV vertex) is the reference's
+// COO sum: per face edge e = (corner e+1, corner e+2) with half-cot weight
+// w_e, (i,j) -= w, (j,i) -= w, (i,i) += w, (j,j) += w in the u and in the v
+// block; per directed boundary edge (a, b), (a_u, b_v) -= 1/2,
+// (b_u, a_v) += 1/2, (a_v, b_u) += 1/2, (b_v, a_u) -= 1/2; per chart two
+// pins (the boundary vertices of smallest and largest initial u, compared in
+// float32, the smallest vertex id on ties) with diagonal weight
+// wpin = 10 max(max |w|, 1e-12) and right-hand side wpin U0. Only UV
+// vertices that a face names have unknowns; the others keep U0.
+//
+// Layout: unknowns grouped by chart (a chart's u unknowns by vertex id, then
+// its v unknowns), so chart c owns the diagonal block [sys_ofs[c],
+// sys_ofs[c+1]). The grouping is a stable radix sort of the vertices by
+// chart; every row lists its diagonal first, then two entries per incident
+// face corner (corners in face order), then one per incident boundary edge
+// end (edges in order): duplicates are kept as separate entries (the product
+// is the same sum), so no per-row merge is needed and the entry order, hence
+// the rounding of every product, is fixed.
+//
+// Steps (one stream, no host round trip):
+//   k_hl_faces   half-cot weights per face (engine/hier.py:362-382 restated),
+//                max |w|, the last face naming each UV vertex, corner counts
+//   k_hl_vchart  chart of each vertex (the last naming face's), chart sizes
+//   k_hl_check   consistency (a face's corners and a boundary edge's ends in
+//                one chart) and the pins' keys (atomic minima of 64-bit
+//                (ordered key, vertex) words)
+//   radix sorts  vertices by chart, corners by vertex, boundary ends by vertex
+//   k_hl_rank    unknown numbers; k_hl_rows<false> (row lengths), scan,
+//                k_hl_rows<true> (entries): the CSR
+//   uva_csr_pcg_blocks, then k_hl_out: U (nv, 2), U0 where not finite.
+#include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "common.cuh"
+#include "scan.cuh"
+
+using namespace uva;
+
+namespace {
+
+constexpr int kTB = 256;
+constexpr uint64_t kNoPin = ~0ull;
+
+unsigned blocks_for(int64_t n) { return static_cast<unsigned>(std::max<int64_t>(1, (n + kTB - 1) / kTB)); }
+
+int bits_for(int64_t maxval) {   // bits holding 0..maxval
+    int b = 1;
+    while (b < 62 && (int64_t{1} << b) <= maxval) ++b;
+    return b;
+}
+
+struct HlArgs {
+    const double* V;       // mesh positions (nvp, 3)
+    const int32_t* F;      // mesh faces (nf, 3)
+    const int32_t* faces;  // (t) rows of F
+    const int32_t* CV;     // (t, 3) UV vertices of the face corners
+    const int32_t* chart;  // (t)
+    const double* U0;      // (nv, 2)
+    const int32_t* ba;     // (nb) directed boundary edges a -> b
+    const int32_t* bb;
+    int64_t nvp, nf, t, nv, nb;
+    int32_t nchart;
+};
+
+// Scratch of one call, carved from one buffer (256-byte aligned pieces).
+struct HlScratch {
+    int32_t *lastf, *cv, *ccnt, *cofs, *npin, *vcnt, *vofs, *bcnt, *bofs, *rowlen, *rowptr, *ci, *sys_ofs, *its,
+        *err, *isums;
+    uint32_t *vkey, *vkey_s, *vval, *vval_s, *ckey, *ckey_s, *cval, *cval_s, *bkey, *bkey_s, *bval, *bval_s;
+    int2* unk;
+    double *w, *va, *b, *x, *pcg;
+    uint64_t *wmax, *pmin, *pmax;
+    void* cub;
+    size_t cub_bytes;
+    int64_t nnz_max;
+};
+
+size_t cub_temp(int64_t n, int end_bit) {
+    size_t bytes = 0;
+    if (n > 0)
+        cub::DeviceRadixSort::SortPairs(nullptr, bytes, static_cast<const uint32_t*>(nullptr),
+                                        static_cast<uint32_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+                                        static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, end_bit);
+    return bytes;
+}
+
+// Lays the scratch out at `base` (nullptr: sizes only); returns the bytes.
+size_t hl_layout(const HlArgs& a, char* base, HlScratch* s) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) -> char* {
+        char* p = base ? base + off : nullptr;
+        off += (bytes + 255) & ~static_cast<size_t>(255);
+        return p;
+    };
+    const int64_t nv = a.nv, t = a.t, nb = a.nb, nc = a.nchart, N = 2 * nv;
+    const int64_t nnz = 2 * (nv + 6 * t + 2 * nb);
+    HlScratch z{};
+    HlScratch& r = s ? *s : z;
+    r.lastf = reinterpret_cast<int32_t*>(take(4 * nv));
+    r.cv = reinterpret_cast<int32_t*>(take(4 * nv));
+    r.ccnt = reinterpret_cast<int32_t*>(take(4 * (nc + 1)));
+    r.cofs = reinterpret_cast<int32_t*>(take(4 * (nc + 1)));
+    r.npin = reinterpret_cast<int32_t*>(take(4 * nv));
+    r.vcnt = reinterpret_cast<int32_t*>(take(4 * (nv + 1)));
+    r.vofs = reinterpret_cast<int32_t*>(take(4 * (nv + 1)));
+    r.bcnt = reinterpret_cast<int32_t*>(take(4 * (nv + 1)));
+    r.bofs = reinterpret_cast<int32_t*>(take(4 * (nv + 1)));
+    r.rowlen = reinterpret_cast<int32_t*>(take(4 * (N + 1)));
+    r.rowptr = reinterpret_cast<int32_t*>(take(4 * (N + 1)));
+    r.ci = reinterpret_cast<int32_t*>(take(4 * nnz));
+    r.sys_ofs = reinterpret_cast<int32_t*>(take(4 * (nc + 1)));
+    r.its = reinterpret_cast<int32_t*>(take(4 * std::max<int64_t>(nc, 1)));
+    r.err = reinterpret_cast<int32_t*>(take(4));
+    r.isums = reinterpret_cast<int32_t*>(take(4 * (xscan_sums(std::max(N, nc) + 1) + 1)));
+    r.vkey = reinterpret_cast<uint32_t*>(take(4 * nv));
+    r.vkey_s = reinterpret_cast<uint32_t*>(take(4 * nv));
+    r.vval = reinterpret_cast<uint32_t*>(take(4 * nv));
+    r.vval_s = reinterpret_cast<uint32_t*>(take(4 * nv));
+    r.ckey = reinterpret_cast<uint32_t*>(take(4 * 3 * t));
+    r.ckey_s = reinterpret_cast<uint32_t*>(take(4 * 3 * t));
+    r.cval = reinterpret_cast<uint32_t*>(take(4 * 3 * t));
+    r.cval_s = reinterpret_cast<uint32_t*>(take(4 * 3 * t));
+    r.bkey = reinterpret_cast<uint32_t*>(take(4 * 2 * nb));
+    r.bkey_s = reinterpret_cast<uint32_t*>(take(4 * 2 * nb));
+    r.bval = reinterpret_cast<uint32_t*>(take(4 * 2 * nb));
+    r.bval_s = reinterpret_cast<uint32_t*>(take(4 * 2 * nb));
+    r.unk = reinterpret_cast<int2*>(take(8 * nv));
+    r.w = reinterpret_cast<double*>(take(8 * 3 * t));
+    r.va = reinterpret_cast<double*>(take(8 * nnz));
+    r.b = reinterpret_cast<double*>(take(8 * N));
+    r.x = reinterpret_cast<double*>(take(8 * N));
+    r.pcg = reinterpret_cast<double*>(take(8 * 3 * N));
+    r.wmax = reinterpret_cast<uint64_t*>(take(8));
+    r.pmin = reinterpret_cast<uint64_t*>(take(8 * std::max<int64_t>(nc, 1)));
+    r.pmax = reinterpret_cast<uint64_t*>(take(8 * std::max<int64_t>(nc, 1)));
+    r.cub_bytes = std::max({cub_temp(nv, bits_for(nc)), cub_temp(3 * t, bits_for(nv)), cub_temp(2 * nb, bits_for(nv))});
+    r.cub = take(std::max<size_t>(r.cub_bytes, 16));
+    r.nnz_max = nnz;
+    return off;
+}
+
+__device__ __forceinline__ void flag(int32_t* err, int bit) { atomicOr(err, bit); }
+
+// Half-cot weights of one mesh face (engine/hier.py:362-382): the face in
+// its own frame, corners (0,0), (l1,0), (e2.ex, e2.ey); 0 for faces too thin
+// for a frame; cotangents clipped to [-1e4, 1e4] (NaN kept, like np.clip).
+__device__ void face_cots(const double* V, const int32_t* Fr, double w[3]) {
+    const double* p0 = V + 3 * static_cast<int64_t>(Fr[0]);
+    const double* p1 = V + 3 * static_cast<int64_t>(Fr[1]);
+    const double* p2 = V + 3 * static_cast<int64_t>(Fr[2]);
+    const double e1x = p1[0] - p0[0], e1y = p1[1] - p0[1], e1z = p1[2] - p0[2];
+    const double e2x = p2[0] - p0[0], e2y = p2[1] - p0[1], e2z = p2[2] - p0[2];
+    const double l1 = sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
+    const double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+    const double dbl = sqrt(nx * nx + ny * ny + nz * nz);
+    const bool ok = dbl > 1e-14 * fmax(l1 * l1, 1e-300) && isfinite(dbl) && l1 > 0.0;
+    w[0] = w[1] = w[2] = 0.0;
+    if (!ok) return;
+    const double ld = fmax(l1, 1e-30), dd = fmax(dbl, 1e-30);
+    const double exx = e1x / ld, exy = e1y / ld, exz = e1z / ld;
+    const double mx = nx / dd, my = ny / dd, mz = nz / dd;
+    const double eyx = my * exz - mz * exy, eyy = mz * exx - mx * exz, eyz = mx * exy - my * exx;
+    const double X[3][2] = {{0.0, 0.0}, {l1, 0.0}, {e2x * exx + e2y * exy + e2z * exz, e2x * eyx + e2y * eyy + e2z * eyz}};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int i = (k + 1) % 3, j = (k + 2) % 3;
+        const double ax = X[i][0] - X[k][0], ay = X[i][1] - X[k][1];
+        const double bx = X[j][0] - X[k][0], by = X[j][1] - X[k][1];
+        const double cr = fmax(fabs(ax * by - ay * bx), 1e-30);
+        double c = (ax * bx + ay * by) / cr;
+        c = c < -1e4 ? -1e4 : (c > 1e4 ? 1e4 : c);
+        w[k] = 0.5 * c;
+    }
+}
+
+__global__ void k_hl_faces(HlArgs a, HlScratch s) {
+    const int64_t f = static_cast<int64_t>(blockIdx.x) * kTB + threadIdx.x;
+    uint64_t wm = 0;
+    if (f < a.t) {
+        double w[3] = {0.0, 0.0, 0.0};
+        const int32_t fid = a.faces[f];
+        if (fid < 0 || fid >= a.nf) {
+            flag(s.err, 2);
+        } else {
+            const int32_t* Fr = a.F + 3 * static_cast<int64_t>(fid);
+            if (Fr[0] < 0 || Fr[0] >= a.nvp || Fr[1] < 0 || Fr[1] >= a.nvp || Fr[2] < 0 || Fr[2] >= a.nvp)
+                flag(s.err, 2);
+            else
+                face_cots(a.V, Fr, w);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            s.w[3 * f + k] = w[k];
+            const uint64_t bits = static_cast<uint64_t>(__double_as_longlong(fabs(w[k])));
+            wm = bits > wm ? bits : wm;   // |w| >= 0: the bit patterns order like the values, NaN above all
+            const int32_t c = a.CV[3 * f + k];
+            if (c < 0 || c >= a.nv) {
+                flag(s.err, 2);
+                s.ckey[3 * f + k] = static_cast<uint32_t>(a.nv);   // sorts after every vertex
+            } else {
+                atomicMax(s.lastf + c, static_cast<int32_t>(f));
+                atomicAdd(s.vcnt + c, 1);
+                s.ckey[3 * f + k] = static_cast<uint32_t>(c);
+            }
+            s.cval[3 * f + k] = static_cast<uint32_t>(3 * f + k);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const uint64_t y = __shfl_xor_sync(0xffffffffu, wm, o);
+        wm = y > wm ? y : wm;
+    }
+    if ((threadIdx.x & 31) == 0 && wm) atomicMax(reinterpret_cast<unsigned long long*>(s.wmax), wm);
+}
+
+__global__ void k_hl_vchart(HlArgs a, HlScratch s) {
+    const int64_t v = static_cast<int64_t>(blockIdx.x) * kTB + threadIdx.x;
+    if (v >= a.nv) return;
+    const int32_t lf = s.lastf[v];
+    int32_t c = -1;
+    if (lf >= 0) {
+        c = a.chart[lf];
+        if (c < 0 || c >= a.nchart) {
+            flag(s.err, 4);
+            c = -1;
+        }
+    }
+    s.cv[v] = c;
+    s.vkey[v] = static_cast<uint32_t>(c >= 0 ? c : a.nchart);
+    s.vval[v] = static_cast<uint32_t>(v);
+    if (c >= 0) atomicAdd(s.ccnt + c, 1);
+}
+
+// float32 key of a pin candidate as an unsigned word in the order of the
+// values (-0 and +0 equal); NaN gets `nan_word`.
+__device__ __forceinline__ uint32_t key_word(double u, uint32_t nan_word) {
+    float k = __double2float_rn(u);
+    if (isnan(k)) return nan_word;
+    if (k == 0.0f) k = 0.0f;
+    const uint32_t b = __float_as_uint(k);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__global__ void k_hl_check(HlArgs a, HlScratch s) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * kTB + threadIdx.x;
+    if (i < a.t) {   // a face's corners in one chart (else the system couples two charts)
+        const int32_t c0 = a.CV[3 * i], c1 = a.CV[3 * i + 1], c2 = a.CV[3 * i + 2];
+        if (c0 >= 0 && c0 < a.nv && c1 >= 0 && c1 < a.nv && c2 >= 0 && c2 < a.nv) {
+            const int32_t k0 = s.cv[c0], k1 = s.cv[c1], k2 = s.cv[c2];
+            if (k0 != k1 || k1 != k2) flag(s.err, 1);
+        }
+        return;
+    }
+    const int64_t e = i - a.t;
+    if (e >= a.nb) return;
+    const int32_t u = a.ba[e], v = a.bb[e];
+    const bool uok = u >= 0 && u < a.nv, vok = v >= 0 && v < a.nv;
+    if (!uok || !vok) flag(s.err, 2);
+    s.bkey[e] = static_cast<uint32_t>(uok ? u : a.nv);
+    s.bkey[a.nb + e] = static_cast<uint32_t>(vok ? v : a.nv);
+    s.bval[e] = static_cast<uint32_t>(e);
+    s.bval[a.nb + e] = static_cast<uint32_t>(a.nb + e);
+    if (uok) atomicAdd(s.bcnt + u, 1);
+    if (vok) atomicAdd(s.bcnt + v, 1);
+    if (!uok || !vok) return;
+    const int32_t cu = s.cv[u], cvv = s.cv[v];
+    if (cu >= 0 && cvv >= 0 && cu != cvv) flag(s.err, 1);
+    if (cu < 0) return;
+    // pins: smallest key first, then smallest vertex; largest key first (NaN
+    // last), then smallest vertex
+    const double u0 = a.U0[2 * static_cast<int64_t>(u)];
+    const uint64_t lo = static_cast<uint64_t>(static_cast<uint32_t>(u));
+    atomicMin(reinterpret_cast<unsigned long long*>(s.pmin + cu),
+              (static_cast<uint64_t>(key_word(u0, 0xFFFFFFFFu)) << 32) | lo);
+    atomicMin(reinterpret_cast<unsigned long long*>(s.pmax + cu),
+              (static_cast<uint64_t>(0xFFFFFFFFu - key_word(u0, 0u)) << 32) | lo);
+}
+
+__global__ void k_hl_pins(HlArgs a, HlScratch s) {
+    const int64_t c = static_cast<int64_t>(blockIdx.x) * kTB + threadIdx.x;
+    if (c >= a.nchart) return;
+    if (s.pmin[c] != kNoPin) atomicAdd(s.npin + static_cast<uint32_t>(s.pmin[c]), 1);
+    if (s.pmax[c] != kNoPin) atomicAdd(s.npin + static_cast<uint32_t>(s.pmax[c]), 1);
+}
+
+// Unknown numbers of every UV vertex from the chart-sorted vertex list, and
+// the first row of every chart's block.
+__global__ void k_hl_rank(HlArgs a, HlScratch s) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * kTB + threadIdx.x;
+    if (i <= a.nchart) s.sys_ofs[i] = 2 * s.cofs[i];
+    if (i >= a.nv) return;
+    const uint32_t c = s.vkey_s[i], v = s.vval_s[i];
+    if (c >= static_cast<uint32_t>(a.nchart)) {
+        s.unk[v] = make_int2(-1, -1);
+        return;
+    }
+    const int32_t loc = static_cast<int32_t>(i) - s.cofs[c];
+    const int32_t base = 2 * s.cofs[c];
+    s.unk[v] = make_int2(base + loc, base + s.ccnt[c] + loc);
+}
+
+// The entries of vertex v's u row and v row (the same length): FILL false
+// counts them, FILL true writes them.
+template <bool FILL>
+__global__ void k_hl_rows(HlArgs a, HlScratch s) {
+    const int64_t v = static_cast<int64_t>(blockIdx.x) * kTB + threadIdx.x;
+    if (v >= a.nv) return;
+    const int2 me = s.unk[v];
+    if (me.x < 0) return;
+    const int32_t c = s.cv[v];
+    int32_t ku = 0, kv = 0;
+    if (FILL) {
+        ku = s.rowptr[me.x];
+        kv = s.rowptr[me.y];
+        s.ci[ku++] = me.x;   // the diagonal first; its value at the end
+        s.ci[kv++] = me.y;
+    }
+    int32_t len = 1;
+    double d = 0.0;
+    const int32_t c0 = s.vofs[v], c1 = c0 + s.vcnt[v];
+    for (int32_t p = c0; p < c1; ++p) {
+        const uint32_t j = s.cval_s[p];
+        const int64_t f = j / 3;
+        const int k = static_cast<int>(j - 3 * f);
+        // corner k lies on edge (k+2)%3 (to corner k+1) and edge (k+1)%3 (to corner k+2)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int e = h == 0 ? (k + 2) % 3 : (k + 1) % 3;
+            const int32_t nb = a.CV[3 * f + (h == 0 ? (k + 1) % 3 : (k + 2) % 3)];
+            const double we = s.w[3 * f + e];
+            d += we;
+            if (nb < 0 || nb >= a.nv || s.cv[nb] != c) continue;
+            ++len;
+            if (FILL) {
+                const int2 o = s.unk[nb];
+                s.ci[ku] = o.x; s.va[ku++] = -we;
+                s.ci[kv] = o.y; s.va[kv++] = -we;
+            }
+        }
+    }
+    const int32_t b0 = s.bofs[v], b1 = b0 + s.bcnt[v];
+    for (int32_t p = b0; p < b1; ++p) {
+        const uint32_t j = s.bval_s[p];
+        const bool is_a = j < static_cast<uint32_t>(a.nb);   // v is the edge's start
+        const int64_t e = is_a ? j : j - a.nb;
+        const int32_t o = is_a ? a.bb[e] : a.ba[e];
+        if (o < 0 || o >= a.nv || s.cv[o] != c) continue;
+        ++len;
+        if (FILL) {
+            const int2 q = s.unk[o];
+            s.ci[ku] = q.y; s.va[ku++] = is_a ? -0.5 : 0.5;
+            s.ci[kv] = q.x; s.va[kv++] = is_a ? 0.5 : -0.5;
+        }
+    }
+    if (!FILL) {
+        s.rowlen[me.x] = len;
+        s.rowlen[me.y] = len;
+        return;
+    }
+    const double wm = __longlong_as_double(static_cast<long long>(*s.wmax));
+    const double wpin = 10.0 * (isnan(wm) ? wm : (wm > 1e-12 ? wm : 1e-12));
+    const int np = s.npin[v];
+    const double ux = a.U0[2 * v], uy = a.U0[2 * v + 1];
+    double bx = 0.0, by = 0.0;
+    for (int q = 0; q < np; ++q) {
+        d += wpin;
+        bx += wpin * ux;
+        by += wpin * uy;
+    }
+    s.va[s.rowptr[me.x]] = d;
+    s.va[s.rowptr[me.y]] = d;
+    s.b[me.x] = bx; s.b[me.y] = by;
+    s.x[me.x] = ux; s.x[me.y] = uy;
+}
+
+__global__ void k_hl_out(HlArgs a, HlScratch s, double* U) {
+    const int64_t v = static_cast<int64_t>(blockIdx.x) * kTB + threadIdx.x;
+    if (v >= a.nv) return;
+    const int2 me = s.unk[v];
+    const double ux = a.U0[2 * v], uy = a.U0[2 * v + 1];
+    double x = ux, y = uy;
+    if (me.x >= 0) { x = s.x[me.x]; y = s.x[me.y]; }
+    U[2 * v] = isfinite(x) ? x : ux;
+    U[2 * v + 1] = isfinite(y) ? y : uy;
+}
+
+bool hl_args_ok(const HlArgs& a) {
+    if (a.nv < 0 || a.t < 0 || a.nb < 0 || a.nchart < 0 || a.nvp < 0 || a.nf < 0) return false;
+    if (a.t > 0 && (!a.faces || !a.CV || !a.chart || !a.V || !a.F)) return false;
+    if (a.nb > 0 && (!a.ba || !a.bb)) return false;
+    if (a.nv > 0 && !a.U0) return false;
+    return true;
+}
+
+bool hl_fits(const HlArgs& a) {   // int32 rows, entries and sort items
+    const int64_t lim = INT32_MAX / 2;
+    return a.nv < lim / 2 && 3 * a.t < lim && 2 * a.nb < lim && 2 * (a.nv + 6 * a.t + 2 * a.nb) < lim &&
+           a.nchart < lim;
+}
+
+}  // namespace
+
+extern "C" int uva_hier_lscm_scratch_bytes(int64_t nv, int64_t t, int64_t nb, int32_t nchart, int64_t* bytes) {
+    HlArgs a{};
+    a.nv = nv; a.t = t; a.nb = nb; a.nchart = nchart;
+    if (!bytes || nv < 0 || t < 0 || nb < 0 || nchart < 0) {
+        uva_set_error("uva_hier_lscm_scratch_bytes: bad arguments");
+        return UVA_E_ARG;
+    }
+    if (!hl_fits(a)) { uva_set_error("uva_hier_lscm_scratch_bytes: too large for int32 indices"); return UVA_E_TOOBIG; }
+    *bytes = static_cast<int64_t>(hl_layout(a, nullptr, nullptr));
+    return UVA_OK;
+}
+
+extern "C" int uva_hier_lscm(const double* V, int64_t nvp, const int32_t* F, int64_t nf, const int32_t* faces,
+                             const int32_t* CV, const int32_t* chart, int64_t t, int64_t nv, int32_t nchart,
+                             const double* U0, const int32_t* ba, const int32_t* bb, int64_t nb, double tol,
+                             int32_t maxiter, void* scratch, int64_t scratch_bytes, double* U, int32_t* flags,
+                             void* stream) {
+    HlArgs a{V, F, faces, CV, chart, U0, ba, bb, nvp, nf, t, nv, nb, nchart};
+    if (!hl_args_ok(a) || !flags || (nv > 0 && (!U || !scratch)) || maxiter < 0) {
+        uva_set_error("uva_hier_lscm: bad arguments");
+        return UVA_E_ARG;
+    }
+    if (!hl_fits(a)) { uva_set_error("uva_hier_lscm: too large for int32 indices"); return UVA_E_TOOBIG; }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(flags, 0, sizeof(int32_t), st) != cudaSuccess) return uva_cuda_status(cudaGetLastError(), "uva_hier_lscm");
+    if (nv == 0) return UVA_OK;
+    HlScratch s{};
+    const size_t need = hl_layout(a, static_cast<char*>(scratch), &s);
+    if (scratch_bytes < static_cast<int64_t>(need)) { uva_set_error("uva_hier_lscm: scratch too small"); return UVA_E_ARG; }
+    s.err = flags;
+    auto zero = [&](void* p, size_t bytes) { return cudaMemsetAsync(p, 0, bytes, st); };
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    ok(cudaMemsetAsync(s.lastf, 0xFF, 4 * nv, st));
+    ok(zero(s.ccnt, 4 * (nchart + 1)));
+    ok(zero(s.npin, 4 * nv));
+    ok(zero(s.vcnt, 4 * (nv + 1)));
+    ok(zero(s.bcnt, 4 * (nv + 1)));
+    ok(zero(s.rowlen, 4 * (2 * nv + 1)));
+    ok(zero(s.wmax, 8));
+    if (nchart > 0) {
+        ok(cudaMemsetAsync(s.pmin, 0xFF, 8 * static_cast<size_t>(nchart), st));
+        ok(cudaMemsetAsync(s.pmax, 0xFF, 8 * static_cast<size_t>(nchart), st));
+    }
+    if (e != cudaSuccess) return uva_cuda_status(e, "uva_hier_lscm/memset");
+    if (t > 0) k_hl_faces<<<blocks_for(t), kTB, 0, st>>>(a, s);
+    k_hl_vchart<<<blocks_for(nv), kTB, 0, st>>>(a, s);
+    if (t + nb > 0) k_hl_check<<<blocks_for(t + nb), kTB, 0, st>>>(a, s);
+    if (nchart > 0) k_hl_pins<<<blocks_for(nchart), kTB, 0, st>>>(a, s);
+    UVA_CHECK_LAUNCH("uva_hier_lscm/faces");
+    // stable radix sorts: vertices by chart (then id), corners and boundary ends by vertex (then position)
+    size_t cb = s.cub_bytes;
+    ok(cub::DeviceRadixSort::SortPairs(s.cub, cb, s.vkey, s.vkey_s, s.vval, s.vval_s, static_cast<int>(nv), 0,
+                                       bits_for(nchart), st));
+    if (t > 0) {
+        cb = s.cub_bytes;
+        ok(cub::DeviceRadixSort::SortPairs(s.cub, cb, s.ckey, s.ckey_s, s.cval, s.cval_s, static_cast<int>(3 * t), 0,
+                                           bits_for(nv), st));
+    }
+    if (nb > 0) {
+        cb = s.cub_bytes;
+        ok(cub::DeviceRadixSort::SortPairs(s.cub, cb, s.bkey, s.bkey_s, s.bval, s.bval_s, static_cast<int>(2 * nb), 0,
+                                           bits_for(nv), st));
+    }
+    if (e != cudaSuccess) return uva_cuda_status(e, "uva_hier_lscm/sort");
+    xscan<int32_t>(s.ccnt, s.cofs, s.isums, nullptr, nchart + 1, st);
+    xscan<int32_t>(s.vcnt, s.vofs, s.isums, nullptr, nv + 1, st);
+    xscan<int32_t>(s.bcnt, s.bofs, s.isums, nullptr, nv + 1, st);
+    k_hl_rank<<<blocks_for(std::max<int64_t>(nv, nchart + 1)), kTB, 0, st>>>(a, s);
+    k_hl_rows<false><<<blocks_for(nv), kTB, 0, st>>>(a, s);
+    xscan<int32_t>(s.rowlen, s.rowptr, s.isums, nullptr, 2 * nv + 1, st);
+    k_hl_rows<true><<<blocks_for(nv), kTB, 0, st>>>(a, s);
+    UVA_CHECK_LAUNCH("uva_hier_lscm/assemble");
+    if (nchart > 0) {
+        const int rc = uva_csr_pcg_blocks(nchart, s.sys_ofs, static_cast<int32_t>(2 * nv), s.rowptr, s.ci, s.va, s.b,
+                                          s.x, tol, maxiter, s.pcg, s.its, stream);
+        if (rc != UVA_OK) return rc;
+    }
+    k_hl_out<<<blocks_for(nv), kTB, 0, st>>>(a, s, U);
+    UVA_CHECK_LAUNCH("uva_hier_lscm/out");
+    return UVA_OK;
+}

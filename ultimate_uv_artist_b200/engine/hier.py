@@ -186,10 +186,11 @@ class Solver:
     residual checked in FP64, where the reference runs ``cg_iters`` (20)
     Jacobi-CG iterations on the whole subset in FP32; ``cg_iters`` is kept
     for signature compatibility. ``lscm`` assembles the reference's
-    soft-pinned LSCM system on the host and solves it with the FP64
-    Jacobi-PCG kernel, one CTA per chart (uva_csr_pcg_blocks), to a 1e-10
-    relative residual per chart, where the reference stops its FP32 CG on
-    the whole system at 1e-6 or 600 iterations.
+    soft-pinned LSCM system on the device (uva_hier_lscm: weights, pins,
+    unknowns grouped by chart, CSR) and solves it with the FP64 Jacobi-PCG
+    kernel, one CTA per chart, to a 1e-10 relative residual per chart, where
+    the reference stops its FP32 CG on the whole system at 1e-6 or 600
+    iterations.
     """
 
     def __init__(self, topo, dev=None):
@@ -296,118 +297,61 @@ class Solver:
     def lscm(self, faces, CV, nv, chart, nchart, U0, ba, bb, iters=600):
         """Free-boundary conformal map of every chart at once: the LSCM energy
         with two soft pins per chart, the boundary vertices of smallest and
-        largest initial u (engine/hier.py:511-583). ``iters`` is accepted for
+        largest initial u (engine/hier.py:534-585). The system is assembled
+        and solved on the device (uva_hier_lscm); ``iters`` is accepted for
         signature compatibility (see the class docstring)."""
         import ctypes as C
-        import scipy.sparse as sp
         import torch
         from .. import _lib
         nv, nchart = int(nv), int(nchart)
-        faces = np.asarray(faces, np.int64)
+        faces = np.asarray(faces, np.int64).reshape(-1)
         CV = np.asarray(CV, np.int64).reshape(-1, 3)
-        chart = np.asarray(chart, np.int64)
-        U0 = np.asarray(U0, np.float64).reshape(-1, 2)
-        ba = np.asarray(ba, np.int64); bb = np.asarray(bb, np.int64)
+        chart = np.asarray(chart, np.int64).reshape(-1)
+        U0 = np.ascontiguousarray(np.asarray(U0, np.float64).reshape(-1, 2))
+        ba = np.asarray(ba, np.int64).reshape(-1); bb = np.asarray(bb, np.int64).reshape(-1)
         if nv == 0:
             return U0.copy()
-        # cot weights of the faces, like the batch setup (engine/gpu.py:88-116)
-        w = _face_cots(self.V, self.F[faces])
-        I = np.concatenate([CV[:, 1], CV[:, 2], CV[:, 0]])
-        J = np.concatenate([CV[:, 2], CV[:, 0], CV[:, 1]])
-        Wl = np.concatenate([w[:, 0], w[:, 1], w[:, 2]])
-        hb = np.full(len(ba), 0.5)
-        rows = [I, J, I, J, I + nv, J + nv, I + nv, J + nv, ba, bb, ba + nv, bb + nv]
-        cols = [J, I, I, J, J + nv, I + nv, I + nv, J + nv, bb + nv, ba + nv, bb, ba]
-        vals = [-Wl, -Wl, Wl, Wl, -Wl, -Wl, Wl, Wl, -hb, hb, hb, -hb]
-        # two pins per chart: boundary vertices extreme along the initial u axis
-        cv = -np.ones(nv, np.int64)
-        if len(CV):
-            rev = CV.reshape(-1)[::-1]
-            uniq, first = np.unique(rev, return_index=True)
-            cv[uniq] = np.repeat(chart, 3)[::-1][first]
-        bv = np.unique(ba)
-        pins = []
-        if len(bv):
-            key = U0[bv, 0].astype(np.float32)      # the reference compares float32 keys
-            cb = cv[bv]
-            o_mn = np.lexsort((bv, key, cb))          # per chart: smallest u first
-            o_mx = np.lexsort((bv, -key, cb))         # per chart: largest u first
-            first_mn = o_mn[np.r_[True, cb[o_mn][1:] != cb[o_mn][:-1]]]
-            first_mx = o_mx[np.r_[True, cb[o_mx][1:] != cb[o_mx][:-1]]]
-            pins = np.concatenate([bv[first_mn], bv[first_mx]])
-        pins = np.asarray(pins, np.int64)
-        wpin = max(np.abs(Wl).max() if len(Wl) else 0.0, 1e-12) * 10
-        rows += [pins, pins + nv]; cols += [pins, pins + nv]; vals += [np.full(2 * len(pins), wpin)]
-        H = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
-                          shape=(2 * nv, 2 * nv)).tocsr()
-        H.sum_duplicates()
-        H.sort_indices()
-        b = np.zeros(2 * nv)
-        np.add.at(b, pins, wpin * U0[pins, 0])
-        np.add.at(b, pins + nv, wpin * U0[pins, 1])
-        x0 = np.concatenate([U0[:, 0], U0[:, 1]])
-        # unknowns of UV vertices that no face names have no equation: they
-        # keep U0. The system is block-diagonal by chart: each chart's u and v
-        # unknowns form one block, solved by its own CTA.
-        used = np.zeros(2 * nv, bool)
-        used[np.concatenate([CV.reshape(-1), CV.reshape(-1) + nv])] = True
-        idx = np.nonzero(used)[0]
-        if len(idx) == 0:
-            return U0.copy()
-        uc = np.concatenate([cv, cv])[idx]                 # chart of every unknown
-        idx = idx[np.argsort(uc, kind="stable")]
-        sys_ofs = np.zeros(nchart + 1, np.int64)
-        np.cumsum(np.bincount(np.concatenate([cv, cv])[idx], minlength=nchart), out=sys_ofs[1:])
-        H = H[idx][:, idx].tocsr()
-        H.sort_indices()
-        blk = np.repeat(np.arange(nchart), np.diff(sys_ofs))   # block of every (permuted) unknown
-        if len(H.indices) and (blk[H.indices] != np.repeat(blk, np.diff(H.indptr))).any():
-            raise ValueError("hier.Solver.lscm: a UV vertex is shared by faces of different charts")
-        b = b[idx]
-        x_all = x0.copy()
-        x0 = x0[idx]
+        t, nb = len(faces), len(ba)
+        if len(CV) != t or len(chart) != t or len(bb) != nb or len(U0) != nv:
+            raise ValueError("hier.Solver.lscm: faces, CV, chart, ba / bb or U0 of inconsistent lengths")
+        for name, a, hi in (("faces", faces, len(self.F)), ("CV", CV, nv), ("ba", ba, nv), ("bb", bb, nv)):
+            if a.size and (a.min() < -hi or a.max() >= hi):
+                raise IndexError(f"hier.Solver.lscm: {name} out of range")
+        # negative indices count from the end, as numpy indexing does
+        faces = np.where(faces < 0, faces + len(self.F), faces)
+        CV = np.where(CV < 0, CV + nv, CV)
+        ba = np.where(ba < 0, ba + nv, ba); bb = np.where(bb < 0, bb + nv, bb)
         d = self.dev
-        rp = torch.from_numpy(H.indptr.astype(np.int32)).to(d)
-        ci = torch.from_numpy(H.indices.astype(np.int32)).to(d)
-        va = torch.from_numpy(H.data.astype(np.float64)).to(d)
-        bd = torch.from_numpy(b).to(d)
-        xd = torch.from_numpy(x0).to(d)
-        so = torch.from_numpy(sys_ofs.astype(np.int32)).to(d)
-        N = len(idx)
-        scratch = torch.empty(3 * N, dtype=torch.float64, device=d)
-        its = torch.zeros(max(nchart, 1), dtype=torch.int32, device=d)
+        Vd, Fd = self._mesh_on_device()
+        up = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dt)).to(d)
+        fd, cvd, chd = up(faces, np.int32), up(CV, np.int32), up(chart, np.int32)
+        bad, bbd, u0d = up(ba, np.int32), up(bb, np.int32), up(U0, np.float64)
         L = _lib.lib()
+        nbytes = C.c_int64()
+        _lib.check(L.uva_hier_lscm_scratch_bytes(nv, t, nb, nchart, C.byref(nbytes)), "uva_hier_lscm_scratch_bytes")
+        scratch = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=d)
+        out = torch.empty((nv, 2), dtype=torch.float64, device=d)
+        flags = torch.empty(1, dtype=torch.int32, device=d)
         st = torch.cuda.current_stream(d)
-        _lib.check(L.uva_csr_pcg_blocks(nchart, so.data_ptr(), N, rp.data_ptr(), ci.data_ptr(), va.data_ptr(),
-                                        bd.data_ptr(), xd.data_ptr(), 1e-10, max(20000, 40 * int(np.sqrt(N))),
-                                        scratch.data_ptr(), its.data_ptr(), C.c_void_p(st.cuda_stream)),
-                   "uva_csr_pcg_blocks")
-        x_all[idx] = xd.cpu().numpy()
-        U = np.stack([x_all[:nv], x_all[nv:]], 1)
-        return np.where(np.isfinite(U), U, U0)
+        maxiter = max(20000, 40 * int(np.sqrt(2 * nv)))
+        _lib.check(L.uva_hier_lscm(Vd.data_ptr(), len(self.V), Fd.data_ptr(), len(self.F), fd.data_ptr(),
+                                   cvd.data_ptr(), chd.data_ptr(), t, nv, nchart, u0d.data_ptr(), bad.data_ptr(),
+                                   bbd.data_ptr(), nb, 1e-10, maxiter, scratch.data_ptr(), int(nbytes.value),
+                                   out.data_ptr(), flags.data_ptr(), C.c_void_p(st.cuda_stream)), "uva_hier_lscm")
+        U = out.cpu().numpy()
+        f = int(flags.item())
+        if f & 6:
+            raise ValueError("hier.Solver.lscm: a mesh face index or chart id out of range")
+        if f & 1:
+            raise ValueError("hier.Solver.lscm: a UV vertex is shared by faces of different charts")
+        return U
 
-
-def _face_cots(V, Ff):
-    """Half cotangent weights (t, 3) of edge k (opposite corner k), 0 for
-    triangles too thin for a frame (engine/hier.py:362-382)."""
-    p0, p1, p2 = V[Ff[:, 0]], V[Ff[:, 1]], V[Ff[:, 2]]
-    e1 = p1 - p0; e2 = p2 - p0
-    l1 = np.linalg.norm(e1, axis=1)
-    nrm = np.cross(e1, e2)
-    dbl = np.linalg.norm(nrm, axis=1)
-    ok = (dbl > 1e-14 * np.maximum(l1 * l1, 1e-300)) & np.isfinite(dbl) & (l1 > 0)
-    with np.errstate(divide="ignore", invalid="ignore"):
-        ex = e1 / np.maximum(l1, 1e-30)[:, None]
-        ey = np.cross(nrm / np.maximum(dbl, 1e-30)[:, None], ex)
-    X = np.zeros((len(Ff), 3, 2))
-    X[:, 1, 0] = l1; X[:, 2, 0] = (e2 * ex).sum(1); X[:, 2, 1] = (e2 * ey).sum(1)
-    X[~ok] = 0
-    cots = []
-    for k in range(3):
-        i, j, o = (k + 1) % 3, (k + 2) % 3, k
-        a = X[:, i] - X[:, o]; b = X[:, j] - X[:, o]
-        cr = np.maximum(np.abs(a[:, 0] * b[:, 1] - a[:, 1] * b[:, 0]), 1e-30)
-        cots.append(np.clip((a * b).sum(1) / cr, -1e4, 1e4))
-    w = 0.5 * np.stack(cots, 1)
-    w[~ok] = 0
-    return w
+    def _mesh_on_device(self):
+        """The mesh's positions (FP64) and faces (int32) on the device, once."""
+        import torch
+        if getattr(self, "_dmesh", None) is None:
+            if len(self.F) and (self.F.min() < 0 or self.F.max() >= len(self.V)):
+                raise IndexError("hier.Solver: mesh faces out of range")
+            self._dmesh = (torch.from_numpy(np.ascontiguousarray(self.V)).to(self.dev),
+                           torch.from_numpy(np.ascontiguousarray(self.F, np.int32)).to(self.dev))
+        return self._dmesh
