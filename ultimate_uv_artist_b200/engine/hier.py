@@ -212,10 +212,8 @@ class Solver:
         if n and (CV.min() < 0 or CV.max() >= nv or chart.min() < 0 or chart.max() >= nchart):
             raise ValueError("hier.Solver: CV or chart out of range")
         vchart = -np.ones(nv, np.int64)
-        if n:
-            rev = CV.reshape(-1)[::-1]
-            uniq, first = np.unique(rev, return_index=True)
-            vchart[uniq] = np.repeat(chart, 3)[::-1][first]
+        if n:   # any naming face's chart: the check below rejects vertices named by two charts
+            vchart[CV.reshape(-1)] = np.repeat(chart, 3)
         if n and (vchart[CV] != chart[:, None]).any():
             raise ValueError("hier.Solver: a UV vertex is shared by faces of different charts")
         used = np.nonzero(vchart >= 0)[0]
@@ -229,8 +227,10 @@ class Solver:
         np.cumsum(np.bincount(chart, minlength=nchart), out=tofs[1:])
         Tb = newid[CV[forder]]
         T_local = Tb - vofs[chart[forder]][:, None]
-        P = np.empty((len(order), 3))
-        P[newid[CV.reshape(-1)]] = self.V[self.F[faces][:, [0, 1, 2]].reshape(-1)]
+        corner = np.empty(nv, np.int64)   # a corner naming each UV vertex (the last one)
+        corner[CV.reshape(-1)] = np.arange(3 * n)
+        c = corner[order]
+        P = self.V[self.F[faces[c // 3], c % 3]]
         return order, P, T_local, vofs, tofs, forder
 
     # ---------------------------------------------------------------- relax
