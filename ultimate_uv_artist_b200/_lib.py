@@ -110,6 +110,7 @@ _SIGS = {
     "uva_shrink": [vp, vp, vp, i32, C.c_float, C.c_float, vp],
     "uva_seg_scratch_bytes": [i32, i32, vp],
     "uva_csr_pcg_blocks": [i32, vp, i32, vp, vp, vp, vp, vp, C.c_double, i32, vp, vp, vp],
+    "uva_hier_boundary_corners": [vp, vp, C.c_int64, vp, vp, vp, vp, C.c_int64, C.c_int64, vp, vp, vp, vp],
     "uva_hier_lscm_scratch_bytes": [C.c_int64, C.c_int64, C.c_int64, i32, vp],
     "uva_hier_lscm": [vp, C.c_int64, vp, C.c_int64, vp, vp, vp, C.c_int64, C.c_int64, i32, vp, vp, vp, C.c_int64,
                       C.c_double, i32, vp, C.c_int64, vp, vp, vp],

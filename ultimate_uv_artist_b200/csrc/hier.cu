@@ -391,6 +391,52 @@ __global__ void k_hl_out(HlArgs a, HlScratch s, double* U) {
     U[2 * v + 1] = isfinite(y) ? y : uy;
 }
 
+// Boundary corners of hier.chart_checks / boundary_directed
+// (engine/hier.py:275-291): corner edge k of local face i is interior when
+// the face g across it (FF) is in the subset (loc[g] = j >= 0) and in the
+// same chart, and g's first corner on the mesh vertex F[f, k] carries the
+// same UV vertex. Also the last corner (face order) naming each UV vertex.
+__global__ void k_hl_isb(const int32_t* F, const int32_t* FF, int64_t nf, const int32_t* faces, const int32_t* loc,
+                         const int32_t* chart, const int32_t* CV, int64_t n, int64_t nv, uint8_t* isb,
+                         int32_t* lastc, int32_t* err) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * kTB + threadIdx.x;
+    if (i >= n) return;
+    const int32_t f = faces[i];
+    const bool fok = f >= 0 && f < nf;
+    if (!fok) flag(err, 2);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int32_t cvk = CV[3 * i + k];
+        if (nv > 0) {   // nv = 0: no vertex charts wanted
+            if (cvk < 0 || cvk >= nv) flag(err, 2);
+            else atomicMax(lastc + cvk, static_cast<int32_t>(3 * i + k));
+        }
+        uint8_t b = 1;
+        const int32_t g = fok ? FF[3 * static_cast<int64_t>(f) + k] : -1;
+        if (g >= nf) {
+            flag(err, 2);
+        } else if (g >= 0) {
+            const int32_t j = loc[g];
+            if (j >= n) {
+                flag(err, 2);
+            } else if (j >= 0 && chart[j] == chart[i]) {
+                const int32_t v = F[3 * static_cast<int64_t>(f) + k];
+                const int32_t* Fg = F + 3 * static_cast<int64_t>(g);
+                const int kk = Fg[0] == v ? 0 : (Fg[1] == v ? 1 : (Fg[2] == v ? 2 : -1));
+                if (kk >= 0 && CV[3 * static_cast<int64_t>(j) + kk] == cvk) b = 0;
+            }
+        }
+        isb[3 * i + k] = b;
+    }
+}
+
+__global__ void k_hl_lastc_chart(int64_t nv, const int32_t* chart, int32_t* vchart) {
+    const int64_t v = static_cast<int64_t>(blockIdx.x) * kTB + threadIdx.x;
+    if (v >= nv) return;
+    const int32_t c = vchart[v];   // the last corner naming v, or -1
+    vchart[v] = c >= 0 ? chart[c / 3] : -1;
+}
+
 bool hl_args_ok(const HlArgs& a) {
     if (a.nv < 0 || a.t < 0 || a.nb < 0 || a.nchart < 0 || a.nvp < 0 || a.nf < 0) return false;
     if (a.t > 0 && (!a.faces || !a.CV || !a.chart || !a.V || !a.F)) return false;
@@ -487,5 +533,28 @@ extern "C" int uva_hier_lscm(const double* V, int64_t nvp, const int32_t* F, int
     }
     k_hl_out<<<blocks_for(nv), kTB, 0, st>>>(a, s, U);
     UVA_CHECK_LAUNCH("uva_hier_lscm/out");
+    return UVA_OK;
+}
+
+extern "C" int uva_hier_boundary_corners(const int32_t* F, const int32_t* FF, int64_t nf, const int32_t* faces,
+                                         const int32_t* loc, const int32_t* chart, const int32_t* CV, int64_t n,
+                                         int64_t nv, uint8_t* isb, int32_t* vchart, int32_t* flags, void* stream) {
+    if (n < 0 || nv < 0 || nf < 0 || !flags || (n > 0 && (!F || !FF || !faces || !loc || !chart || !CV || !isb)) ||
+        (nv > 0 && !vchart)) {
+        uva_set_error("uva_hier_boundary_corners: bad arguments");
+        return UVA_E_ARG;
+    }
+    if (3 * n >= INT32_MAX || nf >= INT32_MAX / 3) {
+        uva_set_error("uva_hier_boundary_corners: too large for int32 indices");
+        return UVA_E_TOOBIG;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(flags, 0, sizeof(int32_t), st);
+    if (e == cudaSuccess && nv > 0) e = cudaMemsetAsync(vchart, 0xFF, 4 * static_cast<size_t>(nv), st);
+    if (e != cudaSuccess) return uva_cuda_status(e, "uva_hier_boundary_corners/memset");
+    if (n > 0)
+        k_hl_isb<<<blocks_for(n), kTB, 0, st>>>(F, FF, nf, faces, loc, chart, CV, n, nv, isb, vchart, flags);
+    if (nv > 0) k_hl_lastc_chart<<<blocks_for(nv), kTB, 0, st>>>(nv, chart, vchart);
+    UVA_CHECK_LAUNCH("uva_hier_boundary_corners");
     return UVA_OK;
 }

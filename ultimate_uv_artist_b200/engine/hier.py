@@ -20,32 +20,54 @@ import numpy as np
 from .. import segments
 
 
-def _boundary_corners(F, FF, faces, loc, chart, CV):
+def _boundary_corners(F, FF, faces, loc, chart, CV, nv=None):
     """isb (n, 3): corner edge k of local face i is a boundary edge unless the
     neighbour across it (FF) is a face of the same chart whose corner on the
     shared vertex F[f, k] (its first match) has the same UV vertex
-    (engine/hier.py:275-291)."""
-    F = np.asarray(F, np.int64)
-    FF = np.asarray(FF, np.int64)
-    faces = np.asarray(faces, np.int64)
-    loc = np.asarray(loc, np.int64)
-    chart = np.asarray(chart, np.int64)
+    (engine/hier.py:275-291). With ``nv``, also vchart (nv,): the chart of
+    the last corner (face order) naming each UV vertex, -1 for none. One
+    device pass (uva_hier_boundary_corners)."""
+    import ctypes as C
+    import torch
+    from .. import _lib
+    from ..device import require_cuda
+    F = np.asarray(F, np.int64).reshape(-1, 3)
+    FF = np.asarray(FF, np.int64).reshape(-1, 3)
+    faces = np.asarray(faces, np.int64).reshape(-1)
+    loc = np.asarray(loc, np.int64).reshape(-1)
+    chart = np.asarray(chart, np.int64).reshape(-1)
     CV = np.asarray(CV, np.int64).reshape(-1, 3)
-    n = len(faces)
+    n, nf = len(faces), len(F)
+    nvv = 0 if nv is None else int(nv)
     if n == 0:
-        return np.zeros((0, 3), bool)
-    g = FF[faces]                                   # (n, 3) neighbour faces
-    gs = np.where(g >= 0, g, 0)
-    j = np.where(g >= 0, loc[gs], -1)               # their local indices
-    js = np.where(j >= 0, j, 0)
-    same = (j >= 0) & (chart[js] == chart[:, None])
-    a = F[faces]                                    # (n, 3) corner vertices
-    match = F[gs] == a[:, :, None]                  # (n, 3, 3): F[g, kk] == F[f, k]
-    has = match.any(2)
-    kk = match.argmax(2)                            # first matching corner of g
-    cvj = CV[js, kk]
-    interior = same & has & (cvj == CV)
-    return ~interior
+        isb = np.zeros((0, 3), bool)
+        return isb if nv is None else (isb, -np.ones(nvv, np.int64))
+    if len(CV) != n or len(chart) != n or len(FF) != nf:
+        raise ValueError("hier: faces, CV, chart or FF of inconsistent lengths")
+    if faces.min() < -nf or faces.max() >= nf:
+        raise IndexError("hier: faces out of range")
+    faces = np.where(faces < 0, faces + nf, faces)        # numpy indexing counts from the end
+    if len(loc) < nf:   # only the neighbours' entries are read
+        if (FF[faces] >= len(loc)).any():
+            raise IndexError("hier: loc shorter than a neighbour face id")
+        loc = np.concatenate([loc, -np.ones(nf - len(loc), np.int64)])
+    dev = require_cuda(None)
+    up = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.int32)).to(dev)
+    Fd, FFd, fd, ld, cd, cvd = up(F), up(FF), up(faces), up(loc), up(chart), up(CV)
+    isb = torch.empty((n, 3), dtype=torch.uint8, device=dev)
+    vchart = torch.empty(max(nvv, 1), dtype=torch.int32, device=dev)
+    flags = torch.empty(1, dtype=torch.int32, device=dev)
+    st = torch.cuda.current_stream(dev)
+    _lib.check(_lib.lib().uva_hier_boundary_corners(Fd.data_ptr(), FFd.data_ptr(), nf, fd.data_ptr(), ld.data_ptr(),
+                                                    cd.data_ptr(), cvd.data_ptr(), n, nvv, isb.data_ptr(),
+                                                    vchart.data_ptr(), flags.data_ptr(), C.c_void_p(st.cuda_stream)),
+               "uva_hier_boundary_corners")
+    out = isb.cpu().numpy().astype(bool)
+    if int(flags.item()):
+        raise IndexError("hier: an FF, loc or CV index is out of range")
+    if nv is None:
+        return out
+    return out, vchart[:nvv].cpu().numpy().astype(np.int64)
 
 
 def boundary_directed(F, FF, faces, loc, chart, CV):
@@ -120,22 +142,18 @@ def chart_checks(F, FF, faces, loc, chart, CV, UV, nchart, nv):
 
 
 def _boundary_topology(F, FF, faces, loc, chart, CV, nchart, nv):
-    """The host half of chart_checks: (chi, loops, ba, bb, bc) with the
-    boundary edges ba -> bb of chart bc in face order."""
+    """chart_checks without the segment test: (chi, loops, ba, bb, bc) with
+    the boundary edges ba -> bb of chart bc in face order. The corner test
+    and the vertex charts run on the device; the per-chart counts and the
+    boundary loops on the host."""
     CV = np.asarray(CV, np.int64).reshape(-1, 3)
     chart = np.asarray(chart, np.int64)
     nchart, nv = int(nchart), int(nv)
     n = len(CV)
-    isb = _boundary_corners(F, FF, faces, loc, chart, CV)
+    # vchart[v]: chart of the last corner (face order) that names v
+    isb, vchart = _boundary_corners(F, FF, faces, loc, chart, CV, nv)
     Fc = np.bincount(chart, minlength=nchart).astype(np.int64) if n else np.zeros(nchart, np.int64)
     nb_c = np.bincount(chart, weights=isb.sum(1), minlength=nchart).astype(np.int64) if n else np.zeros(nchart, np.int64)
-    # vchart[v]: chart of the last corner (face order) that names v
-    flat = CV.reshape(-1)
-    vchart = -np.ones(nv, np.int64)
-    if n:
-        rev = flat[::-1]
-        uniq, first = np.unique(rev, return_index=True)
-        vchart[uniq] = np.repeat(chart, 3)[::-1][first]
     Vc = np.bincount(vchart[vchart >= 0], minlength=nchart).astype(np.int64)
     chi = Vc - (3 * Fc + nb_c) // 2 + Fc
     ba = CV[isb]
