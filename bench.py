@@ -65,6 +65,8 @@ def _args():
     ap.add_argument("--pack-charts", type=int, default=3000)
     ap.add_argument("--pack-only", action="store_true",
                     help="only the packing leg, as one JSON line (for launch lists of the packer)")
+    ap.add_argument("--hier-only", action="store_true",
+                    help="only the hier.Solver leg, as one JSON line (for launch lists of its kernels)")
     return ap.parse_args()
 
 
@@ -839,6 +841,12 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.hier_only:
+        if rank == 0:
+            print(json.dumps({"hier_solver": bench_hier(dev)}))
+        if ws > 1:
+            dist.destroy_process_group()
+        return
     if args.pack_only:
         if rank == 0:
             print(json.dumps({"pack": bench_pack(dev, args.pack_charts, cpu=not args.no_cpu_baseline)}))
