@@ -351,7 +351,7 @@ class Solver:
         out = torch.empty((nv, 2), dtype=torch.float64, device=d)
         flags = torch.empty(1, dtype=torch.int32, device=d)
         st = torch.cuda.current_stream(d)
-        maxiter = max(20000, 40 * int(np.sqrt(2 * nv)))
+        maxiter = max(20000, 40 * int(np.sqrt(2 * nv)))   # 2 nv bounds the unknowns (the used ones are counted on the device)
         _lib.check(L.uva_hier_lscm(Vd.data_ptr(), len(self.V), Fd.data_ptr(), len(self.F), fd.data_ptr(),
                                    cvd.data_ptr(), chd.data_ptr(), t, nv, nchart, u0d.data_ptr(), bad.data_ptr(),
                                    bbd.data_ptr(), nb, 1e-10, maxiter, scratch.data_ptr(), int(nbytes.value),
