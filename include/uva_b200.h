@@ -483,24 +483,14 @@ int uva_csr_pcg_blocks(int32_t nsys, const int32_t* sys_ofs, int32_t n, const in
  * the device: half-cot weights of the mesh faces `faces` (rows of F, (nf,3),
  * positions V (nvp,3)), the soft-pinned LSCM system of every chart (UV
  * corners CV (t,3), chart per face, directed boundary edges ba -> bb (nb)),
- * unknowns grouped by chart, then uva_csr_pcg_blocks to ||r_c|| <= tol
- * ||b_c|| per chart (at most maxiter iterations). U (nv,2): the solution,
- * U0 for UV vertices no face names and for non-finite values. flags (one
- * device int32, zeroed here): bit 0 a UV vertex or boundary edge joins two
- * charts, bit 1 an index out of range (faces, F, CV, ba, bb), bit 2 a chart
- * id out of range; offending entries are left out, so the solve stays in
- * bounds. Index arrays are int32. scratch: uva_hier_lscm_scratch_bytes.   */
-/* Boundary corners of hier.chart_checks / boundary_directed
- * (engine/hier.py:275-291): isb[3i+k] = 1 unless the face across corner
- * edge k of local face i (FF of mesh face faces[i]) is a subset face
- * (loc >= 0) of the same chart whose first corner on mesh vertex
- * F[faces[i], k] has UV vertex CV[i, k]. vchart (nv): the chart of the last
- * corner (face order) naming each UV vertex, -1 for none. flags (one device
- * int32, zeroed here): bit 1 an index out of range (faces, FF, loc, CV).
- * nv = 0: no vertex charts (vchart may be null).                          */
-int uva_hier_boundary_corners(const int32_t* F, const int32_t* FF, int64_t nf, const int32_t* faces,
-                              const int32_t* loc, const int32_t* chart, const int32_t* CV, int64_t n, int64_t nv,
-                              uint8_t* isb, int32_t* vchart, int32_t* flags, void* stream);
+ * one row per UV vertex shared by its u and v unknowns, then FP64
+ * Jacobi-PCG per chart (one CTA) to ||r_c|| <= tol ||b_c|| (at most maxiter
+ * iterations). U (nv,2): the solution, U0 for UV vertices no face names and
+ * for non-finite values. flags (one device int32, zeroed here): bit 0 a UV
+ * vertex or boundary edge joins two charts, bit 1 an index out of range
+ * (faces, F, CV, ba, bb), bit 2 a chart id out of range; offending entries
+ * are left out, so the solve stays in bounds. Index arrays are int32.
+ * scratch: uva_hier_lscm_scratch_bytes.                                    */
 int uva_hier_lscm_scratch_bytes(int64_t nv, int64_t t, int64_t nb, int32_t nchart, int64_t* bytes);
 int uva_hier_lscm(const double* V, int64_t nvp, const int32_t* F, int64_t nf, const int32_t* faces, const int32_t* CV,
                   const int32_t* chart, int64_t t, int64_t nv, int32_t nchart, const double* U0, const int32_t* ba,

@@ -141,3 +141,20 @@ def test_lscm_rejects_shared_vertices_and_bad_indices(cuda):
     U = S.lscm(faces, CV, nv, chart, nchart, U0, ba, bb)
     assert np.isfinite(U).all()
     assert S.lscm(faces[:0], CV[:0], 0, chart[:0], 0, U0[:0], ba[:0], bb[:0]).shape == (0, 2)
+
+
+def test_lscm_degenerate_face_and_self_loop_edge(cuda):
+    """A face whose UV corners repeat a vertex (its self edge folds into the
+    diagonal) and a boundary edge from a vertex to itself (its two couplings
+    cancel), against the oracle's COO-summed system."""
+    from oracle import hier as oh
+    from ultimate_uv_artist_b200.engine import hier
+    V, F, faces, CV, nv, chart, nchart, U0, ba, bb = _mesh_case(nx=24, ny=16, block=8, seed=6500)
+    CV = CV.copy()
+    CV[5, 2] = CV[5, 1]
+    ba = np.r_[ba, ba[0]]; bb = np.r_[bb, ba[0]]
+    S = hier.Solver(SimpleNamespace(V=V, F=F), dev=cuda)
+    U = S.lscm(faces, CV, nv, chart, nchart, U0, ba, bb)
+    Uo = oh.lscm(V, F, faces, CV, nv, chart, nchart, U0, ba, bb)
+    used = np.unique(CV)
+    assert np.abs(U[used] - Uo[used]).max() <= 1e-6 * np.abs(Uo[used]).max()

@@ -1,6 +1,6 @@
 // hier.Solver.lscm on the device (engine/hier.py:534-585): the soft-pinned
-// LSCM system of every chart assembled from the faces, then solved per chart
-// by the FP64 Jacobi-PCG of chart_ops.cu (uva_csr_pcg_blocks).
+// LSCM system of every chart assembled from the faces and solved per chart
+// by FP64 Jacobi-PCG, one CTA per chart.
 //
 // The system (2 nv unknowns: u then v of each UV vertex) is the reference's
 // COO sum: per face edge e = (corner e+1, corner e+2) with half-cot weight
@@ -12,14 +12,15 @@
 // wpin = 10 max(max |w|, 1e-12) and right-hand side wpin U0. Only UV
 // vertices that a face names have unknowns; the others keep U0.
 //
-// Layout: unknowns grouped by chart (a chart's u unknowns by vertex id, then
-// its v unknowns), so chart c owns the diagonal block [sys_ofs[c],
-// sys_ofs[c+1]). The grouping is a stable radix sort of the vertices by
-// chart; every row lists its diagonal first, then two entries per incident
-// face corner (corners in face order), then one per incident boundary edge
-// end (edges in order): duplicates are kept as separate entries (the product
-// is the same sum), so no per-row merge is needed and the entry order, hence
-// the rounding of every product, is fixed.
+// Layout: the UV vertices grouped by chart (a stable radix sort by chart, so
+// by id inside a chart); vertex slot = position in that list. The u row and
+// the v row of a vertex share their Laplacian entries, so each vertex keeps
+// one row: the diagonal, then its neighbours in first-seen order (corners in
+// face order, duplicates summed in that order), then its boundary couplings
+// (edge order; value c for the u row against the neighbour's v, -c for the
+// v row against its u). A chart whose vectors and rows fit in shared memory
+// (about 165 B per vertex) iterates there; larger charts run the same
+// iteration on global scratch.
 //
 // Steps (one stream, no host round trip):
 //   k_hl_faces   half-cot weights per face (engine/hier.py:362-382 restated),
@@ -29,9 +30,9 @@
 //                one chart) and the pins' keys (atomic minima of 64-bit
 //                (ordered key, vertex) words)
 //   radix sorts  vertices by chart, corners by vertex, boundary ends by vertex
-//   k_hl_rank    unknown numbers; k_hl_rows<false> (row lengths), scan,
-//                k_hl_rows<true> (entries): the CSR
-//   uva_csr_pcg_blocks, then k_hl_out: U (nv, 2), U0 where not finite.
+//   k_hl_slot    vertex slots; k_hl_lap<false> (row lengths), scans,
+//                k_hl_lap<true> (rows, diagonal, right-hand side, start)
+//   k_hl_pcg     the per-chart PCG; k_hl_out: U (nv, 2), U0 where not finite.
 #include <cuda_runtime.h>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -72,15 +73,13 @@ struct HlArgs {
 
 // Scratch of one call, carved from one buffer (256-byte aligned pieces).
 struct HlScratch {
-    int32_t *lastf, *cv, *ccnt, *cofs, *npin, *vcnt, *vofs, *bcnt, *bofs, *rowlen, *rowptr, *ci, *sys_ofs, *its,
-        *err, *isums;
+    int32_t *lastf, *cv, *ccnt, *cofs, *npin, *vcnt, *vofs, *bcnt, *bofs, *slot, *llen, *lrow, *lcol, *clen, *cptr,
+        *ccol, *its, *err, *isums;
     uint32_t *vkey, *vkey_s, *vval, *vval_s, *ckey, *ckey_s, *cval, *cval_s, *bkey, *bkey_s, *bval, *bval_s;
-    int2* unk;
-    double *w, *va, *b, *x, *pcg;
+    double *w, *lval, *cpl, *dg, *bu, *bv, *xu, *xv, *gvec;
     uint64_t *wmax, *pmin, *pmax;
     void* cub;
     size_t cub_bytes;
-    int64_t nnz_max;
 };
 
 size_t cub_temp(int64_t n, int end_bit) {
@@ -100,50 +99,27 @@ size_t hl_layout(const HlArgs& a, char* base, HlScratch* s) {
         off += (bytes + 255) & ~static_cast<size_t>(255);
         return p;
     };
-    const int64_t nv = a.nv, t = a.t, nb = a.nb, nc = a.nchart, N = 2 * nv;
-    const int64_t nnz = 2 * (nv + 6 * t + 2 * nb);
+    const int64_t nv = a.nv, t = a.t, nb = a.nb, nc = a.nchart;
     HlScratch z{};
     HlScratch& r = s ? *s : z;
-    r.lastf = reinterpret_cast<int32_t*>(take(4 * nv));
-    r.cv = reinterpret_cast<int32_t*>(take(4 * nv));
-    r.ccnt = reinterpret_cast<int32_t*>(take(4 * (nc + 1)));
-    r.cofs = reinterpret_cast<int32_t*>(take(4 * (nc + 1)));
-    r.npin = reinterpret_cast<int32_t*>(take(4 * nv));
-    r.vcnt = reinterpret_cast<int32_t*>(take(4 * (nv + 1)));
-    r.vofs = reinterpret_cast<int32_t*>(take(4 * (nv + 1)));
-    r.bcnt = reinterpret_cast<int32_t*>(take(4 * (nv + 1)));
-    r.bofs = reinterpret_cast<int32_t*>(take(4 * (nv + 1)));
-    r.rowlen = reinterpret_cast<int32_t*>(take(4 * (N + 1)));
-    r.rowptr = reinterpret_cast<int32_t*>(take(4 * (N + 1)));
-    r.ci = reinterpret_cast<int32_t*>(take(4 * nnz));
-    r.sys_ofs = reinterpret_cast<int32_t*>(take(4 * (nc + 1)));
-    r.its = reinterpret_cast<int32_t*>(take(4 * std::max<int64_t>(nc, 1)));
-    r.err = reinterpret_cast<int32_t*>(take(4));
-    r.isums = reinterpret_cast<int32_t*>(take(4 * (xscan_sums(std::max(N, nc) + 1) + 1)));
-    r.vkey = reinterpret_cast<uint32_t*>(take(4 * nv));
-    r.vkey_s = reinterpret_cast<uint32_t*>(take(4 * nv));
-    r.vval = reinterpret_cast<uint32_t*>(take(4 * nv));
-    r.vval_s = reinterpret_cast<uint32_t*>(take(4 * nv));
-    r.ckey = reinterpret_cast<uint32_t*>(take(4 * 3 * t));
-    r.ckey_s = reinterpret_cast<uint32_t*>(take(4 * 3 * t));
-    r.cval = reinterpret_cast<uint32_t*>(take(4 * 3 * t));
-    r.cval_s = reinterpret_cast<uint32_t*>(take(4 * 3 * t));
-    r.bkey = reinterpret_cast<uint32_t*>(take(4 * 2 * nb));
-    r.bkey_s = reinterpret_cast<uint32_t*>(take(4 * 2 * nb));
-    r.bval = reinterpret_cast<uint32_t*>(take(4 * 2 * nb));
-    r.bval_s = reinterpret_cast<uint32_t*>(take(4 * 2 * nb));
-    r.unk = reinterpret_cast<int2*>(take(8 * nv));
-    r.w = reinterpret_cast<double*>(take(8 * 3 * t));
-    r.va = reinterpret_cast<double*>(take(8 * nnz));
-    r.b = reinterpret_cast<double*>(take(8 * N));
-    r.x = reinterpret_cast<double*>(take(8 * N));
-    r.pcg = reinterpret_cast<double*>(take(8 * 3 * N));
+    auto i32 = [&](int64_t n) { return reinterpret_cast<int32_t*>(take(4 * n)); };
+    auto u32 = [&](int64_t n) { return reinterpret_cast<uint32_t*>(take(4 * n)); };
+    auto f64 = [&](int64_t n) { return reinterpret_cast<double*>(take(8 * n)); };
+    r.lastf = i32(nv); r.cv = i32(nv); r.ccnt = i32(nc + 1); r.cofs = i32(nc + 1); r.npin = i32(nv);
+    r.vcnt = i32(nv + 1); r.vofs = i32(nv + 1); r.bcnt = i32(nv + 1); r.bofs = i32(nv + 1); r.slot = i32(nv);
+    r.llen = i32(nv + 1); r.lrow = i32(nv + 1); r.lcol = i32(6 * t); r.clen = i32(nv + 1); r.cptr = i32(nv + 1);
+    r.ccol = i32(2 * nb); r.its = i32(std::max<int64_t>(nc, 1)); r.err = i32(1);
+    r.isums = i32(xscan_sums(std::max(nv, nc) + 1) + 1);
+    r.vkey = u32(nv); r.vkey_s = u32(nv); r.vval = u32(nv); r.vval_s = u32(nv);
+    r.ckey = u32(3 * t); r.ckey_s = u32(3 * t); r.cval = u32(3 * t); r.cval_s = u32(3 * t);
+    r.bkey = u32(2 * nb); r.bkey_s = u32(2 * nb); r.bval = u32(2 * nb); r.bval_s = u32(2 * nb);
+    r.w = f64(3 * t); r.lval = f64(6 * t); r.cpl = f64(2 * nb); r.dg = f64(nv); r.bu = f64(nv); r.bv = f64(nv);
+    r.xu = f64(nv); r.xv = f64(nv); r.gvec = f64(6 * nv);
     r.wmax = reinterpret_cast<uint64_t*>(take(8));
     r.pmin = reinterpret_cast<uint64_t*>(take(8 * std::max<int64_t>(nc, 1)));
     r.pmax = reinterpret_cast<uint64_t*>(take(8 * std::max<int64_t>(nc, 1)));
     r.cub_bytes = std::max({cub_temp(nv, bits_for(nc)), cub_temp(3 * t, bits_for(nv)), cub_temp(2 * nb, bits_for(nv))});
     r.cub = take(std::max<size_t>(r.cub_bytes, 16));
-    r.nnz_max = nnz;
     return off;
 }
 
@@ -290,61 +266,75 @@ __global__ void k_hl_pins(HlArgs a, HlScratch s) {
     if (s.pmax[c] != kNoPin) atomicAdd(s.npin + static_cast<uint32_t>(s.pmax[c]), 1);
 }
 
-// Unknown numbers of every UV vertex from the chart-sorted vertex list, and
-// the first row of every chart's block.
-__global__ void k_hl_rank(HlArgs a, HlScratch s) {
+// Slot of every UV vertex: its position in the chart-sorted vertex list
+// (chart c owns slots [cofs[c], cofs[c+1])), -1 for vertices no face names.
+__global__ void k_hl_slot(HlArgs a, HlScratch s) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * kTB + threadIdx.x;
-    if (i <= a.nchart) s.sys_ofs[i] = 2 * s.cofs[i];
     if (i >= a.nv) return;
     const uint32_t c = s.vkey_s[i], v = s.vval_s[i];
-    if (c >= static_cast<uint32_t>(a.nchart)) {
-        s.unk[v] = make_int2(-1, -1);
-        return;
-    }
-    const int32_t loc = static_cast<int32_t>(i) - s.cofs[c];
-    const int32_t base = 2 * s.cofs[c];
-    s.unk[v] = make_int2(base + loc, base + s.ccnt[c] + loc);
+    s.slot[v] = c < static_cast<uint32_t>(a.nchart) ? static_cast<int32_t>(i) : -1;
 }
 
-// The entries of vertex v's u row and v row (the same length): FILL false
-// counts them, FILL true writes them.
+// Laplacian candidate j of a vertex: corner p = first + j / 2 of the vertex
+// lies on edge (k+2)%3 (to corner k+1, side 0) and edge (k+1)%3 (to corner
+// k+2, side 1).
+struct Cand {
+    int32_t nb;
+    double w;
+};
+
+__device__ __forceinline__ Cand lap_cand(const HlArgs& a, const HlScratch& s, int32_t first, int32_t j) {
+    const uint32_t cj = s.cval_s[first + (j >> 1)];
+    const int64_t f = cj / 3;
+    const int k = static_cast<int>(cj - 3 * f);
+    const int h = j & 1;
+    return Cand{a.CV[3 * f + (h == 0 ? (k + 1) % 3 : (k + 2) % 3)], s.w[3 * f + (h == 0 ? (k + 2) % 3 : (k + 1) % 3)]};
+}
+
+// One row per used vertex: FILL false counts the distinct same-chart
+// neighbours and the couplings, FILL true writes them with the diagonal,
+// the right-hand side and the start. Degenerate faces' self edges fold into
+// the diagonal (so the Jacobi diagonal equals the matrix's).
+constexpr int kCandBuf = 24;
+
 template <bool FILL>
-__global__ void k_hl_rows(HlArgs a, HlScratch s) {
+__global__ void k_hl_lap(HlArgs a, HlScratch s) {
     const int64_t v = static_cast<int64_t>(blockIdx.x) * kTB + threadIdx.x;
     if (v >= a.nv) return;
-    const int2 me = s.unk[v];
-    if (me.x < 0) return;
-    const int32_t c = s.cv[v];
-    int32_t ku = 0, kv = 0;
-    if (FILL) {
-        ku = s.rowptr[me.x];
-        kv = s.rowptr[me.y];
-        s.ci[ku++] = me.x;   // the diagonal first; its value at the end
-        s.ci[kv++] = me.y;
-    }
-    int32_t len = 1;
-    double d = 0.0;
-    const int32_t c0 = s.vofs[v], c1 = c0 + s.vcnt[v];
-    for (int32_t p = c0; p < c1; ++p) {
-        const uint32_t j = s.cval_s[p];
-        const int64_t f = j / 3;
-        const int k = static_cast<int>(j - 3 * f);
-        // corner k lies on edge (k+2)%3 (to corner k+1) and edge (k+1)%3 (to corner k+2)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int e = h == 0 ? (k + 2) % 3 : (k + 1) % 3;
-            const int32_t nb = a.CV[3 * f + (h == 0 ? (k + 1) % 3 : (k + 2) % 3)];
-            const double we = s.w[3 * f + e];
-            d += we;
-            if (nb < 0 || nb >= a.nv || s.cv[nb] != c) continue;
-            ++len;
-            if (FILL) {
-                const int2 o = s.unk[nb];
-                s.ci[ku] = o.x; s.va[ku++] = -we;
-                s.ci[kv] = o.y; s.va[kv++] = -we;
-            }
+    const int32_t sl = s.slot[v];
+    if (sl < 0) return;
+    const int32_t c = s.cv[v], base = s.cofs[c];
+    const int32_t first = s.vofs[v], m = 2 * s.vcnt[v];
+    Cand buf[kCandBuf];
+    const bool cached = m <= kCandBuf;
+    if (cached)
+        for (int32_t j = 0; j < m; ++j) buf[j] = lap_cand(a, s, first, j);
+    auto cand = [&](int32_t j) { return cached ? buf[j] : lap_cand(a, s, first, j); };
+    int32_t ko = FILL ? s.lrow[sl] : 0, len = 0;
+    double d = 0.0, dself = 0.0;
+    for (int32_t j = 0; j < m; ++j) {
+        const Cand cj = cand(j);
+        d += cj.w;
+        if (cj.nb < 0 || cj.nb >= a.nv || s.cv[cj.nb] != c) continue;
+        bool dup = false;
+        for (int32_t i = 0; i < j && !dup; ++i) dup = cand(i).nb == cj.nb;
+        if (dup) continue;   // summed at its first occurrence
+        double sum = cj.w;
+        for (int32_t i = j + 1; i < m; ++i) {
+            const Cand ci = cand(i);
+            if (ci.nb == cj.nb) sum += ci.w;
+        }
+        if (cj.nb == v) {
+            dself -= sum;
+            continue;
+        }
+        ++len;
+        if (FILL) {
+            s.lcol[ko] = s.slot[cj.nb] - base;
+            s.lval[ko++] = -sum;
         }
     }
+    int32_t kc = FILL ? s.cptr[sl] : 0, clen = 0;
     const int32_t b0 = s.bofs[v], b1 = b0 + s.bcnt[v];
     for (int32_t p = b0; p < b1; ++p) {
         const uint32_t j = s.bval_s[p];
@@ -352,16 +342,15 @@ __global__ void k_hl_rows(HlArgs a, HlScratch s) {
         const int64_t e = is_a ? j : j - a.nb;
         const int32_t o = is_a ? a.bb[e] : a.ba[e];
         if (o < 0 || o >= a.nv || s.cv[o] != c) continue;
-        ++len;
+        ++clen;
         if (FILL) {
-            const int2 q = s.unk[o];
-            s.ci[ku] = q.y; s.va[ku++] = is_a ? -0.5 : 0.5;
-            s.ci[kv] = q.x; s.va[kv++] = is_a ? 0.5 : -0.5;
+            s.ccol[kc] = s.slot[o] - base;
+            s.cpl[kc++] = is_a ? -0.5 : 0.5;   // u row against o's v; the v row takes the opposite sign against o's u
         }
     }
     if (!FILL) {
-        s.rowlen[me.x] = len;
-        s.rowlen[me.y] = len;
+        s.llen[sl] = len;
+        s.clen[sl] = clen;
         return;
     }
     const double wm = __longlong_as_double(static_cast<long long>(*s.wmax));
@@ -374,19 +363,142 @@ __global__ void k_hl_rows(HlArgs a, HlScratch s) {
         bx += wpin * ux;
         by += wpin * uy;
     }
-    s.va[s.rowptr[me.x]] = d;
-    s.va[s.rowptr[me.y]] = d;
-    s.b[me.x] = bx; s.b[me.y] = by;
-    s.x[me.x] = ux; s.x[me.y] = uy;
+    s.dg[sl] = d + dself;
+    s.bu[sl] = bx; s.bv[sl] = by;
+    s.xu[sl] = ux; s.xv[sl] = uy;
+}
+
+// ---- per-chart Jacobi-PCG on the paired rows, one CTA per chart. Shared
+// memory, when the chart fits: 9 vectors (x, r, p, q for u and v, the
+// diagonal) and the rows (starts relative to the chart's first entry, local
+// columns); otherwise the vectors live in global scratch and the rows are
+// read in place (absolute starts).
+constexpr int kHlNT = 1024;
+constexpr size_t kHlSmem = 220 * 1024;
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_hl_pcg(HlArgs a, HlScratch s, double tol, int maxiter) {
+    __shared__ double red[2 * 4 * (NT / 32)];
+    extern __shared__ double dsm[];
+    int phase = 0;
+    const int c = blockIdx.x;
+    if (c >= a.nchart) return;
+    const int32_t s0 = s.cofs[c], n = s.cofs[c + 1] - s0;
+    const int32_t e0 = s.lrow[s0], ne = s.lrow[s0 + n] - e0;
+    const int32_t f0 = s.cptr[s0], nf = s.cptr[s0 + n] - f0;
+    const size_t need = 8 * (9 * static_cast<size_t>(n) + ne + nf) + 4 * (2 * (static_cast<size_t>(n) + 1) + ne + nf);
+    const bool fit = need <= kHlSmem;
+    double *xu, *xv, *ru, *rv, *pu, *pv, *qu, *qv, *dg;
+    const int32_t *lr, *lc, *cr, *cc;
+    const double *lv, *cp;
+    if (fit) {
+        double* p = dsm;
+        xu = p; p += n; xv = p; p += n; ru = p; p += n; rv = p; p += n; pu = p; p += n; pv = p; p += n;
+        qu = p; p += n; qv = p; p += n; dg = p; p += n;
+        double* lvs = p; p += ne;
+        double* cps = p; p += nf;
+        int32_t* ip = reinterpret_cast<int32_t*>(p);
+        int32_t* lrs = ip; ip += n + 1;
+        int32_t* crs = ip; ip += n + 1;
+        int32_t* lcs = ip; ip += ne;
+        int32_t* ccs = ip;
+        for (int i = threadIdx.x; i <= n; i += NT) {
+            lrs[i] = s.lrow[s0 + i] - e0;
+            crs[i] = s.cptr[s0 + i] - f0;
+        }
+        for (int k = threadIdx.x; k < ne; k += NT) { lcs[k] = s.lcol[e0 + k]; lvs[k] = s.lval[e0 + k]; }
+        for (int k = threadIdx.x; k < nf; k += NT) { ccs[k] = s.ccol[f0 + k]; cps[k] = s.cpl[f0 + k]; }
+        for (int i = threadIdx.x; i < n; i += NT) {
+            xu[i] = s.xu[s0 + i]; xv[i] = s.xv[s0 + i]; dg[i] = s.dg[s0 + i];
+        }
+        lr = lrs; cr = crs; lc = lcs; cc = ccs; lv = lvs; cp = cps;
+        __syncthreads();
+    } else {
+        const int64_t nv = a.nv;
+        xu = s.xu + s0; xv = s.xv + s0; dg = s.dg + s0;
+        ru = s.gvec + s0; rv = ru + nv; pu = rv + nv; pv = pu + nv; qu = pv + nv; qv = qu + nv;
+        lr = s.lrow + s0; cr = s.cptr + s0; lc = s.lcol; cc = s.ccol; lv = s.lval; cp = s.cpl;
+    }
+    // (A y)_i for the u and v rows of vertex i
+    auto apply = [&](int i, const double* yu, const double* yv, double& ou, double& ov) {
+        const double d = dg[i];
+        double su = d * yu[i], sv = d * yv[i];
+        for (int k = lr[i]; k < lr[i + 1]; ++k) {
+            const int j = lc[k];
+            const double w = lv[k];
+            su += w * yu[j];
+            sv += w * yv[j];
+        }
+        for (int k = cr[i]; k < cr[i + 1]; ++k) {
+            const int j = cc[k];
+            const double w = cp[k];
+            su += w * yv[j];
+            sv -= w * yu[j];
+        }
+        ou = su;
+        ov = sv;
+    };
+    auto jac = [&](int i) { const double d = dg[i]; return fabs(d) > 1e-300 ? d : 1.0; };
+    double acc[2] = {0.0, 0.0};
+    for (int i = threadIdx.x; i < n; i += NT) {
+        double au, av;
+        apply(i, xu, xv, au, av);
+        const double bu = s.bu[s0 + i], bv = s.bv[s0 + i];
+        const double r0 = bu - au, r1 = bv - av, dj = jac(i);
+        ru[i] = r0; rv[i] = r1;
+        pu[i] = r0 / dj; pv[i] = r1 / dj;
+        acc[0] += r0 * pu[i] + r1 * pv[i];
+        acc[1] += bu * bu + bv * bv;
+    }
+    block_sum<NT, 2>(acc, red, phase);   // also publishes p
+    double rz = acc[0];
+    const double bb = fmax(acc[1], 1e-300);
+    int it = 0;
+    for (; it < maxiter; ++it) {
+        double pq[1] = {0.0};
+        for (int i = threadIdx.x; i < n; i += NT) {
+            double a0, a1;
+            apply(i, pu, pv, a0, a1);
+            qu[i] = a0; qv[i] = a1;
+            pq[0] += pu[i] * a0 + pv[i] * a1;
+        }
+        block_sum<NT, 1>(pq, red, phase);
+        if (!(pq[0] > 0.0)) break;
+        const double alpha = rz / pq[0];
+        double nz[2] = {0.0, 0.0};
+        for (int i = threadIdx.x; i < n; i += NT) {
+            xu[i] += alpha * pu[i];
+            xv[i] += alpha * pv[i];
+            const double r0 = ru[i] - alpha * qu[i], r1 = rv[i] - alpha * qv[i], dj = jac(i);
+            ru[i] = r0; rv[i] = r1;
+            nz[0] += (r0 * r0 + r1 * r1) / dj;
+            nz[1] += r0 * r0 + r1 * r1;
+        }
+        block_sum<NT, 2>(nz, red, phase);
+        if (nz[1] <= tol * tol * bb) { ++it; break; }
+        const double beta = nz[0] / rz;
+        rz = nz[0];
+        for (int i = threadIdx.x; i < n; i += NT) {
+            const double dj = jac(i);
+            pu[i] = ru[i] / dj + beta * pu[i];
+            pv[i] = rv[i] / dj + beta * pv[i];
+        }
+        __syncthreads();
+    }
+    if (fit) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += NT) { s.xu[s0 + i] = xu[i]; s.xv[s0 + i] = xv[i]; }
+    }
+    if (threadIdx.x == 0) s.its[c] = it;
 }
 
 __global__ void k_hl_out(HlArgs a, HlScratch s, double* U) {
     const int64_t v = static_cast<int64_t>(blockIdx.x) * kTB + threadIdx.x;
     if (v >= a.nv) return;
-    const int2 me = s.unk[v];
+    const int32_t sl = s.slot[v];
     const double ux = a.U0[2 * v], uy = a.U0[2 * v + 1];
     double x = ux, y = uy;
-    if (me.x >= 0) { x = s.x[me.x]; y = s.x[me.y]; }
+    if (sl >= 0) { x = s.xu[sl]; y = s.xv[sl]; }
     U[2 * v] = isfinite(x) ? x : ux;
     U[2 * v + 1] = isfinite(y) ? y : uy;
 }
@@ -491,7 +603,8 @@ extern "C" int uva_hier_lscm(const double* V, int64_t nvp, const int32_t* F, int
     ok(zero(s.npin, 4 * nv));
     ok(zero(s.vcnt, 4 * (nv + 1)));
     ok(zero(s.bcnt, 4 * (nv + 1)));
-    ok(zero(s.rowlen, 4 * (2 * nv + 1)));
+    ok(zero(s.llen, 4 * (nv + 1)));
+    ok(zero(s.clen, 4 * (nv + 1)));
     ok(zero(s.wmax, 8));
     if (nchart > 0) {
         ok(cudaMemsetAsync(s.pmin, 0xFF, 8 * static_cast<size_t>(nchart), st));
@@ -521,15 +634,17 @@ extern "C" int uva_hier_lscm(const double* V, int64_t nvp, const int32_t* F, int
     xscan<int32_t>(s.ccnt, s.cofs, s.isums, nullptr, nchart + 1, st);
     xscan<int32_t>(s.vcnt, s.vofs, s.isums, nullptr, nv + 1, st);
     xscan<int32_t>(s.bcnt, s.bofs, s.isums, nullptr, nv + 1, st);
-    k_hl_rank<<<blocks_for(std::max<int64_t>(nv, nchart + 1)), kTB, 0, st>>>(a, s);
-    k_hl_rows<false><<<blocks_for(nv), kTB, 0, st>>>(a, s);
-    xscan<int32_t>(s.rowlen, s.rowptr, s.isums, nullptr, 2 * nv + 1, st);
-    k_hl_rows<true><<<blocks_for(nv), kTB, 0, st>>>(a, s);
+    k_hl_slot<<<blocks_for(nv), kTB, 0, st>>>(a, s);
+    k_hl_lap<false><<<blocks_for(nv), kTB, 0, st>>>(a, s);
+    xscan<int32_t>(s.llen, s.lrow, s.isums, nullptr, nv + 1, st);
+    xscan<int32_t>(s.clen, s.cptr, s.isums, nullptr, nv + 1, st);
+    k_hl_lap<true><<<blocks_for(nv), kTB, 0, st>>>(a, s);
     UVA_CHECK_LAUNCH("uva_hier_lscm/assemble");
     if (nchart > 0) {
-        const int rc = uva_csr_pcg_blocks(nchart, s.sys_ofs, static_cast<int32_t>(2 * nv), s.rowptr, s.ci, s.va, s.b,
-                                          s.x, tol, maxiter, s.pcg, s.its, stream);
-        if (rc != UVA_OK) return rc;
+        ok(cudaFuncSetAttribute(k_hl_pcg<kHlNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kHlSmem)));
+        if (e != cudaSuccess) return uva_cuda_status(e, "uva_hier_lscm/cudaFuncSetAttribute");
+        k_hl_pcg<kHlNT><<<static_cast<unsigned>(nchart), kHlNT, kHlSmem, st>>>(a, s, tol, maxiter);
+        UVA_CHECK_LAUNCH("uva_hier_lscm/pcg");
     }
     k_hl_out<<<blocks_for(nv), kTB, 0, st>>>(a, s, U);
     UVA_CHECK_LAUNCH("uva_hier_lscm/out");
