@@ -67,6 +67,8 @@ def _args():
                     help="only the packing leg, as one JSON line (for launch lists of the packer)")
     ap.add_argument("--hier-only", action="store_true",
                     help="only the hier.Solver leg, as one JSON line (for launch lists of its kernels)")
+    ap.add_argument("--validate-only", action="store_true",
+                    help="only the validation leg, as one JSON line (for launch lists of its kernels)")
     return ap.parse_args()
 
 
@@ -849,6 +851,12 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.validate_only:
+        if rank == 0:
+            print(json.dumps({"validate": bench_validation(dev)}))
+        if ws > 1:
+            dist.destroy_process_group()
+        return
     if args.hier_only:
         if rank == 0:
             print(json.dumps({"hier_solver": bench_hier(dev)}))
