@@ -411,6 +411,8 @@ def bench_validation(dev, steps=3):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
     c = dv.host_counts()
+    metrics.min_gutter_device(UV64, dv.F, dv.labels, int(c[6]), 4096)   # warm-up (first-call allocations)
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2 = torch.cuda.Event(enable_timing=True); e3 = torch.cuda.Event(enable_timing=True)
     e2.record()

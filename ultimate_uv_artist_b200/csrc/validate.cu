@@ -149,16 +149,28 @@ __global__ void k_v_rows(int n, const float* UV, unsigned long long* counts) {
     count_add(counts + UVA_VC_OUTSIDE, out);
 }
 
+// The maximum is taken over the warp first (bit patterns of non-negative
+// doubles order like the values; NaN and negatives are left out, as in
+// atomic_max_nonneg), then one atomic per warp: a single address took one
+// atomic per face before.
 __global__ void k_v_area3(int m, const double* V, const int32_t* F, double* a3, double* amax) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= m) return;
-    const int i0 = F[3 * t], i1 = F[3 * t + 1], i2 = F[3 * t + 2];
-    const double ax = V[3 * i1] - V[3 * i0], ay = V[3 * i1 + 1] - V[3 * i0 + 1], az = V[3 * i1 + 2] - V[3 * i0 + 2];
-    const double bx = V[3 * i2] - V[3 * i0], by = V[3 * i2 + 1] - V[3 * i0 + 1], bz = V[3 * i2 + 2] - V[3 * i0 + 2];
-    const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
-    const double a = 0.5 * sqrt(cx * cx + cy * cy + cz * cz);
-    a3[t] = a;
-    atomic_max_nonneg(amax, a);
+    unsigned long long w = 0;   // +0.0: amax starts there
+    if (t < m) {
+        const int i0 = F[3 * t], i1 = F[3 * t + 1], i2 = F[3 * t + 2];
+        const double ax = V[3 * i1] - V[3 * i0], ay = V[3 * i1 + 1] - V[3 * i0 + 1], az = V[3 * i1 + 2] - V[3 * i0 + 2];
+        const double bx = V[3 * i2] - V[3 * i0], by = V[3 * i2 + 1] - V[3 * i0 + 1], bz = V[3 * i2 + 2] - V[3 * i0 + 2];
+        const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+        const double a = 0.5 * sqrt(cx * cx + cy * cy + cz * cz);
+        a3[t] = a;
+        if (a >= 0.0) w = static_cast<unsigned long long>(__double_as_longlong(a));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long y = __shfl_xor_sync(0xffffffffu, w, o);
+        w = y > w ? y : w;
+    }
+    if ((threadIdx.x & 31) == 0 && w) atomicMax(reinterpret_cast<unsigned long long*>(amax), w);
 }
 
 // engine/validate.py:149-172: signed area, sliver, has3d, skip; cell boxes.
