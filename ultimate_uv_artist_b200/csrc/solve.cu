@@ -39,58 +39,72 @@ namespace {
 // PARAM semantics: engine/param.py:19-44 (no mask, 1e-300 clamps).
 __global__ void k_frames(uva_batch b, double* wmax_isl) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= b.t) return;
-    const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
-    const int v0 = b.vofs[tv.w];
-    const double* P = b.P;
-    const double p0x = P[3 * (v0 + tv.x)], p0y = P[3 * (v0 + tv.x) + 1], p0z = P[3 * (v0 + tv.x) + 2];
-    const double e1x = P[3 * (v0 + tv.y)] - p0x, e1y = P[3 * (v0 + tv.y) + 1] - p0y, e1z = P[3 * (v0 + tv.y) + 2] - p0z;
-    const double e2x = P[3 * (v0 + tv.z)] - p0x, e2y = P[3 * (v0 + tv.z) + 1] - p0y, e2z = P[3 * (v0 + tv.z) + 2] - p0z;
-    const bool batch = b.semantics == UVA_SEM_BATCH;
-    double l1 = sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
-    const double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
-    const double dbl = sqrt(nx * nx + ny * ny + nz * nz);
-    const double clampl = batch ? 1e-30 : 1e-300;
-    if (batch) l1 = fmax(l1, 1e-30);
-    const double il = 1.0 / fmax(l1, clampl);
-    const double exx = e1x * il, exy = e1y * il, exz = e1z * il;
-    const double in = 1.0 / fmax(dbl, clampl);
-    const double ux = nx * in, uy = ny * in, uz = nz * in;
-    const double eyx = uy * exz - uz * exy, eyy = uz * exx - ux * exz, eyz = ux * exy - uy * exx;
-    double X1 = l1, X2 = e2x * exx + e2y * exy + e2z * exz, Y2 = e2x * eyx + e2y * eyy + e2z * eyz;
-    bool ok = true;
-    if (batch) {
-        ok = (dbl > 1e-14 * fmax(l1 * l1, 1e-300)) && isfinite(dbl);
-        if (!ok) { X1 = 0.0; X2 = 0.0; Y2 = 0.0; }
-    }
-    // cotangent of the angle at corner o opposite edge k (corners k+1, k+2)
-    const double cx[3] = {0.0, X1, X2}, cy[3] = {0.0, 0.0, Y2};
-    double w[3];
-    const double crmin = batch ? 1e-30 : 1e-300;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int i = (k + 1) % 3, j = (k + 2) % 3;
-        const double ax = cx[i] - cx[k], ay = cy[i] - cy[k], bx = cx[j] - cx[k], by = cy[j] - cy[k];
-        const double cr = fmax(fabs(ax * by - ay * bx), crmin);
-        double c = (ax * bx + ay * by) / cr;
-        c = fmin(fmax(c, -1e4), 1e4);
-        w[k] = ok ? 0.5 * c : 0.0;
-    }
-    if (batch) {
-        // Jacobian denominators as engine/gpu.py:117-120 clamps them
-        X1 = fmax(X1, 1e-30);
-        if (!(fabs(Y2) > 1e-30)) Y2 = 1e-30;
-    }
-    reinterpret_cast<double4*>(b.frame)[f] = make_double4(X1, X2, Y2, 0.5 * dbl);
-    reinterpret_cast<double4*>(b.wtri)[f] = make_double4(w[0], w[1], w[2], ok ? 1.0 : 0.0);
+    int isl = -1;
     double m = 0.0;
+    if (f < b.t) {
+        const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
+        const int v0 = b.vofs[tv.w];
+        const double* P = b.P;
+        const double p0x = P[3 * (v0 + tv.x)], p0y = P[3 * (v0 + tv.x) + 1], p0z = P[3 * (v0 + tv.x) + 2];
+        const double e1x = P[3 * (v0 + tv.y)] - p0x, e1y = P[3 * (v0 + tv.y) + 1] - p0y, e1z = P[3 * (v0 + tv.y) + 2] - p0z;
+        const double e2x = P[3 * (v0 + tv.z)] - p0x, e2y = P[3 * (v0 + tv.z) + 1] - p0y, e2z = P[3 * (v0 + tv.z) + 2] - p0z;
+        const bool batch = b.semantics == UVA_SEM_BATCH;
+        double l1 = sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
+        const double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+        const double dbl = sqrt(nx * nx + ny * ny + nz * nz);
+        const double clampl = batch ? 1e-30 : 1e-300;
+        if (batch) l1 = fmax(l1, 1e-30);
+        const double il = 1.0 / fmax(l1, clampl);
+        const double exx = e1x * il, exy = e1y * il, exz = e1z * il;
+        const double in = 1.0 / fmax(dbl, clampl);
+        const double ux = nx * in, uy = ny * in, uz = nz * in;
+        const double eyx = uy * exz - uz * exy, eyy = uz * exx - ux * exz, eyz = ux * exy - uy * exx;
+        double X1 = l1, X2 = e2x * exx + e2y * exy + e2z * exz, Y2 = e2x * eyx + e2y * eyy + e2z * eyz;
+        bool ok = true;
+        if (batch) {
+            ok = (dbl > 1e-14 * fmax(l1 * l1, 1e-300)) && isfinite(dbl);
+            if (!ok) { X1 = 0.0; X2 = 0.0; Y2 = 0.0; }
+        }
+        // cotangent of the angle at corner o opposite edge k (corners k+1, k+2)
+        const double cx[3] = {0.0, X1, X2}, cy[3] = {0.0, 0.0, Y2};
+        double w[3];
+        const double crmin = batch ? 1e-30 : 1e-300;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int e = b.tri_edge[3 * f + k];
-        if (e >= 0) atomicAdd(&b.wedge[e], w[k]);
-        m = fmax(m, fabs(w[k]));
+        for (int k = 0; k < 3; ++k) {
+            const int i = (k + 1) % 3, j = (k + 2) % 3;
+            const double ax = cx[i] - cx[k], ay = cy[i] - cy[k], bx = cx[j] - cx[k], by = cy[j] - cy[k];
+            const double cr = fmax(fabs(ax * by - ay * bx), crmin);
+            double c = (ax * bx + ay * by) / cr;
+            c = fmin(fmax(c, -1e4), 1e4);
+            w[k] = ok ? 0.5 * c : 0.0;
+        }
+        if (batch) {
+            // Jacobian denominators as engine/gpu.py:117-120 clamps them
+            X1 = fmax(X1, 1e-30);
+            if (!(fabs(Y2) > 1e-30)) Y2 = 1e-30;
+        }
+        reinterpret_cast<double4*>(b.frame)[f] = make_double4(X1, X2, Y2, 0.5 * dbl);
+        reinterpret_cast<double4*>(b.wtri)[f] = make_double4(w[0], w[1], w[2], ok ? 1.0 : 0.0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int e = b.tri_edge[3 * f + k];
+            if (e >= 0) atomicAdd(&b.wedge[e], w[k]);
+            m = fmax(m, fabs(w[k]));
+        }
+        isl = tv.w;
     }
-    atomic_max_nonneg(&wmax_isl[tv.w], m);
+    // the island's max |w|: a segmented maximum over the warp (triangles of
+    // an island are contiguous), then one atomic per island and warp instead
+    // of one per triangle on the island's slot
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_down_sync(0xffffffffu, m, o);
+        const int yi = __shfl_down_sync(0xffffffffu, isl, o);
+        if (lane + o < 32 && yi == isl) m = fmax(m, y);
+    }
+    const int prev = __shfl_up_sync(0xffffffffu, isl, 1);
+    if (isl >= 0 && (lane == 0 || prev != isl)) atomic_max_nonneg(&wmax_isl[isl], m);
 }
 
 // Pin weight: BATCH one global max |w| clamped at 1e-12 (gpu.py:138);
