@@ -192,32 +192,61 @@ __global__ void k_met_islands(int ni, const double* isum, double* sums, QIn qd) 
 }
 
 // ------------------------------------------------------------------ chart quality
+// Per-key sums of K values over a warp whose lanes hold their keys in
+// contiguous runs (key -1: none): a segmented reduction, then the first lane
+// of each run adds the run's sums at dst + stride * key. Batch triangles are
+// grouped by island, so an island takes one atomic per value and warp.
+template <int K>
+__device__ __forceinline__ void warp_run_sums(double* dst, int stride, int key, double (&v)[K]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int yk = __shfl_down_sync(0xffffffffu, key, o);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const double y = __shfl_down_sync(0xffffffffu, v[k], o);
+            if (lane + o < 32 && yk == key) v[k] += y;
+        }
+    }
+    const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+    if (key >= 0 && (lane == 0 || prev != key)) {
+        double* d = dst + static_cast<size_t>(stride) * key;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if (v[k] != 0.0) atomicAdd(d + k, v[k]);
+    }
+}
+
 // engine/param.py:520-551 for every island of a batch (frames from the setup).
 __global__ void k_quality_a(const uva_batch b, double* tri, double* isum) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= b.t) return;
-    const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
-    const int v0 = b.vofs[tv.w];
-    const double4 fr = reinterpret_cast<const double4*>(b.frame)[f];
-    const double2* U = reinterpret_cast<const double2*>(b.U);
-    const double2 a0 = U[v0 + tv.x], a1 = U[v0 + tv.y], a2 = U[v0 + tv.z];
-    const bool ok = fabs(fr.x * fr.z) > 1e-300;
-    const double x1s = ok ? fr.x : 1.0, y2s = ok ? fr.z : 1.0;
-    const double j00 = (a1.x - a0.x) / x1s, j10 = (a1.y - a0.y) / x1s;
-    const double j01 = ((a2.x - a0.x) - j00 * fr.y) / y2s, j11 = ((a2.y - a0.y) - j10 * fr.y) / y2s;
-    const double E = (j00 + j11) / 2, F = (j00 - j11) / 2, G = (j10 + j01) / 2, H = (j10 - j01) / 2;
-    const double Q = sqrt(E * E + H * H), R = sqrt(F * F + G * G);
-    const double s1 = Q + R, s2 = fabs(Q - R);
-    const double sa = 0.5 * ((a1.x - a0.x) * (a2.y - a0.y) - (a2.x - a0.x) * (a1.y - a0.y));
-    double* o = tri + 6 * static_cast<size_t>(f);
-    o[0] = s1; o[1] = s2; o[2] = sa; o[3] = fr.w;
-    double* s = isum + 8 * static_cast<size_t>(tv.w);
-    atomicAdd(s, fr.w);                       // A
-    atomicAdd(s + 1, fabs(sa));               // uvA
-    if (sa > 0.0) atomicAdd(s + 2, 1.0);      // positive count
-    if (sa < 0.0) atomicAdd(s + 3, 1.0);      // negative count
-    if (sa <= 0.0) atomicAdd(s + 4, 1.0);     // non-positive count
-    if (sa >= 0.0) atomicAdd(s + 5, 1.0);     // non-negative count
+    int key = -1;
+    double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (f < b.t) {
+        const int4 tv = reinterpret_cast<const int4*>(b.tri4)[f];
+        const int v0 = b.vofs[tv.w];
+        const double4 fr = reinterpret_cast<const double4*>(b.frame)[f];
+        const double2* U = reinterpret_cast<const double2*>(b.U);
+        const double2 a0 = U[v0 + tv.x], a1 = U[v0 + tv.y], a2 = U[v0 + tv.z];
+        const bool ok = fabs(fr.x * fr.z) > 1e-300;
+        const double x1s = ok ? fr.x : 1.0, y2s = ok ? fr.z : 1.0;
+        const double j00 = (a1.x - a0.x) / x1s, j10 = (a1.y - a0.y) / x1s;
+        const double j01 = ((a2.x - a0.x) - j00 * fr.y) / y2s, j11 = ((a2.y - a0.y) - j10 * fr.y) / y2s;
+        const double E = (j00 + j11) / 2, F = (j00 - j11) / 2, G = (j10 + j01) / 2, H = (j10 - j01) / 2;
+        const double Q = sqrt(E * E + H * H), R = sqrt(F * F + G * G);
+        const double s1 = Q + R, s2 = fabs(Q - R);
+        const double sa = 0.5 * ((a1.x - a0.x) * (a2.y - a0.y) - (a2.x - a0.x) * (a1.y - a0.y));
+        double* o = tri + 6 * static_cast<size_t>(f);
+        o[0] = s1; o[1] = s2; o[2] = sa; o[3] = fr.w;
+        key = tv.w;
+        v[0] = fr.w;                      // A
+        v[1] = fabs(sa);                  // uvA
+        v[2] = sa > 0.0 ? 1.0 : 0.0;      // positive count
+        v[3] = sa < 0.0 ? 1.0 : 0.0;      // negative count
+        v[4] = sa <= 0.0 ? 1.0 : 0.0;     // non-positive count
+        v[5] = sa >= 0.0 ? 1.0 : 0.0;     // non-negative count
+    }
+    warp_run_sums<6>(isum, 8, key, v);
 }
 
 __global__ void k_quality_b(const uva_batch b, const double* tri, double* isum, QIn qa, QIn qr, double* per_aniso,
