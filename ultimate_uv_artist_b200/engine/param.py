@@ -402,9 +402,16 @@ def chart_quality_batch(db, U=None):
     pr = torch.empty(max(db.t, 1), dtype=torch.float64, device=dev)
     _lib.check(L.uva_chart_quality(C.byref(db.desc), _p(out), _p(pa), _p(pr), _p(scratch), nb.value, _stream(dev)),
                "uva_chart_quality")
-    o = out.cpu().numpy()
-    pa = pa[:db.t].cpu().numpy()
-    pr = pr[:db.t].cpu().numpy()
+    # per-triangle values into page-locked host memory (torch's caching host
+    # allocator reuses it once the caller drops the arrays): no page faults
+    # on fresh pageable memory, asynchronous DMA on the current stream
+    from ..device import host_empty
+    pa_h, pr_h = host_empty(db.t, np.float64), host_empty(db.t, np.float64)
+    if db.t:
+        torch.from_numpy(pa_h).copy_(pa[:db.t], non_blocking=True)
+        torch.from_numpy(pr_h).copy_(pr[:db.t], non_blocking=True)
+    o = out.cpu().numpy()   # synchronises the stream: the copies above are done
+    pa, pr = pa_h, pr_h
     tofs = db.plan.tofs
     res = []
     for i in range(db.nc):
