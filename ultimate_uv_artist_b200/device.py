@@ -61,6 +61,21 @@ def host_empty(shape, dtype):
 
 _TORCH_OF = {np.dtype(np.int32): torch.int32, np.dtype(np.int64): torch.int64, np.dtype(np.float32): torch.float32,
              np.dtype(np.float64): torch.float64, np.dtype(np.uint8): torch.uint8}
+_NUMPY_OF = {v: k for k, v in _TORCH_OF.items()}
+
+
+def to_host(t):
+    """A device tensor's contents as a numpy array in page-locked memory
+    (torch's caching host allocator, so repeated calls reuse it instead of
+    page-faulting fresh pageable memory): one asynchronous copy on the
+    current stream, then a wait for it."""
+    if t.dtype not in _NUMPY_OF:
+        return t.cpu().numpy()
+    out = host_empty(tuple(t.shape), _NUMPY_OF[t.dtype])
+    if t.numel():
+        torch.from_numpy(out).copy_(t, non_blocking=True)
+        torch.cuda.current_stream(t.device).synchronize()
+    return out
 
 
 class Plan:

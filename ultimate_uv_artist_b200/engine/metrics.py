@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 from .. import _lib, meshops
-from ..device import require_cuda
+from ..device import require_cuda, to_host
 
 vp = C.c_void_p
 
@@ -168,7 +168,7 @@ def _distortion(V, F, UV, islands, n_islands, per_tri="host", keep_per_tri=False
                "uva_distortion_report")
     if keep_per_tri:
         return out.cpu().numpy(), per[:m]
-    return out.cpu().numpy(), (per[:m].cpu().numpy() if want else None)
+    return out.cpu().numpy(), (to_host(per[:m]) if want else None)
 
 
 def _distortion_fields(m, s, with_islands):
@@ -291,7 +291,7 @@ def _raster_labels(uv, faces, lab_of_face, res, img):
     F = torch.from_numpy(np.ascontiguousarray(faces, np.int32).reshape(-1, 3)).to(dev)
     lab = torch.from_numpy(np.ascontiguousarray(lab_of_face, np.int32)).to(dev)
     out, _ = _gutter_raw(UV, F, lab, int(res), 1)
-    res_img = out.cpu().numpy()
+    res_img = to_host(out)
     np.copyto(img, np.where(res_img >= 0, res_img, img))
 
 
@@ -339,4 +339,4 @@ def min_gutter(uv, faces, islands, res=4096):
     lab = torch.from_numpy(np.ascontiguousarray(islands, np.int32)).to(dev)
     g = min_gutter_device(UV, F, lab, int(lab.max().item()) + 1 if len(lab) else 0, int(res))
     img, _ = _gutter_raw(UV, F, lab, int(res), 1)
-    return g, img.cpu().numpy()
+    return g, to_host(img)
