@@ -983,6 +983,15 @@ def main():
             dist.all_reduce(x, op=dist.ReduceOp.MAX)
             e2e_val = units_all / float(x[0])
 
+    # our kernels per step: setup (k_frames, k_wpin, k_vert_isl, k_rows,
+    # k_far_pair, then k_coarse for the whole-CTA classes and for the rest),
+    # then k_islands for LSCM and for ARAP, each with k_wide before it when
+    # the batch has islands of the whole-GPU class
+    co = [int(db.desc.class_ofs[c]) for c in range(5)]
+    big = min(max(co[2], 0), db.nc)
+    n_coarse = int(big > 0) + int(db.nc - big > 0)
+    n_wide = 2 if co[1] > co[0] else 0
+    launches_per_step = 5 + n_coarse + 2 + n_wide
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -1106,7 +1115,7 @@ def main():
                               "max_resid": float(st_lscm["resid"].max())},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": 8 * args.steps,   # setup 6 (frames, wpin, vert_isl, rows, far_pair, coarse) + LSCM + ARAP
+            "gpu_launches": launches_per_step * args.steps,
             "lscm_ms": lscm_ms, "arap_ms": arap_ms,
             "graph": graphs is not None,
             "plain_gpu": plain,
